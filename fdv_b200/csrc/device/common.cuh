@@ -1,0 +1,159 @@
+// Shared device-side definitions of the fdv analysis kernels (sm_100a).
+//
+// All pixel work is 8/16/32-bit integer arithmetic; the rate-distortion
+// decisions are IEEE double comparisons evaluated with explicitly rounded
+// intrinsics so that no fused multiply-add can change a tie
+// (J = D + lambda * bits, fdv.h:2527, :4043, :5390, :5866, :5932).
+#pragma once
+#include <cstdint>
+
+#define FDVB_FULL 0xffffffffu
+
+namespace fdvb {
+
+// ----------------------------------------------------------- constants --
+// H.264 4x4 forward multipliers and dequant rescale by [qp % 6][class]
+// (fdv.h:2405-2421), the 4x4 and 8x8 zigzag scans (fdv.h:1699, :2153).
+__constant__ int c_MF[6][3] = {{13107, 5243, 8066}, {11916, 4660, 7490}, {10082, 4194, 6554},
+                               {9362, 3647, 5825},  {8192, 3355, 5243},  {7282, 2893, 4559}};
+__constant__ int c_DQV[6][3] = {{10, 16, 13}, {11, 18, 14}, {13, 20, 16},
+                                {14, 23, 18}, {16, 25, 20}, {18, 29, 23}};
+__constant__ int c_ZZ4[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+__constant__ int c_IZZ4[16] = {0, 1, 5, 6, 2, 4, 7, 12, 3, 8, 11, 13, 9, 10, 14, 15};
+__constant__ int c_ZZ8[64] = {
+     0,  1,  8, 16,  9,  2,  3, 10, 17, 24, 32, 25, 18, 11,  4,  5,
+    12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13,  6,  7, 14, 21, 28,
+    35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
+    58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+// 8x8 DCT basis and quantiser steps, computed on the host (fdvb_c8_tables).
+__constant__ int32_t c_C8[64];
+__constant__ int32_t c_QSTEP8[52];
+
+// Cost constants (fdv.h:3350-3355).
+constexpr int kBitsMode = 3, kBitsFlag = 2;
+
+// ------------------------------------------------------------- helpers --
+__device__ __forceinline__ int clipb(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+__device__ __forceinline__ uint32_t zz_enc(int v) { return ((uint32_t)v << 1) ^ (uint32_t)(v >> 31); }
+__device__ __forceinline__ int leb_size(uint32_t u) { return u < 0x80u ? 1 : (u < 0x4000u ? 2 : (u < 0x200000u ? 3 : (u < 0x10000000u ? 4 : 5))); }
+// 2 * floor(log2(v + 1)) + 1: the exp-Golomb length the reference charges (fdv.h:2487).
+__device__ __forceinline__ int bits_val(uint32_t v) { return 2 * (31 - __clz(v + 1u)) + 1; }
+__device__ __forceinline__ int leb_write(uint8_t *b, uint32_t u) {
+    int n = 0;
+    while (u >= 0x80u) { b[n++] = (uint8_t)(u | 0x80u); u >>= 7; }
+    b[n++] = (uint8_t)u;
+    return n;
+}
+__device__ __forceinline__ int pos_class(int idx) {
+    int i = idx >> 2, j = idx & 3;
+    if (!(i & 1) && !(j & 1)) return 0;
+    if ((i & 1) && (j & 1)) return 1;
+    return 2;
+}
+// J = D + lambda * bits with the same two roundings as the reference's C.
+__device__ __forceinline__ double rd_cost(double D, double lambda, int bits) {
+    return __dadd_rn(D, __dmul_rn(lambda, (double)bits));
+}
+
+// ------------------------------------------------------------ 4x4 core --
+__device__ __forceinline__ int fwd1(int x0, int x1, int x2, int x3, int m) {
+    int a0 = x0 + x3, a3 = x0 - x3, a1 = x1 + x2, a2 = x1 - x2;
+    return m == 0 ? a0 + a1 : (m == 1 ? a3 * 2 + a2 : (m == 2 ? a0 - a1 : a3 - a2 * 2));
+}
+__device__ __forceinline__ int inv1(int d0, int d1, int d2, int d3, int m) {
+    int z0 = d0 + d2, z1 = d0 - d2, z2 = (d1 >> 1) - d3, z3 = d1 + (d3 >> 1);
+    return m == 0 ? z0 + z3 : (m == 1 ? z1 + z2 : (m == 2 ? z1 - z2 : z0 - z3));
+}
+// Whole-block inverse on one thread (used by RDOQ candidate lanes).
+__device__ __forceinline__ void idct4_thread(const int d[16], int r[16]) {
+    int t[16];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        int z0 = d[i * 4 + 0] + d[i * 4 + 2], z1 = d[i * 4 + 0] - d[i * 4 + 2];
+        int z2 = (d[i * 4 + 1] >> 1) - d[i * 4 + 3], z3 = d[i * 4 + 1] + (d[i * 4 + 3] >> 1);
+        t[i * 4 + 0] = z0 + z3; t[i * 4 + 1] = z1 + z2; t[i * 4 + 2] = z1 - z2; t[i * 4 + 3] = z0 - z3;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        int z0 = t[0 * 4 + j] + t[2 * 4 + j], z1 = t[0 * 4 + j] - t[2 * 4 + j];
+        int z2 = (t[1 * 4 + j] >> 1) - t[3 * 4 + j], z3 = t[1 * 4 + j] + (t[3 * 4 + j] >> 1);
+        r[0 * 4 + j] = (int16_t)((z0 + z3 + 32) >> 6);
+        r[1 * 4 + j] = (int16_t)((z1 + z2 + 32) >> 6);
+        r[2 * 4 + j] = (int16_t)((z1 - z2 + 32) >> 6);
+        r[3 * 4 + j] = (int16_t)((z0 - z3 + 32) >> 6);
+    }
+}
+__device__ __forceinline__ int quant4(int w, int idx, int qp) {
+    int m = qp % 6, qbits = 15 + qp / 6, f = (1 << qbits) / 3;
+    int sign = w < 0 ? -1 : 1;
+    long long aw = (long long)(w < 0 ? -w : w);
+    return (int16_t)(sign * (int)((aw * c_MF[m][pos_class(idx)] + f) >> qbits));
+}
+__device__ __forceinline__ int dequant4(int lv, int idx, int qp) {
+    return (int32_t)(lv * c_DQV[qp % 6][pos_class(idx)]) * (int32_t)(1 << (qp / 6));
+}
+
+// ---------------------------------------------------- device structures --
+// A reference frame: luma integer plane G and its three half-pel planes
+// (H.264 b, h, j -- fdv.h:2949-2959), plus the two chroma planes, all padded
+// by `border` replicated samples; pointers address pixel (0,0).
+struct RefPlanes {
+    const uint8_t *G, *B, *H, *J, *U, *V;
+    int ys, cs;          // luma / chroma strides
+};
+
+// Per-macroblock motion kept for merge candidates (fdv.h:5680) plus the mode.
+struct MBInfo {
+    int16_t x, y;
+    uint8_t ref, inter, mode, pad;
+};
+
+// Stream capacities of one macroblock's output slot.  Structure streams are
+// indexed by model exactly as the frame blob carries them (fdv.h:4170,
+// :6198-6210): mode contexts 0-3, reference, MV x, MV y, intra sub-mode, merge
+// index; then the seven coefficient streams.  Level bytes are bounded by two
+// LEB bytes per coefficient (|level| < 8192 for 8-bit input); three are
+// reserved and overruns are detected and reported.
+constexpr int kSlotCap[16] = {1, 1, 1, 1, 1, 8, 8, 1, 1, 16, 768, 8, 1152, 8, 8, 384};
+constexpr int slot_off(int k) {
+    int o = 0;
+    for (int i = 0; i < k; ++i) o += kSlotCap[i];
+    return o;
+}
+__constant__ int c_SlotCap[16] = {1, 1, 1, 1, 1, 8, 8, 1, 1, 16, 768, 8, 1152, 8, 8, 384};
+constexpr int kSlotData = slot_off(16);                       // 2375
+constexpr int kSlotBytes = ((kSlotData + 32 + 127) / 128) * 128;  // lengths + data, 128-aligned
+__constant__ int c_SlotOff[17] = {slot_off(0), slot_off(1), slot_off(2), slot_off(3), slot_off(4),
+                                  slot_off(5), slot_off(6), slot_off(7), slot_off(8), slot_off(9),
+                                  slot_off(10), slot_off(11), slot_off(12), slot_off(13), slot_off(14),
+                                  slot_off(15), slot_off(16)};
+// Slot layout: uint16 len[16] at offset 0, data from offset 32.
+__device__ __forceinline__ uint16_t *slot_len(uint8_t *slot) { return reinterpret_cast<uint16_t *>(slot); }
+__device__ __forceinline__ uint8_t *slot_data(uint8_t *slot, int k) { return slot + 32 + c_SlotOff[k]; }
+
+// Error bits reported through the engine's status word.
+enum : unsigned {
+    kErrWaitTimeout = 1u,    // a wavefront wait gave up
+    kErrSlotOverflow = 2u,   // a symbol stream exceeded its per-block slot
+};
+
+// Bounded spin until *flag >= need.  Gives up after `limit_ns` of wall time
+// (device global timer) or when another block has already raised an error.
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool wait_at_least(const int *flag, int need, unsigned *err,
+                                              unsigned long long limit_ns) {
+    if (*(volatile const int *)flag >= need) { __threadfence(); return true; }
+    unsigned long long t0 = globaltimer();
+    for (;;) {
+        if (*(volatile const int *)flag >= need) { __threadfence(); return true; }
+        if (*(volatile unsigned *)err) return false;
+        if (globaltimer() - t0 > limit_ns) { atomicOr(err, kErrWaitTimeout); return false; }
+        __nanosleep(64);
+    }
+}
+
+}  // namespace fdvb

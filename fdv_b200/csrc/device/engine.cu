@@ -1,0 +1,448 @@
+// The batched GPU encoder engine: owns the device state of a set of
+// independent encoder units (the horizontal bands of a tile-parallel stream,
+// or whole streams) and advances all of them by one frame per step.
+//
+// One step, on one CUDA stream:
+//   1. source frames host -> device;
+//   2. analysis: the P-frame wavefront kernel over every P unit's macroblock
+//      rows and the intra CTU-wavefront kernel over every key-frame unit's
+//      plane CTU rows;
+//   3. deblock, vertical edges then horizontal edges, every plane;
+//   4. compaction of the per-block symbol slots into the per-stream byte
+//      arrays the entropy tail reads, written straight into mapped host memory;
+//   5. reference preparation: the deblocked reconstruction becomes the
+//      unit's new nearest reference (integer + half-pel planes).
+// The reference pool rotates exactly as fdv_video_encode's (fdv.h:6842-6846).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../host/engine.h"
+#include "../host/fdvb_internal.h"
+#include "common.cuh"
+#include "engine_dev.cuh"
+
+namespace fdvb {
+// kernels (pframe.cu, iframe.cu, frame_ops.cu)
+void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
+                   unsigned long long wait_ns, int grid, cudaStream_t st);
+struct IPlaneDev;
+struct ITask;
+size_t iframe_smem_bytes();
+int iframe_slot_bytes();
+void iframe_slot_offsets(int off[12]);
+void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticket, unsigned *err,
+                   unsigned long long wait_ns, int grid, cudaStream_t st);
+struct PrepTask;
+struct DbTask;
+struct CompactTask;
+void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st);
+void launch_deblock(const void *tasks, int ntasks, cudaStream_t st);
+void launch_compact(const void *tasks, int ntasks, unsigned *err, cudaStream_t st);
+void upload_tables(const int32_t c8[64], const int32_t q8[52]);
+}  // namespace fdvb
+
+using namespace fdvb;
+
+namespace {
+
+thread_local std::string g_err;
+
+#define CK(x)                                                                                     \
+    do {                                                                                          \
+        cudaError_t e_ = (x);                                                                     \
+        if (e_ != cudaSuccess) {                                                                  \
+            g_err = std::string(#x) + ": " + cudaGetErrorString(e_);                              \
+            return -3;                                                                            \
+        }                                                                                         \
+    } while (0)
+
+// Host mirrors of device descriptor layouts (must match iframe.cu / frame_ops.cu).
+struct IPlaneDevH {
+    const uint8_t *src;
+    uint8_t *rec;
+    uint8_t *mmap;
+    int *progress;
+    uint8_t *slots;
+    int w, h, cols, rows, qp;
+    double lambda;
+};
+struct ITaskH { int plane, row; };
+struct PrepTaskH {
+    const uint8_t *rec[3];
+    uint8_t *G, *B, *H, *J, *U, *V;
+    int w, h, ys, cs, border;
+};
+struct DbTaskH { uint8_t *p; int w, h, qp; };
+struct CompactTaskH {
+    const uint8_t *slots;
+    int nslots, slot_bytes, nstreams;
+    const int *off;
+    uint8_t *out;
+    size_t cap;
+};
+
+struct RefSlot {
+    uint8_t *mem = nullptr;
+    RefPlanes rp{};
+    uint8_t *G, *B, *H, *J, *U, *V;
+};
+
+struct Unit {
+    int w, h, mbw, mbh, cw, ch;
+    uint8_t *cur = nullptr, *rec = nullptr;
+    RefSlot ref[2];
+    int near_i = 0, nref = 0;
+    MBInfo *mbi = nullptr;
+    int *progress = nullptr;      // P rows, then I rows for Y, U, V
+    uint8_t *slots = nullptr;     // P macroblock slots
+    uint8_t *islots[3] = {nullptr, nullptr, nullptr};
+    uint8_t *mmap[3] = {nullptr, nullptr, nullptr};
+    int icols[3], irows[3], pw[3], ph[3];
+    uint8_t *out_h = nullptr, *out_d = nullptr;
+    size_t out_cap = 0, out_off_i[3] = {0, 0, 0};
+    int last_intra = 0, last_qp = 0;
+    fdvb_streams ps{}, is[3]{};
+};
+
+}  // namespace
+
+struct fdvb_engine {
+    int device = 0, range = 16, border = 32, nsm = 0;
+    cudaStream_t st = nullptr;
+    std::vector<Unit> units;
+    UnitDev *d_units = nullptr;
+    RowTask *d_rows = nullptr;
+    IPlaneDevH *d_planes = nullptr;
+    ITaskH *d_itasks = nullptr;
+    PrepTaskH *d_prep = nullptr;
+    DbTaskH *d_db = nullptr;
+    CompactTaskH *d_cmp = nullptr;
+    int *d_ticket = nullptr;
+    unsigned *d_err = nullptr;
+    int *d_poff = nullptr, *d_ioff = nullptr;
+    int maxrows = 0, maxitasks = 0;
+    unsigned long long wait_ns = 4000000000ull;
+};
+
+static int round_up(int v, int a) { return (v + a - 1) / a * a; }
+
+extern "C" const char *fdvb_engine_error(void) { return g_err.c_str(); }
+
+static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
+    u.w = w; u.h = h; u.mbw = w / 16; u.mbh = h / 16; u.cw = w / 2; u.ch = h / 2;
+    const size_t fs = (size_t)w * h * 3 / 2;
+    CK(cudaMalloc(&u.cur, fs));
+    CK(cudaMalloc(&u.rec, fs));
+    CK(cudaMemset(u.rec, 0, fs));
+    const int B = E->border;
+    const int ys = round_up(w + 2 * B, 64), cs = round_up(u.cw + 2 * B, 64);
+    const size_t lsz = (size_t)ys * (h + 2 * B), csz = (size_t)cs * (u.ch + 2 * B);
+    for (int r = 0; r < 2; ++r) {
+        RefSlot &s = u.ref[r];
+        CK(cudaMalloc(&s.mem, 4 * lsz + 2 * csz));
+        CK(cudaMemset(s.mem, 0, 4 * lsz + 2 * csz));
+        uint8_t *m = s.mem;
+        s.G = m + (size_t)B * ys + B; m += lsz;
+        s.B = m + (size_t)B * ys + B; m += lsz;
+        s.H = m + (size_t)B * ys + B; m += lsz;
+        s.J = m + (size_t)B * ys + B; m += lsz;
+        s.U = m + (size_t)B * cs + B; m += csz;
+        s.V = m + (size_t)B * cs + B;
+        s.rp.G = s.G; s.rp.B = s.B; s.rp.H = s.H; s.rp.J = s.J; s.rp.U = s.U; s.rp.V = s.V;
+        s.rp.ys = ys; s.rp.cs = cs;
+    }
+    const int nmb = u.mbw * u.mbh;
+    CK(cudaMalloc(&u.mbi, sizeof(MBInfo) * nmb));
+    CK(cudaMalloc(&u.slots, (size_t)kSlotBytes * nmb));
+    u.pw[0] = w; u.ph[0] = h; u.pw[1] = u.pw[2] = u.cw; u.ph[1] = u.ph[2] = u.ch;
+    int nprog = u.mbh;
+    for (int p = 0; p < 3; ++p) {
+        u.icols[p] = (u.pw[p] + 63) / 64; u.irows[p] = (u.ph[p] + 63) / 64;
+        nprog += u.irows[p];
+        CK(cudaMalloc(&u.islots[p], (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p]));
+        CK(cudaMalloc(&u.mmap[p], (size_t)(u.pw[p] / 4) * (u.ph[p] / 4)));
+    }
+    CK(cudaMalloc(&u.progress, sizeof(int) * nprog));
+    // host-mapped output: P-frame streams, or the three planes of a key frame
+    size_t pcap = 64 + (size_t)nmb * kSlotData;
+    size_t icap[3];
+    for (int p = 0; p < 3; ++p) icap[p] = 64 + (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p];
+    u.out_off_i[0] = 0; u.out_off_i[1] = icap[0]; u.out_off_i[2] = icap[0] + icap[1];
+    u.out_cap = std::max(pcap, icap[0] + icap[1] + icap[2]);
+    CK(cudaHostAlloc(&u.out_h, u.out_cap, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(&u.out_d, u.out_h, 0));
+    return 0;
+}
+
+static void free_unit(Unit &u) {
+    cudaFree(u.cur); cudaFree(u.rec);
+    for (int r = 0; r < 2; ++r) cudaFree(u.ref[r].mem);
+    cudaFree(u.mbi); cudaFree(u.slots); cudaFree(u.progress);
+    for (int p = 0; p < 3; ++p) { cudaFree(u.islots[p]); cudaFree(u.mmap[p]); }
+    if (u.out_h) cudaFreeHost(u.out_h);
+}
+
+extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
+    if (nunits <= 0 || !w || !h) { g_err = "bad arguments"; return nullptr; }
+    if (range != 16 && range != 32 && range != 64) { g_err = "search range must be 16, 32 or 64"; return nullptr; }
+    for (int i = 0; i < nunits; ++i)
+        if (w[i] <= 0 || h[i] <= 0 || (w[i] & 15) || (h[i] & 15) || w[i] > 8192 || h[i] > 8192) {
+            g_err = "unit dimensions must be positive multiples of 16, at most 8192";
+            return nullptr;
+        }
+    auto *E = new fdvb_engine();
+    E->device = device;
+    E->range = range;
+    E->border = range + 16;
+    if (cudaSetDevice(device) != cudaSuccess) { g_err = "cudaSetDevice failed (no GPU?)"; delete E; return nullptr; }
+    cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess) { g_err = "stream create failed"; delete E; return nullptr; }
+    int32_t c8[64], q8[52];
+    fdvb_c8_tables(c8, q8);
+    upload_tables(c8, q8);
+    E->units.resize(nunits);
+    int maxrows = 0, maxitasks = 0;
+    for (int i = 0; i < nunits; ++i) {
+        if (alloc_unit(E, E->units[i], w[i], h[i]) != 0) { fdvb_engine_destroy(E); return nullptr; }
+        maxrows += E->units[i].mbh;
+        for (int p = 0; p < 3; ++p) maxitasks += E->units[i].irows[p];
+    }
+    E->maxrows = maxrows; E->maxitasks = maxitasks;
+    bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_rows, sizeof(RowTask) * maxrows) == cudaSuccess &&
+              cudaMalloc(&E->d_planes, sizeof(IPlaneDevH) * 3 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_itasks, sizeof(ITaskH) * maxitasks) == cudaSuccess &&
+              cudaMalloc(&E->d_prep, sizeof(PrepTaskH) * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_db, sizeof(DbTaskH) * 3 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_cmp, sizeof(CompactTaskH) * 3 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_ticket, sizeof(int) * 2) == cudaSuccess &&
+              cudaMalloc(&E->d_err, sizeof(unsigned)) == cudaSuccess &&
+              cudaMalloc(&E->d_poff, sizeof(int) * 16) == cudaSuccess &&
+              cudaMalloc(&E->d_ioff, sizeof(int) * 12) == cudaSuccess;
+    if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
+    int poff[16], ioff[12];
+    for (int k = 0; k < 16; ++k) { int o = 0; for (int i = 0; i < k; ++i) o += kSlotCap[i]; poff[k] = o; }
+    iframe_slot_offsets(ioff);
+    cudaMemcpy(E->d_poff, poff, sizeof poff, cudaMemcpyHostToDevice);
+    cudaMemcpy(E->d_ioff, ioff, sizeof ioff, cudaMemcpyHostToDevice);
+    cudaMemset(E->d_err, 0, sizeof(unsigned));
+    if (cudaDeviceSynchronize() != cudaSuccess) { g_err = "device init failed"; fdvb_engine_destroy(E); return nullptr; }
+    return E;
+}
+
+extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
+    if (!E) return;
+    if (E->st) cudaStreamSynchronize(E->st);
+    for (auto &u : E->units) free_unit(u);
+    cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
+    cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
+    cudaFree(E->d_poff); cudaFree(E->d_ioff);
+    if (E->st) cudaStreamDestroy(E->st);
+    delete E;
+}
+
+extern "C" int fdvb_engine_units(const fdvb_engine *E) { return E ? (int)E->units.size() : 0; }
+
+// Parse a compacted output region: uint32 len[n] then the streams.
+static void parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
+    const uint32_t *len = reinterpret_cast<const uint32_t *>(p);
+    const uint8_t *d = p + 4 * n;
+    for (int k = 0; k < 16; ++k) { s->s[k] = nullptr; s->n[k] = 0; }
+    for (int k = 0; k < n; ++k) { s->s[k] = d; s->n[k] = len[k]; d += len[k]; }
+}
+
+static int prep_refs(fdvb_engine *E, const std::vector<int> &which) {
+    std::vector<PrepTaskH> pt;
+    int maxw = 0, maxh = 0;
+    for (int i : which) {
+        Unit &u = E->units[i];
+        RefSlot &s = u.ref[1 - u.near_i];
+        PrepTaskH t;
+        t.rec[0] = u.rec; t.rec[1] = u.rec + (size_t)u.w * u.h; t.rec[2] = t.rec[1] + (size_t)u.cw * u.ch;
+        t.G = s.G; t.B = s.B; t.H = s.H; t.J = s.J; t.U = s.U; t.V = s.V;
+        t.w = u.w; t.h = u.h; t.ys = s.rp.ys; t.cs = s.rp.cs; t.border = E->border;
+        pt.push_back(t);
+        maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h);
+    }
+    if (pt.empty()) return 0;
+    CK(cudaMemcpyAsync(E->d_prep, pt.data(), sizeof(PrepTaskH) * pt.size(), cudaMemcpyHostToDevice, E->st));
+    launch_refprep(E->d_prep, (int)pt.size(), maxw, maxh, E->border, E->st);
+    CK(cudaGetLastError());
+    for (int i : which) {
+        Unit &u = E->units[i];
+        u.near_i = 1 - u.near_i;
+    }
+    return 0;
+}
+
+extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                                const double *lscale, const int *force_skip) {
+    if (!E) return -1;
+    const int nu = (int)E->units.size();
+    for (int i = 0; i < nu; ++i) {
+        if (qp[i] < 0 || qp[i] > 51) { g_err = "qp out of range"; return -1; }
+        bool fs = force_skip && force_skip[i];
+        if (!fs && (!planes || !planes[3 * i] || !planes[3 * i + 1] || !planes[3 * i + 2])) {
+            g_err = "missing source frame";
+            return -1;
+        }
+        if (fs && (is_intra[i] || E->units[i].nref == 0)) { g_err = "a held frame needs a reference"; return -1; }
+        if (!is_intra[i] && E->units[i].nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
+    }
+    CK(cudaSetDevice(E->device));
+    // 1. sources
+    for (int i = 0; i < nu; ++i) {
+        Unit &u = E->units[i];
+        if (force_skip && force_skip[i]) continue;
+        const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
+        CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, cudaMemcpyHostToDevice, E->st));
+    }
+    // 2. descriptors
+    std::vector<UnitDev> ud(nu);
+    std::vector<RowTask> rows;
+    std::vector<IPlaneDevH> iplanes;
+    std::vector<ITaskH> itasks;
+    std::vector<CompactTaskH> cmp;
+    std::vector<DbTaskH> db;
+    for (int i = 0; i < nu; ++i) {
+        Unit &u = E->units[i];
+        UnitDev &d = ud[i];
+        d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh;
+        d.cur[0] = u.cur; d.cur[1] = u.cur + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
+        d.rec[0] = u.rec; d.rec[1] = u.rec + (size_t)u.w * u.h; d.rec[2] = d.rec[1] + (size_t)u.cw * u.ch;
+        const int navail = u.nref >= 2 ? 2 : 1;
+        d.ref[0] = u.ref[u.near_i].rp;
+        d.ref[1] = navail == 2 ? u.ref[1 - u.near_i].rp : u.ref[u.near_i].rp;
+        d.mbi = u.mbi; d.progress = u.progress; d.slots = u.slots;
+        d.lambda = fdvb_lambda(qp[i], lscale ? lscale[i] : 1.0);
+        d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
+        u.last_intra = is_intra[i];
+        u.last_qp = qp[i];
+        if (!is_intra[i]) {
+            for (int r = 0; r < u.mbh; ++r) rows.push_back({i, r});
+            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d, u.out_cap};
+            cmp.push_back(c);
+        } else {
+            int prog = u.mbh;
+            for (int p = 0; p < 3; ++p) {
+                IPlaneDevH P;
+                P.src = d.cur[p]; P.rec = d.rec[p]; P.mmap = u.mmap[p]; P.progress = u.progress + prog;
+                P.slots = u.islots[p]; P.w = u.pw[p]; P.h = u.ph[p]; P.cols = u.icols[p]; P.rows = u.irows[p];
+                P.qp = qp[i]; P.lambda = fdvb_lambda(qp[i], 1.0);
+                int pid = (int)iplanes.size();
+                iplanes.push_back(P);
+                for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
+                prog += u.irows[p];
+                CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
+                               u.out_d + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p]};
+                cmp.push_back(c);
+            }
+        }
+        for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[i]});
+        int nprog = u.mbh + u.irows[0] + u.irows[1] + u.irows[2];
+        CK(cudaMemsetAsync(u.progress, 0, sizeof(int) * nprog, E->st));
+    }
+    // Interleave the rows of different units so the early rows of every unit
+    // start first (each unit's rows stay in order, which is all the ticket
+    // scheme needs).
+    {
+        std::vector<RowTask> inter;
+        int maxh = 0;
+        for (auto &u : E->units) maxh = std::max(maxh, u.mbh);
+        for (int r = 0; r < maxh; ++r)
+            for (auto &t : rows) if (t.row == r) inter.push_back(t);
+        rows.swap(inter);
+        std::vector<ITaskH> it2;
+        int maxr = 0;
+        for (auto &t : itasks) maxr = std::max(maxr, t.row + 1);
+        for (int r = 0; r < maxr; ++r)
+            for (auto &t : itasks) if (t.row == r) it2.push_back(t);
+        itasks.swap(it2);
+    }
+    CK(cudaMemcpyAsync(E->d_units, ud.data(), sizeof(UnitDev) * nu, cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
+    CK(cudaMemsetAsync(E->d_err, 0, sizeof(unsigned), E->st));
+    if (!rows.empty()) {
+        CK(cudaMemcpyAsync(E->d_rows, rows.data(), sizeof(RowTask) * rows.size(), cudaMemcpyHostToDevice, E->st));
+        int grid = std::min((int)rows.size(), E->nsm);
+        launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->st);
+        CK(cudaGetLastError());
+    }
+    if (!itasks.empty()) {
+        CK(cudaMemcpyAsync(E->d_planes, iplanes.data(), sizeof(IPlaneDevH) * iplanes.size(), cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemcpyAsync(E->d_itasks, itasks.data(), sizeof(ITaskH) * itasks.size(), cudaMemcpyHostToDevice, E->st));
+        int grid = std::min((int)itasks.size(), E->nsm);
+        launch_iframe(E->d_planes, E->d_itasks, (int)itasks.size(), E->d_ticket + 1, E->d_err, E->wait_ns, grid, E->st);
+        CK(cudaGetLastError());
+    }
+    // 3. deblock, 4. compact
+    CK(cudaMemcpyAsync(E->d_db, db.data(), sizeof(DbTaskH) * db.size(), cudaMemcpyHostToDevice, E->st));
+    launch_deblock(E->d_db, (int)db.size(), E->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(E->d_cmp, cmp.data(), sizeof(CompactTaskH) * cmp.size(), cudaMemcpyHostToDevice, E->st));
+    launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
+    CK(cudaGetLastError());
+    // 5. the new reference
+    std::vector<int> all(nu);
+    for (int i = 0; i < nu; ++i) all[i] = i;
+    if (prep_refs(E, all) != 0) return -3;
+    for (int i = 0; i < nu; ++i) {
+        Unit &u = E->units[i];
+        u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+    }
+    CK(cudaStreamSynchronize(E->st));
+    unsigned err = 0;
+    CK(cudaMemcpy(&err, E->d_err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err) {
+        g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out" : "symbol slot overflow";
+        return -4;
+    }
+    for (int i = 0; i < nu; ++i) {
+        Unit &u = E->units[i];
+        if (!u.last_intra) parse_streams(u.out_h, 16, &u.ps);
+        else for (int p = 0; p < 3; ++p) parse_streams(u.out_h + u.out_off_i[p], 12, &u.is[p]);
+    }
+    return 0;
+}
+
+extern "C" const fdvb_streams *fdvb_engine_pstreams(fdvb_engine *E, int unit) {
+    if (!E || unit < 0 || unit >= (int)E->units.size() || E->units[unit].last_intra) return nullptr;
+    return &E->units[unit].ps;
+}
+extern "C" const fdvb_streams *fdvb_engine_istreams(fdvb_engine *E, int unit, int plane) {
+    if (!E || unit < 0 || unit >= (int)E->units.size() || !E->units[unit].last_intra || plane < 0 || plane > 2)
+        return nullptr;
+    return &E->units[unit].is[plane];
+}
+extern "C" int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420) {
+    if (!E || unit < 0 || unit >= (int)E->units.size() || !i420) return -1;
+    Unit &u = E->units[unit];
+    CK(cudaMemcpy(i420, u.rec, (size_t)u.w * u.h * 3 / 2, cudaMemcpyDeviceToHost));
+    return 0;
+}
+// Seed a unit's reference pool from host frames (tight I420): nearest, and the
+// second one (NULL = none).  The next step then codes a P-frame against them.
+extern "C" int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *near_i420, const uint8_t *far_i420) {
+    if (!E || unit < 0 || unit >= (int)E->units.size() || !near_i420) return -1;
+    Unit &u = E->units[unit];
+    const size_t fs = (size_t)u.w * u.h * 3 / 2;
+    std::vector<int> one{unit};
+    u.near_i = 0;
+    if (far_i420) {
+        // far first: prep writes slot 1 - near_i and then flips near_i
+        CK(cudaMemcpyAsync(u.rec, far_i420, fs, cudaMemcpyHostToDevice, E->st));
+        if (prep_refs(E, one) != 0) return -3;
+    }
+    CK(cudaMemcpyAsync(u.rec, near_i420, fs, cudaMemcpyHostToDevice, E->st));
+    if (prep_refs(E, one) != 0) return -3;
+    CK(cudaStreamSynchronize(E->st));
+    u.nref = far_i420 ? 2 : 1;
+    return 0;
+}

@@ -1,0 +1,26 @@
+// Device-side descriptors of the batched encoder engine.
+#pragma once
+#include "common.cuh"
+
+namespace fdvb {
+
+// One encoder unit (a horizontal band of a stream, or a whole stream) as the
+// analysis kernels see it for the current frame.
+struct UnitDev {
+    int w, h, mbw, mbh;
+    const uint8_t *cur[3];      // source planes, tight
+    uint8_t *rec[3];            // reconstruction, tight
+    RefPlanes ref[2];           // nearest, and second (== nearest when only one is valid)
+    MBInfo *mbi;                // per macroblock, this frame
+    int *progress;              // per macroblock row: macroblocks finished
+    uint8_t *slots;             // per macroblock symbol slot (P-frames)
+    double lambda;
+    int qp, navail, force_skip, range;
+};
+
+struct RowTask { int unit, row; };
+
+// Stream ids of the P-frame slot (fdv.h:4170, :6198-6210).
+enum { PS_REF = 4, PS_MVX = 5, PS_MVY = 6, PS_SUB = 7, PS_MERGE = 8, PS_CN = 9 };
+
+}  // namespace fdvb

@@ -1,0 +1,163 @@
+// Per-frame passes around the analysis kernels.
+//
+//  * refprep: the deblocked reconstruction becomes a reference frame -- the
+//    integer plane with its border replicated (load_ref/plane_extend,
+//    fdv.h:5183-5193, :1603-1624) and the three H.264 half-pel planes b, h, j
+//    (fdv.h:2932-2959), computed once per frame instead of per probe.
+//  * deblock: the 8x8-grid edge filter (fdv.h:3491-3501, :3617-3625), edge
+//    parallel: every vertical edge of the plane, then every horizontal edge.
+//    Within a pass no two edges touch the same sample (edges are 8 apart and a
+//    filter reads +-2 and writes +-1 samples), so each pass is data-parallel;
+//    only the order of the passes matters.
+//  * compact: per-macroblock symbol slots are concatenated, per stream, in
+//    raster order -- the order the reference appends them -- directly into
+//    host-mapped memory.
+#include "common.cuh"
+#include "engine_dev.cuh"
+
+namespace fdvb {
+
+struct PrepTask {
+    const uint8_t *rec[3];
+    uint8_t *G, *B, *H, *J, *U, *V;   // pointers at pixel (0,0)
+    int w, h, ys, cs, border;
+};
+
+__device__ __forceinline__ int rpx(const uint8_t *p, int w, int h, int x, int y) {
+    x = x < 0 ? 0 : (x >= w ? w - 1 : x);
+    y = y < 0 ? 0 : (y >= h ? h - 1 : y);
+    return p[(size_t)y * w + x];
+}
+__device__ __forceinline__ int tap6(int a, int b, int c, int d, int e, int f) {
+    return a - 5 * b + 20 * c + 20 * d - 5 * e + f;
+}
+__device__ __forceinline__ int hfr(const uint8_t *p, int w, int h, int x, int y) {
+    return tap6(rpx(p, w, h, x - 2, y), rpx(p, w, h, x - 1, y), rpx(p, w, h, x, y),
+                rpx(p, w, h, x + 1, y), rpx(p, w, h, x + 2, y), rpx(p, w, h, x + 3, y));
+}
+
+// Grid: x over padded columns, y over padded rows, z = task.  Luma planes.
+__global__ void refprep_luma_kernel(const PrepTask *tasks) {
+    const PrepTask &T = tasks[blockIdx.z];
+    const int B = T.border, pw = T.w + 2 * B, ph = T.h + 2 * B;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= pw || py >= ph) return;
+    const int x = px - B, y = py - B;
+    const uint8_t *r = T.rec[0];
+    const int w = T.w, h = T.h;
+    const long o = (long)y * T.ys + x;
+    T.G[o] = (uint8_t)rpx(r, w, h, x, y);
+    T.B[o] = (uint8_t)clipb((hfr(r, w, h, x, y) + 16) >> 5);
+    int v = tap6(rpx(r, w, h, x, y - 2), rpx(r, w, h, x, y - 1), rpx(r, w, h, x, y),
+                 rpx(r, w, h, x, y + 1), rpx(r, w, h, x, y + 2), rpx(r, w, h, x, y + 3));
+    T.H[o] = (uint8_t)clipb((v + 16) >> 5);
+    int jj = tap6(hfr(r, w, h, x, y - 2), hfr(r, w, h, x, y - 1), hfr(r, w, h, x, y),
+                  hfr(r, w, h, x, y + 1), hfr(r, w, h, x, y + 2), hfr(r, w, h, x, y + 3));
+    T.J[o] = (uint8_t)clipb((jj + 512) >> 10);
+}
+
+__global__ void refprep_chroma_kernel(const PrepTask *tasks) {
+    const PrepTask &T = tasks[blockIdx.z];
+    const int B = T.border, cw = T.w / 2, ch = T.h / 2, pw = cw + 2 * B, ph = ch + 2 * B;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= pw || py >= ph) return;
+    const int x = px - B, y = py - B;
+    const long o = (long)y * T.cs + x;
+    T.U[o] = (uint8_t)rpx(T.rec[1], cw, ch, x, y);
+    T.V[o] = (uint8_t)rpx(T.rec[2], cw, ch, x, y);
+}
+
+// ------------------------------------------------------------- deblock --
+struct DbTask {
+    uint8_t *p;
+    int w, h, qp;
+};
+
+__device__ __forceinline__ void filter_edge(uint8_t *a, long step, int alpha, int beta, int tc) {
+    int p1 = a[-2 * step], p0 = a[-step], q0 = a[0], q1 = a[step];
+    if (abs(p0 - q0) < alpha && abs(p1 - p0) < beta && abs(q1 - q0) < beta) {
+        int d = ((q0 - p0) * 4 + (p1 - q1) + 4) >> 3;
+        d = d < -tc ? -tc : (d > tc ? tc : d);
+        a[-step] = (uint8_t)clipb(p0 + d);
+        a[0] = (uint8_t)clipb(q0 - d);
+    }
+}
+
+// Vertical edges: one thread per (row, edge x = 8, 16, ...).  Grid z = task.
+__global__ void deblock_v_kernel(const DbTask *tasks) {
+    const DbTask &T = tasks[blockIdx.z];
+    const int ne = T.w / 8 - 1;
+    if (ne <= 0) return;
+    const long n = (long)ne * T.h;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        int y = (int)(i / ne), e = (int)(i % ne);
+        filter_edge(T.p + (long)y * T.w + 8 * (e + 1), 1, 6 + T.qp, 2 + T.qp / 4, 1 + T.qp / 10);
+    }
+}
+// Horizontal edges: one thread per (edge y = 8, 16, ..., column).
+__global__ void deblock_h_kernel(const DbTask *tasks) {
+    const DbTask &T = tasks[blockIdx.z];
+    const int ne = T.h / 8 - 1;
+    if (ne <= 0) return;
+    const long n = (long)ne * T.w;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        int e = (int)(i / T.w), x = (int)(i % T.w);
+        filter_edge(T.p + (long)8 * (e + 1) * T.w + x, T.w, 6 + T.qp, 2 + T.qp / 4, 1 + T.qp / 10);
+    }
+}
+
+// ------------------------------------------------------------- compact --
+// Streams of one unit-frame: `nstreams` streams, slot k of block b at
+// slots + b*slot_bytes, lengths uint16 at slot start, data at 32 + off[k].
+struct CompactTask {
+    const uint8_t *slots;
+    int nslots, slot_bytes, nstreams;
+    const int *off;        // device array [nstreams] of data offsets within a slot
+    uint8_t *out;          // host-mapped: uint32 len[nstreams], then the streams back to back
+    size_t cap;
+};
+
+// One block per task, 1024 threads: 64 threads per stream scan the slot
+// lengths, then each thread copies its chunk of slots.
+__global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks, unsigned *err) {
+    const CompactTask &T = tasks[blockIdx.x];
+    const int tid = threadIdx.x, k = tid >> 6, t = tid & 63;
+    __shared__ unsigned s_tot[16][64];
+    __shared__ unsigned s_base[17];
+    const int nb = T.nslots, chunk = (nb + 63) / 64, b0 = t * chunk, b1 = min(nb, b0 + chunk);
+    unsigned mine = 0;
+    if (k < T.nstreams)
+        for (int b = b0; b < b1; ++b) mine += reinterpret_cast<const uint16_t *>(T.slots + (size_t)b * T.slot_bytes)[k];
+    s_tot[k][t] = mine;
+    __syncthreads();
+    if (tid < 16) {
+        unsigned acc = 0;
+        for (int i = 0; i < 64; ++i) { unsigned v = s_tot[tid][i]; s_tot[tid][i] = acc; acc += v; }
+        s_base[tid] = acc;  // stream total, turned into a base below
+    }
+    __syncthreads();
+    if (tid == 0) {
+        unsigned acc = 0;
+        for (int s = 0; s < T.nstreams; ++s) { unsigned tot = s_base[s]; s_base[s] = acc; acc += tot; }
+        s_base[16] = acc;
+    }
+    __syncthreads();
+    const size_t hdr = 4 * (size_t)T.nstreams;
+    if (hdr + s_base[16] > T.cap) { if (tid == 0) atomicOr(err, kErrSlotOverflow); return; }
+    if (tid < T.nstreams) {
+        unsigned len = (tid + 1 < T.nstreams ? s_base[tid + 1] : s_base[16]) - s_base[tid];
+        reinterpret_cast<unsigned *>(T.out)[tid] = len;
+    }
+    if (k < T.nstreams) {
+        uint8_t *dst = T.out + hdr + s_base[k] + s_tot[k][t];
+        for (int b = b0; b < b1; ++b) {
+            const uint8_t *slot = T.slots + (size_t)b * T.slot_bytes;
+            int n = reinterpret_cast<const uint16_t *>(slot)[k];
+            const uint8_t *src = slot + 32 + T.off[k];
+            for (int i = 0; i < n; ++i) dst[i] = src[i];
+            dst += n;
+        }
+    }
+}
+
+}  // namespace fdvb

@@ -1,0 +1,410 @@
+// The public C ABI of libfdvb200: the fdv.h encode entry points on top of the
+// batched GPU engine, the inner engine ABI, the host entropy tail and the
+// synthetic content generator (include/fdv_b200.h).
+//
+// The stream containers written here follow the reference byte for byte:
+//   video stream     [nframes u16][w u16][h u16][qp u8][keyint u8] then per
+//                    frame [blob_len u32][blob]                     fdv.h:6764-6805
+//   key-frame blob   three [len u32][intra plane blob], Y U V       fdv.h:5529-5538
+//   tiled container  [w u16][h u16][nframes u16][qp u8][keyint u8][nbands u16]
+//                    [band_mbrows u16] then per band [len u32][video stream]
+//                                                                   fdv.h:7098-7101, :7174-7236
+//   file head        "FDV1" [version u8][kind u8][fps u16][payload_len u32]
+//                                                                   fdv.h:7448-7464
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+#include "fdvb_internal.h"
+
+namespace {
+
+thread_local std::string g_api_err;
+int g_range = 16;
+int g_device = 0;
+
+void set_err(const char *m) { g_api_err = m; }
+void set_engine_err() { g_api_err = std::string("engine: ") + fdvb_engine_error(); }
+
+// One unit's host-side stream state: the entropy cache and the coded bytes.
+struct UnitStream {
+    std::unique_ptr<fdvb_tabcache> tc{new fdvb_tabcache()};
+    std::vector<uint8_t> bytes;
+    int w = 0, h = 0;
+    size_t tmp_cap = 0;
+    std::vector<uint8_t> tmp;
+    int fail = 0;
+};
+
+void stream_header(std::vector<uint8_t> &b, int nframes, int w, int h, int qp, int keyint) {
+    uint8_t hd[8];
+    size_t o = 0;
+    o = fdvb_put16(hd, o, (unsigned)nframes);
+    o = fdvb_put16(hd, o, (unsigned)w);
+    o = fdvb_put16(hd, o, (unsigned)h);
+    hd[o++] = (uint8_t)qp;
+    hd[o++] = (uint8_t)keyint;
+    b.insert(b.end(), hd, hd + o);
+}
+
+// Entropy-code unit u's analysis output of the engine's last step and append
+// [blob_len u32][blob] to its stream (the tail of fdv_video_encode's frame loop).
+int code_unit_frame(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp) {
+    size_t blob = 0;
+    if (us.tmp.size() < us.tmp_cap) us.tmp.resize(us.tmp_cap);
+    if (is_intra) {
+        // A key frame restarts the table chain and the adaptive history.
+        memset(us.tc.get(), 0, sizeof(fdvb_tabcache));
+        const int pw[3] = {us.w, us.w / 2, us.w / 2}, ph[3] = {us.h, us.h / 2, us.h / 2};
+        size_t o = 0;
+        for (int p = 0; p < 3; ++p) {
+            const fdvb_streams *s = fdvb_engine_istreams(E, u, p);
+            if (!s) return -1;
+            size_t bcap = (size_t)pw[p] * ph[p] * 2 + 4096;
+            std::vector<uint8_t> pb(bcap);
+            size_t bl = fdvb_image_blob(s, pw[p], ph[p], qp, pb.data(), bcap, nullptr);
+            if (!bl || o + 4 + bl > us.tmp_cap) return -1;
+            o = fdvb_put32(us.tmp.data(), o, (uint32_t)bl);
+            memcpy(us.tmp.data() + o, pb.data(), bl);
+            o += bl;
+        }
+        blob = o;
+    } else {
+        const fdvb_streams *s = fdvb_engine_pstreams(E, u);
+        if (!s) return -1;
+        blob = fdvb_pframe_blob(s, qp, us.tc.get(), us.tmp.data(), us.tmp_cap, nullptr);
+        if (!blob) return -1;
+    }
+    uint8_t l4[4];
+    fdvb_put32(l4, 0, (uint32_t)blob);
+    us.bytes.insert(us.bytes.end(), l4, l4 + 4);
+    us.bytes.insert(us.bytes.end(), us.tmp.begin(), us.tmp.begin() + (long)blob);
+    return 0;
+}
+
+// Entropy-code every unit, spreading units over up to nthreads host threads.
+int code_all(fdvb_engine *E, std::vector<UnitStream> &us, int is_intra, int qp, int nthreads) {
+    const int n = (int)us.size();
+    int nt = std::max(1, std::min(nthreads, n));
+    if (nt == 1) {
+        for (int u = 0; u < n; ++u) if (code_unit_frame(E, u, us[u], is_intra, qp) != 0) return -1;
+        return 0;
+    }
+    std::vector<int> rc(nt, 0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (int u = t; u < n; u += nt) if (code_unit_frame(E, u, us[u], is_intra, qp) != 0) rc[t] = -1;
+        });
+    for (auto &x : th) x.join();
+    for (int r : rc) if (r) return -1;
+    return 0;
+}
+
+int default_threads() {
+    unsigned hc = std::thread::hardware_concurrency();
+    return hc ? (int)hc : 1;
+}
+
+}  // namespace
+
+struct fdv_encoder {
+    int w = 0, h = 0, qp = 0, keyint = 0, n = 0, key_due = 0;
+    int nbands = 0, band_mbrows = 0, nthreads = 1;   // nbands == 0: single stream
+    fdvb_engine *E = nullptr;
+    std::vector<UnitStream> us;
+    std::vector<int> by0, bh;
+};
+
+extern "C" {
+
+const char *fdvb_last_error(void) { return g_api_err.c_str(); }
+
+int fdvb_set_search_range(int range) {
+    if (range != 16 && range != 32 && range != 64) { set_err("search range must be 16, 32 or 64"); return -1; }
+    int old = g_range;
+    g_range = range;
+    return old;
+}
+int fdvb_get_search_range(void) { return g_range; }
+int fdvb_set_device(int device) {
+    if (device < 0) return -1;
+    int old = g_device;
+    g_device = device;
+    return old;
+}
+
+size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payload, size_t payload_len) {
+    if (!out || payload_len > 0xffffffffu || cap < 12 + payload_len) return 0;
+    if (kind != 0 && kind != 1) return 0;
+    if (fps <= 0 || fps > 65535) fps = 25;
+    memmove(out + 12, payload, payload_len);
+    memcpy(out, "FDV1", 4);
+    out[4] = 1;
+    out[5] = (uint8_t)kind;
+    size_t o = 6;
+    o = fdvb_put16(out, o, (unsigned)fps);
+    fdvb_put32(out, o, (uint32_t)payload_len);
+    return 12 + payload_len;
+}
+
+// Encode nframes over a set of horizontal bands (nbands == 1: the plain
+// stream) and leave each band's video stream in us[b].bytes.
+static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
+                        int bh_full, int nthreads, std::vector<UnitStream> &us) {
+    const int nb = (h + bh_full - 1) / bh_full, cw = w / 2, ch = h / 2;
+    std::vector<int> W(nb, w), H(nb), Y0(nb);
+    for (int b = 0; b < nb; ++b) { Y0[b] = b * bh_full; H[b] = std::min(bh_full, h - Y0[b]); }
+    fdvb_engine *E = fdvb_engine_create(nb, W.data(), H.data(), g_range, g_device);
+    if (!E) { set_engine_err(); return -1; }
+    us.clear();
+    us.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        us[b].w = w; us[b].h = H[b];
+        us[b].tmp_cap = (size_t)w * H[b] * 3 + 8192;
+        stream_header(us[b].bytes, nframes, w, H[b], qp, keyint);
+    }
+    std::vector<const uint8_t *> planes(3 * nb);
+    std::vector<int> intra(nb), qps(nb, qp);
+    int rc = 0;
+    for (int f = 0; f < nframes && rc == 0; ++f) {
+        const uint8_t *fy = frames[f], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+        const int is_intra = (f == 0) || (keyint > 0 && f % keyint == 0);
+        for (int b = 0; b < nb; ++b) {
+            planes[3 * b] = fy + (size_t)Y0[b] * w;
+            planes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+            planes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+            intra[b] = is_intra;
+        }
+        if (fdvb_engine_step(E, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) { set_engine_err(); rc = -1; break; }
+        if (code_all(E, us, is_intra, qp, nthreads) != 0) { set_err("entropy coding failed"); rc = -1; }
+    }
+    fdvb_engine_destroy(E);
+    return rc;
+}
+
+size_t fdv_video_encode(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
+                        uint8_t *out, size_t cap) {
+    if (!frames || !out || nframes <= 0 || w <= 0 || h <= 0 || (w & 15) || (h & 15)) { set_err("bad arguments"); return 0; }
+    if (qp < 0 || qp > 51 || nframes > 65535 || w > 8192 || h > 8192) { set_err("bad arguments"); return 0; }
+    if (keyint < 0) keyint = 0;
+    if (keyint > 255) keyint = 255;
+    std::vector<UnitStream> us;
+    if (encode_bands(frames, nframes, w, h, qp, keyint, h, 1, us) != 0) return 0;
+    const auto &b = us[0].bytes;
+    if (b.size() > cap) { set_err("output buffer too small"); return 0; }
+    memcpy(out, b.data(), b.size());
+    return b.size();
+}
+
+size_t fdv_vtile_encode(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
+                        int band_mbrows, int nthreads, uint8_t *out, size_t cap) {
+    if (!frames || !out || nframes <= 0 || w <= 0 || h <= 0 || (w & 15) || (h & 15) || band_mbrows < 1) {
+        set_err("bad arguments");
+        return 0;
+    }
+    if (cap < 12 || qp < 0 || qp > 51 || nframes > 65535 || w > 8192 || h > 8192) { set_err("bad arguments"); return 0; }
+    const int bh_full = band_mbrows * 16, nbands = (h + bh_full - 1) / bh_full;
+    if (keyint < 0) keyint = 0;
+    if (keyint > 255) keyint = 255;
+    if (nthreads < 1) nthreads = 1;
+    std::vector<UnitStream> us;
+    if (encode_bands(frames, nframes, w, h, qp, keyint, bh_full, nthreads, us) != 0) return 0;
+    size_t o = 0;
+    o = fdvb_put16(out, o, (unsigned)w);
+    o = fdvb_put16(out, o, (unsigned)h);
+    o = fdvb_put16(out, o, (unsigned)nframes);
+    out[o++] = (uint8_t)qp;
+    out[o++] = (uint8_t)keyint;
+    o = fdvb_put16(out, o, (unsigned)nbands);
+    o = fdvb_put16(out, o, (unsigned)band_mbrows);
+    for (int b = 0; b < nbands; ++b) {
+        const auto &s = us[b].bytes;
+        if (o + 4 + s.size() > cap) { set_err("output buffer too small"); return 0; }
+        o = fdvb_put32(out, o, (uint32_t)s.size());
+        memcpy(out + o, s.data(), s.size());
+        o += s.size();
+    }
+    return o;
+}
+
+// ------------------------------------------------------------ streaming --
+static fdv_encoder *enc_new(int w, int h, int qp, int keyint, int band_mbrows, int nthreads, bool tiled) {
+    if (w <= 0 || h <= 0 || (w & 15) || (h & 15) || w > 8192 || h > 8192) { set_err("bad dimensions"); return nullptr; }
+    if (qp < 0 || qp > 51) { set_err("bad qp"); return nullptr; }
+    if (tiled && band_mbrows < 1) { set_err("bad band_mbrows"); return nullptr; }
+    if (keyint < 0) keyint = 0;
+    if (keyint > 255) keyint = 255;
+    auto *e = new fdv_encoder();
+    e->w = w; e->h = h; e->qp = qp; e->keyint = keyint;
+    const int bh_full = tiled ? band_mbrows * 16 : h;
+    const int nb = (h + bh_full - 1) / bh_full;
+    if (tiled && nb > 65535) { delete e; set_err("too many bands"); return nullptr; }
+    e->nbands = tiled ? nb : 0;
+    e->band_mbrows = band_mbrows;
+    e->nthreads = nthreads < 1 ? 1 : nthreads;
+    std::vector<int> W(nb, w), H(nb);
+    for (int b = 0; b < nb; ++b) { e->by0.push_back(b * bh_full); H[b] = std::min(bh_full, h - b * bh_full); e->bh.push_back(H[b]); }
+    e->E = fdvb_engine_create(nb, W.data(), H.data(), g_range, g_device);
+    if (!e->E) { set_engine_err(); delete e; return nullptr; }
+    e->us.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        e->us[b].w = w; e->us[b].h = H[b];
+        e->us[b].tmp_cap = (size_t)w * H[b] * 3 + 8192;
+        stream_header(e->us[b].bytes, 0, w, H[b], qp, keyint);   // frame count patched at finish
+    }
+    return e;
+}
+
+fdv_encoder *fdv_enc_open(int w, int h, int qp, int keyint) { return enc_new(w, h, qp, keyint, 0, 1, false); }
+fdv_encoder *fdv_enc_open_tiled(int w, int h, int qp, int keyint, int band_mbrows, int nthreads) {
+    return enc_new(w, h, qp, keyint, band_mbrows, nthreads, true);
+}
+
+void fdv_enc_close(fdv_encoder *e) {
+    if (!e) return;
+    fdvb_engine_destroy(e->E);
+    delete e;
+}
+
+int fdv_enc_count(const fdv_encoder *e) { return e ? e->n : 0; }
+size_t fdv_enc_bytes(const fdv_encoder *e) {
+    if (!e) return 0;
+    size_t t = 0;
+    for (const auto &u : e->us) t += u.bytes.size();
+    return t;
+}
+int fdv_enc_set_bitrate(fdv_encoder *e, int bits_per_second, int fps, double bufsecs) {
+    (void)e; (void)bits_per_second; (void)fps; (void)bufsecs;
+    set_err("average-bitrate control is not provided by this library");
+    return -1;
+}
+
+// enc_push (fdv.h:8231-8377) for every band at once; a held frame re-emits
+// the reference as all-SKIP and carries a due key frame to the next real one.
+static int enc_push(fdv_encoder *e, const uint8_t *i420, int force_skip) {
+    if (!e || (!i420 && !force_skip)) return -1;
+    if (e->n >= 65535) { set_err("frame count limit"); return -1; }
+    const int f = e->n;
+    int is_intra = (f == 0) || e->key_due || (e->keyint > 0 && f % e->keyint == 0);
+    if (force_skip) { e->key_due = is_intra; is_intra = 0; }
+    else e->key_due = 0;
+    const int nb = (int)e->us.size(), w = e->w, h = e->h, cw = w / 2, ch = h / 2;
+    std::vector<const uint8_t *> planes(3 * nb, nullptr);
+    std::vector<int> intra(nb, is_intra), qps(nb, e->qp), fs(nb, force_skip);
+    if (i420) {
+        const uint8_t *fy = i420, *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+        for (int b = 0; b < nb; ++b) {
+            planes[3 * b] = fy + (size_t)e->by0[b] * w;
+            planes[3 * b + 1] = fu + (size_t)(e->by0[b] / 2) * cw;
+            planes[3 * b + 2] = fv + (size_t)(e->by0[b] / 2) * cw;
+        }
+    }
+    if (fdvb_engine_step(e->E, planes.data(), intra.data(), qps.data(), nullptr, fs.data()) != 0) { set_engine_err(); return -1; }
+    if (code_all(e->E, e->us, is_intra, e->qp, e->nthreads) != 0) { set_err("entropy coding failed"); return -1; }
+    ++e->n;
+    return 0;
+}
+
+int fdv_enc_frame(fdv_encoder *e, const uint8_t *i420) {
+    if (!e || !i420) return -1;
+    return enc_push(e, i420, 0);
+}
+int fdv_enc_repeat(fdv_encoder *e) {
+    if (!e || e->n == 0) return -1;
+    return enc_push(e, nullptr, 1);
+}
+
+uint8_t *fdv_enc_finish(fdv_encoder *e, int fps, size_t *len) {
+    if (!e) return nullptr;
+    if (e->n == 0) { fdv_enc_close(e); return nullptr; }
+    for (auto &u : e->us) fdvb_put16(u.bytes.data(), 0, (unsigned)e->n);
+    size_t payload = 0;
+    if (e->nbands == 0) payload = e->us[0].bytes.size();
+    else { payload = 12; for (auto &u : e->us) payload += 4 + u.bytes.size(); }
+    size_t cap = 12 + payload;
+    uint8_t *buf = static_cast<uint8_t *>(malloc(cap));
+    if (!buf) { fdv_enc_close(e); return nullptr; }
+    size_t o = 12;
+    if (e->nbands == 0) {
+        memcpy(buf + o, e->us[0].bytes.data(), payload);
+    } else {
+        o = fdvb_put16(buf, o, (unsigned)e->w);
+        o = fdvb_put16(buf, o, (unsigned)e->h);
+        o = fdvb_put16(buf, o, (unsigned)e->n);
+        buf[o++] = (uint8_t)e->qp;
+        buf[o++] = (uint8_t)e->keyint;
+        o = fdvb_put16(buf, o, (unsigned)e->nbands);
+        o = fdvb_put16(buf, o, (unsigned)e->band_mbrows);
+        for (auto &u : e->us) {
+            o = fdvb_put32(buf, o, (uint32_t)u.bytes.size());
+            memcpy(buf + o, u.bytes.data(), u.bytes.size());
+            o += u.bytes.size();
+        }
+    }
+    size_t flen = fdv_wrap(buf, cap, e->nbands == 0 ? 0 : 1, fps, buf + 12, payload);
+    fdv_enc_close(e);
+    if (!flen) { free(buf); return nullptr; }
+    if (len) *len = flen;
+    return buf;
+}
+
+// --------------------------------------------------------- engine ABI --
+fdvg_ctx *fdvg_create(int nunits, const int *w, const int *h, int range, int device) {
+    fdvb_engine *E = fdvb_engine_create(nunits, w, h, range, device);
+    if (!E) set_engine_err();
+    return E;
+}
+void fdvg_destroy(fdvg_ctx *g) { fdvb_engine_destroy(g); }
+int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
+               const double *lscale, const int *force_skip) {
+    int rc = fdvb_engine_step(g, planes, is_intra, qp, lscale, force_skip);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_pframe_streams(fdvg_ctx *g, int u, const uint8_t **s16, size_t *n16) {
+    const fdvb_streams *s = fdvb_engine_pstreams(g, u);
+    if (!s || !s16 || !n16) { set_err("no P-frame streams for this unit"); return -1; }
+    for (int k = 0; k < 16; ++k) { s16[k] = s->s[k]; n16[k] = s->n[k]; }
+    return 0;
+}
+int fdvg_iframe_streams(fdvg_ctx *g, int u, int plane, const uint8_t **s12, size_t *n12) {
+    const fdvb_streams *s = fdvb_engine_istreams(g, u, plane);
+    if (!s || !s12 || !n12) { set_err("no key-frame streams for this unit/plane"); return -1; }
+    for (int k = 0; k < 12; ++k) { s12[k] = s->s[k]; n12[k] = s->n[k]; }
+    return 0;
+}
+int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420) {
+    int rc = fdvb_engine_recon(g, u, i420);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *far_i420) {
+    int rc = fdvb_engine_set_refs(g, u, near_i420, far_i420);
+    if (rc) set_engine_err();
+    return rc;
+}
+
+// ---------------------------------------------------- entropy tail ABI --
+fdvb_tabcache *fdvb_tabcache_new(void) { return new fdvb_tabcache(); }
+void fdvb_tabcache_reset(fdvb_tabcache *tc) { if (tc) memset(tc, 0, sizeof *tc); }
+void fdvb_tabcache_free(fdvb_tabcache *tc) { delete tc; }
+size_t fdvb_entropy_pframe(const uint8_t *const *s16, const size_t *n16, int qp, fdvb_tabcache *tc,
+                           uint8_t *out, size_t cap) {
+    fdvb_streams st;
+    for (int k = 0; k < 16; ++k) { st.s[k] = s16[k]; st.n[k] = n16[k]; }
+    return fdvb_pframe_blob(&st, qp, tc, out, cap, nullptr);
+}
+size_t fdvb_entropy_image(const uint8_t *const *s12, const size_t *n12, int w, int h, int qp,
+                          uint8_t *out, size_t cap) {
+    fdvb_streams st;
+    for (int k = 0; k < 16; ++k) { st.s[k] = k < 12 ? s12[k] : nullptr; st.n[k] = k < 12 ? n12[k] : 0; }
+    return fdvb_image_blob(&st, w, h, qp, out, cap, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,20 @@
+// The GPU engine's host-side interface (implemented in device/engine.cu).
+#pragma once
+#include <cstdint>
+
+#include "fdvb_internal.h"
+
+struct fdvb_engine;
+
+extern "C" {
+fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device);
+void fdvb_engine_destroy(fdvb_engine *E);
+int fdvb_engine_units(const fdvb_engine *E);
+int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                     const double *lscale, const int *force_skip);
+const fdvb_streams *fdvb_engine_pstreams(fdvb_engine *E, int unit);
+const fdvb_streams *fdvb_engine_istreams(fdvb_engine *E, int unit, int plane);
+int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420);
+int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *near_i420, const uint8_t *far_i420);
+const char *fdvb_engine_error(void);
+}

@@ -1,0 +1,150 @@
+/* fdv_b200 -- the fdv encoder analysis loop on NVIDIA B200 (sm_100a).
+ *
+ * A drop-in for the encode side of the fdv codec (yhbsh/fdv, include/fdv.h):
+ * the same entry points, argument meanings, return conventions and byte
+ * streams, with the per-frame analysis loop -- motion search, motion
+ * compensation, the 4x4/8x8 transforms with quantisation and RDOQ, mode
+ * decision, reconstruction and deblocking -- running as CUDA kernels, and the
+ * rANS / adaptive entropy coding of the decided symbols on the host.
+ *
+ * Every function here is a plain C symbol of libfdvb200.so.  Pointers are host
+ * pointers; frames are I420 (w*h luma bytes, then (w/2)*(h/2) U, then V).
+ * Functions that return a size return 0 on error; functions that return int
+ * return 0 on success and a negative value on error; fdvb_last_error() then
+ * describes the failure.  Nothing aborts the process.
+ *
+ * Streams are byte-identical to the reference encoder's for the same frames,
+ * QP, key interval, band layout and motion search range.  The reference fixes
+ * its search range at compile time (FDV_ME_RANGE, fdv.h:5163-5170; 16 by
+ * default); fdvb_set_search_range() is the run-time equivalent. */
+#ifndef FDV_B200_H
+#define FDV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------ the fdv.h encode API -- */
+
+/* Encode nframes I420 frames as one video stream.  Replaces
+ * fdv_video_encode, fdv.h:903 (implementation fdv.h:6741-6854).  frame f is a
+ * key frame iff f == 0 or (keyint > 0 && f % keyint == 0); keyint is clamped
+ * to 0..255.  w and h must be multiples of 16.  Returns the stream length, or
+ * 0 on error (bad arguments, out of room, device failure). */
+size_t fdv_video_encode(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
+                        uint8_t *out, size_t cap);
+
+/* Encode as a tile-parallel container of independent horizontal bands of
+ * band_mbrows macroblock rows.  Replaces fdv_vtile_encode, fdv.h:973
+ * (implementation fdv.h:7161-7243).  All bands are analysed together on the
+ * GPU; nthreads bounds the host threads used for entropy coding and never
+ * changes the output. */
+size_t fdv_vtile_encode(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
+                        int band_mbrows, int nthreads, uint8_t *out, size_t cap);
+
+/* Streaming encoder.  Replaces the fdv_enc_* family, fdv.h:1157-1198
+ * (implementation fdv.h:8129-8459).  Output is byte-identical to
+ * fdv_video_encode (or fdv_vtile_encode for a tiled encoder) over the same
+ * frames. */
+typedef struct fdv_encoder fdv_encoder;
+fdv_encoder *fdv_enc_open(int w, int h, int qp, int keyint);                       /* fdv.h:1160 */
+fdv_encoder *fdv_enc_open_tiled(int w, int h, int qp, int keyint, int band_mbrows,
+                                int nthreads);                                     /* fdv.h:1186 */
+int fdv_enc_frame(fdv_encoder *e, const uint8_t *i420);                           /* fdv.h:1163 */
+int fdv_enc_repeat(fdv_encoder *e);                                                /* fdv.h:1169 */
+/* Average-bitrate control (fdv.h:1176) is not provided by this library: the
+ * call returns -1 and the encoder keeps its fixed QP. */
+int fdv_enc_set_bitrate(fdv_encoder *e, int bits_per_second, int fps, double bufsecs);
+int fdv_enc_count(const fdv_encoder *e);                                           /* fdv.h:1189 */
+size_t fdv_enc_bytes(const fdv_encoder *e);                                        /* fdv.h:1190 */
+uint8_t *fdv_enc_finish(fdv_encoder *e, int fps, size_t *len);                    /* fdv.h:1195 */
+void fdv_enc_close(fdv_encoder *e);                                                /* fdv.h:1198 */
+
+/* The 12-byte .fdv file head.  Replaces fdv_wrap, fdv.h:1094. */
+size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payload, size_t payload_len);
+
+/* ---------------------------------------------------------- settings -- */
+
+/* Motion search radius in pels: 16 (the reference's default), 32 or 64.
+ * The run-time form of FDV_ME_RANGE (fdv.h:5169).  Returns the previous
+ * value, or -1 for an unsupported radius.  Affects encoders opened after the
+ * call. */
+int fdvb_set_search_range(int range);
+int fdvb_get_search_range(void);
+/* CUDA device used by encoders opened after the call (default 0). */
+int fdvb_set_device(int device);
+/* Description of the last failure on the calling thread. */
+const char *fdvb_last_error(void);
+
+/* -------------------------------------------- the inner engine ABI -- */
+
+/* A batch of independent encoder units (bands of a stream, or streams),
+ * advanced one frame per call.  This is the seam that replaces the body of
+ * the reference's static pframe_encode macroblock loop and deblock
+ * (fdv.h:5797-6170) and fdv_image_encode's intra walk and deblock
+ * (fdv.h:4849-4879): the analysis runs on the GPU and each unit's decided
+ * symbols come back as the byte streams the reference's entropy tail
+ * (fdv.h:6172-6426 and :4881-5032) partitions and codes. */
+typedef struct fdvb_engine fdvg_ctx;
+fdvg_ctx *fdvg_create(int nunits, const int *w, const int *h, int range, int device);
+void fdvg_destroy(fdvg_ctx *g);
+/* One frame for every unit.  planes[3*u + p] is unit u's plane p (Y, U, V),
+ * rows contiguous (stride w, w/2, w/2); all may be NULL for a held frame
+ * (force_skip[u] != 0, fdv_enc_repeat).  is_intra[u] selects a key frame.
+ * lscale may be NULL (1.0: the fractional-lambda multiplier of fdv.h:5804). */
+int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
+               const double *lscale, const int *force_skip);
+/* The last frame's symbol streams of unit u.  P-frame: 16 streams in the
+ * blob's order (9 structure streams by model, then 4x4 counts, 4x4 levels,
+ * 8x8 counts, 8x8 levels, region flags, chroma counts, chroma levels).  Key
+ * frame: plane p's 12 streams (split flags of 4 levels, big-leaf modes, the
+ * two 4x4 mode contexts, counts, levels, 8x8 counts, 8x8 levels, flags).
+ * Pointers stay valid until the next fdvg_frame. */
+int fdvg_pframe_streams(fdvg_ctx *g, int u, const uint8_t **s16, size_t *n16);
+int fdvg_iframe_streams(fdvg_ctx *g, int u, int plane, const uint8_t **s12, size_t *n12);
+/* The last frame's deblocked reconstruction of unit u (tight I420). */
+int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420);
+/* Seed unit u's reference pool (nearest, and optionally the second). */
+int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *far_i420);
+
+/* --------------------------------------------- the host entropy tail -- */
+
+/* Entropy state carried between P-frames (fdv.h:590-601). */
+typedef struct fdvb_tabcache fdvb_tabcache;
+fdvb_tabcache *fdvb_tabcache_new(void);
+void fdvb_tabcache_reset(fdvb_tabcache *tc);
+void fdvb_tabcache_free(fdvb_tabcache *tc);
+/* A P-frame blob from its 16 streams (fdv.h:6172-6426). */
+size_t fdvb_entropy_pframe(const uint8_t *const *s16, const size_t *n16, int qp, fdvb_tabcache *tc,
+                           uint8_t *out, size_t cap);
+/* An intra plane blob from its 12 streams (fdv.h:4881-5032). */
+size_t fdvb_entropy_image(const uint8_t *const *s12, const size_t *n12, int w, int h, int qp,
+                          uint8_t *out, size_t cap);
+
+/* -------------------------------------------- synthetic test content -- */
+
+/* Seeded moving-rectangle content: band-limited noise background (sigma 3 px,
+ * luma mean 128 / sd 30, chroma sd 10), nrects textured rectangles with sides
+ * in [rect_min, rect_max] moving at up to vmax_qpel quarter-pels per frame per
+ * axis, a global pan of (pan_qx, pan_qy) quarter-pels per frame, and a fixed
+ * textured region over static_pct % of the frame. */
+typedef struct fdvb_scene_state fdvb_scene_state;
+typedef struct fdvb_scene_params {
+    int w, h, nframes;
+    int nrects, rect_min, rect_max;
+    int vmax_qpel;
+    int pan_qx, pan_qy;
+    int static_pct;
+    unsigned long long seed;
+} fdvb_scene_params;
+fdvb_scene_state *fdvb_scene_open(const fdvb_scene_params *params);
+int fdvb_scene_frame(const fdvb_scene_state *s, int f, uint8_t *i420);
+void fdvb_scene_close(fdvb_scene_state *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDV_B200_H */
