@@ -127,6 +127,12 @@ struct fdvb_engine {
     int *d_poff = nullptr, *d_ioff = nullptr;
     int maxrows = 0, maxitasks = 0;
     unsigned long long wait_ns = 4000000000ull;
+    // timing (CUDA events on the engine's stream) and launch counts
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double step_ms = 0, pk_ms = 0, ik_ms = 0;
+    long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
+    int src_on_device = 0;
+    int stall_unit = -1, stall_row = -1;
 };
 
 static int round_up(int v, int a) { return (v + a - 1) / a * a; }
@@ -202,6 +208,7 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     if (cudaSetDevice(device) != cudaSuccess) { g_err = "cudaSetDevice failed (no GPU?)"; delete E; return nullptr; }
     cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess) { g_err = "stream create failed"; delete E; return nullptr; }
+    for (auto &e : E->ev) cudaEventCreate(&e);
     int32_t c8[64], q8[52];
     fdvb_c8_tables(c8, q8);
     upload_tables(c8, q8);
@@ -242,18 +249,21 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
+    for (auto &e : E->ev) if (e) cudaEventDestroy(e);
     if (E->st) cudaStreamDestroy(E->st);
     delete E;
 }
 
 extern "C" int fdvb_engine_units(const fdvb_engine *E) { return E ? (int)E->units.size() : 0; }
 
-// Parse a compacted output region: uint32 len[n] then the streams.
-static void parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
+// Parse a compacted output region: uint32 len[n] then the streams.  Returns
+// the bytes the device wrote.
+static size_t parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
     const uint32_t *len = reinterpret_cast<const uint32_t *>(p);
     const uint8_t *d = p + 4 * n;
     for (int k = 0; k < 16; ++k) { s->s[k] = nullptr; s->n[k] = 0; }
     for (int k = 0; k < n; ++k) { s->s[k] = d; s->n[k] = len[k]; d += len[k]; }
+    return (size_t)(d - p);
 }
 
 static int prep_refs(fdvb_engine *E, const std::vector<int> &which) {
@@ -295,14 +305,16 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
         if (!is_intra[i] && E->units[i].nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
     }
     CK(cudaSetDevice(E->device));
+    CK(cudaEventRecord(E->ev[0], E->st));
     // 1. sources
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         if (force_skip && force_skip[i]) continue;
         const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
-        CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, cudaMemcpyHostToDevice, E->st));
-        CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, cudaMemcpyHostToDevice, E->st));
-        CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, cudaMemcpyHostToDevice, E->st));
+        const cudaMemcpyKind kind = E->src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, kind, E->st));
+        CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, kind, E->st));
+        CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, kind, E->st));
     }
     // 2. descriptors
     std::vector<UnitDev> ud(nu);
@@ -323,6 +335,7 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
         d.mbi = u.mbi; d.progress = u.progress; d.slots = u.slots;
         d.lambda = fdvb_lambda(qp[i], lscale ? lscale[i] : 1.0);
         d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
+        d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
         u.last_intra = is_intra[i];
         u.last_qp = qp[i];
         if (!is_intra[i]) {
@@ -372,32 +385,51 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
     if (!rows.empty()) {
         CK(cudaMemcpyAsync(E->d_rows, rows.data(), sizeof(RowTask) * rows.size(), cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)rows.size(), E->nsm);
+        CK(cudaEventRecord(E->ev[1], E->st));
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->st);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(E->ev[2], E->st));
+        E->launches += 1;
     }
     if (!itasks.empty()) {
         CK(cudaMemcpyAsync(E->d_planes, iplanes.data(), sizeof(IPlaneDevH) * iplanes.size(), cudaMemcpyHostToDevice, E->st));
         CK(cudaMemcpyAsync(E->d_itasks, itasks.data(), sizeof(ITaskH) * itasks.size(), cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)itasks.size(), E->nsm);
+        CK(cudaEventRecord(E->ev[3], E->st));
         launch_iframe(E->d_planes, E->d_itasks, (int)itasks.size(), E->d_ticket + 1, E->d_err, E->wait_ns, grid, E->st);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(E->ev[4], E->st));
+        E->launches += 1;
     }
     // 3. deblock, 4. compact
     CK(cudaMemcpyAsync(E->d_db, db.data(), sizeof(DbTaskH) * db.size(), cudaMemcpyHostToDevice, E->st));
     launch_deblock(E->d_db, (int)db.size(), E->st);
     CK(cudaGetLastError());
+    E->launches += 2;
     CK(cudaMemcpyAsync(E->d_cmp, cmp.data(), sizeof(CompactTaskH) * cmp.size(), cudaMemcpyHostToDevice, E->st));
     launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
     CK(cudaGetLastError());
+    E->launches += 1;
     // 5. the new reference
     std::vector<int> all(nu);
     for (int i = 0; i < nu; ++i) all[i] = i;
     if (prep_refs(E, all) != 0) return -3;
+    E->launches += 2;
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
     }
+    CK(cudaEventRecord(E->ev[5], E->st));
+    E->stall_unit = E->stall_row = -1;     // an injected stall lasts one step
     CK(cudaStreamSynchronize(E->st));
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, E->ev[0], E->ev[5]);
+        E->step_ms += ms;
+        E->steps += 1;
+        if (!rows.empty()) { cudaEventElapsedTime(&ms, E->ev[1], E->ev[2]); E->pk_ms += ms; E->pk_n += 1; }
+        if (!itasks.empty()) { cudaEventElapsedTime(&ms, E->ev[3], E->ev[4]); E->ik_ms += ms; E->ik_n += 1; }
+    }
     unsigned err = 0;
     CK(cudaMemcpy(&err, E->d_err, sizeof err, cudaMemcpyDeviceToHost));
     if (err) {
@@ -406,8 +438,8 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
     }
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
-        if (!u.last_intra) parse_streams(u.out_h, 16, &u.ps);
-        else for (int p = 0; p < 3; ++p) parse_streams(u.out_h + u.out_off_i[p], 12, &u.is[p]);
+        if (!u.last_intra) E->d2h += (long long)parse_streams(u.out_h, 16, &u.ps);
+        else for (int p = 0; p < 3; ++p) E->d2h += (long long)parse_streams(u.out_h + u.out_off_i[p], 12, &u.is[p]);
     }
     return 0;
 }
@@ -445,4 +477,40 @@ extern "C" int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *nea
     CK(cudaStreamSynchronize(E->st));
     u.nref = far_i420 ? 2 : 1;
     return 0;
+}
+
+// Sources of the next steps are device pointers (already resident in HBM).
+extern "C" void fdvb_engine_src_on_device(fdvb_engine *E, int on) { if (E) E->src_on_device = on; }
+
+// Accumulated device time (CUDA events on the engine stream) of the steps, of
+// the P-frame analysis kernel and of the key-frame kernel, with their counts,
+// and the number of kernel launches.
+extern "C" void fdvb_engine_stats(const fdvb_engine *E, double *step_ms, double *pk_ms, long long *pk_n,
+                                  double *ik_ms, long long *ik_n, long long *launches, long long *steps,
+                                  long long *d2h_bytes) {
+    if (!E) return;
+    if (d2h_bytes) *d2h_bytes = E->d2h;
+    if (step_ms) *step_ms = E->step_ms;
+    if (pk_ms) *pk_ms = E->pk_ms;
+    if (pk_n) *pk_n = E->pk_n;
+    if (ik_ms) *ik_ms = E->ik_ms;
+    if (ik_n) *ik_n = E->ik_n;
+    if (launches) *launches = E->launches;
+    if (steps) *steps = E->steps;
+}
+extern "C" void fdvb_engine_stats_reset(fdvb_engine *E) {
+    if (!E) return;
+    E->step_ms = E->pk_ms = E->ik_ms = 0;
+    E->steps = E->pk_n = E->ik_n = E->launches = E->d2h = 0;
+}
+// Bound on a wavefront wait before the kernel reports a timeout.
+extern "C" void fdvb_engine_set_wait_ns(fdvb_engine *E, unsigned long long ns) { if (E) E->wait_ns = ns; }
+
+// Fault injection for tests: in the next step, macroblock row `row` of unit
+// `unit` is skipped, so the rows below it wait on a progress flag that nothing
+// sets; their bounded waits expire and the step returns a timeout error.
+extern "C" void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row) {
+    if (!E) return;
+    E->stall_unit = unit;
+    E->stall_row = row;
 }

@@ -16,6 +16,7 @@ struct UnitDev {
     uint8_t *slots;             // per macroblock symbol slot (P-frames)
     double lambda;
     int qp, navail, force_skip, range;
+    int stall_row;              // test hook: this row never runs (-1: none)
 };
 
 struct RowTask { int unit, row; };

@@ -77,6 +77,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         if (t >= nrows) return;
         const UnitDev &U = units[rows[t].unit];
         const int row = rows[t].row, w = U.w, cw = w / 2, mbw = U.mbw;
+        if (row == U.stall_row) continue;   // injected stall: this row's progress flag is never set
         const double lambda = U.lambda;
         const int qp = U.qp, R = U.range;
         const double lam14 = __dmul_rn(lambda, 14.0), lam16 = __dmul_rn(lambda, 16.0), lam19 = __dmul_rn(lambda, 19.0);

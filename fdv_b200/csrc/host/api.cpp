@@ -390,6 +390,24 @@ int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *f
     return rc;
 }
 
+int fdvg_frame_device(fdvg_ctx *g, const uint8_t *const *dplanes, const int *is_intra, const int *qp,
+                      const double *lscale, const int *force_skip) {
+    fdvb_engine_src_on_device(g, 1);
+    int rc = fdvb_engine_step(g, dplanes, is_intra, qp, lscale, force_skip);
+    fdvb_engine_src_on_device(g, 0);
+    if (rc) set_engine_err();
+    return rc;
+}
+void fdvg_stats(const fdvg_ctx *g, double *step_ms, double *analysis_p_ms, long long *p_launches,
+                double *analysis_i_ms, long long *i_launches, long long *kernel_launches, long long *steps,
+                long long *d2h_bytes) {
+    fdvb_engine_stats(g, step_ms, analysis_p_ms, p_launches, analysis_i_ms, i_launches, kernel_launches, steps,
+                      d2h_bytes);
+}
+void fdvg_stats_reset(fdvg_ctx *g) { fdvb_engine_stats_reset(g); }
+void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns) { fdvb_engine_set_wait_ns(g, ns); }
+void fdvg_inject_stall(fdvg_ctx *g, int u, int row) { fdvb_engine_inject_stall(g, u, row); }
+
 // ---------------------------------------------------- entropy tail ABI --
 fdvb_tabcache *fdvb_tabcache_new(void) { return new fdvb_tabcache(); }
 void fdvb_tabcache_reset(fdvb_tabcache *tc) { if (tc) memset(tc, 0, sizeof *tc); }

@@ -57,6 +57,12 @@ int64_t isqrt64(int64_t v) {
     return r;
 }
 
+// Mirror an index into [0, n) (one reflection, then clamped for tiny n).
+inline int reflect(int i, int n) {
+    i = i < 0 ? -i : (i >= n ? 2 * n - 2 - i : i);
+    return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+
 // Gaussian-ish white noise (sum of four uniforms), low-passed by the separable
 // kernel above, then mapped affinely to (mean, sd) and clipped to [0, 255].
 Tex make_noise_tex(Rng &rng, int w, int h, int mean, int sd) {
@@ -72,7 +78,7 @@ Tex make_noise_tex(Rng &rng, int w, int h, int mean, int sd) {
         for (int x = 0; x < w; ++x) {
             int64_t acc = 0;
             for (int k = -9; k <= 9; ++k) {
-                int xx = x + k; xx = xx < 0 ? -xx : (xx >= w ? 2 * w - 2 - xx : xx);
+                int xx = reflect(x + k, w);
                 acc += (int64_t)kBlur[k < 0 ? -k : k] * n[(size_t)y * w + xx];
             }
             a[(size_t)y * w + x] = (int32_t)(acc >> 12);
@@ -82,7 +88,7 @@ Tex make_noise_tex(Rng &rng, int w, int h, int mean, int sd) {
         for (int x = 0; x < w; ++x) {
             int64_t acc = 0;
             for (int k = -9; k <= 9; ++k) {
-                int yy = y + k; yy = yy < 0 ? -yy : (yy >= h ? 2 * h - 2 - yy : yy);
+                int yy = reflect(y + k, h);
                 acc += (int64_t)kBlur[k < 0 ? -k : k] * a[(size_t)yy * w + x];
             }
             int32_t v = (int32_t)(acc >> 12);

@@ -109,6 +109,26 @@ int fdvg_iframe_streams(fdvg_ctx *g, int u, int plane, const uint8_t **s12, size
 int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420);
 /* Seed unit u's reference pool (nearest, and optionally the second). */
 int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *far_i420);
+/* fdvg_frame with the planes already in device memory (device pointers). */
+int fdvg_frame_device(fdvg_ctx *g, const uint8_t *const *dplanes, const int *is_intra, const int *qp,
+                      const double *lscale, const int *force_skip);
+/* Device time accumulated since creation or the last reset, measured with
+ * CUDA events on the engine's stream: whole steps, the P-frame analysis kernel
+ * and the key-frame analysis kernel (with their launch counts), the total
+ * number of kernel launches, and the symbol bytes the device wrote to host
+ * memory. */
+void fdvg_stats(const fdvg_ctx *g, double *step_ms, double *analysis_p_ms, long long *p_launches,
+                double *analysis_i_ms, long long *i_launches, long long *kernel_launches, long long *steps,
+                long long *d2h_bytes);
+void fdvg_stats_reset(fdvg_ctx *g);
+/* Bound on one wavefront wait inside the analysis kernels (default 4 s);
+ * past it the kernel stops, and fdvg_frame returns an error. */
+void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns);
+/* Fault injection for testing the bounded waits: in the next fdvg_frame,
+ * P-frame macroblock row `row` of unit u is skipped, so the rows below wait on
+ * a progress flag nothing sets; the waits expire and fdvg_frame returns an
+ * error, leaving the engine usable. */
+void fdvg_inject_stall(fdvg_ctx *g, int u, int row);
 
 /* --------------------------------------------- the host entropy tail -- */
 

@@ -1,0 +1,102 @@
+"""Generate tests/golden/golden.json from the reference encoder.
+
+Run in a container that holds the reference sources: the reference is compiled
+from them into oracle/_ref (oracle/build.py) and encodes the seeded workloads;
+this records SHA-256 digests and lengths of its streams and of the rendered
+source frames, plus a few known-answer vectors of its exported kernels.  The
+GPU tests compare the library's output with these digests, so they do not need
+the reference tree at run time.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import fdv_b200 as F  # noqa: E402
+import oracle as O  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
+
+
+def sha(b) -> str:
+    return hashlib.sha256(bytes(b)).hexdigest()
+
+
+# (name, scene kwargs, encode kwargs)
+CASES = [
+    ("cif30", dict(w=352, h=288, nframes=30, nrects=6, seed=1),
+     dict(qp=28, keyint=0, band_mbrows=None, search_range=16)),
+    ("hd720_g12", dict(w=1280, h=720, nframes=12, nrects=40, pan_qx=9, static_pct=40, seed=1),
+     dict(qp=24, keyint=60, band_mbrows=6, search_range=32)),
+    ("pan256_k5", dict(w=256, h=144, nframes=10, nrects=10, pan_qx=9, static_pct=40, seed=5),
+     dict(qp=24, keyint=5, band_mbrows=None, search_range=32)),
+    ("tiny_q0", dict(w=64, h=48, nframes=4, nrects=3, rect_max=24, pan_qx=5, seed=7),
+     dict(qp=0, keyint=0, band_mbrows=None, search_range=16)),
+    ("tiny_q51_r64", dict(w=64, h=48, nframes=4, nrects=3, rect_max=24, pan_qx=5, seed=7),
+     dict(qp=51, keyint=2, band_mbrows=None, search_range=64)),
+    ("bands_q12", dict(w=192, h=160, nframes=6, nrects=8, pan_qx=-6, pan_qy=3, static_pct=20, seed=9),
+     dict(qp=12, keyint=4, band_mbrows=3, search_range=16)),
+]
+
+
+def scene(kw) -> list[np.ndarray]:
+    kw = dict(kw)
+    n = kw.pop("nframes")
+    w, h = kw.pop("w"), kw.pop("h")
+    return F.Scene(w, h, n, **kw).frames(n)
+
+
+def main() -> None:
+    out = {"cases": {}, "kernels": {}}
+    for name, skw, ekw in CASES:
+        fr = scene(skw)
+        w, h = skw["w"], skw["h"]
+        if ekw["band_mbrows"] is None:
+            s = O.ref_video_encode(fr, w, h, ekw["qp"], ekw["keyint"], ekw["search_range"])
+            dec = O.ref_video_decode(s, ekw["search_range"])
+        else:
+            s = O.ref_vtile_encode(fr, w, h, ekw["qp"], ekw["keyint"], ekw["band_mbrows"], 1, ekw["search_range"])
+            dec = O.ref_vtile_decode(s, ekw["search_range"])
+        out["cases"][name] = {
+            "scene": skw, "encode": ekw, "stream_sha256": sha(s), "stream_len": len(s),
+            "frames_sha256": sha(b"".join(f.tobytes() for f in fr)),
+            "decoded_sha256": sha(dec.tobytes()),
+        }
+        print(name, len(s), flush=True)
+    # known answers of the reference's kernels (its own tests pin the first two:
+    # test_enc.c:466-476 flat block -> DC only; :817-826 motion search recovers
+    # a pure translation with SAD 0)
+    L = O.ref(16)
+    res = (C.c_int16 * 16)(*([10] * 16))
+    co = (C.c_int32 * 16)()
+    L.fdv_fdct4x4(res, co)
+    out["kernels"]["fdct4x4_flat10"] = list(co)
+    rng = np.random.default_rng(42)
+    blk = rng.integers(-255, 256, 16).astype(np.int16)
+    co2 = (C.c_int32 * 16)()
+    L.fdv_fdct4x4(blk.ctypes.data_as(C.POINTER(C.c_int16)), co2)
+    lev = (C.c_int16 * 16)()
+    L.fdv_quant4x4(co2, lev, 24)
+    out["kernels"]["fdct4x4_seed42"] = {"in": blk.tolist(), "coeff": list(co2), "level_qp24": list(lev)}
+    c8 = (C.c_int32 * 64)()
+    q8 = (C.c_int32 * 52)()
+    L.fdvref_c8_tables(c8, q8)
+    out["kernels"]["c8"] = list(c8)
+    out["kernels"]["qstep8"] = list(q8)
+    with open(OUT, "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("wrote", OUT)
+
+
+if __name__ == "__main__":
+    main()
