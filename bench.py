@@ -157,6 +157,7 @@ def run_reference(args) -> None:
 
 
 def main() -> None:
+    global NF
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -166,7 +167,6 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI end-to-end leg (profiling runs)")
     ap.add_argument("--frames", type=int, default=NF, help="frames per step (profiling runs use a few)")
     args = ap.parse_args()
-    global NF
     NF = max(1, min(args.frames, 120))
     if args.impl == "reference":
         run_reference(args)
