@@ -52,3 +52,185 @@ void launch_compact(const void *tasks, int ntasks, unsigned *err, cudaStream_t s
 }
 
 }  // namespace fdvb
+
+// ===================================================================
+// Allocation-free P-frame analysis of one unit.
+//
+// Some callers cannot allocate device memory while they encode: a host that
+// owns the GPU's memory itself (a media framework or inference server with its
+// own pool, where a stray cudaMalloc competes with it or is forbidden), a
+// real-time capture path that cannot take cudaMalloc's implicit device
+// synchronisation in the middle of a frame, and code that must not grow the
+// process's device footprint after start-up.  For them this entry point runs
+// the whole P-frame analysis step -- reference preparation, the macroblock
+// wavefront, deblocking and symbol compaction -- with every piece of scratch
+// (padded reference planes, per-macroblock symbol slots, motion map, progress
+// flags, launch descriptors) carved from one file-scope device array, so the
+// call itself allocates nothing.  The caller passes its own device buffers for
+// the inputs and outputs.
+// ===================================================================
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../host/fdvb_internal.h"
+
+namespace {
+
+// 24 MiB: enough for one 1280x720 unit at any supported search range
+// (padded reference planes for two references + one symbol slot per
+// macroblock).  Every GPU that loads the library holds this array until the
+// process exits.
+constexpr size_t kStaticScratchBytes = (size_t)24 << 20;
+
+}  // namespace
+
+static __device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+struct StaticSetup {
+    bool done = false;
+    uint8_t *ptr = nullptr;     // device address of g_static_scratch on this device
+    int nsm = 0;
+};
+StaticSetup g_static_setup[64];
+std::mutex g_static_mu;
+thread_local char g_static_err[256];
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int static_fail(const char *msg) {
+    snprintf(g_static_err, sizeof g_static_err, "%s", msg);
+    return -1;
+}
+
+}  // namespace
+
+extern "C" const char *fdvg_pframe_static_error(void) { return g_static_err; }
+
+extern "C" size_t fdvg_pframe_static_capacity(void) { return kStaticScratchBytes; }
+
+extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, const uint8_t *far_ref,
+                                  uint8_t *rec, int w, int h, int qp, double lscale, int range,
+                                  uint8_t *out, size_t out_cap, void *stream) {
+    using namespace fdvb;
+    g_static_err[0] = 0;
+    if (!cur || !near_ref || !rec || !out) return static_fail("null buffer");
+    if (w <= 0 || h <= 0 || (w & 15) || (h & 15) || w > 8192 || h > 8192)
+        return static_fail("dimensions must be positive multiples of 16");
+    if (qp < 0 || qp > 51) return static_fail("qp out of range");
+    if (range != 16 && range != 32 && range != 64) return static_fail("search range must be 16, 32 or 64");
+    if (out_cap < 64) return static_fail("output buffer too small");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return static_fail("no CUDA device");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    {
+        // Set-up, once per device, with that device current: the array's name
+        // is only a host-side stand-in, so its device address is looked up here
+        // and passed to the kernels.
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        StaticSetup &S = g_static_setup[dev];
+        if (!S.done) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            if (e != cudaSuccess || !p) return static_fail("cudaGetSymbolAddress of the static scratch failed");
+            int32_t c8[64], q8[52];
+            fdvb_c8_tables(c8, q8);
+            if (cudaMemcpyToSymbol(c_C8, c8, sizeof c8) != cudaSuccess ||
+                cudaMemcpyToSymbol(c_QSTEP8, q8, sizeof q8) != cudaSuccess)
+                return static_fail("table upload failed");
+            cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev);
+            S.ptr = static_cast<uint8_t *>(p);
+            S.done = true;
+        }
+    }
+    const StaticSetup &S = g_static_setup[dev];
+
+    // Carve the scratch.
+    const int B = range + 16, cw = w / 2, ch = h / 2, mbw = w / 16, mbh = h / 16, nmb = mbw * mbh;
+    const int ys = (w + 2 * B + 63) / 64 * 64, cs = (cw + 2 * B + 63) / 64 * 64;
+    const size_t lsz = (size_t)ys * (h + 2 * B), csz = (size_t)cs * (ch + 2 * B);
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off = align256(off + n); return o; };
+    size_t o_ref[2], o_mbi, o_slots, o_prog, o_misc, o_unit, o_rows, o_prep, o_db, o_cmp, o_off;
+    for (int r = 0; r < 2; ++r) o_ref[r] = take(4 * lsz + 2 * csz);
+    o_mbi = take(sizeof(MBInfo) * nmb);
+    o_slots = take((size_t)kSlotBytes * nmb);
+    o_prog = take(sizeof(int) * mbh);
+    o_misc = take(16);                       // ticket[2], error word
+    o_unit = take(sizeof(UnitDev));
+    o_rows = take(sizeof(RowTask) * mbh);
+    o_prep = take(sizeof(PrepTask) * 2);
+    o_db = take(sizeof(DbTask) * 3);
+    o_cmp = take(sizeof(CompactTask));
+    o_off = take(sizeof(int) * 16);
+    if (off > kStaticScratchBytes) {
+        snprintf(g_static_err, sizeof g_static_err,
+                 "unit %dx%d at search range %d needs %zu bytes of scratch; the static scratch holds %zu "
+                 "(about 1280x720 at most)", w, h, range, off, kStaticScratchBytes);
+        return -1;
+    }
+    uint8_t *base = S.ptr;
+
+    // Descriptors (host staging on the stack; the stream is synchronised
+    // before they go out of scope).
+    RefPlanes rp[2];
+    PrepTask prep[2];
+    const uint8_t *srcs[2] = {near_ref, far_ref ? far_ref : near_ref};
+    for (int r = 0; r < 2; ++r) {
+        uint8_t *m = base + o_ref[r];
+        RefPlanes &R = rp[r];
+        uint8_t *G = m + (size_t)B * ys + B, *Bp = G + lsz, *Hp = Bp + lsz, *Jp = Hp + lsz;
+        uint8_t *U = m + 4 * lsz + (size_t)B * cs + B, *V = U + csz;
+        R.G = G; R.B = Bp; R.H = Hp; R.J = Jp; R.U = U; R.V = V; R.ys = ys; R.cs = cs;
+        PrepTask &t = prep[r];
+        t.rec[0] = srcs[r]; t.rec[1] = srcs[r] + (size_t)w * h; t.rec[2] = t.rec[1] + (size_t)cw * ch;
+        t.G = G; t.B = Bp; t.H = Hp; t.J = Jp; t.U = U; t.V = V;
+        t.w = w; t.h = h; t.ys = ys; t.cs = cs; t.border = B;
+    }
+    UnitDev u;
+    u.w = w; u.h = h; u.mbw = mbw; u.mbh = mbh;
+    u.cur[0] = cur; u.cur[1] = cur + (size_t)w * h; u.cur[2] = u.cur[1] + (size_t)cw * ch;
+    u.rec[0] = rec; u.rec[1] = rec + (size_t)w * h; u.rec[2] = u.rec[1] + (size_t)cw * ch;
+    u.ref[0] = rp[0];
+    u.ref[1] = far_ref ? rp[1] : rp[0];
+    u.mbi = reinterpret_cast<MBInfo *>(base + o_mbi);
+    u.progress = reinterpret_cast<int *>(base + o_prog);
+    u.slots = base + o_slots;
+    u.lambda = fdvb_lambda(qp, lscale);
+    u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1;
+    RowTask rows[8192 / 16];
+    for (int r = 0; r < mbh; ++r) rows[r] = {0, r};
+    DbTask db[3] = {{rec, w, h, qp}, {rec + (size_t)w * h, cw, ch, qp}, {rec + (size_t)w * h + (size_t)cw * ch, cw, ch, qp}};
+    int poff[16];
+    for (int k = 0; k < 16; ++k) { int o = 0; for (int i = 0; i < k; ++i) o += kSlotCap[i]; poff[k] = o; }
+    CompactTask cmp;
+    cmp.slots = base + o_slots; cmp.nslots = nmb; cmp.slot_bytes = kSlotBytes; cmp.nstreams = 16;
+    cmp.off = reinterpret_cast<const int *>(base + o_off); cmp.out = out; cmp.cap = out_cap;
+
+    int *ticket = reinterpret_cast<int *>(base + o_misc);
+    unsigned *err = reinterpret_cast<unsigned *>(base + o_misc + 8);
+    bool ok = cudaMemcpyAsync(base + o_prep, prep, sizeof prep, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(base + o_unit, &u, sizeof u, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(base + o_rows, rows, sizeof(RowTask) * mbh, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(base + o_db, db, sizeof db, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(base + o_cmp, &cmp, sizeof cmp, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              cudaMemcpyAsync(base + o_off, poff, sizeof poff, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+              // what must start at zero: progress flags, row ticket, error word
+              cudaMemsetAsync(base + o_prog, 0, sizeof(int) * mbh, st) == cudaSuccess &&
+              cudaMemsetAsync(base + o_misc, 0, 16, st) == cudaSuccess;
+    if (!ok) return static_fail("descriptor upload failed");
+    launch_refprep(base + o_prep, far_ref ? 2 : 1, w, h, B, st);
+    launch_pframe(reinterpret_cast<const UnitDev *>(base + o_unit), reinterpret_cast<const RowTask *>(base + o_rows),
+                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, st);
+    launch_deblock(base + o_db, 3, st);
+    launch_compact(base + o_cmp, 1, err, st);
+    if (cudaGetLastError() != cudaSuccess) return static_fail("kernel launch failed");
+    unsigned herr = 0;
+    if (cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return static_fail("device error");
+    if (herr) return static_fail((herr & kErrWaitTimeout) ? "wavefront wait timed out" : "symbol slot overflow");
+    return 0;
+}

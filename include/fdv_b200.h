@@ -130,6 +130,35 @@ void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns);
  * error, leaving the engine usable. */
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row);
 
+/* Allocation-free P-frame analysis of one unit.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory while they
+ * encode -- a host that owns the GPU's memory pool itself, a real-time path
+ * that cannot take cudaMalloc's implicit synchronisation mid-frame -- this
+ * runs the same analysis as fdvg_frame (reference preparation, the macroblock
+ * wavefront, deblocking, symbol compaction) for one w x h unit with all its
+ * scratch in a fixed device array inside the library: 24 MiB
+ * (fdvg_pframe_static_capacity), enough for one 1280x720 unit at any search
+ * range, held by every GPU that loads the library until the process exits.
+ * Larger units are rejected with an error.  The call allocates nothing.
+ *
+ * cur, near_ref, far_ref (NULL: one reference) and rec are device pointers to
+ * tight I420 frames of the unit; rec receives the deblocked reconstruction.
+ * out (device or host-mapped, out_cap bytes) receives uint32 len[16] followed
+ * by the 16 P-frame symbol streams back to back, in fdvg_pframe_streams'
+ * order.  stream is a cudaStream_t (NULL: the default stream); the call
+ * synchronises it before returning 0, or a negative value with
+ * fdvg_pframe_static_error() set.
+ *
+ * The first call on a device looks up the array's device address and uploads
+ * the transform tables with that device current; make it before any stream
+ * capture.  Every call shares the one array and leaves its contents behind:
+ * calls that overlap on the GPU (other threads, other streams of the same
+ * device) race on it and must be serialised by the caller. */
+int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, const uint8_t *far_ref, uint8_t *rec, int w,
+                       int h, int qp, double lscale, int range, uint8_t *out, size_t out_cap, void *stream);
+size_t fdvg_pframe_static_capacity(void);
+const char *fdvg_pframe_static_error(void);
+
 /* --------------------------------------------- the host entropy tail -- */
 
 /* Entropy state carried between P-frames (fdv.h:590-601). */
