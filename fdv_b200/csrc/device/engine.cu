@@ -133,6 +133,7 @@ struct fdvb_engine {
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
     int src_on_device = 0;
     int stall_unit = -1, stall_row = -1;
+    unsigned long long *d_prof = nullptr;   // phase profile accumulators (when enabled)
 };
 
 static int round_up(int v, int a) { return (v + a - 1) / a * a; }
@@ -249,6 +250,7 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
+    if (E->d_prof) cudaFree(E->d_prof);
     for (auto &e : E->ev) if (e) cudaEventDestroy(e);
     if (E->st) cudaStreamDestroy(E->st);
     delete E;
@@ -336,6 +338,7 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
         d.lambda = fdvb_lambda(qp[i], lscale ? lscale[i] : 1.0);
         d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
         d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
+        d.prof = E->d_prof;
         u.last_intra = is_intra[i];
         u.last_qp = qp[i];
         if (!is_intra[i]) {
@@ -513,4 +516,22 @@ extern "C" void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row) {
     if (!E) return;
     E->stall_unit = unit;
     E->stall_row = row;
+}
+
+// Per-phase cycle profile of the P-frame kernel (thread 0 of each block adds
+// clock64 deltas): wait, load, SKIP, searches, residuals, region decisions,
+// commit, output; then macroblock and SKIP-early-out counts.  Enabling it
+// allocates the accumulators; reading returns and clears them.
+extern "C" int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out16) {
+    if (!E) return -1;
+    if (enable && !E->d_prof) {
+        if (cudaMalloc(&E->d_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return -3;
+        cudaMemset(E->d_prof, 0, 16 * sizeof(unsigned long long));
+    }
+    if (out16 && E->d_prof) {
+        cudaMemcpy(out16, E->d_prof, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        cudaMemset(E->d_prof, 0, 16 * sizeof(unsigned long long));
+    }
+    if (!enable && E->d_prof) { cudaFree(E->d_prof); E->d_prof = nullptr; }
+    return 0;
 }

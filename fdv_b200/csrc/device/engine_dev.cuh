@@ -17,7 +17,11 @@ struct UnitDev {
     double lambda;
     int qp, navail, force_skip, range;
     int stall_row;              // test hook: this row never runs (-1: none)
+    unsigned long long *prof;   // optional per-phase cycle accumulators (NULL: off)
 };
+
+// Phases of a macroblock, for the optional cycle profile.
+enum { PP_WAIT = 0, PP_LOAD, PP_SKIP, PP_SEARCH, PP_RESID, PP_DECIDE, PP_COMMIT, PP_OUT, PP_NMB, PP_NSKIP, PP_N = 16 };
 
 struct RowTask { int unit, row; };
 

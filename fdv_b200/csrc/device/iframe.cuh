@@ -73,6 +73,7 @@ __host__ __device__ constexpr int isink_bytes(int d) {
 constexpr int kLeafSinkBytes = isink_ccap(0, 0) + isink_ccap(0, 1) + isink_ccap(0, 2) + isink_ccap(0, 3) + isink_ccap(0, 4);
 
 struct IShared {
+    QP4 q;
     uint8_t tile[65 * kTileW];            // reconstruction: rows -1..63, cols -1..127
     uint8_t src[64 * 64];
     uint8_t mm[17 * 17];                  // mode map: cells -1..15 x -1..15
@@ -241,14 +242,14 @@ __device__ double leaf4(ICtx &c, int bx, int by, ISink *tgt) {
         double best_cost = -1.0;
         int best_c = 0;
         for (int k = 0; k < run; ++k) {
-            warp_block4(&S->src[ty * 64 + tx], 64, S->cp[S->cmode[k]], 4, S->trec4, 4, c.qp, c.lambda, false,
+            warp_block4(&S->src[ty * 64 + tx], 64, S->cp[S->cmode[k]], 4, S->trec4, 4, S->q, c.lambda, false,
                         &S->trial[k], &S->b4, lane);
             double J = rd_cost((double)S->trial[k].ssd, c.lambda, kBitsMode + S->trial[k].bits);
             if (best_cost < 0.0 || J < best_cost) { best_cost = J; best_c = k; }
         }
         const int mode = S->cmode[best_c];
         // re-code the winner with RDOQ straight into the reconstruction tile
-        warp_block4(&S->src[ty * 64 + tx], 64, S->cp[mode], 4, &TL(S, ty, tx), kTileW, c.qp, c.lambda, true,
+        warp_block4(&S->src[ty * 64 + tx], 64, S->cp[mode], 4, &TL(S, ty, tx), kTileW, S->q, c.lambda, true,
                     &S->fin, &S->b4, lane);
         if (lane == 0) {
             cs_put1(&tgt->c, CS_N, (uint8_t)S->fin.count, c.err);
@@ -303,7 +304,7 @@ __device__ double leafn(ICtx &c, int bx, int by, int *mode_out, CoefSink **best_
         for (int m = 0; m < 4; ++m) {
             if (!nn_mode_ok(m, n, ht, hl)) continue;
             int bits = kBitsMode;
-            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->pred[m], n, n, c.qp, c.lambda, false,
+            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->pred[m], n, n, S->q, c.qp, c.lambda, false,
                                                S->trec[m], n, &S->lsink[m], &bits, &S->rs, c.err);
             double J = rd_cost((double)D, c.lambda, bits);
             if (best < 0.0 || J < best) { best = J; bmode = m; bidx = m; }
@@ -320,7 +321,7 @@ __device__ double leafn(ICtx &c, int bx, int by, int *mode_out, CoefSink **best_
             for (int p = tid; p < n * n; p += INT) S->bigpred[p] = (uint8_t)nn_px(S->nn[m], S->nb_top, S->nb_left, p % n, p / n);
             __syncthreads();
             int bits = kBitsMode;
-            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->bigpred, n, n, c.qp, c.lambda, false,
+            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->bigpred, n, n, S->q, c.qp, c.lambda, false,
                                                S->bigrec[t], n, &S->bsink[t], &bits, &S->rs, c.err);
             double J = rd_cost((double)D, c.lambda, bits);
             if (best < 0.0 || J < best) { best = J; bmode = m; bidx = t; }
@@ -424,6 +425,7 @@ iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ ta
         const int r = tasks[t].row;
         ICtx c;
         c.S = S; c.P = &P; c.w = P.w; c.h = P.h; c.qp = P.qp; c.lambda = P.lambda; c.err = err;
+        qp4_setup(&S->q, P.qp, tid);
         const int mmw = P.w / 4, mmh = P.h / 4;
         for (int col = 0; col < P.cols; ++col) {
             if (r > 0) {

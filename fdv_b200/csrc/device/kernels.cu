@@ -30,7 +30,13 @@ void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticke
 
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
                    unsigned long long wait_ns, int grid, cudaStream_t st) {
-    pframe_kernel<<<grid, 256, 0, st>>>(units, rows, nrows, ticket, err, wait_ns);
+    static bool attr = false;
+    const size_t smem = sizeof(PShared);
+    if (!attr) {
+        cudaFuncSetAttribute(pframe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    pframe_kernel<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
 }
 
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st) {
@@ -199,7 +205,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     u.progress = reinterpret_cast<int *>(base + o_prog);
     u.slots = base + o_slots;
     u.lambda = fdvb_lambda(qp, lscale);
-    u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1;
+    u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1; u.prof = nullptr;
     RowTask rows[8192 / 16];
     for (int r = 0; r < mbh; ++r) rows[r] = {0, r};
     DbTask db[3] = {{rec, w, h, qp}, {rec + (size_t)w * h, cw, ch, qp}, {rec + (size_t)w * h + (size_t)cw * ch, cw, ch, qp}};

@@ -9,12 +9,23 @@
 // above-right motion for merge candidates, and the above mode for the mode
 // context.  The waits are bounded and report a timeout instead of hanging.
 //
-// Inside a macroblock the 256 threads run the reference's decision procedure
-// (pframe_encode, fdv.h:5808-6162) with its trials parallelised: the SKIP
-// candidates' predictions, each motion search step's candidate vectors, the
-// sixteen 4x4 blocks and four 8x8 regions of a residual, the RDOQ truncation
-// candidates, the four intra sub-modes' SATD screens.  Decisions are made on
-// shared values with the reference's comparison operators and order.
+// A macroblock runs the reference's decision procedure (pframe_encode,
+// fdv.h:5808-6162) on 512 threads in four phases:
+//   0. SKIP: the merge candidates' predictions and squared errors; if SKIP
+//      wins outright (Js <= lambda * 14) nothing else is evaluated.
+//   1. Searches, concurrently on four groups of four warps: the 16x16 search
+//      on the nearest reference, on the second reference, the chain of four
+//      8x8 quadrant searches, and the SATD screen of the intra sub-modes.
+//   2. Residuals of every candidate at once: up to three 16x16 residuals and
+//      four 8x8 ones -- every 4x4 block on a warp (RDOQ candidates on lanes),
+//      every 8x8 option on 64 threads -- then each candidate's per-region
+//      transform-size decisions.
+//   3. The reference's sequential mode decision replayed on those results:
+//      reference break (lambda * 16), intra gate (lambda * 14), INTER8 gate
+//      (lambda * 19 and the SAD ratio), strict-less selection in the order
+//      SKIP, INTER16, INTRA, INTER8.  Candidates computed but not reached by
+//      that flow are ignored, so the decisions are the reference's.  Then
+//      chroma, reconstruction and the symbols of the chosen mode.
 #include "common.cuh"
 #include "engine_dev.cuh"
 #include "inter.cuh"
@@ -23,36 +34,58 @@
 
 namespace fdvb {
 
+constexpr int PNT = 512;
+using PResid = ResidScratchT<PNT>;
+
 struct PShared {
+    QP4 q;
     uint8_t cur[256], curc[2][64];
-    uint8_t top[16], left[16];
-    uint8_t predS[3][256];
-    uint8_t pr[256];
-    uint8_t recI[2][256];
-    uint8_t predI[4][256];
-    uint8_t recIn[256];
-    uint8_t pred8[4][64];
-    uint8_t rec8[4][64];
-    uint8_t cpred[2][64];
-    uint8_t crec[2][64];
-    uint8_t cpred4[8][16];
-    uint8_t ctop[2][8], cleft[2][8];
-    uint8_t isS[2][12];       // inter16 structure bytes per ping-pong slot
-    uint8_t p8S[20];
-    CoefSink sink[4];         // 0/1 inter16 ping-pong, 2 intra, 3 inter8
-    uint8_t sinkmem[4][kCsBytes];
-    ResidScratch rs;
-    Blk4 cblk[8];
-    int s_sad[8];
-    int satd[64];
-    int ssd3[3];
-    // macroblock state (written by thread 0, read by all after a barrier)
+    uint8_t top[16], left[16], ctop[2][8], cleft[2][8];
+    int tl, ht, hl, ctl[2];
     MBInfo cand[3];
-    int ncand, tl, ht, hl, ctl[2];
+    int ncand, ssd3[3];
+    uint8_t predS[3][256];
+    // phase 1
+    uint8_t pr[3][256];          // 16x16 predictions: nearest ref, second ref, selected intra
+    uint8_t pred8[4][64];        // INTER8 quadrant predictions
+    int mv[2][2], sad[2];
+    int qmv[4][2], ssad;
+    int isel;
+    int satd[64];
+    NNPred nn[4];
+    int gsad[4][8];
+    // phase 2: regions 0-3 nearest ref, 4-7 second ref, 8-11 intra, 12-15 INTER8 quadrants
+    Blk4 blk[64];
+    uint8_t recA[16][64];
+    Reg8 reg[16];
+    Reg8Scratch r8[8];
+    Blk4Scratch b4[16];
+    RegDec dec[16];
+    CoefSink sink[4];
+    uint8_t sinkmem[4][kCsBytes];
+    long long cD[4];
+    int cB[4];
+    // chroma
+    uint8_t cpred[2][64], crec[2][64], cpred4[8][16];
+    Blk4 cblk[8];
+    Reg8 creg[2];
+    RegDec cdec[2];
+    long long ce;
+    int cb;
     int task, row_ok;
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
+
+// Optional phase profile: thread 0 adds the cycles since the last mark.
+struct PhaseClock {
+    unsigned long long *acc;
+    long long t;
+    __device__ void start() { if (acc) t = clock64(); }
+    __device__ void mark(int ph) {
+        if (acc) { long long n = clock64(); atomicAdd(&acc[ph], (unsigned long long)(n - t)); t = n; }
+    }
+};
 
 __device__ void write_slot_structs(uint8_t *slot, int k, const uint8_t *b, int n, unsigned *err) {
     uint16_t *len = slot_len(slot);
@@ -62,11 +95,21 @@ __device__ void write_slot_structs(uint8_t *slot, int k, const uint8_t *b, int n
     len[k] = (uint16_t)(len[k] + n);
 }
 
-__global__ void __launch_bounds__(256, 1)
+// 16x16 prediction of a group of 128 threads (threads 0..63 one word each).
+__device__ __forceinline__ void mc16_group(const RefPlanes &R, int bx, int by, int mvx, int mvy, uint8_t *dst, int gt) {
+    if (gt < 64) {
+        const int row = gt >> 2, col = (gt & 3) * 4, ph = (mvy & 3) * 4 + (mvx & 3);
+        reinterpret_cast<uint32_t *>(dst)[gt] = mc_word(R, bx + col + (mvx >> 2), by + row + (mvy >> 2), ph);
+    }
+}
+
+__global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
               int *ticket, unsigned *err, unsigned long long wait_ns) {
-    __shared__ PShared S;
+    extern __shared__ __align__(16) uint8_t psmem[];
+    PShared &S = *reinterpret_cast<PShared *>(psmem);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = warp >> 2, gw = warp & 3, gt = tid & 127;
     if (tid < 4) cs_init(&S.sink[tid], S.sinkmem[tid], c_CsCap);
     __syncthreads();
     for (;;) {
@@ -79,42 +122,49 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const int row = rows[t].row, w = U.w, cw = w / 2, mbw = U.mbw;
         if (row == U.stall_row) continue;   // injected stall: this row's progress flag is never set
         const double lambda = U.lambda;
-        const int qp = U.qp, R = U.range;
+        const int qp = U.qp, R = U.range, navail = U.navail;
         const double lam14 = __dmul_rn(lambda, 14.0), lam16 = __dmul_rn(lambda, 16.0), lam19 = __dmul_rn(lambda, 19.0);
+        qp4_setup(&S.q, qp, tid);
         int pmvx = 0, pmvy = 0;
+        PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
+            pc.start();
             if (row > 0) {
                 if (tid == 0) S.row_ok = wait_at_least(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
             } else if (tid == 0) S.row_ok = 1;
             __syncthreads();
             if (!S.row_ok) break;
+            pc.mark(PP_WAIT);
             uint8_t *slot = U.slots + (size_t)(row * mbw + mbx) * kSlotBytes;
             if (tid < 16) slot_len(slot)[tid] = 0;
-            // ---- load the macroblock and its current-frame neighbours
-            for (int p = tid; p < 256; p += 256) S.cur[p] = U.cur[0][(size_t)(by + (p >> 4)) * w + bx + (p & 15)];
-            if (tid < 128) {
-                int pl = tid >> 6, p = tid & 63;
-                S.curc[pl][p] = U.cur[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)];
-            }
-            if (tid < 16) {
-                S.top[tid] = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx + tid]) : 0;
-                S.left[tid] = bx > 0 ? ldcg8(&U.rec[0][(size_t)(by + tid) * w + bx - 1]) : 0;
-            } else if (tid < 32) {
-                int k = tid - 16, pl = k >> 3, q = k & 7;
+            // ---- the macroblock, its current-frame neighbours, merge candidates
+            if (tid < 64) {
+                const int r2 = tid >> 2, c2 = (tid & 3) * 4;
+                *reinterpret_cast<uint32_t *>(&S.cur[tid * 4]) =
+                    *reinterpret_cast<const uint32_t *>(&U.cur[0][(size_t)(by + r2) * w + bx + c2]);
+            } else if (tid < 96) {
+                const int k = tid - 64, pl = k >> 4, r2 = (k & 15) >> 1, c2 = (k & 1) * 4;
+                *reinterpret_cast<uint32_t *>(&S.curc[pl][(k & 15) * 4]) =
+                    *reinterpret_cast<const uint32_t *>(&U.cur[1 + pl][(size_t)(cby + r2) * cw + cbx + c2]);
+            } else if (tid < 112) {
+                const int k = tid - 96;
+                S.top[k] = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx + k]) : 0;
+                S.left[k] = bx > 0 ? ldcg8(&U.rec[0][(size_t)(by + k) * w + bx - 1]) : 0;
+            } else if (tid < 128) {
+                const int k = tid - 112, pl = k >> 3, q = k & 7;
                 S.ctop[pl][q] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q]) : 0;
                 S.cleft[pl][q] = cbx > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1]) : 0;
-            }
-            if (tid == 0) {
+            } else if (tid == 128) {
                 S.ht = by > 0; S.hl = bx > 0;
                 S.tl = (by > 0 && bx > 0) ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
                 for (int pl = 0; pl < 2; ++pl)
                     S.ctl[pl] = (cby > 0 && cbx > 0) ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
                 // merge candidates (fdv.h:5711-5729)
-                int n = 0;
-                S.cand[0].x = (int16_t)pmvx; S.cand[0].y = (int16_t)pmvy; S.cand[0].ref = 0; S.cand[0].inter = 1; n = 1;
+                int n = 1;
+                S.cand[0].x = (int16_t)pmvx; S.cand[0].y = (int16_t)pmvy; S.cand[0].ref = 0; S.cand[0].inter = 1;
                 for (int k = 0; k < 2 && n < 3; ++k) {
-                    int cx = mbx + k, cy = row - 1;
+                    const int cx = mbx + k, cy = row - 1;
                     if (cy < 0 || cx >= mbw) continue;
                     const MBInfo *mp = &U.mbi[cy * mbw + cx];
                     MBInfo m;
@@ -129,20 +179,21 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 S.ncand = n;
             }
             __syncthreads();
-            // mode context (fdv.h:4172): left / above macroblock skipped-ness
-            int ctx = 0;
+            int ctx;   // mode context (fdv.h:4172): left / above macroblock skipped-ness
             {
-                int Lm = mbx > 0 ? ldcg8(&U.mbi[row * mbw + mbx - 1].mode) : 0;
-                int Am = row > 0 ? ldcg8(&U.mbi[(row - 1) * mbw + mbx].mode) : 0;
+                const int Lm = mbx > 0 ? ldcg8(&U.mbi[row * mbw + mbx - 1].mode) : 0;
+                const int Am = row > 0 ? ldcg8(&U.mbi[(row - 1) * mbw + mbx].mode) : 0;
                 ctx = (Lm != 0 ? 2 : 0) + (Am != 0 ? 1 : 0);
             }
             const RefPlanes &R0 = U.ref[0];
             if (U.force_skip) {
                 // A held frame: SKIP with the zero vector everywhere (fdv.h:5820-5836).
-                for (int p = tid; p < 256; p += 256)
-                    U.rec[0][(size_t)(by + (p >> 4)) * w + bx + (p & 15)] = R0.G[(long)(by + (p >> 4)) * R0.ys + bx + (p & 15)];
-                if (tid < 128) {
-                    int pl = tid >> 6, p = tid & 63;
+                if (tid < 64) {
+                    const int r2 = tid >> 2, c2 = (tid & 3) * 4;
+                    *reinterpret_cast<uint32_t *>(&U.rec[0][(size_t)(by + r2) * w + bx + c2]) =
+                        ld4u(R0.G + (long)(by + r2) * R0.ys + bx + c2);
+                } else if (tid < 192) {
+                    const int k = tid - 64, pl = k >> 6, p = k & 63;
                     const uint8_t *P = pl ? R0.V : R0.U;
                     U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = P[(long)(cby + (p >> 3)) * R0.cs + cbx + (p & 7)];
                 }
@@ -158,13 +209,15 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 if (tid == 0) atomicExch(&U.progress[row], mbx + 1);
                 continue;
             }
+            pc.mark(PP_LOAD);
+            // ---- phase 0: SKIP (fdv.h:5843-5899)
             const int ncand = S.ncand;
-            // ---- SKIP: merge candidates (fdv.h:5843-5899)
-            for (int p = tid; p < ncand * 256; p += 256) {
-                int mi = p >> 8, q = p & 255;
+            if (tid < ncand * 64) {
+                const int mi = tid >> 6, k = tid & 63;
                 const MBInfo &c = S.cand[mi];
-                int ph = (c.y & 3) * 4 + (c.x & 3);
-                S.predS[mi][q] = (uint8_t)mc_px(U.ref[c.ref], bx + (q & 15) + (c.x >> 2), by + (q >> 4) + (c.y >> 2), ph);
+                const int r2 = k >> 2, c2 = (k & 3) * 4, ph = (c.y & 3) * 4 + (c.x & 3);
+                reinterpret_cast<uint32_t *>(S.predS[mi])[k] =
+                    mc_word(U.ref[c.ref], bx + c2 + (c.x >> 2), by + r2 + (c.y >> 2), ph);
             }
             __syncthreads();
             if (warp < ncand) {
@@ -178,128 +231,144 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             for (int mi = 1; mi < ncand; ++mi) if (S.ssd3[mi] < Ds) { Ds = S.ssd3[mi]; best_mi = mi; }
             const int midx_bits = ncand > 1 ? kBitsMode : 0;
             const double Js = rd_cost((double)Ds, lambda, kBitsMode + midx_bits);
-            double Jbest = Js;
             const bool skip_wins = Js <= lam14;
+            pc.mark(PP_SKIP);
+            if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); if (skip_wins) atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
 
-            // ---- INTER16 over the available references (fdv.h:5901-5943)
-            int mvx = 0, mvy = 0, best_ref = 0, sad16 = 0, best_slot = -1, is_len[2] = {0, 0};
-            double Ji = 1e30;
-            for (int r = 0; r < U.navail && !skip_wins; ++r) {
-                if (r > 0 && Jbest <= lam16) break;
-                const RefPlanes &Rr = U.ref[r];
-                int rmx, rmy;
-                int rsad = me_search(S.cur, 16, Rr, bx, by, 16, 16, R, pmvx, pmvy, &rmx, &rmy, S.s_sad);
-                {
-                    int ph = (rmy & 3) * 4 + (rmx & 3);
-                    int q = tid;
-                    S.pr[q] = (uint8_t)mc_px(Rr, bx + (q & 15) + (rmx >> 2), by + (q >> 4) + (rmy >> 2), ph);
-                }
-                const int ts = best_slot == 0 ? 1 : 0;
-                if (tid == 0) {
-                    cs_reset(&S.sink[ts]);
-                    uint8_t *b = S.isS[ts];
-                    int n = 0;
-                    b[n++] = (uint8_t)r;
-                    n += leb_write(b + n, zz_enc(rmx - pmvx));
-                    n += leb_write(b + n, zz_enc(rmy - pmvy));
-                    is_len[ts] = n;
-                    S.ssd3[0] = n;
+            int chosen = 0, best_ref = 0, mvx = 0, mvy = 0, best_sub = 0;
+            if (!skip_wins) {
+                // ---- phase 1: searches on four warp groups
+                if (grp == 0) {
+                    int mx, my;
+                    int sd = me_search_group<16>(S.cur, U.ref[0], bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9);
+                    if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
+                    mc16_group(U.ref[0], bx, by, mx, my, S.pr[0], gt);
+                } else if (grp == 1) {
+                    if (navail > 1) {
+                        int mx, my;
+                        int sd = me_search_group<16>(S.cur, U.ref[1], bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10);
+                        if (gt == 0) { S.mv[1][0] = mx; S.mv[1][1] = my; S.sad[1] = sd; }
+                        mc16_group(U.ref[1], bx, by, mx, my, S.pr[1], gt);
+                    }
+                } else if (grp == 2) {
+                    int qpx = pmvx, qpy = pmvy, ssad = 0;
+                    for (int q = 0; q < 4; ++q) {
+                        const int qx = (q & 1) * 8, qy = (q >> 1) * 8;
+                        int mx, my;
+                        ssad += me_search_group<8>(S.cur + qy * 16 + qx, R0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
+                                                   S.gsad[2], gw, lane, 11);
+                        if (gt == 0) { S.qmv[q][0] = mx; S.qmv[q][1] = my; }
+                        qpx = mx; qpy = my;
+                        if (gt < 16) {
+                            const int r2 = gt >> 1, c2 = (gt & 1) * 4, ph = (my & 3) * 4 + (mx & 3);
+                            reinterpret_cast<uint32_t *>(S.pred8[q])[gt] =
+                                mc_word(R0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
+                        }
+                    }
+                    if (gt == 0) S.ssad = ssad;
+                } else {
+                    // intra 16x16 sub-modes, SATD-screened (fdv.h:5961-5970)
+                    if (gt < 4) S.nn[gt] = nn_setup(gt, S.top, S.left, S.tl, 16, S.ht, S.hl);
+                    gbar(12, 128);
+                    if (gt < 64) {
+                        const int m = gt >> 4, b = gt & 15, oy = (b >> 2) * 4, ox = (b & 3) * 4;
+                        uint8_t pk[16];
+                        for (int p = 0; p < 16; ++p) pk[p] = (uint8_t)nn_px(S.nn[m], S.top, S.left, ox + (p & 3), oy + (p >> 2));
+                        S.satd[gt] = satd4(S.cur + oy * 16 + ox, 16, pk, 4);
+                    }
+                    gbar(12, 128);
+                    int sel = -1, sbest = 0;
+                    for (int m = 0; m < 4; ++m) {
+                        if (!nn_mode_ok(m, 16, S.ht, S.hl)) continue;
+                        int sa = 0;
+                        for (int b = 0; b < 16; ++b) sa += S.satd[m * 16 + b];
+                        if (sel < 0 || sa < sbest) { sbest = sa; sel = m; }
+                    }
+                    if (gt == 0) S.isel = sel;
+                    if (sel >= 0)
+                        for (int p = gt; p < 256; p += 128) S.pr[2][p] = (uint8_t)nn_px(S.nn[sel], S.top, S.left, p & 15, p >> 4);
                 }
                 __syncthreads();
-                is_len[ts] = S.ssd3[0];
-                int bb = 2 * kBitsMode + bits_val(zz_enc(rmx - pmvx)) + bits_val(zz_enc(rmy - pmvy));
-                long long dd = code_residual(S.cur, 16, S.pr, 16, qp, lambda, false, S.recI[ts], &S.sink[ts], &bb, &S.rs, err);
-                double J = rd_cost((double)dd, lambda, bb);
-                if (J < Jbest) Jbest = J;
-                if (J < Ji) { Ji = J; best_ref = r; mvx = rmx; mvy = rmy; sad16 = rsad; best_slot = ts; }
-            }
-
-            // ---- INTRA 16x16, SATD-screened (fdv.h:5945-5988)
-            double Jintra = 1e30;
-            int best_sub = 0;
-            if (!skip_wins && Jbest > lam14) {
-                __shared__ NNPred s_nn[4];
-                if (tid < 4) s_nn[tid] = nn_setup(tid, S.top, S.left, S.tl, 16, S.ht, S.hl);
-                __syncthreads();
-                for (int p = tid; p < 4 * 256; p += 256) {
-                    int m = p >> 8, q = p & 255;
-                    S.predI[m][q] = (uint8_t)nn_px(s_nn[m], S.top, S.left, q & 15, q >> 4);
+                pc.mark(PP_SEARCH);
+                // ---- phase 2: residuals of every candidate at once
+                const int isel = S.isel, ssad = S.ssad;
+                const bool have1 = navail > 1, haveI = isel >= 0;
+                // INTER8 residuals are needed unless the SAD gate rejects the
+                // split whichever INTER16 reference ends up chosen.
+                auto gate_skip = [&](int s16) { return s16 > 0 && ssad * 10 >= s16 * 9; };
+                const bool need8 = !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
+                const unsigned pres = 0xFu | (have1 ? 0xF0u : 0u) | (haveI ? 0xF00u : 0u) | (need8 ? 0xF000u : 0u);
+                if (tid < 4) cs_reset(&S.sink[tid]);
+                for (int b = warp; b < 64; b += 16) {
+                    const int g = b >> 2, s = b & 3;
+                    if (!((pres >> g) & 1u)) continue;
+                    const int sx = (s & 1) * 4, sy = (s >> 1) * 4;
+                    if (g < 12) {
+                        const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
+                        warp_block4(S.cur + (ry + sy) * 16 + rx + sx, 16, S.pr[c] + (ry + sy) * 16 + rx + sx, 16,
+                                    &S.recA[g][sy * 8 + sx], 8, S.q, lambda, true, &S.blk[b], &S.b4[warp], lane);
+                    } else {
+                        const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
+                        warp_block4(S.cur + (qy + sy) * 16 + qx + sx, 16, S.pred8[q] + sy * 8 + sx, 8,
+                                    &S.recA[g][sy * 8 + sx], 8, S.q, lambda, true, &S.blk[b], &S.b4[warp], lane);
+                    }
+                }
+                for (int round = 0; round < 2; ++round) {
+                    const int g = round * 8 + (tid >> 6);
+                    if ((pres >> g) & 1u) {
+                        const uint8_t *cp, *pp;
+                        int pstr;
+                        if (g < 12) {
+                            const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
+                            cp = S.cur + ry * 16 + rx; pp = S.pr[c] + ry * 16 + rx; pstr = 16;
+                        } else {
+                            const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
+                            cp = S.cur + qy * 16 + qx; pp = S.pred8[q]; pstr = 8;
+                        }
+                        region8(cp, 16, pp, pstr, qp, &S.reg[g], &S.r8[tid >> 6], tid & 63, 1 + (tid >> 6));
+                    }
                 }
                 __syncthreads();
-                if (tid < 64) {
-                    int m = tid >> 4, b = tid & 15, oy = (b >> 2) * 4, ox = (b & 3) * 4;
-                    S.satd[tid] = satd4(S.cur + oy * 16 + ox, 16, S.predI[m] + oy * 16 + ox, 16);
+                pc.mark(PP_RESID);
+                for (int c = 0; c < 4; ++c) {
+                    if (!((pres >> (4 * c)) & 1u)) continue;
+                    decide_regions<PNT>(4, &S.blk[16 * c], &S.reg[4 * c], &S.dec[4 * c], lambda, false, &S.sink[c],
+                                        &S.cD[c], &S.cB[c], err);
                 }
                 __syncthreads();
-                int sel = -1, sbest = 0;
-                for (int m = 0; m < 4; ++m) {
-                    if (!nn_mode_ok(m, 16, S.ht, S.hl)) continue;
-                    int sa = 0;
-                    for (int b = 0; b < 16; ++b) sa += S.satd[m * 16 + b];
-                    if (sel < 0 || sa < sbest) { sbest = sa; sel = m; }
+                pc.mark(PP_DECIDE);
+                // ---- phase 3: the reference's decision on these results
+                double Jbest = Js, Ji = 1e30, Jintra = 1e30, J8 = 1e30;
+                int sad16 = 0;
+                for (int r = 0; r < navail; ++r) {
+                    if (r > 0 && Jbest <= lam16) break;
+                    const int rmx = S.mv[r][0], rmy = S.mv[r][1];
+                    const int bb = 2 * kBitsMode + bits_val(zz_enc(rmx - pmvx)) + bits_val(zz_enc(rmy - pmvy)) + S.cB[r];
+                    const double J = rd_cost((double)S.cD[r], lambda, bb);
+                    if (J < Jbest) Jbest = J;
+                    if (J < Ji) { Ji = J; best_ref = r; mvx = rmx; mvy = rmy; sad16 = S.sad[r]; }
                 }
-                if (sel >= 0) {
-                    if (tid == 0) cs_reset(&S.sink[2]);
-                    __syncthreads();
-                    int bn = 2 * kBitsMode;
-                    long long Dn = code_residual(S.cur, 16, S.predI[sel], 16, qp, lambda, false, S.recIn, &S.sink[2], &bn, &S.rs, err);
-                    Jintra = rd_cost((double)Dn, lambda, bn);
-                    best_sub = sel;
+                if (Jbest > lam14 && haveI) {
+                    Jintra = rd_cost((double)S.cD[2], lambda, 2 * kBitsMode + S.cB[2]);
+                    best_sub = isel;
                     if (Jintra < Jbest) Jbest = Jintra;
                 }
-            }
-
-            // ---- INTER8: four chained quadrant searches on the nearest reference (fdv.h:5990-6033)
-            int qmv[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-            long long D8 = 0;
-            int b8 = kBitsMode, p8len = 0;
-            bool try8 = !skip_wins && Jbest > lam19;
-            if (try8) {
-                int ssad = 0, qpx = pmvx, qpy = pmvy;
-                for (int q = 0; q < 4; ++q) {
-                    int qx = (q & 1) * 8, qy = (q >> 1) * 8, mx, my;
-                    ssad += me_search(S.cur + qy * 16 + qx, 16, R0, bx + qx, by + qy, 8, 8, R, qpx, qpy, &mx, &my, S.s_sad);
-                    qmv[q][0] = mx; qmv[q][1] = my; qpx = mx; qpy = my;
-                }
-                if (sad16 > 0 && ssad * 10 >= sad16 * 9) try8 = false;
-                if (try8) {
-                    if (tid == 0) {
-                        cs_reset(&S.sink[3]);
-                        int n = 0, px = pmvx, py = pmvy;
-                        for (int q = 0; q < 4; ++q) {
-                            n += leb_write(S.p8S + n, zz_enc(qmv[q][0] - px));
-                            n += leb_write(S.p8S + n, zz_enc(qmv[q][1] - py));
-                            px = qmv[q][0]; py = qmv[q][1];
-                        }
-                        S.ssd3[0] = n;
-                    }
-                    {
-                        int q = tid >> 6, p = tid & 63, qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                        int mx = qmv[q][0], my = qmv[q][1], ph = (my & 3) * 4 + (mx & 3);
-                        S.pred8[q][p] = (uint8_t)mc_px(R0, bx + qx + (p & 7) + (mx >> 2), by + qy + (p >> 3) + (my >> 2), ph);
-                    }
-                    __syncthreads();
-                    p8len = S.ssd3[0];
-                    int px = pmvx, py = pmvy;
+                if (Jbest > lam19 && !gate_skip(sad16)) {
+                    int b8 = kBitsMode, px = pmvx, py = pmvy;
                     for (int q = 0; q < 4; ++q) {
-                        int qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                        b8 += bits_val(zz_enc(qmv[q][0] - px)) + bits_val(zz_enc(qmv[q][1] - py));
-                        px = qmv[q][0]; py = qmv[q][1];
-                        D8 += code_residual(S.cur + qy * 16 + qx, 16, S.pred8[q], 8, qp, lambda, false, S.rec8[q], &S.sink[3], &b8, &S.rs, err);
+                        b8 += bits_val(zz_enc(S.qmv[q][0] - px)) + bits_val(zz_enc(S.qmv[q][1] - py));
+                        px = S.qmv[q][0]; py = S.qmv[q][1];
                     }
+                    J8 = rd_cost((double)S.cD[3], lambda, b8 + S.cB[3]);
                 }
+                double Jmin = Js;
+                if (Ji < Jmin) { Jmin = Ji; chosen = 1; }
+                if (Jintra < Jmin) { Jmin = Jintra; chosen = 2; }
+                if (J8 < Jmin) { Jmin = J8; chosen = 3; }
             }
-            const double J8 = try8 ? rd_cost((double)D8, lambda, b8) : 1e30;
 
-            // ---- commit the cheapest (fdv.h:6035-6160)
-            double Jmin = Js;
-            int chosen = 0;
-            if (Ji < Jmin) { Jmin = Ji; chosen = 1; }
-            if (Jintra < Jmin) { Jmin = Jintra; chosen = 2; }
-            if (J8 < Jmin) { Jmin = J8; chosen = 3; }
-            __syncthreads();
-
-            CoefSink *M = chosen == 1 ? &S.sink[best_slot] : (chosen == 2 ? &S.sink[2] : &S.sink[3]);
+            // ---- commit (fdv.h:6049-6160)
+            CoefSink *M = chosen == 1 ? &S.sink[best_ref] : &S.sink[chosen == 2 ? 2 : 3];
             MBInfo info = {0, 0, 0, 0, (uint8_t)chosen, 0};
             if (chosen == 0) {
                 const int smvx = S.cand[best_mi].x, smvy = S.cand[best_mi].y, sref = S.cand[best_mi].ref;
@@ -308,11 +377,13 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     write_slot_structs(slot, ctx, &m0, 1, err);
                     if (ncand > 1) write_slot_structs(slot, PS_MERGE, &mi, 1, err);
                 }
-                U.rec[0][(size_t)(by + (tid >> 4)) * w + bx + (tid & 15)] = S.predS[best_mi][tid];
-                if (tid < 128) {
-                    int pl = tid >> 6, p = tid & 63;
+                if (tid < 64)
+                    *reinterpret_cast<uint32_t *>(&U.rec[0][(size_t)(by + (tid >> 2)) * w + bx + (tid & 3) * 4]) =
+                        reinterpret_cast<const uint32_t *>(S.predS[best_mi])[tid];
+                else if (tid < 192) {
+                    const int k = tid - 64, pl = k >> 6, p = k & 63;
                     const RefPlanes &Rs = U.ref[sref];
-                    int cmx = smvx / 2, cmy = smvy / 2;
+                    const int cmx = smvx / 2, cmy = smvy / 2;
                     U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] =
                         (uint8_t)mc_cpx(pl ? Rs.V : Rs.U, Rs.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
@@ -320,29 +391,40 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 pmvx = smvx; pmvy = smvy;
             } else if (chosen == 1) {
                 if (tid == 0) {
+                    uint8_t b[12];
+                    int n = 0;
+                    b[n++] = (uint8_t)best_ref;
+                    n += leb_write(b + n, zz_enc(mvx - pmvx));
+                    n += leb_write(b + n, zz_enc(mvy - pmvy));
                     uint8_t m1 = 1;
                     write_slot_structs(slot, ctx, &m1, 1, err);
-                    const uint8_t *b = S.isS[best_slot];
                     write_slot_structs(slot, PS_REF, b, 1, err);
                     int part = 0;
-                    for (int q = 1; q < is_len[best_slot]; ++q) {
+                    for (int q = 1; q < n; ++q) {
                         write_slot_structs(slot, part ? PS_MVY : PS_MVX, b + q, 1, err);
                         if (!(b[q] & 0x80)) ++part;
                     }
                 }
-                U.rec[0][(size_t)(by + (tid >> 4)) * w + bx + (tid & 15)] = S.recI[best_slot][tid];
+                {
+                    const int rr = ((tid >> 4) >> 3) * 2 + ((tid & 15) >> 3), q = ((tid >> 4) & 7) * 8 + (tid & 7);
+                    if (tid < 256) {
+                        const int g = 4 * best_ref + rr;
+                        U.rec[0][(size_t)(by + (tid >> 4)) * w + bx + (tid & 15)] =
+                            S.dec[g].choice ? S.reg[g].rec[q] : S.recA[g][q];
+                    }
+                }
                 // chroma INTER: prediction at mv/2, four 4x4 blocks per plane, no RDOQ (fdv.h:5576-5626)
                 const RefPlanes &Rb = U.ref[best_ref];
                 const int cmx = mvx / 2, cmy = mvy / 2;
                 if (tid < 128) {
-                    int pl = tid >> 6, p = tid & 63;
+                    const int pl = tid >> 6, p = tid & 63;
                     S.cpred[pl][p] = (uint8_t)mc_cpx(pl ? Rb.V : Rb.U, Rb.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
                 __syncthreads();
-                {
-                    int pl = warp >> 2, b = warp & 3, oy = (b >> 1) * 4, ox = (b & 1) * 4;
+                if (warp < 8) {
+                    const int pl = warp >> 2, b = warp & 3, oy = (b >> 1) * 4, ox = (b & 1) * 4;
                     warp_block4(S.curc[pl] + oy * 8 + ox, 8, S.cpred[pl] + oy * 8 + ox, 8, S.crec[pl] + oy * 8 + ox, 8,
-                                qp, lambda, false, &S.cblk[warp], &S.rs.b4[warp], lane);
+                                S.q, lambda, false, &S.cblk[warp], &S.b4[warp], lane);
                 }
                 __syncthreads();
                 if (tid == 0) {
@@ -358,7 +440,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     }
                 }
                 if (tid < 128) {
-                    int pl = tid >> 6, p = tid & 63;
+                    const int pl = tid >> 6, p = tid & 63;
                     U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = S.crec[pl][p];
                 }
                 info.x = (int16_t)mvx; info.y = (int16_t)mvy; info.ref = (uint8_t)best_ref; info.inter = 1;
@@ -369,45 +451,68 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     write_slot_structs(slot, ctx, &m2, 1, err);
                     write_slot_structs(slot, PS_SUB, &sb, 1, err);
                 }
-                U.rec[0][(size_t)(by + (tid >> 4)) * w + bx + (tid & 15)] = S.recIn[tid];
-                // chroma intra with the same sub-mode, through the residual coder (fdv.h:6104-6117)
-                for (int pl = 0; pl < 2; ++pl) {
-                    __shared__ NNPred s_cn;
-                    if (tid == 0) s_cn = nn_setup(best_sub, S.ctop[pl], S.cleft[pl], S.ctl[pl], 8, cby > 0, cbx > 0);
-                    __syncthreads();
-                    if (tid < 64) S.cpred[pl][tid] = (uint8_t)nn_px(s_cn, S.ctop[pl], S.cleft[pl], tid & 7, tid >> 3);
-                    __syncthreads();
-                    int bb = 0;
-                    code_residual(S.curc[pl], 8, S.cpred[pl], 8, qp, lambda, true, S.crec[pl], M, &bb, &S.rs, err);
-                    if (tid < 64) U.rec[1 + pl][(size_t)(cby + (tid >> 3)) * cw + cbx + (tid & 7)] = S.crec[pl][tid];
+                if (tid < 256) {
+                    const int rr = ((tid >> 4) >> 3) * 2 + ((tid & 15) >> 3), q = ((tid >> 4) & 7) * 8 + (tid & 7);
+                    const int g = 8 + rr;
+                    U.rec[0][(size_t)(by + (tid >> 4)) * w + bx + (tid & 15)] = S.dec[g].choice ? S.reg[g].rec[q] : S.recA[g][q];
+                }
+                // chroma intra with the same sub-mode through the residual coder, U then V (fdv.h:6104-6117)
+                if (tid < 2) S.nn[tid] = nn_setup(best_sub, S.ctop[tid], S.cleft[tid], S.ctl[tid], 8, cby > 0, cbx > 0);
+                __syncthreads();
+                if (tid < 128) {
+                    const int pl = tid >> 6, p = tid & 63;
+                    S.cpred[pl][p] = (uint8_t)nn_px(S.nn[pl], S.ctop[pl], S.cleft[pl], p & 7, p >> 3);
+                }
+                __syncthreads();
+                if (warp < 8) {
+                    const int pl = warp >> 2, s = warp & 3, sx = (s & 1) * 4, sy = (s >> 1) * 4;
+                    warp_block4(S.curc[pl] + sy * 8 + sx, 8, S.cpred[pl] + sy * 8 + sx, 8, &S.recA[pl][sy * 8 + sx], 8,
+                                S.q, lambda, true, &S.blk[warp], &S.b4[warp], lane);
+                } else if (tid >= 256 && tid < 384) {
+                    const int pl = (tid - 256) >> 6;
+                    region8(S.curc[pl], 8, S.cpred[pl], 8, qp, &S.creg[pl], &S.r8[pl], tid & 63, 1 + pl);
+                }
+                __syncthreads();
+                for (int pl = 0; pl < 2; ++pl)
+                    decide_regions<PNT>(1, &S.blk[4 * pl], &S.creg[pl], &S.cdec[pl], lambda, true, M, &S.ce, &S.cb, err);
+                if (tid < 128) {
+                    const int pl = tid >> 6, q = tid & 63;
+                    U.rec[1 + pl][(size_t)(cby + (q >> 3)) * cw + cbx + (q & 7)] = S.cdec[pl].choice ? S.creg[pl].rec[q] : S.recA[pl][q];
                 }
                 info.inter = 0;
             } else {
                 if (tid == 0) {
+                    uint8_t b[20];
+                    int n = 0, px = pmvx, py = pmvy;
+                    for (int q = 0; q < 4; ++q) {
+                        n += leb_write(b + n, zz_enc(S.qmv[q][0] - px));
+                        n += leb_write(b + n, zz_enc(S.qmv[q][1] - py));
+                        px = S.qmv[q][0]; py = S.qmv[q][1];
+                    }
                     uint8_t m3 = 3;
                     write_slot_structs(slot, ctx, &m3, 1, err);
                     int part = 0;
-                    for (int q = 0; q < p8len; ++q) {
-                        write_slot_structs(slot, (part & 1) ? PS_MVY : PS_MVX, S.p8S + q, 1, err);
-                        if (!(S.p8S[q] & 0x80)) ++part;
+                    for (int q = 0; q < n; ++q) {
+                        write_slot_structs(slot, (part & 1) ? PS_MVY : PS_MVX, b + q, 1, err);
+                        if (!(b[q] & 0x80)) ++part;
                     }
                 }
-                {
-                    int q = tid >> 6, p = tid & 63, qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                    U.rec[0][(size_t)(by + qy + (p >> 3)) * w + bx + qx + (p & 7)] = S.rec8[q][p];
+                if (tid < 256) {
+                    const int q = tid >> 6, p = tid & 63, qx = (q & 1) * 8, qy = (q >> 1) * 8, g = 12 + q;
+                    U.rec[0][(size_t)(by + qy + (p >> 3)) * w + bx + qx + (p & 7)] = S.dec[g].choice ? S.reg[g].rec[p] : S.recA[g][p];
                 }
                 // chroma: 4x4 per quadrant at qmv/2 from the nearest reference, RDOQ'd (fdv.h:6143-6159)
                 if (tid < 128) {
-                    int k = tid >> 4, p = tid & 15, pl = k >> 2, q = k & 3;
-                    int cmx = qmv[q][0] / 2, cmy = qmv[q][1] / 2, qcx = (q & 1) * 4, qcy = (q >> 1) * 4;
+                    const int k = tid >> 4, p = tid & 15, pl = k >> 2, q = k & 3;
+                    const int cmx = S.qmv[q][0] / 2, cmy = S.qmv[q][1] / 2, qcx = (q & 1) * 4, qcy = (q >> 1) * 4;
                     S.cpred4[k][p] = (uint8_t)mc_cpx(pl ? R0.V : R0.U, R0.cs, cbx + qcx + (p & 3) + (cmx >> 2),
                                                      cby + qcy + (p >> 2) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
                 __syncthreads();
-                {
-                    int pl = warp >> 2, q = warp & 3, qcx = (q & 1) * 4, qcy = (q >> 1) * 4;
+                if (warp < 8) {
+                    const int pl = warp >> 2, q = warp & 3, qcx = (q & 1) * 4, qcy = (q >> 1) * 4;
                     warp_block4(S.curc[pl] + qcy * 8 + qcx, 8, S.cpred4[warp], 4, S.crec[pl] + qcy * 8 + qcx, 8,
-                                qp, lambda, true, &S.cblk[warp], &S.rs.b4[warp], lane);
+                                S.q, lambda, true, &S.cblk[warp], &S.b4[warp], lane);
                 }
                 __syncthreads();
                 if (tid == 0) {
@@ -417,13 +522,14 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     }
                 }
                 if (tid < 128) {
-                    int pl = tid >> 6, p = tid & 63;
+                    const int pl = tid >> 6, p = tid & 63;
                     U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = S.crec[pl][p];
                 }
-                info.x = (int16_t)qmv[3][0]; info.y = (int16_t)qmv[3][1]; info.ref = 0; info.inter = 1;
-                pmvx = qmv[3][0]; pmvy = qmv[3][1];
+                info.x = (int16_t)S.qmv[3][0]; info.y = (int16_t)S.qmv[3][1]; info.ref = 0; info.inter = 1;
+                pmvx = S.qmv[3][0]; pmvy = S.qmv[3][1];
             }
             __syncthreads();
+            pc.mark(PP_COMMIT);
             // ---- coefficient streams of the chosen mode into the slot
             if (chosen != 0) {
                 for (int k = 0; k < CS_NUM; ++k) {
@@ -431,7 +537,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     if (n > c_SlotCap[PS_CN + k]) { if (tid == 0) atomicOr(err, kErrSlotOverflow); n = 0; }
                     uint8_t *d = slot_data(slot, PS_CN + k);
                     const uint8_t *s = M->buf[k];
-                    for (int i = tid; i < n; i += 256) d[i] = s[i];
+                    for (int i = tid; i < n; i += PNT) d[i] = s[i];
                     if (tid == 0) slot_len(slot)[PS_CN + k] = (uint16_t)n;
                 }
             }
@@ -439,6 +545,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             __threadfence();
             __syncthreads();
             if (tid == 0) atomicExch(&U.progress[row], mbx + 1);
+            pc.mark(PP_OUT);
         }
         __syncthreads();
     }

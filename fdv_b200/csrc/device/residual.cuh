@@ -43,6 +43,21 @@ __device__ __forceinline__ void cs_put(CoefSink *s, int k, const uint8_t *b, int
 __device__ __forceinline__ void cs_put1(CoefSink *s, int k, uint8_t v, unsigned *err) { cs_put(s, k, &v, 1, err); }
 
 // ----------------------------------------------------- 4x4 block coder --
+// Per-QP constants of the 4x4 quantiser and dequantiser (fdv.h:2430-2444,
+// :2546-2555), per coefficient position, set up once per block of threads.
+struct QP4 {
+    int mf[16];       // MF[qp % 6][class(p)]
+    int dq[16];       // DEQUANT_V[qp % 6][class(p)] << (qp / 6)
+    int f, qbits;
+};
+__device__ __forceinline__ void qp4_setup(QP4 *q, int qp, int t) {
+    if (t < 16) {
+        q->mf[t] = c_MF[qp % 6][pos_class(t)];
+        q->dq[t] = c_DQV[qp % 6][pos_class(t)] << (qp / 6);
+    }
+    if (t == 0) { q->qbits = 15 + qp / 6; q->f = (1 << (15 + qp / 6)) / 3; }
+}
+
 // Result of one 4x4 block: its end-of-block count, level bytes, squared error
 // against the source after clipping, and its rate in fdv_bits_val units.
 struct Blk4 {
@@ -53,17 +68,27 @@ struct Blk4 {
 struct Blk4Scratch {
     int res[16];
     int lev[16];
-    double J[17];
-    int valid[17];
 };
 
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FDVB_FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
 // One warp codes one 4x4 block: forward transform, quantisation, optional RDOQ
-// (fdv.h:2493), dequantisation, inverse transform, reconstruction.  Lane l<16
-// owns coefficient position l; lanes 0..16 evaluate the RDOQ truncation
-// candidate L = lane-1 in parallel and lane 0 replays the reference's
-// sequential selection over them.  Writes rec (uint8, stride rs) and `out`.
+// (fdv.h:2493-2536), dequantisation, inverse transform, reconstruction.  Lane
+// l < 16 owns raster position l and zigzag position l; lanes 0..16 evaluate
+// the RDOQ truncation candidate L = lane - 1 in parallel, their rates come
+// from a suffix sum over the zigzag scan, and every lane replays the
+// reference's sequential selection (bestJ < 0.0 || J < bestJ, in the order
+// L = last .. -1) over the valid candidates.  Level bytes are packed in
+// parallel from a prefix sum of their LEB lengths.  Writes rec (stride rs).
 __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
-                            uint8_t *rec, int rs, int qp, double lambda, bool rdoq,
+                            uint8_t *rec, int rs, const QP4 &Q, double lambda, bool rdoq,
                             Blk4 *out, Blk4Scratch *sc, int lane) {
     const int l = lane & 15, i = l >> 2, j = l & 3;
     const int cv = cur[i * cs + j], pv = pred[i * ps + j];
@@ -73,68 +98,80 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
     int t = fwd1(x0, x1, x2, x3, j);
     int y0 = __shfl_sync(FDVB_FULL, t, 0 * 4 + j), y1 = __shfl_sync(FDVB_FULL, t, 1 * 4 + j);
     int y2 = __shfl_sync(FDVB_FULL, t, 2 * 4 + j), y3 = __shfl_sync(FDVB_FULL, t, 3 * 4 + j);
-    int coef = fwd1(y0, y1, y2, y3, i);
-    int lev = quant4(coef, l, qp);
-    const int iz = c_IZZ4[l];
-    int last = __reduce_max_sync(FDVB_FULL, (lane < 16 && lev != 0) ? iz : -1);
+    const int coef = fwd1(y0, y1, y2, y3, i);
+    int lev;
+    {
+        int sign = coef < 0 ? -1 : 1;
+        long long aw = coef < 0 ? -(long long)coef : (long long)coef;
+        lev = (int16_t)(sign * (int)((aw * Q.mf[l] + Q.f) >> Q.qbits));
+    }
+    // zigzag view: lane k holds the level at zigzag position k
+    const int kz = l;
+    int levz = __shfl_sync(FDVB_FULL, lev, c_ZZ4[kz]);
+    unsigned nzm = __ballot_sync(FDVB_FULL, lane < 16 && levz != 0);
+    int last = nzm ? 31 - __clz(nzm) : -1;
     if (rdoq && last >= 0) {
+        const uint32_t z = zz_enc(levz);
+        const bool in = lane < 16 && kz <= last;
+        const int bits0 = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
+        const int pre = warp_incl_scan(in ? 8 * leb_size(z) : 0, lane);
+        const int tot = __shfl_sync(FDVB_FULL, pre, 31);
+        const int L = lane - 1;
+        int preL = __shfl_sync(FDVB_FULL, pre, L < 0 ? 0 : (L & 31));
+        if (L < 0) preL = 0;
+        const int bitsL = bits0 - (tot - preL);
+        const unsigned vmask = 1u | (nzm << 1);          // candidate c = L + 1
+        const bool valid = lane <= 16 && ((vmask >> lane) & 1u);
         if (lane < 16) { sc->res[l] = res; sc->lev[l] = lev; }
         __syncwarp();
-        int bv = (lane < 16 && iz <= last) ? bits_val(zz_enc(lev)) : 0;
-        int bits0 = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, bv);
-        const int L = lane - 1;
-        bool valid = lane <= 16 && L <= last && (L < 0 || sc->lev[c_ZZ4[L]] != 0);
+        double J = 0.0;
         if (valid) {
-            int bits = bits0;
-            for (int k = L + 1; k <= last; ++k) bits -= 8 * leb_size(zz_enc(sc->lev[c_ZZ4[k]]));
             int d[16], r[16];
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = dequant4(c_IZZ4[p] <= L ? sc->lev[p] : 0, p, qp);
+            for (int p = 0; p < 16; ++p) d[p] = (c_IZZ4[p] <= L ? sc->lev[p] : 0) * Q.dq[p];
             idct4_thread(d, r);
-            long long D = 0;
+            int D = 0;
 #pragma unroll
-            for (int p = 0; p < 16; ++p) { int e = sc->res[p] - r[p]; D += (long long)e * e; }
-            sc->J[lane] = rd_cost((double)D, lambda, bits);
+            for (int p = 0; p < 16; ++p) { int e = sc->res[p] - r[p]; D += e * e; }
+            J = rd_cost((double)D, lambda, bitsL);
         }
-        if (lane <= 16) sc->valid[lane] = valid;
-        __syncwarp();
         int bestL = last;
-        if (lane == 0) {
-            double bestJ = -1.0;
-            for (int Lc = last; Lc >= -1; --Lc) {
-                if (!sc->valid[Lc + 1]) continue;
-                double J = sc->J[Lc + 1];
-                if (bestJ < 0.0 || J < bestJ) { bestJ = J; bestL = Lc; }
-            }
+        double bestJ = -1.0;
+        unsigned m = vmask;
+        while (m) {                                        // uniform across the warp
+            const int c = 31 - __clz(m);
+            m &= ~(1u << c);
+            const double Jc = __shfl_sync(FDVB_FULL, J, c);
+            if (bestJ < 0.0 || Jc < bestJ) { bestJ = Jc; bestL = c - 1; }
         }
-        bestL = __shfl_sync(FDVB_FULL, bestL, 0);
-        if (iz > bestL) lev = 0;
+        if (kz > bestL) levz = 0;
+        if (c_IZZ4[l] > bestL) lev = 0;
         last = bestL;
         __syncwarp();
     }
-    // Reconstruct from the final levels.
-    int dq = dequant4(lane < 16 ? lev : 0, l, qp);
+    // reconstruct from the final levels
+    const int dq = (lane < 16 ? lev : 0) * Q.dq[l];
     int d0 = __shfl_sync(FDVB_FULL, dq, i * 4 + 0), d1 = __shfl_sync(FDVB_FULL, dq, i * 4 + 1);
     int d2 = __shfl_sync(FDVB_FULL, dq, i * 4 + 2), d3 = __shfl_sync(FDVB_FULL, dq, i * 4 + 3);
     int u = inv1(d0, d1, d2, d3, j);
     int e0 = __shfl_sync(FDVB_FULL, u, 0 * 4 + j), e1 = __shfl_sync(FDVB_FULL, u, 1 * 4 + j);
     int e2 = __shfl_sync(FDVB_FULL, u, 2 * 4 + j), e3 = __shfl_sync(FDVB_FULL, u, 3 * 4 + j);
-    int rr = (int16_t)((inv1(e0, e1, e2, e3, i) + 32) >> 6);
-    int r = clipb(pv + rr);
+    const int rr = (int16_t)((inv1(e0, e1, e2, e3, i) + 32) >> 6);
+    const int r = clipb(pv + rr);
     if (lane < 16) rec[i * rs + j] = (uint8_t)r;
-    int dd = cv - r;
-    int ssd = __reduce_add_sync(FDVB_FULL, lane < 16 ? dd * dd : 0);
-    uint32_t z = zz_enc(lev);
-    int bl = (lane < 16 && iz <= last) ? bits_val(z) : 0;
-    int bits = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, bl);
-    // Level bytes in zigzag order: each lane knows its LEB length; lane 0 packs.
-    if (lane < 16) sc->lev[l] = lev;
-    __syncwarp();
+    const int dd = cv - r;
+    const int ssd = __reduce_add_sync(FDVB_FULL, lane < 16 ? dd * dd : 0);
+    // rate and level bytes, zigzag order
+    const uint32_t z = zz_enc(levz);
+    const bool in = lane < 16 && kz <= last;
+    const int bits = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
+    const int len = in ? leb_size(z) : 0;
+    const int end = warp_incl_scan(len, lane);
+    if (in) leb_write(out->bytes + (end - len), z);
+    const int nbytes = __shfl_sync(FDVB_FULL, end, 31);
     if (lane == 0) {
-        int nb = 0;
-        for (int k = 0; k <= last; ++k) nb += leb_write(out->bytes + nb, zz_enc(sc->lev[c_ZZ4[k]]));
         out->count = last + 1;
-        out->nbytes = nb;
+        out->nbytes = nbytes;
         out->ssd = ssd;
         out->bits = bits;
     }
@@ -148,7 +185,7 @@ struct Reg8Scratch {
     int32_t Y[64];
     int32_t L[64];
     long long B[64];
-    int ssd_part[2];
+    int part[2][4];
 };
 struct Reg8 {
     int count, nbytes, bits;
@@ -159,13 +196,14 @@ struct Reg8 {
 
 // 64 threads (t = 0..63) code one 8x8 region with the 8x8 transform: forward
 // DCT in int32, quantise, dequantise (saturating to int32), inverse in int64
-// with >> 36 normalisation, reconstruct.  `bar` names a named barrier shared
-// only by these 64 threads (two warps).
+// with >> 36 normalisation, reconstruct; then count, rate and level bytes in
+// zigzag order from ballots and prefix sums.  `bar` names a named barrier
+// shared only by these 64 threads (two warps).
 __device__ __forceinline__ void bar_sync64(int bar) { asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory"); }
 
 __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps, int qp,
                         Reg8 *out, Reg8Scratch *sc, int t, int bar) {
-    const int r = t >> 3, c = t & 7;
+    const int r = t >> 3, c = t & 7, lane = t & 31, w = t >> 5;
     const int cv = cur[r * cs + c], pv = pred[r * ps + c];
     sc->X[t] = cv - pv;
     bar_sync64(bar);
@@ -183,7 +221,7 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
         for (int x = 0; x < 8; ++x) s += sc->A[r * 8 + x] * c_C8[c * 8 + x];
         Yv = s;
     }
-    int32_t q = c_QSTEP8[qp], f = q / 3;
+    const int32_t q = c_QSTEP8[qp], f = q / 3;
     int sign = Yv < 0 ? -1 : 1;
     int32_t a = Yv < 0 ? -Yv : Yv;
     int lev = (int16_t)(sign * ((a + f) / q));
@@ -205,30 +243,45 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
         for (int v = 0; v < 8; ++v) s += sc->B[r * 8 + v] * (long long)c_C8[v * 8 + c];
         rr = (int16_t)((s + (1LL << 35)) >> 36);
     }
-    int rv = clipb(pv + rr);
+    const int rv = clipb(pv + rr);
     out->rec[t] = (uint8_t)rv;
-    int d = cv - rv;
-    int ssd = __reduce_add_sync(FDVB_FULL, d * d);
-    if ((t & 31) == 0) sc->ssd_part[t >> 5] = ssd;
+    const int d = cv - rv;
+    // zigzag view: thread k holds the level at zigzag position k
+    const int lz = sc->L[c_ZZ8[t]];
+    const unsigned b = __ballot_sync(FDVB_FULL, lz != 0);
+    const int ssd = __reduce_add_sync(FDVB_FULL, d * d);
+    if (lane == 0) { sc->part[w][0] = b ? 32 * w + 31 - __clz(b) : -1; sc->part[w][1] = ssd; }
     bar_sync64(bar);
+    const int last = max(sc->part[0][0], sc->part[1][0]);
+    const uint32_t z = zz_enc(lz);
+    const bool in = t <= last;
+    const int bsum = __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
+    const int len = in ? leb_size(z) : 0;
+    const int end = warp_incl_scan(len, lane);
+    if (lane == 31) { sc->part[w][2] = end; sc->part[w][3] = bsum; }
+    bar_sync64(bar);
+    const int base = w ? sc->part[0][2] : 0;
+    if (in) leb_write(out->bytes + base + end - len, z);
     if (t == 0) {
-        int last1 = 0;
-        for (int k = 0; k < 64; ++k) if (sc->L[c_ZZ8[k]] != 0) last1 = k + 1;
-        int nb = 0, bits = kBitsFlag + bits_val((uint32_t)last1);
-        for (int k = 0; k < last1; ++k) {
-            uint32_t z = zz_enc(sc->L[c_ZZ8[k]]);
-            nb += leb_write(out->bytes + nb, z);
-            bits += bits_val(z);
-        }
-        out->count = last1;
-        out->nbytes = nb;
-        out->bits = bits;
-        out->ssd = (long long)sc->ssd_part[0] + sc->ssd_part[1];
+        out->count = last + 1;
+        out->nbytes = sc->part[0][2] + sc->part[1][2];
+        out->bits = kBitsFlag + bits_val((uint32_t)(last + 1)) + sc->part[0][3] + sc->part[1][3];
+        out->ssd = (long long)sc->part[0][1] + sc->part[1][1];
     }
     bar_sync64(bar);
 }
 
 // --------------------------------------------------- residual (n x n) --
+// The decision of one 8x8 region between its 4x4 option (A) and its 8x8
+// option (B), with the region's byte counts in each stream.
+struct RegDec {
+    int choice, flv;          // 0 = four 4x4 (A), 1 = one 8x8 (B); flag byte value
+    int nl, ol;               // level bytes and their offset in the level stream
+    int oc, ofl;              // offsets in the count stream and the flag stream
+    long long e;
+    int b;
+};
+
 // Scratch for one chunk of up to NT/64 8x8 regions of a code_residual call.
 template <int NT>
 struct ResidScratchT {
@@ -238,24 +291,95 @@ struct ResidScratchT {
     Reg8 reg[RMAX];
     Reg8Scratch r8[RMAX];
     Blk4Scratch b4[NW];
-    int choice[RMAX];
+    RegDec dec[RMAX];
     long long e;
     int b;
 };
-using ResidScratch = ResidScratchT<256>;
+
+// Decide regions [0, nreg) given their A results blk[4*rg..] and B results
+// reg[rg], append their symbols to `sink` in region order, and leave the
+// chunk's distortion and rate in e / b.  Called by all NT threads.
+template <int NT>
+__device__ void decide_regions(int nreg, Blk4 *blk, Reg8 *reg, RegDec *dec, double lambda, bool chroma,
+                               CoefSink *sink, long long *e_out, int *b_out, unsigned *err) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid < nreg) {
+        const int rg = tid;
+        long long eA = 0;
+        int bA = kBitsFlag, lpA = 0;
+        for (int s = 0; s < 4; ++s) { eA += blk[rg * 4 + s].ssd; bA += blk[rg * 4 + s].bits; lpA += blk[rg * 4 + s].nbytes; }
+        const Reg8 &R = reg[rg];
+        long long eB = R.ssd;
+        int bB = R.bits;
+        const bool emptyA = lpA == 0, emptyB = R.count == 0;
+        if (emptyA) bA = kBitsFlag;
+        if (emptyB) bB = kBitsFlag;
+        RegDec &D = dec[rg];
+        if (rd_cost((double)eA, lambda, bA) <= rd_cost((double)eB, lambda, bB)) {
+            D.choice = 0; D.flv = emptyA ? 0 : 1; D.nl = emptyA ? 0 : lpA; D.e = eA; D.b = bA;
+        } else {
+            D.choice = 1; D.flv = emptyB ? 0 : 2; D.nl = emptyB ? 0 : R.nbytes; D.e = eB; D.b = bB;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int kc = chroma ? CS_NC : CS_N, kl = chroma ? CS_LC : CS_L;
+        long long e = 0;
+        int b = 0;
+        bool ovf = false;
+        for (int rg = 0; rg < nreg; ++rg) {
+            RegDec &D = dec[rg];
+            D.ofl = sink->len[CS_FL]++;
+            if (D.flv == 1) { D.oc = sink->len[kc]; sink->len[kc] += 4; D.ol = sink->len[kl]; sink->len[kl] += D.nl; }
+            else if (D.flv == 2) { D.oc = sink->len[CS_N8]; sink->len[CS_N8] += 1; D.ol = sink->len[CS_L8]; sink->len[CS_L8] += D.nl; }
+            e += D.e;
+            b += D.b;
+        }
+        for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) ovf = true;
+        if (ovf) {
+            atomicOr(err, kErrSlotOverflow);
+            for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) sink->len[k] = sink->cap[k];
+            for (int rg = 0; rg < nreg; ++rg) dec[rg].flv = -1;   // write nothing
+        }
+        *e_out = e;
+        *b_out = b;
+    }
+    __syncthreads();
+    // one warp per region copies its flag, counts and level bytes
+    for (int rg = warp; rg < nreg; rg += NT / 32) {
+        const RegDec &D = dec[rg];
+        if (D.flv < 0) continue;
+        if (lane == 0) sink->buf[CS_FL][D.ofl] = (uint8_t)D.flv;
+        if (D.flv == 1) {
+            uint8_t *cnt = sink->buf[chroma ? CS_NC : CS_N] + D.oc;
+            uint8_t *lv = sink->buf[chroma ? CS_LC : CS_L] + D.ol;
+            int o = 0;
+            for (int s2 = 0; s2 < 4; ++s2) {
+                const Blk4 &B4 = blk[rg * 4 + s2];
+                if (lane == 0) cnt[s2] = (uint8_t)B4.count;
+                for (int i = lane; i < B4.nbytes; i += 32) lv[o + i] = B4.bytes[i];
+                o += B4.nbytes;
+            }
+        } else if (D.flv == 2) {
+            if (lane == 0) sink->buf[CS_N8][D.oc] = (uint8_t)reg[rg].count;
+            uint8_t *lv = sink->buf[CS_L8] + D.ol;
+            for (int i = lane; i < D.nl; i += 32) lv[i] = reg[rg].bytes[i];
+        }
+    }
+}
 
 // The whole block (NT threads) codes an n x n residual, n in {8, 16, 32, 64}:
 // per aligned 8x8 region, in raster order, the RD choice between four RDOQ'd
 // 4x4 transforms and one 8x8 transform, with the 3-valued region flag
 // (fdv.h:5300-5414).  Regions are processed NT/64 at a time: every 4x4 block
 // of the chunk on its own warp, every region's 8x8 option on 64 threads, then
-// the decisions in order.  cur has stride cs, pred and rec stride ps / rs.
-// Appends to `sink` (4x4 symbols to the chroma streams when `chroma`),
-// returns the distortion and adds the rate to *bits (uniform on return).
+// the decisions.  cur has stride cs, pred ps, rec rs.  Appends to `sink`
+// (4x4 symbols to the chroma streams when `chroma`), returns the distortion
+// and adds the rate to *bits (uniform on return).
 template <int NT>
-__device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *pred, int ps, int n, int qp,
-                                     double lambda, bool chroma, uint8_t *rec, int rs, CoefSink *sink,
-                                     int *bits, ResidScratchT<NT> *sc, unsigned *err) {
+__device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *pred, int ps, int n,
+                                     const QP4 &Q, int qp, double lambda, bool chroma, uint8_t *rec, int rs,
+                                     CoefSink *sink, int *bits, ResidScratchT<NT> *sc, unsigned *err) {
     constexpr int RMAX = NT / 64, NW = NT / 32;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int rpl = n / 8, nreg_total = rpl * rpl;
@@ -267,57 +391,18 @@ __device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *
             int rg = b >> 2, s = b & 3, gr = r0 + rg;
             int rx = (gr % rpl) * 8, ry = (gr / rpl) * 8, sx = (s & 1) * 4, sy = (s >> 1) * 4;
             warp_block4(cur + (ry + sy) * cs + rx + sx, cs, pred + (ry + sy) * ps + rx + sx, ps,
-                        &sc->recA[rg][sy * 8 + sx], 8, qp, lambda, true, &sc->blk[b], &sc->b4[warp], lane);
+                        &sc->recA[rg][sy * 8 + sx], 8, Q, lambda, true, &sc->blk[b], &sc->b4[warp], lane);
         }
         if (tid < nreg * 64) {
             int rg = tid >> 6, gr = r0 + rg, rx = (gr % rpl) * 8, ry = (gr / rpl) * 8;
             region8(cur + ry * cs + rx, cs, pred + ry * ps + rx, ps, qp, &sc->reg[rg], &sc->r8[rg], tid & 63, 1 + rg);
         }
         __syncthreads();
-        if (tid == 0) {
-            long long e = 0;
-            int b = 0;
-            for (int rg = 0; rg < nreg; ++rg) {
-                long long eA = 0;
-                int bA = kBitsFlag, lpA = 0;
-                for (int s = 0; s < 4; ++s) { eA += sc->blk[rg * 4 + s].ssd; bA += sc->blk[rg * 4 + s].bits; lpA += sc->blk[rg * 4 + s].nbytes; }
-                const Reg8 &R = sc->reg[rg];
-                long long eB = R.ssd;
-                int bB = R.bits;
-                bool emptyA = lpA == 0, emptyB = R.count == 0;
-                if (emptyA) bA = kBitsFlag;
-                if (emptyB) bB = kBitsFlag;
-                if (rd_cost((double)eA, lambda, bA) <= rd_cost((double)eB, lambda, bB)) {
-                    if (emptyA) cs_put1(sink, CS_FL, 0, err);
-                    else {
-                        cs_put1(sink, CS_FL, 1, err);
-                        for (int s = 0; s < 4; ++s) {
-                            const Blk4 &B4 = sc->blk[rg * 4 + s];
-                            cs_put1(sink, chroma ? CS_NC : CS_N, (uint8_t)B4.count, err);
-                            cs_put(sink, chroma ? CS_LC : CS_L, B4.bytes, B4.nbytes, err);
-                        }
-                    }
-                    sc->choice[rg] = 0;
-                    e += eA; b += bA;
-                } else {
-                    if (emptyB) cs_put1(sink, CS_FL, 0, err);
-                    else {
-                        cs_put1(sink, CS_FL, 2, err);
-                        cs_put1(sink, CS_N8, (uint8_t)R.count, err);
-                        cs_put(sink, CS_L8, R.bytes, R.nbytes, err);
-                    }
-                    sc->choice[rg] = 1;
-                    e += eB; b += bB;
-                }
-            }
-            sc->e = e;
-            sc->b = b;
-        }
-        __syncthreads();
+        decide_regions<NT>(nreg, sc->blk, sc->reg, sc->dec, lambda, chroma, sink, &sc->e, &sc->b, err);
         for (int p = tid; p < nreg * 64; p += NT) {
             int rg = p >> 6, q = p & 63, gr = r0 + rg;
             int y = (gr / rpl) * 8 + (q >> 3), x = (gr % rpl) * 8 + (q & 7);
-            rec[y * rs + x] = sc->choice[rg] ? sc->reg[rg].rec[q] : sc->recA[rg][q];
+            rec[y * rs + x] = sc->dec[rg].choice ? sc->reg[rg].rec[q] : sc->recA[rg][q];
         }
         etot += sc->e;
         btot += sc->b;
@@ -325,21 +410,6 @@ __device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *
     }
     *bits += btot;
     return etot;
-}
-
-// The P-frame kernel's form: 256 threads, n in {8, 16}, pred and rec stride n.
-__device__ __forceinline__ long long code_residual(const uint8_t *cur, int cs, const uint8_t *pred, int n, int qp,
-                                                   double lambda, bool chroma, uint8_t *rec, CoefSink *sink,
-                                                   int *bits, ResidScratch *sc, unsigned *err) {
-    return code_residual_t<256>(cur, cs, pred, n, n, qp, lambda, chroma, rec, n, sink, bits, sc, err);
-}
-
-// A single 4x4 residual (n == 4, the chroma quadrants of INTER8): one warp.
-// The caller arranges for exactly one warp to call this.
-__device__ long long code_residual4_warp(const uint8_t *cur, int cs, const uint8_t *pred, int qp,
-                                         double lambda, uint8_t *rec, Blk4 *out, Blk4Scratch *sc, int lane) {
-    warp_block4(cur, cs, pred, 4, rec, 4, qp, lambda, true, out, sc, lane);
-    return out->ssd;
 }
 
 }  // namespace fdvb

@@ -129,6 +129,12 @@ void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns);
  * a progress flag nothing sets; the waits expire and fdvg_frame returns an
  * error, leaving the engine usable. */
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row);
+/* Per-phase cycle profile of the P-frame analysis kernel, for tuning:
+ * enable != 0 turns it on (thread 0 of every block adds clock64 deltas:
+ * wait, load, SKIP, searches, residuals, region decisions, commit, output,
+ * then the macroblock count and the SKIP early-out count); out16 (may be NULL)
+ * receives and clears the 16 accumulators. */
+int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out16);
 
 /* Allocation-free P-frame analysis of one unit.  No counterpart in the
  * reference.  For callers that cannot allocate device memory while they
