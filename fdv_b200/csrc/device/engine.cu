@@ -70,6 +70,7 @@ struct IPlaneDevH {
     uint8_t *slots;
     int w, h, cols, rows, qp;
     double lambda;
+    unsigned long long *prof;
 };
 struct ITaskH { int plane, row; };
 struct PrepTaskH {
@@ -351,7 +352,7 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
                 IPlaneDevH P;
                 P.src = d.cur[p]; P.rec = d.rec[p]; P.mmap = u.mmap[p]; P.progress = u.progress + prog;
                 P.slots = u.islots[p]; P.w = u.pw[p]; P.h = u.ph[p]; P.cols = u.icols[p]; P.rows = u.irows[p];
-                P.qp = qp[i]; P.lambda = fdvb_lambda(qp[i], 1.0);
+                P.qp = qp[i]; P.lambda = fdvb_lambda(qp[i], 1.0); P.prof = E->d_prof ? E->d_prof + 16 : nullptr;
                 int pid = (int)iplanes.size();
                 iplanes.push_back(P);
                 for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
@@ -397,9 +398,8 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
     if (!itasks.empty()) {
         CK(cudaMemcpyAsync(E->d_planes, iplanes.data(), sizeof(IPlaneDevH) * iplanes.size(), cudaMemcpyHostToDevice, E->st));
         CK(cudaMemcpyAsync(E->d_itasks, itasks.data(), sizeof(ITaskH) * itasks.size(), cudaMemcpyHostToDevice, E->st));
-        int grid = std::min((int)itasks.size(), E->nsm);
         CK(cudaEventRecord(E->ev[3], E->st));
-        launch_iframe(E->d_planes, E->d_itasks, (int)itasks.size(), E->d_ticket + 1, E->d_err, E->wait_ns, grid, E->st);
+        launch_iframe(E->d_planes, E->d_itasks, (int)itasks.size(), E->d_ticket + 1, E->d_err, E->wait_ns, E->nsm, E->st);
         CK(cudaGetLastError());
         CK(cudaEventRecord(E->ev[4], E->st));
         E->launches += 1;
@@ -518,19 +518,21 @@ extern "C" void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row) {
     E->stall_row = row;
 }
 
-// Per-phase cycle profile of the P-frame kernel (thread 0 of each block adds
-// clock64 deltas): wait, load, SKIP, searches, residuals, region decisions,
-// commit, output; then macroblock and SKIP-early-out counts.  Enabling it
-// allocates the accumulators; reading returns and clears them.
-extern "C" int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out16) {
+// Per-phase cycle profile (thread 0 of each block adds clock64 deltas).
+// Entries 0..15, P-frame kernel: wait, load, SKIP, searches, residuals, region
+// decisions, commit, output, macroblock count, SKIP early-out count.  Entries
+// 16..31, key-frame kernel: wait, 4x4 leaves, 8/16/32/64 leaves, CTU total,
+// CTU count, 4x4 leaf count.  Enabling it allocates the accumulators; reading
+// returns and clears them.
+extern "C" int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out32) {
     if (!E) return -1;
     if (enable && !E->d_prof) {
-        if (cudaMalloc(&E->d_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return -3;
-        cudaMemset(E->d_prof, 0, 16 * sizeof(unsigned long long));
+        if (cudaMalloc(&E->d_prof, 32 * sizeof(unsigned long long)) != cudaSuccess) return -3;
+        cudaMemset(E->d_prof, 0, 32 * sizeof(unsigned long long));
     }
-    if (out16 && E->d_prof) {
-        cudaMemcpy(out16, E->d_prof, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-        cudaMemset(E->d_prof, 0, 16 * sizeof(unsigned long long));
+    if (out32 && E->d_prof) {
+        cudaMemcpy(out32, E->d_prof, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        cudaMemset(E->d_prof, 0, 32 * sizeof(unsigned long long));
     }
     if (!enable && E->d_prof) { cudaFree(E->d_prof); E->d_prof = nullptr; }
     return 0;

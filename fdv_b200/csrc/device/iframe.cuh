@@ -1,30 +1,42 @@
 // Key-frame analysis: the intra quadtree of the image codec as a persistent
-// wavefront kernel over coding tree units.
+// wavefront kernel over coding tree units, run by clusters of four blocks.
 //
-// Work unit: one 64x64 CTU row of one plane of one encoder unit; rows are
-// taken from an atomic ticket in plane order.  CTU (c, r) starts once row r-1
+// Work unit: one 64x64 CTU row of one plane of one encoder unit; clusters take
+// rows from an atomic ticket in plane order.  CTU (c, r) starts once row r-1
 // has finished CTU c+1 -- the top-right samples a 4x4 leaf on the CTU's top
 // edge may read -- exactly the reference's wavefront (intra_ctu_row,
 // fdv.h:4698-4725), with bounded waits.
 //
-// Inside a CTU the 512 threads walk the quadtree in the reference's order
-// (intra_node, fdv.h:4494-4582): at every node inside the plane the split trial
-// (four children, recursively) and then the leaf trial, kept if strictly
-// cheaper; nodes crossing the plane edge split with no flag; 4x4 leaves choose
-// among the nine directions by SATD screen and RD trial and are re-coded with
-// RDOQ (intra_leaf4, fdv.h:3907-4111).  The recursion is unrolled at compile
-// time (inode<D>).  The CTU's reconstruction, its 4x4 mode map and every
-// trial's symbols live in shared memory; the winner is appended to the CTU's
-// output slot.  A 4x4 leaf runs on one warp; a larger leaf's four sub-modes and
-// their 8x8 regions use all sixteen warps.
+// The quadtree (intra_node, fdv.h:4494-4582) tries, at every node inside the
+// plane, the split (four children, recursively) and the leaf, and keeps the
+// leaf only if it is not more expensive.  A node's leaf trial reads nothing
+// but the samples above and left of the node, which are final when the node
+// starts, so it runs concurrently with the node's split trial:
+//   * block 0, warps 0-3 ("the chain"): the walk in the reference's order, the
+//     4x4 leaves (intra_leaf4, fdv.h:3907-4111), the split/leaf decisions and
+//     the CTU's symbols; it holds the CTU's reconstruction and mode map;
+//   * block 0, warps 4-15: the 8x8 leaf trials; blocks 1, 2, 3 (all 16 warps):
+//     the 16x16, 32x32 and 64x64 leaf trials (intra_leafn, fdv.h:4442-4484),
+//     every allowed mode at once.
+// When the chain enters a node it posts the node's neighbours to the team of
+// that size through distributed shared memory; the team codes the leaf and
+// posts back its cost; the chain reads the winner's reconstruction and symbols
+// from the team's shared memory only if the leaf wins.  Every wait is bounded.
+#include <cooperative_groups.h>
 #include "common.cuh"
 #include "intra.cuh"
 #include "residual.cuh"
 
 namespace fdvb {
 
+namespace cg = cooperative_groups;
+
 constexpr int INT = 512;              // threads per block
+constexpr int ICL = 4;                // blocks per cluster
 constexpr int kTileW = 129;           // tile columns: x in [-1, 127] relative to the CTU
+constexpr int kChainNT = 128;         // chain threads (block 0, warps 0-3)
+constexpr int kH8NT = INT - kChainNT; // 8x8 leaf team (block 0, warps 4-15)
+enum { BAR_CHAIN = 1, BAR_H8 = 2, BAR_TEAM = 3 };
 
 // Stream ids of the intra path (fdv.h:4273-4289).
 enum { IS_SPLIT0 = 0, IS_MODEB = 4, IS_MODE0 = 5, IS_MODE1 = 6, IS_NS = 7 };
@@ -51,10 +63,16 @@ struct IPlaneDev {
     uint8_t *slots;         // per CTU output slot
     int w, h, cols, rows, qp;
     double lambda;
+    unsigned long long *prof;   // optional cycle profile (NULL: off)
 };
+// Profile entries of the key-frame kernel (relative to prof): chain waits for
+// the row above, chain 4x4 leaves, team busy time per leaf size, CTU time,
+// CTU count, 4x4 leaf count, chain waits for team results.
+enum { IP_WAIT = 0, IP_LEAF4, IP_LEAF8, IP_LEAF16, IP_LEAF32, IP_LEAF64, IP_CTU, IP_NCTU, IP_NLEAF4, IP_HWAIT };
 struct ITask { int plane, row; };
 
-// Per-depth sink capacities (node of side n = 64 >> d, see nd_struct/nd_cnt/nd_lvl fdv.h:4312-4314).
+// Per-depth split-trial sink capacities (node of side n = 64 >> d, see
+// nd_struct/nd_cnt/nd_lvl fdv.h:4312-4314).
 __host__ __device__ constexpr int isink_scap(int d, int k) {
     return k < 4 ? (k >= d ? (1 << (2 * (k - d))) : 0)
                  : (k == 4 ? (d <= 0 ? 85 : (d == 1 ? 21 : (d == 2 ? 5 : 1))) : ((64 >> d) / 4) * ((64 >> d) / 4));
@@ -70,56 +88,103 @@ __host__ __device__ constexpr int isink_bytes(int d) {
     for (int k = 0; k < CS_NUM; ++k) t += isink_ccap(d, k);
     return t;
 }
-constexpr int kLeafSinkBytes = isink_ccap(0, 0) + isink_ccap(0, 1) + isink_ccap(0, 2) + isink_ccap(0, 3) + isink_ccap(0, 4);
+// A team's per-mode coefficient sink: the capacities of a 64x64 leaf, stream
+// k at a fixed offset so that the chain can address it in another block.
+__host__ __device__ constexpr int leaf_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += isink_ccap(0, i); return o; }
+constexpr int kLeafSinkBytes = leaf_off(CS_NUM);
 
-struct IShared {
-    QP4 q;
+// A leaf-trial job (written by the chain) and its result (read by the chain).
+struct HJob {
+    int seq;                 // job sequence number, release-stored last
+    int kind;                // 0: code the node's leaf; 1: end of the CTU row
+    int bx, by, ht, hl, tl;
+    uint8_t top[64], left[64];
+};
+struct HelperArea {
+    HJob job;
+    int ok, nm, ml[4];
+    int best_idx, best_mode;
+    double best_J;
+    NNPred nn[4];
+    long long e[4];
+    int b[4];
+    CoefSink sink[4];
+    __align__(16) uint8_t src[64 * 64];
+    __align__(16) uint8_t pred[4][64 * 64];
+    __align__(16) uint8_t rec[4][64 * 64];
+    __align__(16) uint8_t sinkmem[4][kLeafSinkBytes];
+    TeamResidScratch<INT / 32> ts;
+};
+struct ChainArea {
     uint8_t tile[65 * kTileW];            // reconstruction: rows -1..63, cols -1..127
-    uint8_t src[64 * 64];
+    __align__(16) uint8_t src[64 * 64];
     uint8_t mm[17 * 17];                  // mode map: cells -1..15 x -1..15
-    uint8_t stash_rec[64 * 64 + 32 * 32 + 16 * 16 + 8 * 8];
-    uint8_t stash_mm[16 * 16 + 8 * 8 + 4 * 4 + 2 * 2];
-    uint8_t pred[4][16 * 16];             // leaf trial predictions (all four modes when n <= 16)
-    uint8_t trec[4][64 * 64 / 4 > 256 ? 1024 : 1024];
-    uint8_t bigpred[64 * 64];
-    uint8_t bigrec[2][64 * 64];
     ISink ss[4];                          // split trial sinks per depth
     uint8_t ssmem[isink_bytes(0) + isink_bytes(1) + isink_bytes(2) + isink_bytes(3)];
-    CoefSink lsink[4];                    // leaf trial sinks (parallel modes, or ping-pong)
-    uint8_t lsmem[4][isink_ccap(2, 0) + isink_ccap(2, 1) + isink_ccap(2, 2) + isink_ccap(2, 3) + isink_ccap(2, 4)];
-    CoefSink bsink[2];                    // ping-pong for n >= 32
-    uint8_t bsmem[2][kLeafSinkBytes];
-    ResidScratchT<INT> rs;
     ISink out;                            // the CTU's output (global)
-    // 4x4 leaf scratch (warp 0)
+    // 4x4 leaf scratch
+    int T9[9], L5[5];                     // T(-1..7), L(-1..3)
     uint8_t cp[9][16];
-    int csat[9], cmode[9], ncand, ntry;
+    int csat[9], cs[9], cm[9], run, best_c;
     Blk4 trial[9];
-    Blk4 fin;
-    uint8_t trec4[16];
-    Blk4Scratch b4;
-    uint8_t nb_top[64], nb_left[64];
-    int nb_tl, nb_ht, nb_hl;
-    NNPred nn[4];
-    double J[4];
-    int jbits[4];
-    long long jd[4];
+    Blk4 fin[2];
+    uint8_t frec[2][16], junk[4][16];
+    Blk4Scratch b4[4];
     double retJ;
-    int retMode;
-    int task, row_ok;
+    int done[4];                          // per leaf size: last finished job (written by the teams)
+    int issued[4];                        // per leaf size: last posted job
+    int abort, task, row_ok;
+};
+struct IShared {
+    QP4 q;
+    ChainArea C;
+    HelperArea H;
 };
 
-struct ICtx {
+struct CCtx {
     IShared *S;
     const IPlaneDev *P;
     int bx0, by0, w, h, qp;
     double lambda;
     unsigned *err;
+    unsigned long long *prof;
+    unsigned long long hlimit;
 };
 
-__device__ __forceinline__ uint8_t &TL(IShared *S, int ty, int tx) { return S->tile[(ty + 1) * kTileW + tx + 1]; }
-__device__ __forceinline__ uint8_t &MM(IShared *S, int cy, int cx) { return S->mm[(cy + 1) * 17 + cx + 1]; }
+// --------------------------------------------------- cluster plumbing --
+__device__ __forceinline__ void fence_cluster() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+__device__ __forceinline__ void st_release_cluster(int *p, int v) {
+    asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_cluster(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// Bounded wait (one thread) until *p >= need; false on timeout (reported) or
+// when another block has already raised an error.
+__device__ bool wait_cluster_flag(const int *p, int need, unsigned *err, unsigned long long limit_ns) {
+    if (ld_acquire_cluster(p) >= need) return true;
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+        if (ld_acquire_cluster(p) >= need) return true;
+        if (*(volatile unsigned *)err) return false;
+        if (globaltimer() - t0 > limit_ns) { atomicOr(err, kErrWaitTimeout); return false; }
+        __nanosleep(32);
+    }
+}
+// The leaf trials of nodes of side 64 >> L run in cluster block 3 - L.
+__device__ __forceinline__ int level_rank(int L) { return 3 - L; }
 
+__device__ __forceinline__ void cbar() { team_bar(BAR_CHAIN, kChainNT); }
+__device__ __forceinline__ uint8_t &TL(ChainArea &C, int ty, int tx) { return C.tile[(ty + 1) * kTileW + tx + 1]; }
+__device__ __forceinline__ uint8_t &MM(ChainArea &C, int cy, int cx) { return C.mm[(cy + 1) * 17 + cx + 1]; }
+__device__ __forceinline__ long long prof_t0(const unsigned long long *prof, int t) { return (prof && t == 0) ? clock64() : 0; }
+__device__ __forceinline__ void prof_add(unsigned long long *prof, int t, int k, long long t0) {
+    if (prof && t == 0) atomicAdd(&prof[k], (unsigned long long)(clock64() - t0));
+}
+
+// ------------------------------------------------------------- sinks --
 __device__ void isink_reset(ISink *s) {
     for (int k = 0; k < IS_NS; ++k) s->slen[k] = 0;
     cs_reset(&s->c);
@@ -128,37 +193,45 @@ __device__ void isink_put(ISink *s, int k, uint8_t v, unsigned *err) {
     if (s->slen[k] + 1 > s->scap[k]) { atomicOr(err, kErrSlotOverflow); return; }
     s->sbuf[k][s->slen[k]++] = v;
 }
-// dst += src (all threads; lengths updated after a barrier).
-__device__ void isink_append(ISink *dst, const ISink *src, unsigned *err) {
-    const int tid = threadIdx.x;
+// dst += src, by the chain (lengths updated after a barrier).
+__device__ void chain_isink_append(ISink *dst, const ISink *src, unsigned *err) {
+    const int t = threadIdx.x;
     for (int k = 0; k < IS_NS; ++k) {
-        int n = src->slen[k], b = dst->slen[k];
-        if (b + n > dst->scap[k]) { if (tid == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        for (int i = tid; i < n; i += INT) dst->sbuf[k][b + i] = src->sbuf[k][i];
+        const int n = src->slen[k], b = dst->slen[k];
+        if (b + n > dst->scap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
+        for (int i = t; i < n; i += kChainNT) dst->sbuf[k][b + i] = src->sbuf[k][i];
     }
     for (int k = 0; k < CS_NUM; ++k) {
-        int n = src->c.len[k], b = dst->c.len[k];
-        if (b + n > dst->c.cap[k]) { if (tid == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        for (int i = tid; i < n; i += INT) dst->c.buf[k][b + i] = src->c.buf[k][i];
+        const int n = src->c.len[k], b = dst->c.len[k];
+        if (b + n > dst->c.cap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
+        for (int i = t; i < n; i += kChainNT) dst->c.buf[k][b + i] = src->c.buf[k][i];
     }
-    __syncthreads();
-    if (tid == 0) {
+    cbar();
+    if (t == 0) {
         for (int k = 0; k < IS_NS; ++k) if (dst->slen[k] + src->slen[k] <= dst->scap[k]) dst->slen[k] += src->slen[k];
         for (int k = 0; k < CS_NUM; ++k) if (dst->c.len[k] + src->c.len[k] <= dst->c.cap[k]) dst->c.len[k] += src->c.len[k];
     }
-    __syncthreads();
+    cbar();
 }
-__device__ void csink_append(CoefSink *dst, const CoefSink *src, unsigned *err) {
-    const int tid = threadIdx.x;
+// dst += the team's sink `idx` (in cluster block `rank`), by the chain.
+__device__ void chain_append_leaf(CoefSink *dst, IShared *S, int rank, int idx, unsigned *err) {
+    const int t = threadIdx.x;
+    cg::cluster_group cl = cg::this_cluster();
+    const CoefSink *rs = cl.map_shared_rank(&S->H.sink[idx], rank);
+    const uint8_t *rm = cl.map_shared_rank(&S->H.sinkmem[idx][0], rank);
+    int len[CS_NUM];
+    for (int k = 0; k < CS_NUM; ++k) len[k] = rs->len[k];
     for (int k = 0; k < CS_NUM; ++k) {
-        int n = src->len[k], b = dst->len[k];
-        if (b + n > dst->cap[k]) { if (tid == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        for (int i = tid; i < n; i += INT) dst->buf[k][b + i] = src->buf[k][i];
+        const int n = len[k], b = dst->len[k];
+        if (n == 0) continue;
+        if (b + n > dst->cap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
+        const uint8_t *src = rm + leaf_off(k);
+        for (int i = t; i < n; i += kChainNT) dst->buf[k][b + i] = src[i];
     }
-    __syncthreads();
-    if (tid == 0)
-        for (int k = 0; k < CS_NUM; ++k) if (dst->len[k] + src->len[k] <= dst->cap[k]) dst->len[k] += src->len[k];
-    __syncthreads();
+    cbar();
+    if (t == 0)
+        for (int k = 0; k < CS_NUM; ++k) if (dst->len[k] + len[k] <= dst->cap[k]) dst->len[k] += len[k];
+    cbar();
 }
 
 // z-scan index of a 4x4 cell in its CTU (fdv.h:3659) and the availability of
@@ -185,304 +258,403 @@ __device__ __forceinline__ bool mode_ok4(int m, int ht, int htr, int hl, int htl
     }
 }
 
-// One 4x4 leaf (fdv.h:3907-4111) on warp 0; all threads call, the result is
-// returned uniformly.
-__device__ double leaf4(ICtx &c, int bx, int by, ISink *tgt) {
-    IShared *S = c.S;
-    const int tid = threadIdx.x, lane = tid & 31;
+// ------------------------------------------------------- 4x4 leaf --
+// One 4x4 leaf (fdv.h:3907-4111) on the chain's four warps: the nine
+// predictions and their SATD screen on half-warps, the reference's selection
+// sort and ratio prune on one thread, then the RD trials without RDOQ and the
+// RDOQ re-code of the winner.  With at most two trials (QP >= 12) the RDOQ
+// re-codes of both run beside the trials and the winner's is kept.
+__device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
+    ChainArea &C = c.S->C;
+    const QP4 &Q = c.S->q;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    const long long t0 = prof_t0(c.prof, t);
     const int tx = bx - c.bx0, ty = by - c.by0;
-    if (tid < 32) {
-        const int ht = by > 0, hl = bx > 0, htl = ht && hl;
-        const int htr = ht && (bx + 4 < c.w) && cell_done(bx + 4, by - 1, bx, by);
-        // neighbours (gather_neighbors fdv.h:3689-3706)
-        __shared__ uint8_t top[8], left[4];
-        __shared__ int tlv;
-        if (lane < 8) {
-            int v = 0;
-            if (ht) v = (lane < 4 || htr) ? TL(S, ty - 1, tx + lane) : TL(S, ty - 1, tx + 3);
-            top[lane] = (uint8_t)v;
-        } else if (lane < 12) {
-            left[lane - 8] = hl ? TL(S, ty + lane - 8, tx - 1) : 0;
-        } else if (lane == 12) {
-            tlv = htl ? TL(S, ty - 1, tx - 1) : 128;
-        }
-        __syncwarp();
-        // predict the allowed modes and SATD-screen them
-        if (lane < 9) {
-            int m = lane;
-            if (mode_ok4(m, ht, htr, hl, htl)) {
-                int Tn[9], Ln[5];
-                Tn[0] = tlv; for (int k = 0; k < 8; ++k) Tn[k + 1] = top[k];
-                Ln[0] = tlv; for (int k = 0; k < 4; ++k) Ln[k + 1] = left[k];
-                for (int p = 0; p < 16; ++p) S->cp[m][p] = (uint8_t)pred4_px(m, Tn, Ln, top, left, ht, hl, p & 3, p >> 2);
-                S->csat[m] = satd4(&S->src[ty * 64 + tx], 64, S->cp[m], 4);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-            int cs[9], cm[9], nc = 0;
-            for (int m = 0; m < 9; ++m) if (mode_ok4(m, ht, htr, hl, htl)) { cs[nc] = S->csat[m]; cm[nc] = m; ++nc; }
-            int ntry = c.qp < 12 ? nc : (nc < 2 ? nc : 2);
-            for (int a = 0; a < ntry; ++a) {
-                int bst = a;
-                for (int b2 = a + 1; b2 < nc; ++b2) if (cs[b2] < cs[bst]) bst = b2;
-                if (bst != a) { int t = cs[a]; cs[a] = cs[bst]; cs[bst] = t; t = cm[a]; cm[a] = cm[bst]; cm[bst] = t; }
-            }
-            // how many trials run before the SATD prune breaks the loop (fdv.h:3987-3990)
-            int run = 0;
-            for (int k = 0; k < ntry; ++k) {
-                if (k > 0 && c.qp >= 12 && (long long)cs[k] * 4 > (long long)cs[0] * 5) break;
-                ++run;
-            }
-            for (int k = 0; k < run; ++k) S->cmode[k] = cm[k];
-            S->ntry = run;
-        }
-        __syncwarp();
-        const int run = S->ntry;
-        double best_cost = -1.0;
-        int best_c = 0;
-        for (int k = 0; k < run; ++k) {
-            warp_block4(&S->src[ty * 64 + tx], 64, S->cp[S->cmode[k]], 4, S->trec4, 4, S->q, c.lambda, false,
-                        &S->trial[k], &S->b4, lane);
-            double J = rd_cost((double)S->trial[k].ssd, c.lambda, kBitsMode + S->trial[k].bits);
-            if (best_cost < 0.0 || J < best_cost) { best_cost = J; best_c = k; }
-        }
-        const int mode = S->cmode[best_c];
-        // re-code the winner with RDOQ straight into the reconstruction tile
-        warp_block4(&S->src[ty * 64 + tx], 64, S->cp[mode], 4, &TL(S, ty, tx), kTileW, S->q, c.lambda, true,
-                    &S->fin, &S->b4, lane);
-        if (lane == 0) {
-            cs_put1(&tgt->c, CS_N, (uint8_t)S->fin.count, c.err);
-            cs_put(&tgt->c, CS_L, S->fin.bytes, S->fin.nbytes, c.err);
-            int lcx = tx >> 2, lcy = ty >> 2;
-            int Lm = bx > 0 ? MM(S, lcy, lcx - 1) : 0;
-            int Am = by > 0 ? MM(S, lcy - 1, lcx) : 0;
-            isink_put(tgt, Lm == Am ? IS_MODE0 : IS_MODE1, (uint8_t)mode, c.err);
-            MM(S, lcy, lcx) = (uint8_t)mode;
-            S->retJ = rd_cost((double)S->fin.ssd, c.lambda, kBitsMode + S->fin.bits);
+    const int ht = by > 0, hl = bx > 0, htl = ht && hl;
+    const int htr = ht && (bx + 4 < c.w) && cell_done(bx + 4, by - 1, bx, by);
+    // neighbours (gather_neighbors fdv.h:3689-3706)
+    if (t < 8) C.T9[t + 1] = ht ? ((t < 4 || htr) ? TL(C, ty - 1, tx + t) : TL(C, ty - 1, tx + 3)) : 0;
+    else if (t < 12) C.L5[t - 7] = hl ? TL(C, ty + t - 8, tx - 1) : 0;
+    else if (t == 12) { const int v = htl ? TL(C, ty - 1, tx - 1) : 128; C.T9[0] = v; C.L5[0] = v; }
+    cbar();
+    {   // predictions: thread (m, p) for m = 0..7, then mode 8 on threads 0..15
+        const int m = t >> 4, p = t & 15;
+        if (mode_ok4(m, ht, htr, hl, htl)) C.cp[m][p] = (uint8_t)pred4_px(m, C.T9, C.L5, ht, hl, p & 3, p >> 2);
+        if (t < 16 && mode_ok4(8, ht, htr, hl, htl)) C.cp[8][p] = (uint8_t)pred4_px(8, C.T9, C.L5, ht, hl, p & 3, p >> 2);
+    }
+    cbar();
+    {   // SATD (fdv.h:3803-3823): half-warp h screens mode h, then warp 0 mode 8
+        const int l = t & 15, i = l >> 2, j = l & 3, rb = lane & ~3, cb = (lane & 16) + j;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass && w != 0) break;
+            const int m = pass ? 8 : (t >> 4);
+            const int d = (int)C.src[(ty + i) * 64 + tx + j] - (int)C.cp[m][l];
+            const int x0 = __shfl_sync(FDVB_FULL, d, rb), x1 = __shfl_sync(FDVB_FULL, d, rb + 1);
+            const int x2 = __shfl_sync(FDVB_FULL, d, rb + 2), x3 = __shfl_sync(FDVB_FULL, d, rb + 3);
+            const int a0 = x0 + x1, a1 = x0 - x1, a2 = x2 + x3, a3 = x2 - x3;
+            const int hv = j == 0 ? a0 + a2 : (j == 1 ? a1 + a3 : (j == 2 ? a0 - a2 : a1 - a3));
+            const int y0 = __shfl_sync(FDVB_FULL, hv, cb), y1 = __shfl_sync(FDVB_FULL, hv, cb + 4);
+            const int y2 = __shfl_sync(FDVB_FULL, hv, cb + 8), y3 = __shfl_sync(FDVB_FULL, hv, cb + 12);
+            const int b0 = y0 + y1, b1 = y0 - y1, b2 = y2 + y3, b3 = y2 - y3;
+            int s = abs(i == 0 ? b0 + b2 : (i == 1 ? b1 + b3 : (i == 2 ? b0 - b2 : b1 - b3)));
+            s += __shfl_xor_sync(FDVB_FULL, s, 8);
+            s += __shfl_xor_sync(FDVB_FULL, s, 4);
+            s += __shfl_xor_sync(FDVB_FULL, s, 2);
+            s += __shfl_xor_sync(FDVB_FULL, s, 1);
+            if (l == 0) C.csat[m] = s;
         }
     }
-    __syncthreads();
-    double J = S->retJ;
-    __syncthreads();
-    return J;
-}
-
-// Gather a leaf's n top / n left neighbours from the tile (gather_nb fdv.h:5201).
-__device__ void gather_leaf_nb(ICtx &c, int bx, int by, int n) {
-    IShared *S = c.S;
-    const int tid = threadIdx.x, tx = bx - c.bx0, ty = by - c.by0;
-    const int ht = by > 0, hl = bx > 0;
-    if (tid < n) S->nb_top[tid] = ht ? TL(S, ty - 1, tx + tid) : 0;
-    else if (tid >= 64 && tid < 64 + n) S->nb_left[tid - 64] = hl ? TL(S, ty + tid - 64, tx - 1) : 0;
-    if (tid == 0) { S->nb_ht = ht; S->nb_hl = hl; S->nb_tl = (ht && hl) ? TL(S, ty - 1, tx - 1) : 128; }
-    __syncthreads();
-    if (tid < 4) S->nn[tid] = nn_setup(tid, S->nb_top, S->nb_left, S->nb_tl, n, S->nb_ht, S->nb_hl);
-    __syncthreads();
-}
-
-// An n x n leaf (intra_leafn fdv.h:4442-4484): the allowed sub-modes coded
-// through the residual coder, the cheapest (first strictly better) kept.
-// Leaves the winner's reconstruction in the tile and returns its cost; the
-// winner's coefficient sink is *best_sink.
-template <int n>
-__device__ double leafn(ICtx &c, int bx, int by, int *mode_out, CoefSink **best_sink) {
-    IShared *S = c.S;
-    const int tid = threadIdx.x, tx = bx - c.bx0, ty = by - c.by0;
-    gather_leaf_nb(c, bx, by, n);
-    const int ht = S->nb_ht, hl = S->nb_hl;
-    double best = -1.0;
-    int bmode = 0, bidx = 0;
-    if (n <= 16) {
-        // all allowed modes at once: each mode's regions are independent work
-        if (tid < 4) cs_reset(&S->lsink[tid]);
-        for (int p = tid; p < 4 * n * n; p += INT) {
-            int m = p / (n * n), q = p % (n * n);
-            S->pred[m][q] = (uint8_t)nn_px(S->nn[m], S->nb_top, S->nb_left, q % n, q / n);
+    cbar();
+    if (t == 0) {   // the reference's selection sort over the screened modes, then the ratio prune
+        int nc = 0;
+        for (int m = 0; m < 9; ++m)
+            if (mode_ok4(m, ht, htr, hl, htl)) { C.cs[nc] = C.csat[m]; C.cm[nc] = m; ++nc; }
+        const int ntry = c.qp < 12 ? nc : (nc < 2 ? nc : 2);
+        for (int a = 0; a < ntry; ++a) {
+            int bst = a;
+            for (int b2 = a + 1; b2 < nc; ++b2) if (C.cs[b2] < C.cs[bst]) bst = b2;
+            if (bst != a) {
+                int v = C.cs[a]; C.cs[a] = C.cs[bst]; C.cs[bst] = v;
+                v = C.cm[a]; C.cm[a] = C.cm[bst]; C.cm[bst] = v;
+            }
         }
-        __syncthreads();
-        for (int m = 0; m < 4; ++m) {
-            if (!nn_mode_ok(m, n, ht, hl)) continue;
-            int bits = kBitsMode;
-            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->pred[m], n, n, S->q, c.qp, c.lambda, false,
-                                               S->trec[m], n, &S->lsink[m], &bits, &S->rs, c.err);
-            double J = rd_cost((double)D, c.lambda, bits);
-            if (best < 0.0 || J < best) { best = J; bmode = m; bidx = m; }
+        int run = 0;
+        for (int k = 0; k < ntry; ++k) {
+            if (k > 0 && c.qp >= 12 && (long long)C.cs[k] * 4 > (long long)C.cs[0] * 5) break;
+            ++run;
         }
-        for (int p = tid; p < n * n; p += INT) TL(S, ty + p / n, tx + p % n) = S->trec[bidx][p];
-        *best_sink = &S->lsink[bidx];
+        C.run = run;
+    }
+    cbar();
+    const int run = C.run;
+    const uint8_t *sblk = &C.src[ty * 64 + tx];
+    int fsel;
+    if (run <= 2) {
+        const int k = w & 1;
+        if (k < run) {
+            if (w < 2) warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.junk[w], 4, Q, c.lambda, false, &C.trial[k], &C.b4[w], lane);
+            else       warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.frec[k], 4, Q, c.lambda, true, &C.fin[k], &C.b4[w], lane);
+        }
     } else {
-        int cur = 0;
-        bidx = -1;
-        for (int m = 0; m < 4; ++m) {
-            if (!nn_mode_ok(m, n, ht, hl)) continue;
-            const int t = bidx == 0 ? 1 : 0;
-            if (tid == 0) cs_reset(&S->bsink[t]);
-            for (int p = tid; p < n * n; p += INT) S->bigpred[p] = (uint8_t)nn_px(S->nn[m], S->nb_top, S->nb_left, p % n, p / n);
-            __syncthreads();
-            int bits = kBitsMode;
-            long long D = code_residual_t<INT>(&S->src[ty * 64 + tx], 64, S->bigpred, n, n, S->q, c.qp, c.lambda, false,
-                                               S->bigrec[t], n, &S->bsink[t], &bits, &S->rs, c.err);
-            double J = rd_cost((double)D, c.lambda, bits);
-            if (best < 0.0 || J < best) { best = J; bmode = m; bidx = t; }
-            cur = t;
-        }
-        (void)cur;
-        for (int p = tid; p < n * n; p += INT) TL(S, ty + p / n, tx + p % n) = S->bigrec[bidx][p];
-        *best_sink = &S->bsink[bidx];
+        for (int k = w; k < run; k += 4)
+            warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.junk[w], 4, Q, c.lambda, false, &C.trial[k], &C.b4[w], lane);
     }
-    __syncthreads();
-    *mode_out = bmode;
-    return best;
+    cbar();
+    if (t == 0) {
+        double best = -1.0;
+        int bc = 0;
+        for (int k = 0; k < run; ++k) {
+            const double J = rd_cost((double)C.trial[k].ssd, c.lambda, kBitsMode + C.trial[k].bits);
+            if (best < 0.0 || J < best) { best = J; bc = k; }
+        }
+        C.best_c = bc;
+    }
+    cbar();
+    if (run <= 2) {
+        fsel = C.best_c;
+    } else {
+        if (w == 0) warp_block4(sblk, 64, C.cp[C.cm[C.best_c]], 4, C.frec[0], 4, Q, c.lambda, true, &C.fin[0], &C.b4[0], lane);
+        cbar();
+        fsel = 0;
+    }
+    const Blk4 &F = C.fin[fsel];
+    if (t < 16) TL(C, ty + (t >> 2), tx + (t & 3)) = C.frec[fsel][t];
+    if (t == 0) {
+        const int mode = C.cm[C.best_c];
+        cs_put1(&tgt->c, CS_N, (uint8_t)F.count, c.err);
+        cs_put(&tgt->c, CS_L, F.bytes, F.nbytes, c.err);
+        const int lcx = tx >> 2, lcy = ty >> 2;
+        const int Lm = bx > 0 ? MM(C, lcy, lcx - 1) : 0;
+        const int Am = by > 0 ? MM(C, lcy - 1, lcx) : 0;
+        isink_put(tgt, Lm == Am ? IS_MODE0 : IS_MODE1, (uint8_t)mode, c.err);
+        MM(C, lcy, lcx) = (uint8_t)mode;
+        C.retJ = rd_cost((double)F.ssd, c.lambda, kBitsMode + F.bits);
+        if (c.prof) atomicAdd(&c.prof[IP_NLEAF4], 1ull);
+    }
+    cbar();
+    prof_add(c.prof, t, IP_LEAF4, t0);
+    return C.retJ;
 }
 
-__device__ __forceinline__ int nn_to_4x4(int m) { return m == 1 ? 1 : (m == 2 ? 2 : 0); }
+// ------------------------------------------------------ chain: nodes --
+// Post the leaf trial of the node of side n = 64 >> L at (bx, by) to its team.
+__device__ void post_leaf_job(CCtx &c, int L, int bx, int by, int n) {
+    ChainArea &C = c.S->C;
+    const int t = threadIdx.x, tx = bx - c.bx0, ty = by - c.by0;
+    const int ht = by > 0, hl = bx > 0;
+    HJob *J = cg::this_cluster().map_shared_rank(&c.S->H.job, level_rank(L));
+    if (t < n) J->top[t] = ht ? TL(C, ty - 1, tx + t) : 0;
+    if (t >= 64 && t - 64 < n) J->left[t - 64] = hl ? TL(C, ty + t - 64, tx - 1) : 0;
+    if (t == 1) {
+        J->bx = bx; J->by = by; J->ht = ht; J->hl = hl;
+        J->tl = (ht && hl) ? TL(C, ty - 1, tx - 1) : 128;
+        J->kind = 0;
+    }
+    fence_cluster();
+    cbar();
+    if (t == 0) st_release_cluster(&J->seq, ++C.issued[L]);
+}
+// Tell every team that the CTU row is over.
+__device__ void post_row_end(IShared *S) {
+    ChainArea &C = S->C;
+    if (threadIdx.x == 0) {
+        for (int L = 0; L < 4; ++L) {
+            HJob *J = cg::this_cluster().map_shared_rank(&S->H.job, level_rank(L));
+            J->kind = 1;
+            st_release_cluster(&J->seq, ++C.issued[L]);
+        }
+    }
+}
 
-template <int D> struct INode {
-    static __device__ double run(ICtx &c, int bx, int by, ISink *tgt);
+template <int D> struct CNode {
+    static __device__ double run(CCtx &c, int bx, int by, ISink *tgt);
 };
-
-template <> struct INode<4> {
-    static __device__ double run(ICtx &c, int bx, int by, ISink *tgt) { return leaf4(c, bx, by, tgt); }
+template <> struct CNode<4> {
+    static __device__ double run(CCtx &c, int bx, int by, ISink *tgt) {
+        if (c.S->C.abort) return 0.0;
+        return leaf4(c, bx, by, tgt);
+    }
 };
 
 template <int D>
-__device__ double INode<D>::run(ICtx &c, int bx, int by, ISink *tgt) {
+__device__ double CNode<D>::run(CCtx &c, int bx, int by, ISink *tgt) {
     constexpr int n = 64 >> D, hn = n / 2;
     IShared *S = c.S;
-    const int tid = threadIdx.x;
-    if (bx + n > c.w || by + n > c.h) {
+    ChainArea &C = S->C;
+    const int t = threadIdx.x;
+    if (C.abort) return 0.0;
+    if (bx + n > c.w || by + n > c.h) {            // implicit split, no flag
         double J = 0.0;
         for (int k = 0; k < 4; ++k) {
-            int cx = bx + (k & 1) * hn, cy = by + (k >> 1) * hn;
+            const int cx = bx + (k & 1) * hn, cy = by + (k >> 1) * hn;
             if (cx >= c.w || cy >= c.h) continue;
-            J = __dadd_rn(J, INode<D + 1>::run(c, cx, cy, tgt));
+            J = __dadd_rn(J, CNode<D + 1>::run(c, cx, cy, tgt));
         }
         return J;
     }
-    ISink *ss = &S->ss[D];
-    if (tid == 0) isink_reset(ss);
-    __syncthreads();
-    double Jsplit = 0.0;
-    for (int k = 0; k < 4; ++k)
-        Jsplit = __dadd_rn(Jsplit, INode<D + 1>::run(c, bx + (k & 1) * hn, by + (k >> 1) * hn, ss));
-    // stash the split trial's reconstruction and mode map
-    constexpr int rs_off = D == 0 ? 0 : (D == 1 ? 4096 : (D == 2 ? 5120 : 5376));
-    constexpr int ms_off = D == 0 ? 0 : (D == 1 ? 256 : (D == 2 ? 320 : 336));
-    constexpr int cells = n / 4;
-    const int tx = bx - c.bx0, ty = by - c.by0;
-    for (int p = tid; p < n * n; p += INT) S->stash_rec[rs_off + p] = TL(S, ty + p / n, tx + p % n);
-    for (int p = tid; p < cells * cells; p += INT) S->stash_mm[ms_off + p] = MM(S, (ty >> 2) + p / cells, (tx >> 2) + p % cells);
-    __syncthreads();
-    int mode = 0;
-    CoefSink *lbest = nullptr;
-    double Jleaf = leafn<n>(c, bx, by, &mode, &lbest);
-    const bool split = Jsplit < Jleaf;
-    if (tid == 0) isink_put(tgt, IS_SPLIT0 + D, (uint8_t)split, c.err);
+    post_leaf_job(c, D, bx, by, n);
+    ISink *ss = &C.ss[D];
+    if (t == 0) isink_reset(ss);
+    cbar();
+    double Js = 0.0;
+    for (int k = 0; k < 4; ++k) Js = __dadd_rn(Js, CNode<D + 1>::run(c, bx + (k & 1) * hn, by + (k >> 1) * hn, ss));
+    // the leaf trial's result
+    const long long tw = prof_t0(c.prof, t);
+    if (t == 0 && !C.abort && !wait_cluster_flag(&C.done[D], C.issued[D], c.err, c.hlimit)) C.abort = 1;
+    cbar();
+    fence_cluster();
+    prof_add(c.prof, t, IP_HWAIT, tw);
+    if (C.abort) return 0.0;
+    const int rank = level_rank(D);
+    const HelperArea *RH = cg::this_cluster().map_shared_rank(&S->H, rank);
+    const double Jl = RH->best_J;
+    const int bi = RH->best_idx, mode = RH->best_mode;
+    const bool split = Js < Jl;
+    if (t == 0) isink_put(tgt, IS_SPLIT0 + D, (uint8_t)split, c.err);
     if (split) {
-        for (int p = tid; p < n * n; p += INT) TL(S, ty + p / n, tx + p % n) = S->stash_rec[rs_off + p];
-        for (int p = tid; p < cells * cells; p += INT) MM(S, (ty >> 2) + p / cells, (tx >> 2) + p % cells) = S->stash_mm[ms_off + p];
-        __syncthreads();
-        isink_append(tgt, ss, c.err);
-        return Jsplit;
+        chain_isink_append(tgt, ss, c.err);
+        return Js;
     }
-    if (tid == 0) isink_put(tgt, IS_MODEB, (uint8_t)mode, c.err);
-    for (int p = tid; p < cells * cells; p += INT) MM(S, (ty >> 2) + p / cells, (tx >> 2) + p % cells) = (uint8_t)nn_to_4x4(mode);
-    __syncthreads();
-    csink_append(&tgt->c, lbest, c.err);
-    return Jleaf;
+    if (t == 0) isink_put(tgt, IS_MODEB, (uint8_t)mode, c.err);
+    const int tx = bx - c.bx0, ty = by - c.by0;
+    const uint32_t *rw = reinterpret_cast<const uint32_t *>(RH->rec[bi]);
+    for (int p = t; p < n * n / 4; p += kChainNT) {
+        const uint32_t v = rw[p];
+        const int y = (p * 4) / n, x = (p * 4) % n;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) TL(C, ty + y, tx + x + q) = (uint8_t)(v >> (8 * q));
+    }
+    constexpr int cells = n / 4;
+    const int m4 = mode == 1 ? 1 : (mode == 2 ? 2 : 0);   // nn_to_4x4_mode
+    for (int p = t; p < cells * cells; p += kChainNT) MM(C, (ty >> 2) + p / cells, (tx >> 2) + p % cells) = (uint8_t)m4;
+    chain_append_leaf(&tgt->c, S, rank, bi, c.err);
+    return Jl;
 }
 
-__global__ void __launch_bounds__(INT, 1)
+// The chain's walk over one CTU row.
+__device__ void chain_row(IShared *S, const IPlaneDev &P, int r, unsigned *err, unsigned long long wait_ns,
+                          unsigned long long hlimit) {
+    ChainArea &C = S->C;
+    const int t = threadIdx.x;
+    CCtx c;
+    c.S = S; c.P = &P; c.w = P.w; c.h = P.h; c.qp = P.qp; c.lambda = P.lambda; c.err = err; c.prof = P.prof;
+    c.hlimit = hlimit;
+    const int mmw = P.w / 4, mmh = P.h / 4;
+    if (t == 0) C.abort = 0;
+    for (int col = 0; col < P.cols; ++col) {
+        const long long tw = prof_t0(c.prof, t);
+        if (r > 0) {
+            if (t == 0) C.row_ok = wait_at_least(&P.progress[r - 1], min(col + 2, P.cols), err, wait_ns);
+        } else if (t == 0) C.row_ok = 1;
+        cbar();
+        if (!C.row_ok) break;
+        prof_add(c.prof, t, IP_WAIT, tw);
+        const long long tc = prof_t0(c.prof, t);
+        const int bx0 = col * 64, by0 = r * 64;
+        c.bx0 = bx0; c.by0 = by0;
+        // the source block, the reconstruction above / left and their modes
+        for (int p = t; p < 64 * 16; p += kChainNT) {
+            const int y = by0 + p / 16, x = bx0 + (p % 16) * 4;
+            uint32_t v = 0;
+            if (y < P.h) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) if (x + q < P.w) v |= (uint32_t)P.src[(size_t)y * P.w + x + q] << (8 * q);
+            }
+            reinterpret_cast<uint32_t *>(C.src)[p] = v;
+        }
+        for (int p = t; p < kTileW; p += kChainNT) {
+            const int x = bx0 - 1 + p, y = by0 - 1;
+            C.tile[p] = (y >= 0 && x >= 0 && x < P.w) ? __ldcg(&P.rec[(size_t)y * P.w + x]) : 0;
+        }
+        if (t < 64) {
+            const int x = bx0 - 1, y = by0 + t;
+            TL(C, t, -1) = (x >= 0 && y < P.h) ? __ldcg(&P.rec[(size_t)y * P.w + x]) : 0;
+        } else if (t < 64 + 17) {
+            const int p = t - 64, cx = bx0 / 4 - 1 + p, cy = by0 / 4 - 1;
+            C.mm[p] = (cy >= 0 && cx >= 0 && cx < mmw) ? __ldcg(&P.mmap[(size_t)cy * mmw + cx]) : 0;
+        } else if (t < 64 + 17 + 16) {
+            const int p = t - 81, cx = bx0 / 4 - 1, cy = by0 / 4 + p;
+            MM(C, p, -1) = (cx >= 0 && cy < mmh) ? __ldcg(&P.mmap[(size_t)cy * mmw + cx]) : 0;
+        }
+        uint8_t *slot = P.slots + (size_t)(r * P.cols + col) * kISlotBytes;
+        if (t == 0) {
+            ISink *o = &C.out;
+            for (int k = 0; k < IS_NS; ++k) { o->slen[k] = 0; o->scap[k] = c_IStreamCap[k]; o->sbuf[k] = slot + 32 + c_IStreamOff[k]; }
+            int cc[CS_NUM] = {c_IStreamCap[7], c_IStreamCap[8], c_IStreamCap[9], c_IStreamCap[10], c_IStreamCap[11], 0, 0};
+            cs_init(&o->c, slot + 32 + c_IStreamOff[7], cc);
+        }
+        cbar();
+        CNode<0>::run(c, bx0, by0, &C.out);
+        if (C.abort) break;
+        // write back the reconstruction, the mode map and the slot lengths
+        for (int p = t; p < 64 * 64; p += kChainNT) {
+            const int y = by0 + p / 64, x = bx0 + p % 64;
+            if (y < P.h && x < P.w) P.rec[(size_t)y * P.w + x] = TL(C, p / 64, p % 64);
+        }
+        for (int p = t; p < 256; p += kChainNT) {
+            const int cy = by0 / 4 + p / 16, cx = bx0 / 4 + p % 16;
+            if (cy < mmh && cx < mmw) P.mmap[(size_t)cy * mmw + cx] = MM(C, p / 16, p % 16);
+        }
+        if (t < 12) {
+            const int len = t < IS_NS ? C.out.slen[t] : C.out.c.len[t - IS_NS];
+            reinterpret_cast<uint16_t *>(slot)[t] = (uint16_t)len;
+        }
+        __threadfence();
+        cbar();
+        if (t == 0) atomicExch(&P.progress[r], col + 1);
+        prof_add(c.prof, t, IP_CTU, tc);
+        if (c.prof && t == 0) atomicAdd(&c.prof[IP_NCTU], 1ull);
+    }
+    post_row_end(S);
+}
+
+// ------------------------------------------------------- leaf teams --
+// A team codes the leaf trials of one node size until the chain ends the row:
+// every allowed mode (fdv_intra_nn_mode_ok) of the n x n leaf at once through
+// team_residuals, then the reference's choice among them (the first strictly
+// cheaper, fdv.h:4467-4471).  `seen` counts the jobs this team has taken.
+template <int NT, int BAR>
+__device__ void team_loop(IShared *S, const IPlaneDev &P, int L, unsigned *err, unsigned long long hlimit, int tt,
+                          int &seen) {
+    HelperArea &H = S->H;
+    const int n = 64 >> L;
+    cg::cluster_group cl = cg::this_cluster();
+    int *done = cl.map_shared_rank(&S->C.done[L], 0);
+    unsigned long long *prof = P.prof;
+    for (;;) {
+        if (tt == 0) H.ok = wait_cluster_flag(&H.job.seq, seen + 1, err, hlimit);
+        team_bar(BAR, NT);
+        fence_cluster();
+        if (!H.ok) break;
+        ++seen;
+        if (H.job.kind != 0) break;
+        const long long t0 = prof_t0(prof, tt);
+        const int bx = H.job.bx, by = H.job.by, ht = H.job.ht, hl = H.job.hl, tl = H.job.tl;
+        for (int p = tt; p < n * n; p += NT) {
+            const int y = p / n, x = p % n;
+            H.src[y * 64 + x] = P.src[(size_t)(by + y) * P.w + bx + x];
+        }
+        if (tt < 4) {
+            H.nn[tt] = nn_setup(tt, H.job.top, H.job.left, tl, n, ht, hl);
+            cs_reset(&H.sink[tt]);
+        }
+        if (tt == 0) {
+            int nm = 0;
+            for (int m = 0; m < 4; ++m) if (nn_mode_ok(m, n, ht, hl)) H.ml[nm++] = m;
+            H.nm = nm;
+        }
+        team_bar(BAR, NT);
+        const int M = H.nm, nn2 = n * n;
+        for (int p = tt; p < M * nn2; p += NT) {
+            const int i = p / nn2, q = p - i * nn2;
+            H.pred[i][q] = (uint8_t)nn_px(H.nn[H.ml[i]], H.job.top, H.job.left, q % n, q / n);
+        }
+        team_bar(BAR, NT);
+        uint8_t *pr[4] = {H.pred[0], H.pred[1], H.pred[2], H.pred[3]};
+        uint8_t *rc[4] = {H.rec[0], H.rec[1], H.rec[2], H.rec[3]};
+        CoefSink *sk[4] = {&H.sink[0], &H.sink[1], &H.sink[2], &H.sink[3]};
+        team_residuals<NT>(H.src, 64, pr, rc, sk, M, n, S->q, P.qp, P.lambda, H.e, H.b, &H.ts, err, tt, BAR);
+        if (tt == 0) {
+            double best = -1.0;
+            int bi = 0;
+            for (int i = 0; i < M; ++i) {
+                const double J = rd_cost((double)H.e[i], P.lambda, kBitsMode + H.b[i]);
+                if (best < 0.0 || J < best) { best = J; bi = i; }
+            }
+            H.best_J = best;
+            H.best_idx = bi;
+            H.best_mode = H.ml[bi];
+        }
+        fence_cluster();
+        team_bar(BAR, NT);
+        if (tt == 0) st_release_cluster(done, seen);
+        prof_add(prof, tt, IP_LEAF64 - L, t0);
+    }
+}
+
+__global__ void __cluster_dims__(ICL, 1, 1) __launch_bounds__(INT, 1)
 iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ tasks, int ntasks,
               int *ticket, unsigned *err, unsigned long long wait_ns) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     IShared *S = reinterpret_cast<IShared *>(smem_raw);
-    const int tid = threadIdx.x;
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x, rank = (int)cl.block_rank();
+    // team waits may span a whole CTU row, including the chain's own waits
+    const unsigned long long hlimit = 2 * wait_ns + 1000000000ull;
     if (tid == 0) {
-        uint8_t *m = S->ssmem;
+        ChainArea &C = S->C;
+        uint8_t *m = C.ssmem;
         for (int d = 0; d < 4; ++d) {
-            ISink *s = &S->ss[d];
+            ISink *s = &C.ss[d];
             for (int k = 0; k < IS_NS; ++k) { s->slen[k] = 0; s->scap[k] = isink_scap(d, k); s->sbuf[k] = m; m += s->scap[k]; }
             int cc[CS_NUM];
             for (int k = 0; k < CS_NUM; ++k) cc[k] = isink_ccap(d, k);
             cs_init(&s->c, m, cc);
             for (int k = 0; k < CS_NUM; ++k) m += cc[k];
         }
-        int c2[CS_NUM], c0[CS_NUM];
-        for (int k = 0; k < CS_NUM; ++k) { c2[k] = isink_ccap(2, k); c0[k] = isink_ccap(0, k); }
-        for (int i = 0; i < 4; ++i) cs_init(&S->lsink[i], S->lsmem[i], c2);
-        for (int i = 0; i < 2; ++i) cs_init(&S->bsink[i], S->bsmem[i], c0);
+        int c0[CS_NUM];
+        for (int k = 0; k < CS_NUM; ++k) c0[k] = isink_ccap(0, k);
+        for (int i = 0; i < 4; ++i) cs_init(&S->H.sink[i], S->H.sinkmem[i], c0);
+        for (int L = 0; L < 4; ++L) { C.done[L] = 0; C.issued[L] = 0; }
+        S->H.job.seq = 0;
     }
-    __syncthreads();
+    int seen = 0;
+    cl.sync();
     for (;;) {
-        if (tid == 0) S->task = atomicAdd(ticket, 1);
-        __syncthreads();
-        const int t = S->task;
-        __syncthreads();
-        if (t >= ntasks) return;
+        if (rank == 0 && tid == 0) S->C.task = atomicAdd(ticket, 1);
+        cl.sync();
+        const int t = *cl.map_shared_rank(&S->C.task, 0);
+        cl.sync();
+        if (t >= ntasks) break;
         const IPlaneDev &P = planes[tasks[t].plane];
-        const int r = tasks[t].row;
-        ICtx c;
-        c.S = S; c.P = &P; c.w = P.w; c.h = P.h; c.qp = P.qp; c.lambda = P.lambda; c.err = err;
         qp4_setup(&S->q, P.qp, tid);
-        const int mmw = P.w / 4, mmh = P.h / 4;
-        for (int col = 0; col < P.cols; ++col) {
-            if (r > 0) {
-                if (tid == 0) S->row_ok = wait_at_least(&P.progress[r - 1], min(col + 2, P.cols), err, wait_ns);
-            } else if (tid == 0) S->row_ok = 1;
-            __syncthreads();
-            if (!S->row_ok) break;
-            const int bx0 = col * 64, by0 = r * 64;
-            c.bx0 = bx0; c.by0 = by0;
-            // load the source block, the reconstruction above / left and their modes
-            for (int p = tid; p < 64 * 64; p += INT) {
-                int y = by0 + p / 64, x = bx0 + p % 64;
-                S->src[p] = (y < P.h && x < P.w) ? P.src[(size_t)y * P.w + x] : 0;
-            }
-            for (int p = tid; p < kTileW; p += INT) {
-                int x = bx0 - 1 + p, y = by0 - 1;
-                S->tile[p] = (y >= 0 && x >= 0 && x < P.w) ? __ldcg(&P.rec[(size_t)y * P.w + x]) : 0;
-            }
-            for (int p = tid; p < 64; p += INT) {
-                int x = bx0 - 1, y = by0 + p;
-                TL(S, p, -1) = (x >= 0 && y < P.h) ? __ldcg(&P.rec[(size_t)y * P.w + x]) : 0;
-            }
-            for (int p = tid; p < 17; p += INT) {
-                int cx = bx0 / 4 - 1 + p, cy = by0 / 4 - 1;
-                S->mm[p] = (cy >= 0 && cx >= 0 && cx < mmw) ? __ldcg(&P.mmap[(size_t)cy * mmw + cx]) : 0;
-            }
-            for (int p = tid; p < 16; p += INT) {
-                int cx = bx0 / 4 - 1, cy = by0 / 4 + p;
-                MM(S, p, -1) = (cx >= 0 && cy < mmh) ? __ldcg(&P.mmap[(size_t)cy * mmw + cx]) : 0;
-            }
-            uint8_t *slot = P.slots + (size_t)(r * P.cols + col) * kISlotBytes;
-            if (tid == 0) {
-                ISink *o = &S->out;
-                for (int k = 0; k < IS_NS; ++k) { o->slen[k] = 0; o->scap[k] = c_IStreamCap[k]; o->sbuf[k] = slot + 32 + c_IStreamOff[k]; }
-                int cc[CS_NUM] = {c_IStreamCap[7], c_IStreamCap[8], c_IStreamCap[9], c_IStreamCap[10], c_IStreamCap[11], 0, 0};
-                cs_init(&o->c, slot + 32 + c_IStreamOff[7], cc);
-            }
-            __syncthreads();
-            INode<0>::run(c, bx0, by0, &S->out);
-            // write back the reconstruction, the mode map and the slot lengths
-            for (int p = tid; p < 64 * 64; p += INT) {
-                int y = by0 + p / 64, x = bx0 + p % 64;
-                if (y < P.h && x < P.w) P.rec[(size_t)y * P.w + x] = TL(S, p / 64, p % 64);
-            }
-            for (int p = tid; p < 256; p += INT) {
-                int cy = by0 / 4 + p / 16, cx = bx0 / 4 + p % 16;
-                if (cy < mmh && cx < mmw) P.mmap[(size_t)cy * mmw + cx] = MM(S, p / 16, p % 16);
-            }
-            if (tid < 12) {
-                int len = tid < IS_NS ? S->out.slen[tid] : S->out.c.len[tid - IS_NS];
-                reinterpret_cast<uint16_t *>(slot)[tid] = (uint16_t)len;
-            }
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) atomicExch(&P.progress[r], col + 1);
-        }
         __syncthreads();
+        if (rank == 0) {
+            if (tid < kChainNT) chain_row(S, P, tasks[t].row, err, wait_ns, hlimit);
+            else team_loop<kH8NT, BAR_H8>(S, P, 3, err, hlimit, tid - kChainNT, seen);
+        } else {
+            team_loop<INT, BAR_TEAM>(S, P, 3 - rank, err, hlimit, tid, seen);
+        }
     }
 }
 

@@ -59,9 +59,9 @@ __device__ __forceinline__ int nn_px(const NNPred &P, const uint8_t *top, const 
     }
 }
 
-// 4x4 directional prediction of pixel (x, y); T(-1) = L(-1) = corner.
-__device__ int pred4_px(int mode, const int *Tn, const int *Ln, const uint8_t *top, const uint8_t *left,
-                        int ht, int hl, int x, int y) {
+// 4x4 directional prediction of pixel (x, y) from Tn = T(-1..7) and
+// Ln = L(-1..3), T(-1) = L(-1) = the corner.
+__device__ int pred4_px(int mode, const int *Tn, const int *Ln, int ht, int hl, int x, int y) {
 #define T(i) Tn[(i) + 1]
 #define L(i) Ln[(i) + 1]
     switch (mode) {
@@ -98,9 +98,9 @@ __device__ int pred4_px(int mode, const int *Tn, const int *Ln, const uint8_t *t
     }
     default: {
         int s = 0;
-        if (ht && hl) { for (int k = 0; k < 4; ++k) s += top[k] + left[k]; return (s + 4) >> 3; }
-        if (ht) { for (int k = 0; k < 4; ++k) s += top[k]; return (s + 2) >> 2; }
-        if (hl) { for (int k = 0; k < 4; ++k) s += left[k]; return (s + 2) >> 2; }
+        if (ht && hl) { for (int k = 0; k < 4; ++k) s += T(k) + L(k); return (s + 4) >> 3; }
+        if (ht) { for (int k = 0; k < 4; ++k) s += T(k); return (s + 2) >> 2; }
+        if (hl) { for (int k = 0; k < 4; ++k) s += L(k); return (s + 2) >> 2; }
         return 128;
     }
     }

@@ -24,8 +24,10 @@ void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticke
         cudaFuncSetAttribute(iframe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    iframe_kernel<<<grid, INT, smem, st>>>(static_cast<const IPlaneDev *>(planes), static_cast<const ITask *>(tasks),
-                                           ntasks, ticket, err, wait_ns);
+    // clusters of ICL blocks, one CTU row each at a time; `grid` is the SM count
+    const int ncl = std::max(1, std::min(ntasks, grid / ICL));
+    iframe_kernel<<<ncl * ICL, INT, smem, st>>>(static_cast<const IPlaneDev *>(planes), static_cast<const ITask *>(tasks),
+                                                ntasks, ticket, err, wait_ns);
 }
 
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,

@@ -271,6 +271,106 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     bar_sync64(bar);
 }
 
+// One warp codes one 8x8 region with the 8x8 transform: the same arithmetic
+// as region8 (int32 forward DCT, quantiser step QSTEP8[qp] with f = q / 3,
+// dequantisation saturated to int32, int64 inverse with >> 36), lane l owning
+// positions l and l + 32.  No barrier beyond the warp, so any number of warps
+// of a block can run it concurrently.
+struct Reg8WScratch {
+    int32_t X[64];            // residual, later the dequantised coefficients
+    int32_t A[64];
+    int16_t L[64];
+    long long B[64];
+};
+__device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps, int qp,
+                             Reg8 *out, Reg8WScratch *sc, int lane) {
+    const int c = lane & 7, r0 = lane >> 3, r1 = r0 + 4;
+    const int cv0 = cur[r0 * cs + c], pv0 = pred[r0 * ps + c];
+    const int cv1 = cur[r1 * cs + c], pv1 = pred[r1 * ps + c];
+    sc->X[lane] = cv0 - pv0;
+    sc->X[lane + 32] = cv1 - pv1;
+    __syncwarp();
+    {   // A[u][x] = sum_y C8[u][y] X[y][x]   (u = r0, r1; x = c)
+        int32_t a0 = 0, a1 = 0;
+#pragma unroll
+        for (int y = 0; y < 8; ++y) {
+            const int32_t xv = sc->X[y * 8 + c];
+            a0 += c_C8[r0 * 8 + y] * xv;
+            a1 += c_C8[r1 * 8 + y] * xv;
+        }
+        sc->A[lane] = a0;
+        sc->A[lane + 32] = a1;
+    }
+    __syncwarp();
+    {   // Y[u][v] = sum_x A[u][x] C8[v][x]   (u = r0, r1; v = c), quantise, dequantise
+        int32_t y0 = 0, y1 = 0;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            const int32_t cx = c_C8[c * 8 + x];
+            y0 += sc->A[r0 * 8 + x] * cx;
+            y1 += sc->A[r1 * 8 + x] * cx;
+        }
+        const int32_t q = c_QSTEP8[qp], f = q / 3;
+        const int l0 = (int16_t)((y0 < 0 ? -1 : 1) * (((y0 < 0 ? -y0 : y0) + f) / q));
+        const int l1 = (int16_t)((y1 < 0 ? -1 : 1) * (((y1 < 0 ? -y1 : y1) + f) / q));
+        sc->L[lane] = (int16_t)l0;
+        sc->L[lane + 32] = (int16_t)l1;
+        const long long d0 = (long long)l0 * q, d1 = (long long)l1 * q;
+        sc->X[lane] = d0 < INT32_MIN ? INT32_MIN : (d0 > INT32_MAX ? INT32_MAX : (int32_t)d0);
+        sc->X[lane + 32] = d1 < INT32_MIN ? INT32_MIN : (d1 > INT32_MAX ? INT32_MAX : (int32_t)d1);
+    }
+    __syncwarp();
+    {   // B[y][v] = sum_u C8[u][y] Yd[u][v]   (y = r0, r1; v = c)
+        long long b0 = 0, b1 = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long yd = sc->X[u * 8 + c];
+            b0 += (long long)c_C8[u * 8 + r0] * yd;
+            b1 += (long long)c_C8[u * 8 + r1] * yd;
+        }
+        sc->B[lane] = b0;
+        sc->B[lane + 32] = b1;
+    }
+    __syncwarp();
+    int rv0, rv1;
+    {   // X[y][x] = (sum_v B[y][v] C8[v][x] + 2^35) >> 36   (y = r0, r1; x = c)
+        long long s0 = 0, s1 = 0;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            const long long cc = c_C8[v * 8 + c];
+            s0 += sc->B[r0 * 8 + v] * cc;
+            s1 += sc->B[r1 * 8 + v] * cc;
+        }
+        rv0 = clipb(pv0 + (int16_t)((s0 + (1LL << 35)) >> 36));
+        rv1 = clipb(pv1 + (int16_t)((s1 + (1LL << 35)) >> 36));
+    }
+    out->rec[lane] = (uint8_t)rv0;
+    out->rec[lane + 32] = (uint8_t)rv1;
+    const int e0 = cv0 - rv0, e1 = cv1 - rv1;
+    const int ssd = __reduce_add_sync(FDVB_FULL, e0 * e0 + e1 * e1);
+    // zigzag view: lane k holds zigzag positions k and k + 32
+    const int lz0 = sc->L[c_ZZ8[lane]], lz1 = sc->L[c_ZZ8[lane + 32]];
+    const unsigned m0 = __ballot_sync(FDVB_FULL, lz0 != 0), m1 = __ballot_sync(FDVB_FULL, lz1 != 0);
+    const int last = m1 ? 63 - __clz(m1) : (m0 ? 31 - __clz(m0) : -1);
+    const uint32_t z0 = zz_enc(lz0), z1 = zz_enc(lz1);
+    const bool in0 = lane <= last, in1 = lane + 32 <= last;
+    const int bsum = __reduce_add_sync(FDVB_FULL, (in0 ? bits_val(z0) : 0) + (in1 ? bits_val(z1) : 0));
+    const int len0 = in0 ? leb_size(z0) : 0, len1 = in1 ? leb_size(z1) : 0;
+    const int end0 = warp_incl_scan(len0, lane);
+    const int tot0 = __shfl_sync(FDVB_FULL, end0, 31);
+    const int end1 = tot0 + warp_incl_scan(len1, lane);
+    if (in0) leb_write(out->bytes + end0 - len0, z0);
+    if (in1) leb_write(out->bytes + end1 - len1, z1);
+    const int nbytes = __shfl_sync(FDVB_FULL, end1, 31);
+    if (lane == 0) {
+        out->count = last + 1;
+        out->nbytes = nbytes;
+        out->bits = kBitsFlag + bits_val((uint32_t)(last + 1)) + bsum;
+        out->ssd = ssd;
+    }
+    __syncwarp();
+}
+
 // --------------------------------------------------- residual (n x n) --
 // The decision of one 8x8 region between its 4x4 option (A) and its 8x8
 // option (B), with the region's byte counts in each stream.
@@ -296,6 +396,72 @@ struct ResidScratchT {
     int b;
 };
 
+// The RD choice of one 8x8 region between its four 4x4 blocks (A) and its 8x8
+// transform (B), with the empty-region flag value 0 (fdv.h:5379-5411).
+__device__ __forceinline__ void region_choice(const Blk4 *b4, const Reg8 &R, double lambda, RegDec &D) {
+    long long eA = 0;
+    int bA = kBitsFlag, lpA = 0;
+    for (int s = 0; s < 4; ++s) { eA += b4[s].ssd; bA += b4[s].bits; lpA += b4[s].nbytes; }
+    long long eB = R.ssd;
+    int bB = R.bits;
+    const bool emptyA = lpA == 0, emptyB = R.count == 0;
+    if (emptyA) bA = kBitsFlag;
+    if (emptyB) bB = kBitsFlag;
+    if (rd_cost((double)eA, lambda, bA) <= rd_cost((double)eB, lambda, bB)) {
+        D.choice = 0; D.flv = emptyA ? 0 : 1; D.nl = emptyA ? 0 : lpA; D.e = eA; D.b = bA;
+    } else {
+        D.choice = 1; D.flv = emptyB ? 0 : 2; D.nl = emptyB ? 0 : R.nbytes; D.e = eB; D.b = bB;
+    }
+}
+
+// Copy region rg's symbols (flag, counts, level bytes) to the offsets its
+// decision reserved (one warp).
+__device__ __forceinline__ void region_symbols(const RegDec &D, const Blk4 *b4, const Reg8 &R, CoefSink *sink,
+                                               bool chroma, int lane) {
+    if (D.flv < 0) return;
+    if (lane == 0) sink->buf[CS_FL][D.ofl] = (uint8_t)D.flv;
+    if (D.flv == 1) {
+        uint8_t *cnt = sink->buf[chroma ? CS_NC : CS_N] + D.oc;
+        uint8_t *lv = sink->buf[chroma ? CS_LC : CS_L] + D.ol;
+        int o = 0;
+        for (int s2 = 0; s2 < 4; ++s2) {
+            if (lane == 0) cnt[s2] = (uint8_t)b4[s2].count;
+            for (int i = lane; i < b4[s2].nbytes; i += 32) lv[o + i] = b4[s2].bytes[i];
+            o += b4[s2].nbytes;
+        }
+    } else if (D.flv == 2) {
+        if (lane == 0) sink->buf[CS_N8][D.oc] = (uint8_t)R.count;
+        uint8_t *lv = sink->buf[CS_L8] + D.ol;
+        for (int i = lane; i < D.nl; i += 32) lv[i] = R.bytes[i];
+    }
+}
+
+// Reserve the stream offsets of regions dec[0..nreg) in order (one thread);
+// on overflow report it, clamp the lengths and mark the regions unwritten.
+__device__ __forceinline__ void region_offsets(RegDec *dec, int nreg, CoefSink *sink, bool chroma,
+                                               long long *e, int *b, unsigned *err) {
+    const int kc = chroma ? CS_NC : CS_N, kl = chroma ? CS_LC : CS_L;
+    long long es = 0;
+    int bs = 0;
+    for (int rg = 0; rg < nreg; ++rg) {
+        RegDec &D = dec[rg];
+        D.ofl = sink->len[CS_FL]++;
+        if (D.flv == 1) { D.oc = sink->len[kc]; sink->len[kc] += 4; D.ol = sink->len[kl]; sink->len[kl] += D.nl; }
+        else if (D.flv == 2) { D.oc = sink->len[CS_N8]; sink->len[CS_N8] += 1; D.ol = sink->len[CS_L8]; sink->len[CS_L8] += D.nl; }
+        es += D.e;
+        bs += D.b;
+    }
+    bool ovf = false;
+    for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) ovf = true;
+    if (ovf) {
+        atomicOr(err, kErrSlotOverflow);
+        for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) sink->len[k] = sink->cap[k];
+        for (int rg = 0; rg < nreg; ++rg) dec[rg].flv = -1;
+    }
+    *e += es;
+    *b += bs;
+}
+
 // Decide regions [0, nreg) given their A results blk[4*rg..] and B results
 // reg[rg], append their symbols to `sink` in region order, and leave the
 // chunk's distortion and rate in e / b.  Called by all NT threads.
@@ -303,69 +469,16 @@ template <int NT>
 __device__ void decide_regions(int nreg, Blk4 *blk, Reg8 *reg, RegDec *dec, double lambda, bool chroma,
                                CoefSink *sink, long long *e_out, int *b_out, unsigned *err) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid < nreg) {
-        const int rg = tid;
-        long long eA = 0;
-        int bA = kBitsFlag, lpA = 0;
-        for (int s = 0; s < 4; ++s) { eA += blk[rg * 4 + s].ssd; bA += blk[rg * 4 + s].bits; lpA += blk[rg * 4 + s].nbytes; }
-        const Reg8 &R = reg[rg];
-        long long eB = R.ssd;
-        int bB = R.bits;
-        const bool emptyA = lpA == 0, emptyB = R.count == 0;
-        if (emptyA) bA = kBitsFlag;
-        if (emptyB) bB = kBitsFlag;
-        RegDec &D = dec[rg];
-        if (rd_cost((double)eA, lambda, bA) <= rd_cost((double)eB, lambda, bB)) {
-            D.choice = 0; D.flv = emptyA ? 0 : 1; D.nl = emptyA ? 0 : lpA; D.e = eA; D.b = bA;
-        } else {
-            D.choice = 1; D.flv = emptyB ? 0 : 2; D.nl = emptyB ? 0 : R.nbytes; D.e = eB; D.b = bB;
-        }
-    }
+    if (tid < nreg) region_choice(&blk[tid * 4], reg[tid], lambda, dec[tid]);
     __syncthreads();
     if (tid == 0) {
-        const int kc = chroma ? CS_NC : CS_N, kl = chroma ? CS_LC : CS_L;
-        long long e = 0;
-        int b = 0;
-        bool ovf = false;
-        for (int rg = 0; rg < nreg; ++rg) {
-            RegDec &D = dec[rg];
-            D.ofl = sink->len[CS_FL]++;
-            if (D.flv == 1) { D.oc = sink->len[kc]; sink->len[kc] += 4; D.ol = sink->len[kl]; sink->len[kl] += D.nl; }
-            else if (D.flv == 2) { D.oc = sink->len[CS_N8]; sink->len[CS_N8] += 1; D.ol = sink->len[CS_L8]; sink->len[CS_L8] += D.nl; }
-            e += D.e;
-            b += D.b;
-        }
-        for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) ovf = true;
-        if (ovf) {
-            atomicOr(err, kErrSlotOverflow);
-            for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) sink->len[k] = sink->cap[k];
-            for (int rg = 0; rg < nreg; ++rg) dec[rg].flv = -1;   // write nothing
-        }
-        *e_out = e;
-        *b_out = b;
+        *e_out = 0;
+        *b_out = 0;
+        region_offsets(dec, nreg, sink, chroma, e_out, b_out, err);
     }
     __syncthreads();
     // one warp per region copies its flag, counts and level bytes
-    for (int rg = warp; rg < nreg; rg += NT / 32) {
-        const RegDec &D = dec[rg];
-        if (D.flv < 0) continue;
-        if (lane == 0) sink->buf[CS_FL][D.ofl] = (uint8_t)D.flv;
-        if (D.flv == 1) {
-            uint8_t *cnt = sink->buf[chroma ? CS_NC : CS_N] + D.oc;
-            uint8_t *lv = sink->buf[chroma ? CS_LC : CS_L] + D.ol;
-            int o = 0;
-            for (int s2 = 0; s2 < 4; ++s2) {
-                const Blk4 &B4 = blk[rg * 4 + s2];
-                if (lane == 0) cnt[s2] = (uint8_t)B4.count;
-                for (int i = lane; i < B4.nbytes; i += 32) lv[o + i] = B4.bytes[i];
-                o += B4.nbytes;
-            }
-        } else if (D.flv == 2) {
-            if (lane == 0) sink->buf[CS_N8][D.oc] = (uint8_t)reg[rg].count;
-            uint8_t *lv = sink->buf[CS_L8] + D.ol;
-            for (int i = lane; i < D.nl; i += 32) lv[i] = reg[rg].bytes[i];
-        }
-    }
+    for (int rg = warp; rg < nreg; rg += NT / 32) region_symbols(dec[rg], &blk[rg * 4], reg[rg], sink, chroma, lane);
 }
 
 // The whole block (NT threads) codes an n x n residual, n in {8, 16, 32, 64}:
@@ -410,6 +523,80 @@ __device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *
     }
     *bits += btot;
     return etot;
+}
+
+// ---------------------------------------------- team residual coding --
+// A team is NT threads (a multiple of 32) of one block that synchronise on
+// their own named barrier, so several teams of a block run independently.
+__device__ __forceinline__ void team_bar(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Scratch of a team: one chunk of up to TR regions, per-warp coder scratch.
+template <int NW>
+struct TeamResidScratch {
+    static constexpr int TR = 16;
+    Blk4 blk[4 * TR];
+    __align__(16) uint8_t recA[TR][64];
+    Reg8 reg[TR];
+    RegDec dec[TR];
+    Reg8WScratch r8[NW];
+    Blk4Scratch b4[NW];
+};
+
+// M residuals of n x n (n in {8, 16, 32, 64}) coded at once against the same
+// source cur (stride cs): prediction pred[i] (stride n), reconstruction rec[i]
+// (stride n), symbols appended to sink[i], distortion e[i] and rate b[i]
+// (region flags and coefficients; the caller charges the mode symbol).  Each
+// residual follows code_residual (fdv.h:5300-5414): 8x8 regions in raster
+// order, each the RD choice between four RDOQ'd 4x4 blocks and one 8x8
+// transform.  Work goes out in chunks of TR regions, five warp tasks per
+// region (four 4x4 blocks, the 8x8 option); TR is a multiple of (n/8)^2 or
+// divides it, so a chunk never splits one residual's regions unevenly.
+// Called by all NT threads of the team (tt = 0..NT-1) with barrier `bar`.
+template <int NT, int NWS>
+__device__ void team_residuals(const uint8_t *cur, int cs, uint8_t *const *pred, uint8_t *const *rec,
+                               CoefSink *const *sink, int M, int n, const QP4 &Q, int qp, double lambda,
+                               long long *e, int *b, TeamResidScratch<NWS> *sc, unsigned *err, int tt,
+                               int bar) {
+    constexpr int NW = NT / 32, TR = TeamResidScratch<NWS>::TR;
+    static_assert(NW <= NWS, "scratch for every warp of the team");
+    const int wt = tt >> 5, lane = tt & 31;
+    const int rpl = n / 8, rpm = rpl * rpl, total = M * rpm;
+    if (tt < M) { e[tt] = 0; b[tt] = 0; }
+    for (int g0 = 0; g0 < total; g0 += TR) {
+        const int R = min(TR, total - g0);
+        for (int k = wt; k < 5 * R; k += NW) {
+            const int i = k / 5, sub = k - 5 * i, g = g0 + i, m = g / rpm, rg = g - m * rpm;
+            const int rx = (rg % rpl) * 8, ry = (rg / rpl) * 8;
+            const uint8_t *cb = cur + ry * cs + rx, *pb = pred[m] + ry * n + rx;
+            if (sub < 4) {
+                const int sx = (sub & 1) * 4, sy = (sub >> 1) * 4;
+                warp_block4(cb + sy * cs + sx, cs, pb + sy * n + sx, n, &sc->recA[i][sy * 8 + sx], 8, Q, lambda, true,
+                            &sc->blk[4 * i + sub], &sc->b4[wt], lane);
+            } else {
+                warp_region8(cb, cs, pb, n, qp, &sc->reg[i], &sc->r8[wt], lane);
+            }
+        }
+        team_bar(bar, NT);
+        if (tt < R) region_choice(&sc->blk[4 * tt], sc->reg[tt], lambda, sc->dec[tt]);
+        team_bar(bar, NT);
+        const int seg = min(rpm, R), nseg = R / seg;
+        if (tt < nseg) {
+            const int m = (g0 + tt * seg) / rpm;
+            region_offsets(&sc->dec[tt * seg], seg, sink[m], false, &e[m], &b[m], err);
+        }
+        team_bar(bar, NT);
+        for (int i = wt; i < R; i += NW) {
+            const int g = g0 + i, m = g / rpm, rg = g - m * rpm;
+            const int rx = (rg % rpl) * 8, ry = (rg / rpl) * 8;
+            const RegDec &D = sc->dec[i];
+            region_symbols(D, &sc->blk[4 * i], sc->reg[i], sink[m], false, lane);
+            for (int q = lane; q < 64; q += 32)
+                rec[m][(ry + (q >> 3)) * n + rx + (q & 7)] = D.choice ? sc->reg[i].rec[q] : sc->recA[i][q];
+        }
+        team_bar(bar, NT);
+    }
 }
 
 }  // namespace fdvb

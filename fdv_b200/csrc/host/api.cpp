@@ -407,7 +407,7 @@ void fdvg_stats(const fdvg_ctx *g, double *step_ms, double *analysis_p_ms, long 
 void fdvg_stats_reset(fdvg_ctx *g) { fdvb_engine_stats_reset(g); }
 void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns) { fdvb_engine_set_wait_ns(g, ns); }
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row) { fdvb_engine_inject_stall(g, u, row); }
-int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out16) { return fdvb_engine_profile(g, enable, out16); }
+int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out32) { return fdvb_engine_profile(g, enable, out32); }
 
 // ---------------------------------------------------- entropy tail ABI --
 fdvb_tabcache *fdvb_tabcache_new(void) { return new fdvb_tabcache(); }

@@ -23,5 +23,5 @@ void fdvb_engine_stats(const fdvb_engine *E, double *step_ms, double *pk_ms, lon
 void fdvb_engine_stats_reset(fdvb_engine *E);
 void fdvb_engine_set_wait_ns(fdvb_engine *E, unsigned long long ns);
 void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row);
-int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out16);
+int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out32);
 }

@@ -129,12 +129,14 @@ void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns);
  * a progress flag nothing sets; the waits expire and fdvg_frame returns an
  * error, leaving the engine usable. */
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row);
-/* Per-phase cycle profile of the P-frame analysis kernel, for tuning:
- * enable != 0 turns it on (thread 0 of every block adds clock64 deltas:
- * wait, load, SKIP, searches, residuals, region decisions, commit, output,
- * then the macroblock count and the SKIP early-out count); out16 (may be NULL)
- * receives and clears the 16 accumulators. */
-int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out16);
+/* Per-phase cycle profile of the analysis kernels, for tuning: enable != 0
+ * turns it on (thread 0 of every block adds clock64 deltas).  out32 (may be
+ * NULL) receives and clears 32 accumulators: [0..9] P-frame kernel (wait,
+ * load, SKIP, searches, residuals, region decisions, commit, output,
+ * macroblock count, SKIP early-out count); [16..24] key-frame kernel (wait,
+ * 4x4 leaves, 8x8/16x16/32x32/64x64 leaves, CTU total, CTU count, 4x4 leaf
+ * count). */
+int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out32);
 
 /* Allocation-free P-frame analysis of one unit.  No counterpart in the
  * reference.  For callers that cannot allocate device memory while they
