@@ -18,16 +18,31 @@ __constant__ int c_MF[6][3] = {{13107, 5243, 8066}, {11916, 4660, 7490}, {10082,
                                {9362, 3647, 5825},  {8192, 3355, 5243},  {7282, 2893, 4559}};
 __constant__ int c_DQV[6][3] = {{10, 16, 13}, {11, 18, 14}, {13, 20, 16},
                                 {14, 23, 18}, {16, 25, 20}, {18, 29, 23}};
-__constant__ int c_ZZ4[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
-__constant__ int c_IZZ4[16] = {0, 1, 5, 6, 2, 4, 7, 12, 3, 8, 11, 13, 9, 10, 14, 15};
-__constant__ int c_ZZ8[64] = {
+// Lookups indexed by lane go through registers or L1, never the constant
+// cache (which serialises different addresses within a warp): the 4x4 scans
+// are nibble-packed immediates, the 8x8 scan and basis live in global memory.
+constexpr int kZZ4[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+constexpr int kIZZ4[16] = {0, 1, 5, 6, 2, 4, 7, 12, 3, 8, 11, 13, 9, 10, 14, 15};
+constexpr unsigned long long nib_pack(const int (&a)[16]) {
+    unsigned long long v = 0;
+    for (int i = 15; i >= 0; --i) v = (v << 4) | (unsigned long long)a[i];
+    return v;
+}
+constexpr unsigned long long kZZ4P = nib_pack(kZZ4), kIZZ4P = nib_pack(kIZZ4);
+__device__ __forceinline__ int zz4(int k) { return (int)((kZZ4P >> (4 * k)) & 15u); }
+__device__ __forceinline__ int izz4(int k) { return (int)((kIZZ4P >> (4 * k)) & 15u); }
+__device__ const uint8_t g_ZZ8[64] = {
      0,  1,  8, 16,  9,  2,  3, 10, 17, 24, 32, 25, 18, 11,  4,  5,
     12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13,  6,  7, 14, 21, 28,
     35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
     58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
-// 8x8 DCT basis and quantiser steps, computed on the host (fdvb_c8_tables).
-__constant__ int32_t c_C8[64];
+// 8x8 DCT basis (and its transpose) and quantiser steps, computed on the
+// host (fdvb_c8_tables).
+__device__ int32_t g_C8[64], g_C8T[64];
 __constant__ int32_t c_QSTEP8[52];
+__device__ __forceinline__ int32_t c8(int i) { return __ldg(&g_C8[i]); }
+__device__ __forceinline__ int32_t c8t(int i) { return __ldg(&g_C8T[i]); }
+__device__ __forceinline__ int zz8(int k) { return __ldg(&g_ZZ8[k]); }
 
 // Cost constants (fdv.h:3350-3355).
 constexpr int kBitsMode = 3, kBitsFlag = 2;

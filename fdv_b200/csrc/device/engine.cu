@@ -3,7 +3,7 @@
 // or whole streams) and advances all of them by one frame per step.
 //
 // One step, on one CUDA stream:
-//   1. source frames host -> device;
+//   1. source frames host -> device (through a pinned staging buffer);
 //   2. analysis: the P-frame wavefront kernel over every P unit's macroblock
 //      rows and the intra CTU-wavefront kernel over every key-frame unit's
 //      plane CTU rows;
@@ -13,6 +13,12 @@
 //   5. reference preparation: the deblocked reconstruction becomes the
 //      unit's new nearest reference (integer + half-pel planes).
 // The reference pool rotates exactly as fdv_video_encode's (fdv.h:6842-6846).
+//
+// A step is a submit (everything above enqueued, nothing waited on) and a
+// collect (wait for the oldest submitted frame, check its error word, point
+// the stream views at its output).  Two frames can be in flight: staging,
+// output buffers and events are double-buffered, so a host can entropy-code
+// frame f while the GPU analyses frame f + 1.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,7 +49,7 @@ struct CompactTask;
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st);
 void launch_deblock(const void *tasks, int ntasks, cudaStream_t st);
 void launch_compact(const void *tasks, int ntasks, unsigned *err, cudaStream_t st);
-void upload_tables(const int32_t c8[64], const int32_t q8[52]);
+int upload_tables(const int32_t c8[64], const int32_t q8[52]);
 }  // namespace fdvb
 
 using namespace fdvb;
@@ -104,10 +110,21 @@ struct Unit {
     uint8_t *islots[3] = {nullptr, nullptr, nullptr};
     uint8_t *mmap[3] = {nullptr, nullptr, nullptr};
     int icols[3], irows[3], pw[3], ph[3];
-    uint8_t *out_h = nullptr, *out_d = nullptr;
+    uint8_t *out_h[2] = {nullptr, nullptr}, *out_d[2] = {nullptr, nullptr};   // per in-flight slot
     size_t out_cap = 0, out_off_i[3] = {0, 0, 0};
     int last_intra = 0, last_qp = 0;
     fdvb_streams ps{}, is[3]{};
+};
+
+// One in-flight frame: pinned staging of its sources and descriptors, its
+// error word, its events, and what its units were.
+struct Slot {
+    uint8_t *stage = nullptr;
+    size_t stage_cap = 0;
+    unsigned *err_h = nullptr;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::vector<int> intra;
+    bool has_p = false, has_i = false;
 };
 
 }  // namespace
@@ -128,8 +145,9 @@ struct fdvb_engine {
     int *d_poff = nullptr, *d_ioff = nullptr;
     int maxrows = 0, maxitasks = 0;
     unsigned long long wait_ns = 4000000000ull;
+    Slot slot[2];
+    int head = 0, inflight = 0;    // oldest in-flight slot, number in flight
     // timing (CUDA events on the engine's stream) and launch counts
-    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     double step_ms = 0, pk_ms = 0, ik_ms = 0;
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
     int src_on_device = 0;
@@ -182,8 +200,10 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     for (int p = 0; p < 3; ++p) icap[p] = 64 + (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p];
     u.out_off_i[0] = 0; u.out_off_i[1] = icap[0]; u.out_off_i[2] = icap[0] + icap[1];
     u.out_cap = std::max(pcap, icap[0] + icap[1] + icap[2]);
-    CK(cudaHostAlloc(&u.out_h, u.out_cap, cudaHostAllocMapped));
-    CK(cudaHostGetDevicePointer(&u.out_d, u.out_h, 0));
+    for (int k = 0; k < 2; ++k) {
+        CK(cudaHostAlloc(&u.out_h[k], u.out_cap, cudaHostAllocMapped));
+        CK(cudaHostGetDevicePointer(&u.out_d[k], u.out_h[k], 0));
+    }
     return 0;
 }
 
@@ -192,7 +212,15 @@ static void free_unit(Unit &u) {
     for (int r = 0; r < 2; ++r) cudaFree(u.ref[r].mem);
     cudaFree(u.mbi); cudaFree(u.slots); cudaFree(u.progress);
     for (int p = 0; p < 3; ++p) { cudaFree(u.islots[p]); cudaFree(u.mmap[p]); }
-    if (u.out_h) cudaFreeHost(u.out_h);
+    for (int k = 0; k < 2; ++k) if (u.out_h[k]) cudaFreeHost(u.out_h[k]);
+}
+
+// Bytes of the descriptor area of a slot's staging buffer (each array 64-byte aligned).
+static size_t stage_desc_bytes(int nu, int maxrows, int maxitasks) {
+    auto a = [](size_t n) { return (n + 63) / 64 * 64; };
+    return a(sizeof(UnitDev) * nu) + a(sizeof(RowTask) * maxrows) + a(sizeof(IPlaneDevH) * 3 * nu) +
+           a(sizeof(ITaskH) * maxitasks) + a(sizeof(PrepTaskH) * nu) + a(sizeof(DbTaskH) * 3 * nu) +
+           a(sizeof(CompactTaskH) * 3 * nu);
 }
 
 extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
@@ -210,10 +238,10 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     if (cudaSetDevice(device) != cudaSuccess) { g_err = "cudaSetDevice failed (no GPU?)"; delete E; return nullptr; }
     cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess) { g_err = "stream create failed"; delete E; return nullptr; }
-    for (auto &e : E->ev) cudaEventCreate(&e);
+    for (auto &sl : E->slot) for (auto &e : sl.ev) cudaEventCreate(&e);
     int32_t c8[64], q8[52];
     fdvb_c8_tables(c8, q8);
-    upload_tables(c8, q8);
+    if (upload_tables(c8, q8) != 0) { g_err = "table upload failed"; fdvb_engine_destroy(E); return nullptr; }
     E->units.resize(nunits);
     int maxrows = 0, maxitasks = 0;
     for (int i = 0; i < nunits; ++i) {
@@ -234,6 +262,18 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
               cudaMalloc(&E->d_poff, sizeof(int) * 16) == cudaSuccess &&
               cudaMalloc(&E->d_ioff, sizeof(int) * 12) == cudaSuccess;
     if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
+    size_t src_bytes = 0;
+    for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
+    for (auto &sl : E->slot) {
+        sl.stage_cap = (src_bytes + 63) / 64 * 64 + stage_desc_bytes(nunits, maxrows, maxitasks);
+        if (cudaHostAlloc(&sl.stage, sl.stage_cap, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&sl.err_h, 64, cudaHostAllocDefault) != cudaSuccess) {
+            g_err = "pinned allocation failed";
+            fdvb_engine_destroy(E);
+            return nullptr;
+        }
+        sl.intra.assign(nunits, 0);
+    }
     int poff[16], ioff[12];
     for (int k = 0; k < 16; ++k) { int o = 0; for (int i = 0; i < k; ++i) o += kSlotCap[i]; poff[k] = o; }
     iframe_slot_offsets(ioff);
@@ -252,7 +292,11 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
     if (E->d_prof) cudaFree(E->d_prof);
-    for (auto &e : E->ev) if (e) cudaEventDestroy(e);
+    for (auto &sl : E->slot) {
+        for (auto &e : sl.ev) if (e) cudaEventDestroy(e);
+        if (sl.stage) cudaFreeHost(sl.stage);
+        if (sl.err_h) cudaFreeHost(sl.err_h);
+    }
     if (E->st) cudaStreamDestroy(E->st);
     delete E;
 }
@@ -269,7 +313,10 @@ static size_t parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
     return (size_t)(d - p);
 }
 
-static int prep_refs(fdvb_engine *E, const std::vector<int> &which) {
+// Enqueue the reference preparation of units `which`; the task array is
+// staged in `stage` (pinned, slot-owned) when given, else copied from the stack
+// (callers that synchronise before returning).
+static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *stage = nullptr) {
     std::vector<PrepTaskH> pt;
     int maxw = 0, maxh = 0;
     for (int i : which) {
@@ -283,7 +330,9 @@ static int prep_refs(fdvb_engine *E, const std::vector<int> &which) {
         maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h);
     }
     if (pt.empty()) return 0;
-    CK(cudaMemcpyAsync(E->d_prep, pt.data(), sizeof(PrepTaskH) * pt.size(), cudaMemcpyHostToDevice, E->st));
+    const void *src = pt.data();
+    if (stage) { memcpy(stage, pt.data(), sizeof(PrepTaskH) * pt.size()); src = stage; }
+    CK(cudaMemcpyAsync(E->d_prep, src, sizeof(PrepTaskH) * pt.size(), cudaMemcpyHostToDevice, E->st));
     launch_refprep(E->d_prep, (int)pt.size(), maxw, maxh, E->border, E->st);
     CK(cudaGetLastError());
     for (int i : which) {
@@ -293,9 +342,10 @@ static int prep_refs(fdvb_engine *E, const std::vector<int> &which) {
     return 0;
 }
 
-extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
-                                const double *lscale, const int *force_skip) {
+extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                                  const double *lscale, const int *force_skip) {
     if (!E) return -1;
+    if (E->inflight >= 2) { g_err = "two frames already in flight"; return -1; }
     const int nu = (int)E->units.size();
     for (int i = 0; i < nu; ++i) {
         if (qp[i] < 0 || qp[i] > 51) { g_err = "qp out of range"; return -1; }
@@ -308,17 +358,35 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
         if (!is_intra[i] && E->units[i].nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
     }
     CK(cudaSetDevice(E->device));
-    CK(cudaEventRecord(E->ev[0], E->st));
-    // 1. sources
+    const int si = (E->head + E->inflight) & 1;
+    Slot &SL = E->slot[si];
+    CK(cudaEventRecord(SL.ev[0], E->st));
+    // 1. sources (host sources through the slot's pinned staging buffer)
+    uint8_t *stage = SL.stage;
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         if (force_skip && force_skip[i]) continue;
         const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
-        const cudaMemcpyKind kind = E->src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, kind, E->st));
-        CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, kind, E->st));
-        CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, kind, E->st));
+        if (E->src_on_device) {
+            CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, cudaMemcpyDeviceToDevice, E->st));
+            CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, cudaMemcpyDeviceToDevice, E->st));
+            CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, cudaMemcpyDeviceToDevice, E->st));
+        } else {
+            memcpy(stage, planes[3 * i], ys);
+            memcpy(stage + ys, planes[3 * i + 1], cs);
+            memcpy(stage + ys + cs, planes[3 * i + 2], cs);
+            CK(cudaMemcpyAsync(u.cur, stage, ys + 2 * cs, cudaMemcpyHostToDevice, E->st));
+            stage += ys + 2 * cs;
+        }
     }
+    stage = SL.stage + (stage - SL.stage + 63) / 64 * 64;
+    // descriptors are staged too: each array copied to the pinned buffer
+    auto staged = [&](const void *src, size_t n) -> const void * {
+        memcpy(stage, src, n);
+        const void *r = stage;
+        stage += (n + 63) / 64 * 64;
+        return r;
+    };
     // 2. descriptors
     std::vector<UnitDev> ud(nu);
     std::vector<RowTask> rows;
@@ -340,11 +408,11 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
         d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
         d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
         d.prof = E->d_prof;
-        u.last_intra = is_intra[i];
+        SL.intra[i] = is_intra[i];
         u.last_qp = qp[i];
         if (!is_intra[i]) {
             for (int r = 0; r < u.mbh; ++r) rows.push_back({i, r});
-            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d, u.out_cap};
+            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[si], u.out_cap};
             cmp.push_back(c);
         } else {
             int prog = u.mbh;
@@ -358,7 +426,7 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
                 for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
                 prog += u.irows[p];
                 CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
-                               u.out_d + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p]};
+                               u.out_d[si] + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p]};
                 cmp.push_back(c);
             }
         }
@@ -383,68 +451,98 @@ extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, co
             for (auto &t : itasks) if (t.row == r) it2.push_back(t);
         itasks.swap(it2);
     }
-    CK(cudaMemcpyAsync(E->d_units, ud.data(), sizeof(UnitDev) * nu, cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemcpyAsync(E->d_units, staged(ud.data(), sizeof(UnitDev) * nu), sizeof(UnitDev) * nu, cudaMemcpyHostToDevice, E->st));
     CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
     CK(cudaMemsetAsync(E->d_err, 0, sizeof(unsigned), E->st));
     if (!rows.empty()) {
-        CK(cudaMemcpyAsync(E->d_rows, rows.data(), sizeof(RowTask) * rows.size(), cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemcpyAsync(E->d_rows, staged(rows.data(), sizeof(RowTask) * rows.size()), sizeof(RowTask) * rows.size(),
+                           cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)rows.size(), E->nsm);
-        CK(cudaEventRecord(E->ev[1], E->st));
+        CK(cudaEventRecord(SL.ev[1], E->st));
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->st);
         CK(cudaGetLastError());
-        CK(cudaEventRecord(E->ev[2], E->st));
+        CK(cudaEventRecord(SL.ev[2], E->st));
         E->launches += 1;
     }
     if (!itasks.empty()) {
-        CK(cudaMemcpyAsync(E->d_planes, iplanes.data(), sizeof(IPlaneDevH) * iplanes.size(), cudaMemcpyHostToDevice, E->st));
-        CK(cudaMemcpyAsync(E->d_itasks, itasks.data(), sizeof(ITaskH) * itasks.size(), cudaMemcpyHostToDevice, E->st));
-        CK(cudaEventRecord(E->ev[3], E->st));
+        CK(cudaMemcpyAsync(E->d_planes, staged(iplanes.data(), sizeof(IPlaneDevH) * iplanes.size()),
+                           sizeof(IPlaneDevH) * iplanes.size(), cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemcpyAsync(E->d_itasks, staged(itasks.data(), sizeof(ITaskH) * itasks.size()),
+                           sizeof(ITaskH) * itasks.size(), cudaMemcpyHostToDevice, E->st));
+        CK(cudaEventRecord(SL.ev[3], E->st));
         launch_iframe(E->d_planes, E->d_itasks, (int)itasks.size(), E->d_ticket + 1, E->d_err, E->wait_ns, E->nsm, E->st);
         CK(cudaGetLastError());
-        CK(cudaEventRecord(E->ev[4], E->st));
+        CK(cudaEventRecord(SL.ev[4], E->st));
         E->launches += 1;
     }
     // 3. deblock, 4. compact
-    CK(cudaMemcpyAsync(E->d_db, db.data(), sizeof(DbTaskH) * db.size(), cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemcpyAsync(E->d_db, staged(db.data(), sizeof(DbTaskH) * db.size()), sizeof(DbTaskH) * db.size(),
+                       cudaMemcpyHostToDevice, E->st));
     launch_deblock(E->d_db, (int)db.size(), E->st);
     CK(cudaGetLastError());
     E->launches += 2;
-    CK(cudaMemcpyAsync(E->d_cmp, cmp.data(), sizeof(CompactTaskH) * cmp.size(), cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemcpyAsync(E->d_cmp, staged(cmp.data(), sizeof(CompactTaskH) * cmp.size()), sizeof(CompactTaskH) * cmp.size(),
+                       cudaMemcpyHostToDevice, E->st));
     launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
     CK(cudaGetLastError());
     E->launches += 1;
     // 5. the new reference
     std::vector<int> all(nu);
     for (int i = 0; i < nu; ++i) all[i] = i;
-    if (prep_refs(E, all) != 0) return -3;
+    if (prep_refs(E, all, stage) != 0) return -3;
     E->launches += 2;
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
     }
-    CK(cudaEventRecord(E->ev[5], E->st));
+    CK(cudaMemcpyAsync(SL.err_h, E->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
+    CK(cudaEventRecord(SL.ev[5], E->st));
+    SL.has_p = !rows.empty();
+    SL.has_i = !itasks.empty();
     E->stall_unit = E->stall_row = -1;     // an injected stall lasts one step
-    CK(cudaStreamSynchronize(E->st));
+    E->inflight += 1;
+    return 0;
+}
+
+// Wait for the oldest submitted frame; on success the stream views
+// (fdvb_engine_pstreams / _istreams) describe it.
+extern "C" int fdvb_engine_collect(fdvb_engine *E) {
+    if (!E) return -1;
+    if (E->inflight == 0) { g_err = "no frame in flight"; return -1; }
+    Slot &SL = E->slot[E->head];
+    const int si = E->head;
+    E->head ^= 1;
+    E->inflight -= 1;
+    CK(cudaEventSynchronize(SL.ev[5]));
     {
         float ms = 0;
-        cudaEventElapsedTime(&ms, E->ev[0], E->ev[5]);
+        cudaEventElapsedTime(&ms, SL.ev[0], SL.ev[5]);
         E->step_ms += ms;
         E->steps += 1;
-        if (!rows.empty()) { cudaEventElapsedTime(&ms, E->ev[1], E->ev[2]); E->pk_ms += ms; E->pk_n += 1; }
-        if (!itasks.empty()) { cudaEventElapsedTime(&ms, E->ev[3], E->ev[4]); E->ik_ms += ms; E->ik_n += 1; }
+        if (SL.has_p) { cudaEventElapsedTime(&ms, SL.ev[1], SL.ev[2]); E->pk_ms += ms; E->pk_n += 1; }
+        if (SL.has_i) { cudaEventElapsedTime(&ms, SL.ev[3], SL.ev[4]); E->ik_ms += ms; E->ik_n += 1; }
     }
-    unsigned err = 0;
-    CK(cudaMemcpy(&err, E->d_err, sizeof err, cudaMemcpyDeviceToHost));
+    const unsigned err = *SL.err_h;
     if (err) {
         g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out" : "symbol slot overflow";
         return -4;
     }
-    for (int i = 0; i < nu; ++i) {
+    for (int i = 0; i < (int)E->units.size(); ++i) {
         Unit &u = E->units[i];
-        if (!u.last_intra) E->d2h += (long long)parse_streams(u.out_h, 16, &u.ps);
-        else for (int p = 0; p < 3; ++p) E->d2h += (long long)parse_streams(u.out_h + u.out_off_i[p], 12, &u.is[p]);
+        u.last_intra = SL.intra[i];
+        if (!u.last_intra) E->d2h += (long long)parse_streams(u.out_h[si], 16, &u.ps);
+        else for (int p = 0; p < 3; ++p) E->d2h += (long long)parse_streams(u.out_h[si] + u.out_off_i[p], 12, &u.is[p]);
     }
     return 0;
+}
+
+extern "C" int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                                const double *lscale, const int *force_skip) {
+    if (!E) return -1;
+    if (E->inflight) { g_err = "a frame is still in flight"; return -1; }
+    const int rc = fdvb_engine_submit(E, planes, is_intra, qp, lscale, force_skip);
+    if (rc != 0) return rc;
+    return fdvb_engine_collect(E);
 }
 
 extern "C" const fdvb_streams *fdvb_engine_pstreams(fdvb_engine *E, int unit) {
@@ -459,6 +557,7 @@ extern "C" const fdvb_streams *fdvb_engine_istreams(fdvb_engine *E, int unit, in
 extern "C" int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420) {
     if (!E || unit < 0 || unit >= (int)E->units.size() || !i420) return -1;
     Unit &u = E->units[unit];
+    CK(cudaStreamSynchronize(E->st));
     CK(cudaMemcpy(i420, u.rec, (size_t)u.w * u.h * 3 / 2, cudaMemcpyDeviceToHost));
     return 0;
 }
@@ -466,6 +565,7 @@ extern "C" int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420) {
 // second one (NULL = none).  The next step then codes a P-frame against them.
 extern "C" int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *near_i420, const uint8_t *far_i420) {
     if (!E || unit < 0 || unit >= (int)E->units.size() || !near_i420) return -1;
+    if (E->inflight) { g_err = "a frame is still in flight"; return -1; }
     Unit &u = E->units[unit];
     const size_t fs = (size_t)u.w * u.h * 3 / 2;
     std::vector<int> one{unit};

@@ -68,7 +68,8 @@ struct IPlaneDev {
 // Profile entries of the key-frame kernel (relative to prof): chain waits for
 // the row above, chain 4x4 leaves, team busy time per leaf size, CTU time,
 // CTU count, 4x4 leaf count, chain waits for team results.
-enum { IP_WAIT = 0, IP_LEAF4, IP_LEAF8, IP_LEAF16, IP_LEAF32, IP_LEAF64, IP_CTU, IP_NCTU, IP_NLEAF4, IP_HWAIT };
+enum { IP_WAIT = 0, IP_LEAF4, IP_LEAF8, IP_LEAF16, IP_LEAF32, IP_LEAF64, IP_CTU, IP_NCTU, IP_NLEAF4, IP_HWAIT,
+       IP_L4SCREEN, IP_L4SELECT, IP_L4TRIAL, IP_L4COMMIT, IP_L4RUN1, IP_L4RUN2 };
 struct ITask { int plane, row; };
 
 // Per-depth split-trial sink capacities (node of side n = 64 >> d, see
@@ -103,8 +104,6 @@ struct HJob {
 struct HelperArea {
     HJob job;
     int ok, nm, ml[4];
-    int best_idx, best_mode;
-    double best_J;
     NNPred nn[4];
     long long e[4];
     int b[4];
@@ -123,7 +122,7 @@ struct ChainArea {
     uint8_t ssmem[isink_bytes(0) + isink_bytes(1) + isink_bytes(2) + isink_bytes(3)];
     ISink out;                            // the CTU's output (global)
     // 4x4 leaf scratch
-    int T9[9], L5[5];                     // T(-1..7), L(-1..3)
+    int T9w[4][9], L5w[4][5];             // per warp: T(-1..7), L(-1..3)
     uint8_t cp[9][16];
     int csat[9], cs[9], cm[9], run, best_c;
     Blk4 trial[9];
@@ -133,6 +132,8 @@ struct ChainArea {
     double retJ;
     int done[4];                          // per leaf size: last finished job (written by the teams)
     int issued[4];                        // per leaf size: last posted job
+    double res_J[4];                      // per leaf size: the team's result (written by the team)
+    int res_idx[4], res_mode[4];
     int abort, task, row_ok;
 };
 struct IShared {
@@ -217,8 +218,8 @@ __device__ void chain_isink_append(ISink *dst, const ISink *src, unsigned *err) 
 __device__ void chain_append_leaf(CoefSink *dst, IShared *S, int rank, int idx, unsigned *err) {
     const int t = threadIdx.x;
     cg::cluster_group cl = cg::this_cluster();
-    const CoefSink *rs = cl.map_shared_rank(&S->H.sink[idx], rank);
-    const uint8_t *rm = cl.map_shared_rank(&S->H.sinkmem[idx][0], rank);
+    const CoefSink *rs = rank ? cl.map_shared_rank(&S->H.sink[idx], rank) : &S->H.sink[idx];
+    const uint8_t *rm = rank ? cl.map_shared_rank(&S->H.sinkmem[idx][0], rank) : &S->H.sinkmem[idx][0];
     int len[CS_NUM];
     for (int k = 0; k < CS_NUM; ++k) len[k] = rs->len[k];
     for (int k = 0; k < CS_NUM; ++k) {
@@ -259,11 +260,16 @@ __device__ __forceinline__ bool mode_ok4(int m, int ht, int htr, int hl, int htl
 }
 
 // ------------------------------------------------------- 4x4 leaf --
-// One 4x4 leaf (fdv.h:3907-4111) on the chain's four warps: the nine
-// predictions and their SATD screen on half-warps, the reference's selection
-// sort and ratio prune on one thread, then the RD trials without RDOQ and the
-// RDOQ re-code of the winner.  With at most two trials (QP >= 12) the RDOQ
-// re-codes of both run beside the trials and the winner's is kept.
+// One 4x4 leaf (fdv.h:3907-4111) on the chain's four warps.  Every warp reads
+// the neighbours itself; half-warp h of warp w predicts and SATD-screens mode
+// 2w + h (warp 0 also mode 8).  From QP 12 up the screen keeps at most two
+// candidates: every warp derives the reference's selection-sort order and
+// ratio prune with two warp minimums, and the trials run at once -- the RD
+// trials without RDOQ on warps 0-1, the RDOQ re-codes of both candidates on
+// warps 2-3 -- so one barrier separates the screen from the trials and one
+// the trials from the commit, which every warp applies to its own view of the
+// tile.  Below QP 12 every screened mode is tried in the sorted order and the
+// winner re-coded after.
 __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     ChainArea &C = c.S->C;
     const QP4 &Q = c.S->q;
@@ -272,23 +278,21 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     const int tx = bx - c.bx0, ty = by - c.by0;
     const int ht = by > 0, hl = bx > 0, htl = ht && hl;
     const int htr = ht && (bx + 4 < c.w) && cell_done(bx + 4, by - 1, bx, by);
-    // neighbours (gather_neighbors fdv.h:3689-3706)
-    if (t < 8) C.T9[t + 1] = ht ? ((t < 4 || htr) ? TL(C, ty - 1, tx + t) : TL(C, ty - 1, tx + 3)) : 0;
-    else if (t < 12) C.L5[t - 7] = hl ? TL(C, ty + t - 8, tx - 1) : 0;
-    else if (t == 12) { const int v = htl ? TL(C, ty - 1, tx - 1) : 128; C.T9[0] = v; C.L5[0] = v; }
-    cbar();
-    {   // predictions: thread (m, p) for m = 0..7, then mode 8 on threads 0..15
-        const int m = t >> 4, p = t & 15;
-        if (mode_ok4(m, ht, htr, hl, htl)) C.cp[m][p] = (uint8_t)pred4_px(m, C.T9, C.L5, ht, hl, p & 3, p >> 2);
-        if (t < 16 && mode_ok4(8, ht, htr, hl, htl)) C.cp[8][p] = (uint8_t)pred4_px(8, C.T9, C.L5, ht, hl, p & 3, p >> 2);
-    }
-    cbar();
-    {   // SATD (fdv.h:3803-3823): half-warp h screens mode h, then warp 0 mode 8
-        const int l = t & 15, i = l >> 2, j = l & 3, rb = lane & ~3, cb = (lane & 16) + j;
+    // neighbours (gather_neighbors fdv.h:3689-3706), one copy per warp
+    int *T9 = C.T9w[w], *L5 = C.L5w[w];
+    if (lane < 8) T9[lane + 1] = ht ? ((lane < 4 || htr) ? TL(C, ty - 1, tx + lane) : TL(C, ty - 1, tx + 3)) : 0;
+    else if (lane < 12) L5[lane - 7] = hl ? TL(C, ty + lane - 8, tx - 1) : 0;
+    else if (lane == 12) { const int v = htl ? TL(C, ty - 1, tx - 1) : 128; T9[0] = v; L5[0] = v; }
+    __syncwarp();
+    {   // predictions and SATD (fdv.h:3803-3823)
+        const int l = lane & 15, i = l >> 2, j = l & 3, rb = lane & ~3, cb = (lane & 16) + j;
+        const int sv = C.src[(ty + i) * 64 + tx + j];
         for (int pass = 0; pass < 2; ++pass) {
             if (pass && w != 0) break;
-            const int m = pass ? 8 : (t >> 4);
-            const int d = (int)C.src[(ty + i) * 64 + tx + j] - (int)C.cp[m][l];
+            const int m = pass ? 8 : 2 * w + (lane >> 4);
+            const int pv = mode_ok4(m, ht, htr, hl, htl) ? pred4_px(m, T9, L5, ht, hl, j, i) : 0;
+            C.cp[m][l] = (uint8_t)pv;
+            const int d = sv - pv;
             const int x0 = __shfl_sync(FDVB_FULL, d, rb), x1 = __shfl_sync(FDVB_FULL, d, rb + 1);
             const int x2 = __shfl_sync(FDVB_FULL, d, rb + 2), x3 = __shfl_sync(FDVB_FULL, d, rb + 3);
             const int a0 = x0 + x1, a1 = x0 - x1, a2 = x2 + x3, a3 = x2 - x3;
@@ -296,71 +300,92 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
             const int y0 = __shfl_sync(FDVB_FULL, hv, cb), y1 = __shfl_sync(FDVB_FULL, hv, cb + 4);
             const int y2 = __shfl_sync(FDVB_FULL, hv, cb + 8), y3 = __shfl_sync(FDVB_FULL, hv, cb + 12);
             const int b0 = y0 + y1, b1 = y0 - y1, b2 = y2 + y3, b3 = y2 - y3;
-            int s = abs(i == 0 ? b0 + b2 : (i == 1 ? b1 + b3 : (i == 2 ? b0 - b2 : b1 - b3)));
-            s += __shfl_xor_sync(FDVB_FULL, s, 8);
-            s += __shfl_xor_sync(FDVB_FULL, s, 4);
-            s += __shfl_xor_sync(FDVB_FULL, s, 2);
-            s += __shfl_xor_sync(FDVB_FULL, s, 1);
-            if (l == 0) C.csat[m] = s;
+            int sa = abs(i == 0 ? b0 + b2 : (i == 1 ? b1 + b3 : (i == 2 ? b0 - b2 : b1 - b3)));
+            sa += __shfl_xor_sync(FDVB_FULL, sa, 8);
+            sa += __shfl_xor_sync(FDVB_FULL, sa, 4);
+            sa += __shfl_xor_sync(FDVB_FULL, sa, 2);
+            sa += __shfl_xor_sync(FDVB_FULL, sa, 1);
+            if (l == 0) C.csat[m] = sa;
         }
     }
     cbar();
-    if (t == 0) {   // the reference's selection sort over the screened modes, then the ratio prune
-        int nc = 0;
-        for (int m = 0; m < 9; ++m)
-            if (mode_ok4(m, ht, htr, hl, htl)) { C.cs[nc] = C.csat[m]; C.cm[nc] = m; ++nc; }
-        const int ntry = c.qp < 12 ? nc : (nc < 2 ? nc : 2);
-        for (int a = 0; a < ntry; ++a) {
-            int bst = a;
-            for (int b2 = a + 1; b2 < nc; ++b2) if (C.cs[b2] < C.cs[bst]) bst = b2;
-            if (bst != a) {
-                int v = C.cs[a]; C.cs[a] = C.cs[bst]; C.cs[bst] = v;
-                v = C.cm[a]; C.cm[a] = C.cm[bst]; C.cm[bst] = v;
-            }
-        }
-        int run = 0;
-        for (int k = 0; k < ntry; ++k) {
-            if (k > 0 && c.qp >= 12 && (long long)C.cs[k] * 4 > (long long)C.cs[0] * 5) break;
-            ++run;
-        }
-        C.run = run;
-    }
-    cbar();
-    const int run = C.run;
+    long long tp = prof_t0(c.prof, t);
+    prof_add(c.prof, t, IP_L4SCREEN, t0);
     const uint8_t *sblk = &C.src[ty * 64 + tx];
-    int fsel;
-    if (run <= 2) {
-        const int k = w & 1;
-        if (k < run) {
-            if (w < 2) warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.junk[w], 4, Q, c.lambda, false, &C.trial[k], &C.b4[w], lane);
-            else       warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.frec[k], 4, Q, c.lambda, true, &C.fin[k], &C.b4[w], lane);
+    int mode, fsel;
+    if (c.qp >= 12) {
+        // The selection sort (fdv.h:3962-3975) for two places: the first
+        // minimum, then the first minimum of the rest in the order left by the
+        // swap (the first candidate moved to the winner's place); the prune
+        // keeps the second only if its SATD is within 5/4 of the first's.
+        const bool vm = lane < 9 && mode_ok4(lane, ht, htr, hl, htl);
+        const unsigned vmask = __ballot_sync(FDVB_FULL, vm);
+        const unsigned sv = vm ? (unsigned)C.csat[lane] : 0u;
+        const unsigned k0 = __reduce_min_sync(FDVB_FULL, vm ? (sv << 4) | lane : 0xffffffffu);
+        const int m0 = k0 & 15, s0 = k0 >> 4;
+        const int first = __ffs(vmask) - 1;
+        const int p0 = __popc(vmask & ((1u << m0) - 1));
+        const int pos = lane == first ? p0 : __popc(vmask & ((1u << lane) - 1));
+        const unsigned k1 = __reduce_min_sync(FDVB_FULL, (vm && lane != m0) ? (sv << 8) | (pos << 4) | lane : 0xffffffffu);
+        const int m1 = k1 & 15, s1 = k1 >> 8;
+        const int run = (__popc(vmask) >= 2 && !((long long)s1 * 4 > (long long)s0 * 5)) ? 2 : 1;
+        if (c.prof && t == 0) atomicAdd(&c.prof[run == 1 ? IP_L4RUN1 : IP_L4RUN2], 1ull);
+        prof_add(c.prof, t, IP_L4SELECT, tp);
+        tp = prof_t0(c.prof, t);
+        if (run == 1) {
+            if (w == 0) warp_block4(sblk, 64, C.cp[m0], 4, C.frec[0], 4, Q, c.lambda, true, &C.fin[0], &C.b4[0], lane);
+        } else {
+            const int k = w & 1, mk = k ? m1 : m0;
+            if (w < 2) warp_block4(sblk, 64, C.cp[mk], 4, C.junk[w], 4, Q, c.lambda, false, &C.trial[k], &C.b4[w], lane);
+            else       warp_block4(sblk, 64, C.cp[mk], 4, C.frec[k], 4, Q, c.lambda, true, &C.fin[k], &C.b4[w], lane);
         }
+        cbar();
+        fsel = 0;
+        if (run == 2) {   // trial costs are positive: the second wins only if strictly cheaper
+            const double J0 = rd_cost((double)C.trial[0].ssd, c.lambda, kBitsMode + C.trial[0].bits);
+            const double J1 = rd_cost((double)C.trial[1].ssd, c.lambda, kBitsMode + C.trial[1].bits);
+            fsel = J1 < J0 ? 1 : 0;
+        }
+        mode = fsel ? m1 : m0;
     } else {
+        if (t == 0) {   // the reference's selection sort over every screened mode
+            int nc = 0;
+            for (int m = 0; m < 9; ++m)
+                if (mode_ok4(m, ht, htr, hl, htl)) { C.cs[nc] = C.csat[m]; C.cm[nc] = m; ++nc; }
+            for (int a = 0; a < nc; ++a) {
+                int bst = a;
+                for (int b2 = a + 1; b2 < nc; ++b2) if (C.cs[b2] < C.cs[bst]) bst = b2;
+                if (bst != a) {
+                    int v = C.cs[a]; C.cs[a] = C.cs[bst]; C.cs[bst] = v;
+                    v = C.cm[a]; C.cm[a] = C.cm[bst]; C.cm[bst] = v;
+                }
+            }
+            C.run = nc;
+        }
+        cbar();
+        const int run = C.run;
         for (int k = w; k < run; k += 4)
             warp_block4(sblk, 64, C.cp[C.cm[k]], 4, C.junk[w], 4, Q, c.lambda, false, &C.trial[k], &C.b4[w], lane);
-    }
-    cbar();
-    if (t == 0) {
+        cbar();
         double best = -1.0;
         int bc = 0;
         for (int k = 0; k < run; ++k) {
             const double J = rd_cost((double)C.trial[k].ssd, c.lambda, kBitsMode + C.trial[k].bits);
             if (best < 0.0 || J < best) { best = J; bc = k; }
         }
-        C.best_c = bc;
-    }
-    cbar();
-    if (run <= 2) {
-        fsel = C.best_c;
-    } else {
-        if (w == 0) warp_block4(sblk, 64, C.cp[C.cm[C.best_c]], 4, C.frec[0], 4, Q, c.lambda, true, &C.fin[0], &C.b4[0], lane);
+        mode = C.cm[bc];
+        if (w == 0) warp_block4(sblk, 64, C.cp[mode], 4, C.frec[0], 4, Q, c.lambda, true, &C.fin[0], &C.b4[0], lane);
         cbar();
         fsel = 0;
     }
+    prof_add(c.prof, t, IP_L4TRIAL, tp);
+    tp = prof_t0(c.prof, t);
+    // commit: every warp writes the winner into the tile (the next leaf's
+    // neighbours come from this warp's own writes), thread 0 the symbols
     const Blk4 &F = C.fin[fsel];
-    if (t < 16) TL(C, ty + (t >> 2), tx + (t & 3)) = C.frec[fsel][t];
+    if (lane < 16) TL(C, ty + (lane >> 2), tx + (lane & 3)) = C.frec[fsel][lane];
+    __syncwarp();
     if (t == 0) {
-        const int mode = C.cm[C.best_c];
         cs_put1(&tgt->c, CS_N, (uint8_t)F.count, c.err);
         cs_put(&tgt->c, CS_L, F.bytes, F.nbytes, c.err);
         const int lcx = tx >> 2, lcy = ty >> 2;
@@ -368,17 +393,17 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
         const int Am = by > 0 ? MM(C, lcy - 1, lcx) : 0;
         isink_put(tgt, Lm == Am ? IS_MODE0 : IS_MODE1, (uint8_t)mode, c.err);
         MM(C, lcy, lcx) = (uint8_t)mode;
-        C.retJ = rd_cost((double)F.ssd, c.lambda, kBitsMode + F.bits);
         if (c.prof) atomicAdd(&c.prof[IP_NLEAF4], 1ull);
     }
-    cbar();
+    prof_add(c.prof, t, IP_L4COMMIT, tp);
     prof_add(c.prof, t, IP_LEAF4, t0);
-    return C.retJ;
+    return rd_cost((double)F.ssd, c.lambda, kBitsMode + F.bits);
 }
 
 // ------------------------------------------------------ chain: nodes --
-// Post the leaf trial of the node of side n = 64 >> L at (bx, by) to its team.
-__device__ void post_leaf_job(CCtx &c, int L, int bx, int by, int n) {
+// Post the leaf trial of the node of side n = 64 >> L at (bx, by) to its team
+// and clear the node's split-trial sink.
+__device__ void post_leaf_job(CCtx &c, int L, int bx, int by, int n, ISink *ss) {
     ChainArea &C = c.S->C;
     const int t = threadIdx.x, tx = bx - c.bx0, ty = by - c.by0;
     const int ht = by > 0, hl = bx > 0;
@@ -390,7 +415,8 @@ __device__ void post_leaf_job(CCtx &c, int L, int bx, int by, int n) {
         J->tl = (ht && hl) ? TL(C, ty - 1, tx - 1) : 128;
         J->kind = 0;
     }
-    fence_cluster();
+    if (t == 2) isink_reset(ss);
+    if (L < 3) fence_cluster();
     cbar();
     if (t == 0) st_release_cluster(&J->seq, ++C.issued[L]);
 }
@@ -432,23 +458,19 @@ __device__ double CNode<D>::run(CCtx &c, int bx, int by, ISink *tgt) {
         }
         return J;
     }
-    post_leaf_job(c, D, bx, by, n);
     ISink *ss = &C.ss[D];
-    if (t == 0) isink_reset(ss);
-    cbar();
+    post_leaf_job(c, D, bx, by, n, ss);
     double Js = 0.0;
     for (int k = 0; k < 4; ++k) Js = __dadd_rn(Js, CNode<D + 1>::run(c, bx + (k & 1) * hn, by + (k >> 1) * hn, ss));
     // the leaf trial's result
     const long long tw = prof_t0(c.prof, t);
     if (t == 0 && !C.abort && !wait_cluster_flag(&C.done[D], C.issued[D], c.err, c.hlimit)) C.abort = 1;
     cbar();
-    fence_cluster();
     prof_add(c.prof, t, IP_HWAIT, tw);
     if (C.abort) return 0.0;
     const int rank = level_rank(D);
-    const HelperArea *RH = cg::this_cluster().map_shared_rank(&S->H, rank);
-    const double Jl = RH->best_J;
-    const int bi = RH->best_idx, mode = RH->best_mode;
+    const double Jl = C.res_J[D];
+    const int bi = C.res_idx[D], mode = C.res_mode[D];
     const bool split = Js < Jl;
     if (t == 0) isink_put(tgt, IS_SPLIT0 + D, (uint8_t)split, c.err);
     if (split) {
@@ -456,6 +478,11 @@ __device__ double CNode<D>::run(CCtx &c, int bx, int by, ISink *tgt) {
         return Js;
     }
     if (t == 0) isink_put(tgt, IS_MODEB, (uint8_t)mode, c.err);
+    const HelperArea *RH = &S->H;
+    if (rank != 0) {
+        fence_cluster();
+        RH = cg::this_cluster().map_shared_rank(&S->H, rank);
+    }
     const int tx = bx - c.bx0, ty = by - c.by0;
     const uint32_t *rw = reinterpret_cast<const uint32_t *>(RH->rec[bi]);
     for (int p = t; p < n * n / 4; p += kChainNT) {
@@ -559,7 +586,7 @@ __device__ void team_loop(IShared *S, const IPlaneDev &P, int L, unsigned *err, 
     HelperArea &H = S->H;
     const int n = 64 >> L;
     cg::cluster_group cl = cg::this_cluster();
-    int *done = cl.map_shared_rank(&S->C.done[L], 0);
+    ChainArea *RC = cl.map_shared_rank(&S->C, 0);
     unsigned long long *prof = P.prof;
     for (;;) {
         if (tt == 0) H.ok = wait_cluster_flag(&H.job.seq, seen + 1, err, hlimit);
@@ -601,13 +628,13 @@ __device__ void team_loop(IShared *S, const IPlaneDev &P, int L, unsigned *err, 
                 const double J = rd_cost((double)H.e[i], P.lambda, kBitsMode + H.b[i]);
                 if (best < 0.0 || J < best) { best = J; bi = i; }
             }
-            H.best_J = best;
-            H.best_idx = bi;
-            H.best_mode = H.ml[bi];
+            RC->res_J[L] = best;
+            RC->res_idx[L] = bi;
+            RC->res_mode[L] = H.ml[bi];
         }
-        fence_cluster();
+        if (L < 3) fence_cluster();
         team_bar(BAR, NT);
-        if (tt == 0) st_release_cluster(done, seen);
+        if (tt == 0) st_release_cluster(&RC->done[L], seen);
         prof_add(prof, tt, IP_LEAF64 - L, t0);
     }
 }

@@ -11,9 +11,15 @@
 
 namespace fdvb {
 
-void upload_tables(const int32_t c8[64], const int32_t q8[52]) {
-    cudaMemcpyToSymbol(c_C8, c8, sizeof(int32_t) * 64);
-    cudaMemcpyToSymbol(c_QSTEP8, q8, sizeof(int32_t) * 52);
+int upload_tables(const int32_t c8[64], const int32_t q8[52]) {
+    int32_t c8t[64];
+    for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) c8t[j * 8 + i] = c8[i * 8 + j];
+    if (cudaMemcpyToSymbol(g_C8, c8, sizeof(int32_t) * 64) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_C8T, c8t, sizeof(int32_t) * 64) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_QSTEP8, q8, sizeof(int32_t) * 52) != cudaSuccess)
+        return -1;
+    return 0;
 }
 
 void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticket, unsigned *err,
@@ -145,9 +151,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
             if (e != cudaSuccess || !p) return static_fail("cudaGetSymbolAddress of the static scratch failed");
             int32_t c8[64], q8[52];
             fdvb_c8_tables(c8, q8);
-            if (cudaMemcpyToSymbol(c_C8, c8, sizeof c8) != cudaSuccess ||
-                cudaMemcpyToSymbol(c_QSTEP8, q8, sizeof q8) != cudaSuccess)
-                return static_fail("table upload failed");
+            if (upload_tables(c8, q8) != 0) return static_fail("table upload failed");
             cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev);
             S.ptr = static_cast<uint8_t *>(p);
             S.done = true;

@@ -78,14 +78,24 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
     }
     return v;
 }
+// Inclusive scan over lanes 0..15 (lanes 16..31 hold partial sums).
+__device__ __forceinline__ int scan16(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int t = __shfl_up_sync(FDVB_FULL, v, o);
+        if ((lane & 15) >= o) v += t;
+    }
+    return v;
+}
 
 // One warp codes one 4x4 block: forward transform, quantisation, optional RDOQ
 // (fdv.h:2493-2536), dequantisation, inverse transform, reconstruction.  Lane
 // l < 16 owns raster position l and zigzag position l; lanes 0..16 evaluate
 // the RDOQ truncation candidate L = lane - 1 in parallel, their rates come
-// from a suffix sum over the zigzag scan, and every lane replays the
-// reference's sequential selection (bestJ < 0.0 || J < bestJ, in the order
-// L = last .. -1) over the valid candidates.  Level bytes are packed in
+// from a suffix sum over the zigzag scan.  The reference's sequential
+// selection (bestJ < 0.0 || J < bestJ, in the order L = last .. -1) is a
+// butterfly minimum when no cost is negative and is replayed step by step
+// otherwise (a rate can go negative).  Level bytes are packed in
 // parallel from a prefix sum of their LEB lengths.  Writes rec (stride rs).
 __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
                             uint8_t *rec, int rs, const QP4 &Q, double lambda, bool rdoq,
@@ -107,15 +117,15 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
     }
     // zigzag view: lane k holds the level at zigzag position k
     const int kz = l;
-    int levz = __shfl_sync(FDVB_FULL, lev, c_ZZ4[kz]);
+    int levz = __shfl_sync(FDVB_FULL, lev, zz4(kz));
     unsigned nzm = __ballot_sync(FDVB_FULL, lane < 16 && levz != 0);
     int last = nzm ? 31 - __clz(nzm) : -1;
     if (rdoq && last >= 0) {
         const uint32_t z = zz_enc(levz);
         const bool in = lane < 16 && kz <= last;
         const int bits0 = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
-        const int pre = warp_incl_scan(in ? 8 * leb_size(z) : 0, lane);
-        const int tot = __shfl_sync(FDVB_FULL, pre, 31);
+        const int pre = scan16(in ? 8 * leb_size(z) : 0, lane);
+        const int tot = __shfl_sync(FDVB_FULL, pre, 15);
         const int L = lane - 1;
         int preL = __shfl_sync(FDVB_FULL, pre, L < 0 ? 0 : (L & 31));
         if (L < 0) preL = 0;
@@ -128,7 +138,7 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
         if (valid) {
             int d[16], r[16];
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = (c_IZZ4[p] <= L ? sc->lev[p] : 0) * Q.dq[p];
+            for (int p = 0; p < 16; ++p) d[p] = (izz4(p) <= L ? sc->lev[p] : 0) * Q.dq[p];
             idct4_thread(d, r);
             int D = 0;
 #pragma unroll
@@ -136,16 +146,30 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
             J = rd_cost((double)D, lambda, bitsL);
         }
         int bestL = last;
-        double bestJ = -1.0;
-        unsigned m = vmask;
-        while (m) {                                        // uniform across the warp
-            const int c = 31 - __clz(m);
-            m &= ~(1u << c);
-            const double Jc = __shfl_sync(FDVB_FULL, J, c);
-            if (bestJ < 0.0 || Jc < bestJ) { bestJ = Jc; bestL = c - 1; }
+        if (!__any_sync(FDVB_FULL, valid && J < 0.0)) {
+            // every cost non-negative: the sequential rule is the minimum, ties
+            // going to the first candidate in its order (the highest c).  The
+            // bit patterns of non-negative doubles order like their values, so
+            // the minimum is taken on the high word, then the low word.
+            const unsigned long long jb = (unsigned long long)__double_as_longlong(J);
+            const unsigned hi = valid ? (unsigned)(jb >> 32) : 0xffffffffu;
+            const unsigned mh = __reduce_min_sync(FDVB_FULL, hi);
+            const unsigned lo = (valid && hi == mh) ? (unsigned)jb : 0xffffffffu;
+            const unsigned ml = __reduce_min_sync(FDVB_FULL, lo);
+            const unsigned bc = __reduce_max_sync(FDVB_FULL, (valid && hi == mh && lo == ml) ? (unsigned)lane + 1u : 0u);
+            bestL = (int)bc - 2;
+        } else {
+            double bestJ = -1.0;
+            unsigned m = vmask;
+            while (m) {                                    // uniform across the warp
+                const int c = 31 - __clz(m);
+                m &= ~(1u << c);
+                const double Jc = __shfl_sync(FDVB_FULL, J, c);
+                if (bestJ < 0.0 || Jc < bestJ) { bestJ = Jc; bestL = c - 1; }
+            }
         }
         if (kz > bestL) levz = 0;
-        if (c_IZZ4[l] > bestL) lev = 0;
+        if (izz4(l) > bestL) lev = 0;
         last = bestL;
         __syncwarp();
     }
@@ -166,9 +190,9 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
     const bool in = lane < 16 && kz <= last;
     const int bits = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
     const int len = in ? leb_size(z) : 0;
-    const int end = warp_incl_scan(len, lane);
+    const int end = scan16(len, lane);
     if (in) leb_write(out->bytes + (end - len), z);
-    const int nbytes = __shfl_sync(FDVB_FULL, end, 31);
+    const int nbytes = __shfl_sync(FDVB_FULL, end, 15);
     if (lane == 0) {
         out->count = last + 1;
         out->nbytes = nbytes;
@@ -210,7 +234,7 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     {   // A[u][x] = sum_y C8[u][y] X[y][x]   (u = r, x = c)
         int32_t s = 0;
 #pragma unroll
-        for (int y = 0; y < 8; ++y) s += c_C8[r * 8 + y] * sc->X[y * 8 + c];
+        for (int y = 0; y < 8; ++y) s += c8(r * 8 + y) * sc->X[y * 8 + c];
         sc->A[t] = s;
     }
     bar_sync64(bar);
@@ -218,7 +242,7 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     {   // Y[u][v] = sum_x A[u][x] C8[v][x]   (u = r, v = c)
         int32_t s = 0;
 #pragma unroll
-        for (int x = 0; x < 8; ++x) s += sc->A[r * 8 + x] * c_C8[c * 8 + x];
+        for (int x = 0; x < 8; ++x) s += sc->A[r * 8 + x] * c8t(x * 8 + c);
         Yv = s;
     }
     const int32_t q = c_QSTEP8[qp], f = q / 3;
@@ -232,7 +256,7 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     {   // B[y][v] = sum_u C8[u][y] Y[u][v]   (y = r, v = c)
         long long s = 0;
 #pragma unroll
-        for (int u = 0; u < 8; ++u) s += (long long)c_C8[u * 8 + r] * sc->Y[u * 8 + c];
+        for (int u = 0; u < 8; ++u) s += (long long)c8(u * 8 + r) * sc->Y[u * 8 + c];
         sc->B[t] = s;
     }
     bar_sync64(bar);
@@ -240,14 +264,14 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     {   // X[y][x] = (sum_v B[y][v] C8[v][x] + 2^35) >> 36   (y = r, x = c)
         long long s = 0;
 #pragma unroll
-        for (int v = 0; v < 8; ++v) s += sc->B[r * 8 + v] * (long long)c_C8[v * 8 + c];
+        for (int v = 0; v < 8; ++v) s += sc->B[r * 8 + v] * (long long)c8(v * 8 + c);
         rr = (int16_t)((s + (1LL << 35)) >> 36);
     }
     const int rv = clipb(pv + rr);
     out->rec[t] = (uint8_t)rv;
     const int d = cv - rv;
     // zigzag view: thread k holds the level at zigzag position k
-    const int lz = sc->L[c_ZZ8[t]];
+    const int lz = sc->L[zz8(t)];
     const unsigned b = __ballot_sync(FDVB_FULL, lz != 0);
     const int ssd = __reduce_add_sync(FDVB_FULL, d * d);
     if (lane == 0) { sc->part[w][0] = b ? 32 * w + 31 - __clz(b) : -1; sc->part[w][1] = ssd; }
@@ -295,8 +319,8 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
 #pragma unroll
         for (int y = 0; y < 8; ++y) {
             const int32_t xv = sc->X[y * 8 + c];
-            a0 += c_C8[r0 * 8 + y] * xv;
-            a1 += c_C8[r1 * 8 + y] * xv;
+            a0 += c8(r0 * 8 + y) * xv;
+            a1 += c8(r1 * 8 + y) * xv;
         }
         sc->A[lane] = a0;
         sc->A[lane + 32] = a1;
@@ -306,7 +330,7 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
         int32_t y0 = 0, y1 = 0;
 #pragma unroll
         for (int x = 0; x < 8; ++x) {
-            const int32_t cx = c_C8[c * 8 + x];
+            const int32_t cx = c8t(x * 8 + c);
             y0 += sc->A[r0 * 8 + x] * cx;
             y1 += sc->A[r1 * 8 + x] * cx;
         }
@@ -325,8 +349,8 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const long long yd = sc->X[u * 8 + c];
-            b0 += (long long)c_C8[u * 8 + r0] * yd;
-            b1 += (long long)c_C8[u * 8 + r1] * yd;
+            b0 += (long long)c8(u * 8 + r0) * yd;
+            b1 += (long long)c8(u * 8 + r1) * yd;
         }
         sc->B[lane] = b0;
         sc->B[lane + 32] = b1;
@@ -337,7 +361,7 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
         long long s0 = 0, s1 = 0;
 #pragma unroll
         for (int v = 0; v < 8; ++v) {
-            const long long cc = c_C8[v * 8 + c];
+            const long long cc = c8(v * 8 + c);
             s0 += sc->B[r0 * 8 + v] * cc;
             s1 += sc->B[r1 * 8 + v] * cc;
         }
@@ -349,7 +373,7 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
     const int e0 = cv0 - rv0, e1 = cv1 - rv1;
     const int ssd = __reduce_add_sync(FDVB_FULL, e0 * e0 + e1 * e1);
     // zigzag view: lane k holds zigzag positions k and k + 32
-    const int lz0 = sc->L[c_ZZ8[lane]], lz1 = sc->L[c_ZZ8[lane + 32]];
+    const int lz0 = sc->L[zz8(lane)], lz1 = sc->L[zz8(lane + 32)];
     const unsigned m0 = __ballot_sync(FDVB_FULL, lz0 != 0), m1 = __ballot_sync(FDVB_FULL, lz1 != 0);
     const int last = m1 ? 63 - __clz(m1) : (m0 ? 31 - __clz(m0) : -1);
     const uint32_t z0 = zz_enc(lz0), z1 = zz_enc(lz1);

@@ -12,9 +12,13 @@
 //   file head        "FDV1" [version u8][kind u8][fps u16][payload_len u32]
 //                                                                   fdv.h:7448-7464
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -111,6 +115,109 @@ int default_threads() {
     return hc ? (int)hc : 1;
 }
 
+// A fixed team of host threads (the caller plus n - 1 workers) that runs the
+// tasks 0..ntasks-1 of one job at a time; run() returns when all are done.
+class Pool {
+  public:
+    explicit Pool(int n) {
+        for (int i = 1; i < n; ++i) th_.emplace_back([this] { work(); });
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            quit_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void run(int ntasks, const std::function<void(int)> &fn) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            fn_ = &fn;
+            ntasks_ = ntasks;
+            next_.store(0);
+            left_ = ntasks;
+            ++gen_;
+        }
+        cv_.notify_all();
+        drain();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [this] { return left_ == 0; });
+        fn_ = nullptr;
+    }
+
+  private:
+    void drain() {
+        for (;;) {
+            const int i = next_.fetch_add(1);
+            if (i >= ntasks_) return;
+            (*fn_)(i);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--left_ == 0) done_cv_.notify_all();
+        }
+    }
+    void work() {
+        long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+                if (quit_) return;
+                seen = gen_;
+            }
+            drain();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)> *fn_ = nullptr;
+    std::atomic<int> next_{0};
+    int ntasks_ = 0, left_ = 0;
+    long gen_ = 0;
+    bool quit_ = false;
+};
+
+// Engines are kept between calls (keyed by device, search range and unit
+// sizes): creating one allocates device and pinned memory, which costs more
+// than coding a short clip.  Taken out while in use; at most kCacheMax kept.
+struct CachedEngine {
+    int device, range;
+    std::vector<int> w, h;
+    fdvb_engine *E;
+};
+constexpr size_t kCacheMax = 4;
+std::mutex g_cache_mu;
+std::vector<CachedEngine> *g_cache = new std::vector<CachedEngine>();   // never destroyed: outlives the CUDA runtime
+
+fdvb_engine *engine_acquire(int n, const int *w, const int *h, int range, int device) {
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (size_t i = 0; i < g_cache->size(); ++i) {
+            CachedEngine &c = (*g_cache)[i];
+            if (c.device == device && c.range == range && (int)c.w.size() == n &&
+                std::equal(c.w.begin(), c.w.end(), w) && std::equal(c.h.begin(), c.h.end(), h)) {
+                fdvb_engine *E = c.E;
+                g_cache->erase(g_cache->begin() + (long)i);
+                return E;
+            }
+        }
+    }
+    return fdvb_engine_create(n, w, h, range, device);
+}
+void engine_release(fdvb_engine *E, int n, const int *w, const int *h, int range, int device) {
+    fdvb_engine *evict = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        g_cache->push_back({device, range, std::vector<int>(w, w + n), std::vector<int>(h, h + n), E});
+        if (g_cache->size() > kCacheMax) {
+            evict = g_cache->front().E;
+            g_cache->erase(g_cache->begin());
+        }
+    }
+    if (evict) fdvb_engine_destroy(evict);
+}
+
 }  // namespace
 
 struct fdv_encoder {
@@ -124,6 +231,15 @@ struct fdv_encoder {
 extern "C" {
 
 const char *fdvb_last_error(void) { return g_api_err.c_str(); }
+
+void fdvb_release_engines(void) {
+    std::vector<CachedEngine> v;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        v.swap(*g_cache);
+    }
+    for (auto &c : v) fdvb_engine_destroy(c.E);
+}
 
 int fdvb_set_search_range(int range) {
     if (range != 16 && range != 32 && range != 64) { set_err("search range must be 16, 32 or 64"); return -1; }
@@ -154,13 +270,15 @@ size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payl
 }
 
 // Encode nframes over a set of horizontal bands (nbands == 1: the plain
-// stream) and leave each band's video stream in us[b].bytes.
+// stream) and leave each band's video stream in us[b].bytes.  The GPU analyses
+// frame f while the host entropy-codes frame f - 1 (bands in parallel).
 static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
                         int bh_full, int nthreads, std::vector<UnitStream> &us) {
     const int nb = (h + bh_full - 1) / bh_full, cw = w / 2, ch = h / 2;
     std::vector<int> W(nb, w), H(nb), Y0(nb);
     for (int b = 0; b < nb; ++b) { Y0[b] = b * bh_full; H[b] = std::min(bh_full, h - Y0[b]); }
-    fdvb_engine *E = fdvb_engine_create(nb, W.data(), H.data(), g_range, g_device);
+    const int range = g_range, device = g_device;
+    fdvb_engine *E = engine_acquire(nb, W.data(), H.data(), range, device);
     if (!E) { set_engine_err(); return -1; }
     us.clear();
     us.resize(nb);
@@ -171,20 +289,35 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     }
     std::vector<const uint8_t *> planes(3 * nb);
     std::vector<int> intra(nb), qps(nb, qp);
-    int rc = 0;
-    for (int f = 0; f < nframes && rc == 0; ++f) {
-        const uint8_t *fy = frames[f], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
-        const int is_intra = (f == 0) || (keyint > 0 && f % keyint == 0);
-        for (int b = 0; b < nb; ++b) {
-            planes[3 * b] = fy + (size_t)Y0[b] * w;
-            planes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
-            planes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
-            intra[b] = is_intra;
+    Pool pool(std::max(1, std::min(nthreads, nb)));
+    std::vector<int> urc(nb);
+    int rc = 0, inflight = 0, prev_intra = 0;
+    for (int f = 0; f <= nframes && rc == 0; ++f) {
+        int is_intra = 0;
+        if (f < nframes) {
+            const uint8_t *fy = frames[f], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+            is_intra = (f == 0) || (keyint > 0 && f % keyint == 0);
+            for (int b = 0; b < nb; ++b) {
+                planes[3 * b] = fy + (size_t)Y0[b] * w;
+                planes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+                planes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+                intra[b] = is_intra;
+            }
+            if (fdvb_engine_submit(E, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) { set_engine_err(); rc = -1; break; }
+            ++inflight;
         }
-        if (fdvb_engine_step(E, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) { set_engine_err(); rc = -1; break; }
-        if (code_all(E, us, is_intra, qp, nthreads) != 0) { set_err("entropy coding failed"); rc = -1; }
+        if (f > 0) {
+            --inflight;
+            if (fdvb_engine_collect(E) != 0) { set_engine_err(); rc = -1; break; }
+            std::fill(urc.begin(), urc.end(), 0);
+            pool.run(nb, [&](int u) { urc[u] = code_unit_frame(E, u, us[u], prev_intra, qp); });
+            for (int r : urc) if (r) { set_err("entropy coding failed"); rc = -1; }
+        }
+        prev_intra = is_intra;
     }
-    fdvb_engine_destroy(E);
+    while (inflight-- > 0) fdvb_engine_collect(E);
+    if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
+    else fdvb_engine_destroy(E);
     return rc;
 }
 

@@ -12,6 +12,9 @@ void fdvb_engine_destroy(fdvb_engine *E);
 int fdvb_engine_units(const fdvb_engine *E);
 int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
                      const double *lscale, const int *force_skip);
+int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                       const double *lscale, const int *force_skip);
+int fdvb_engine_collect(fdvb_engine *E);
 const fdvb_streams *fdvb_engine_pstreams(fdvb_engine *E, int unit);
 const fdvb_streams *fdvb_engine_istreams(fdvb_engine *E, int unit, int plane);
 int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420);
