@@ -35,7 +35,7 @@
 namespace fdvb {
 // kernels (pframe.cu, iframe.cu, frame_ops.cu)
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, cudaStream_t st);
+                   unsigned long long wait_ns, int grid, int range, cudaStream_t st);
 struct IPlaneDev;
 struct ITask;
 size_t iframe_smem_bytes();
@@ -459,7 +459,7 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
                            cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)rows.size(), E->nsm);
         CK(cudaEventRecord(SL.ev[1], E->st));
-        launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->st);
+        launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range, E->st);
         CK(cudaGetLastError());
         CK(cudaEventRecord(SL.ev[2], E->st));
         E->launches += 1;

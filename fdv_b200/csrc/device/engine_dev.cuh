@@ -21,7 +21,8 @@ struct UnitDev {
 };
 
 // Phases of a macroblock, for the optional cycle profile.
-enum { PP_WAIT = 0, PP_LOAD, PP_SKIP, PP_SEARCH, PP_RESID, PP_DECIDE, PP_COMMIT, PP_OUT, PP_NMB, PP_NSKIP, PP_N = 16 };
+enum { PP_WAIT = 0, PP_LOAD, PP_SKIP, PP_SEARCH, PP_RESID, PP_DECIDE, PP_COMMIT, PP_OUT, PP_NMB, PP_NSKIP,
+       PP_G0, PP_G1, PP_G2, PP_G3, PP_IT16, PP_IT8, PP_N = 16 };
 
 struct RowTask { int unit, row; };
 

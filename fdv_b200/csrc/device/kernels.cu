@@ -4,6 +4,9 @@
 // engine uses.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
+
 #include "common.cuh"
 #include "frame_ops.cuh"
 #include "iframe.cuh"
@@ -36,15 +39,27 @@ void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticke
                                                 ntasks, ticket, err, wait_ns);
 }
 
+// The P-frame kernel stages the references' luma in shared memory when the
+// search range allows it (up to 32); a range of 64 reads them from global
+// memory.  All units of one launch share the range.
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, cudaStream_t st) {
-    static bool attr = false;
-    const size_t smem = sizeof(PShared);
-    if (!attr) {
-        cudaFuncSetAttribute(pframe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
+                   unsigned long long wait_ns, int grid, int range, cudaStream_t st) {
+    static std::mutex mu;
+    static bool attr[64][2] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool win = range <= 32;
+    const size_t smem = win ? (size_t)kPWinOff + kPWinBytes : sizeof(PShared);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64 && !attr[dev][win]) {
+            if (win) cudaFuncSetAttribute(pframe_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            else cudaFuncSetAttribute(pframe_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr[dev][win] = true;
+        }
     }
-    pframe_kernel<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
+    if (win) pframe_kernel<true><<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
+    else pframe_kernel<false><<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
 }
 
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st) {
@@ -235,7 +250,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     if (!ok) return static_fail("descriptor upload failed");
     launch_refprep(base + o_prep, far_ref ? 2 : 1, w, h, B, st);
     launch_pframe(reinterpret_cast<const UnitDev *>(base + o_unit), reinterpret_cast<const RowTask *>(base + o_rows),
-                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, st);
+                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, range, st);
     launch_deblock(base + o_db, 3, st);
     launch_compact(base + o_cmp, 1, err, st);
     if (cudaGetLastError() != cudaSuccess) return static_fail("kernel launch failed");

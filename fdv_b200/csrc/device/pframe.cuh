@@ -53,7 +53,7 @@ struct PShared {
     int isel;
     int satd[64];
     NNPred nn[4];
-    int gsad[4][8];
+    int gsad[4][16];
     // phase 2: regions 0-3 nearest ref, 4-7 second ref, 8-11 intra, 12-15 INTER8 quadrants
     Blk4 blk[64];
     uint8_t recA[16][64];
@@ -96,18 +96,70 @@ __device__ void write_slot_structs(uint8_t *slot, int k, const uint8_t *b, int n
 }
 
 // 16x16 prediction of a group of 128 threads (threads 0..63 one word each).
-__device__ __forceinline__ void mc16_group(const RefPlanes &R, int bx, int by, int mvx, int mvy, uint8_t *dst, int gt) {
+template <class Src>
+__device__ __forceinline__ void mc16_group(const Src &R, int bx, int by, int mvx, int mvy, uint8_t *dst, int gt) {
     if (gt < 64) {
         const int row = gt >> 2, col = (gt & 3) * 4, ph = (mvy & 3) * 4 + (mvx & 3);
         reinterpret_cast<uint32_t *>(dst)[gt] = mc_word(R, bx + col + (mvx >> 2), by + row + (mvy >> 2), ph);
     }
 }
 
+// ----------------------------------------------- reference window --
+// With a search range up to 32 the luma planes of both references around the
+// current macroblock are staged in shared memory: a ring of kWinRing columns
+// (eight 16-column strips) by 2 * range + 23 rows per plane, which covers every
+// sample a vector within the search range (plus the quarter-pel refinement
+// and the interpolation taps) can touch.  Macroblock x reads strips x-3..x+3;
+// while it runs, strip x+4 is copied in (cp.async) for macroblock x+1, into the
+// ring slot of strip x-4, which is no longer read.
+constexpr int kPWinOff = (int)((sizeof(PShared) + 127) / 128 * 128);
+constexpr int kPWinBytes = 8 * kWinPlane;   // 2 references x 4 planes
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copy strips s0..s1 (clipped to the padded plane) of the window rows
+// wy0 .. wy0 + wrows - 1 of nref references (all threads; one commit group).
+__device__ void win_fill(uint8_t *win, const UnitDev &U, int nref, int s0, int s1, int wy0, int wrows, int tid) {
+    const int B = U.range + 16, smin = -B / 16, smax = (U.w + B) / 16 - 1;
+    s0 = s0 < smin ? smin : s0;
+    s1 = s1 > smax ? smax : s1;
+    if (s1 >= s0) {
+        const int per = nref * 4 * wrows, total = (s1 - s0 + 1) * per;
+        for (int i = tid; i < total; i += PNT) {
+            const int si = i / per, rem = i - si * per, pr = rem / wrows, row = rem - pr * wrows;
+            const int r = pr >> 2, p = pr & 3, x = 16 * (s0 + si);
+            const RefPlanes &RP = U.ref[r];
+            const uint8_t *pl = p == 0 ? RP.G : (p == 1 ? RP.B : (p == 2 ? RP.H : RP.J));
+            cp_async16(win + (r * 4 + p) * kWinPlane + row * kWinStride + (x & (kWinRing - 1)),
+                       pl + (long)(wy0 + row) * RP.ys + x);
+        }
+    }
+    cp_async_commit();
+}
+
+template <bool WIN> struct LumaOf { using T = GlobalLuma; };
+template <> struct LumaOf<true> { using T = WindowLuma; };
+template <bool WIN>
+__device__ __forceinline__ typename LumaOf<WIN>::T luma_src(const RefPlanes &R, const uint8_t *win, int r, int wy0, int wrows);
+template <>
+__device__ __forceinline__ GlobalLuma luma_src<false>(const RefPlanes &R, const uint8_t *, int, int, int) { return GlobalLuma(R); }
+template <>
+__device__ __forceinline__ WindowLuma luma_src<true>(const RefPlanes &, const uint8_t *win, int r, int wy0, int wrows) {
+    return WindowLuma{win + r * 4 * kWinPlane, wy0, wrows - 1};
+}
+
+template <bool WIN>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
               int *ticket, unsigned *err, unsigned long long wait_ns) {
-    extern __shared__ __align__(16) uint8_t psmem[];
+    extern __shared__ __align__(128) uint8_t psmem[];
     PShared &S = *reinterpret_cast<PShared *>(psmem);
+    uint8_t *win = psmem + kPWinOff;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int grp = warp >> 2, gw = warp & 3, gt = tid & 127;
     if (tid < 4) cs_init(&S.sink[tid], S.sinkmem[tid], c_CsCap);
@@ -117,7 +169,10 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         __syncthreads();
         const int t = S.task;
         __syncthreads();
-        if (t >= nrows) return;
+        if (t >= nrows) {
+            if (WIN) cp_async_wait_all();
+            return;
+        }
         const UnitDev &U = units[rows[t].unit];
         const int row = rows[t].row, w = U.w, cw = w / 2, mbw = U.mbw;
         if (row == U.stall_row) continue;   // injected stall: this row's progress flag is never set
@@ -125,16 +180,26 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const int qp = U.qp, R = U.range, navail = U.navail;
         const double lam14 = __dmul_rn(lambda, 14.0), lam16 = __dmul_rn(lambda, 16.0), lam19 = __dmul_rn(lambda, 19.0);
         qp4_setup(&S.q, qp, tid);
+        const int nref = navail > 1 ? 2 : 1, wy0 = row * 16 - R - 3, wrows = 2 * R + 23;
+        if (WIN) {
+            cp_async_wait_all();   // this block's copies for an earlier row have landed
+            __syncthreads();
+            win_fill(win, U, nref, -3, 4, wy0, wrows, tid);   // macroblock 0's strips and macroblock 1's
+        }
+        const typename LumaOf<WIN>::T L0 = luma_src<WIN>(U.ref[0], win, 0, wy0, wrows);
+        const typename LumaOf<WIN>::T L1 = luma_src<WIN>(U.ref[1], win, nref - 1, wy0, wrows);
         int pmvx = 0, pmvy = 0;
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
             pc.start();
+            if (WIN) cp_async_wait_all();   // this thread's strip copies; the barrier below publishes them
             if (row > 0) {
                 if (tid == 0) S.row_ok = wait_at_least(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
             } else if (tid == 0) S.row_ok = 1;
             __syncthreads();
             if (!S.row_ok) break;
+            if (WIN && mbx >= 1) win_fill(win, U, nref, mbx + 4, mbx + 4, wy0, wrows, tid);
             pc.mark(PP_WAIT);
             uint8_t *slot = U.slots + (size_t)(row * mbw + mbx) * kSlotBytes;
             if (tid < 16) slot_len(slot)[tid] = 0;
@@ -217,7 +282,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const MBInfo &c = S.cand[mi];
                 const int r2 = k >> 2, c2 = (k & 3) * 4, ph = (c.y & 3) * 4 + (c.x & 3);
                 reinterpret_cast<uint32_t *>(S.predS[mi])[k] =
-                    mc_word(U.ref[c.ref], bx + c2 + (c.x >> 2), by + r2 + (c.y >> 2), ph);
+                    mc_word(c.ref ? L1 : L0, bx + c2 + (c.x >> 2), by + r2 + (c.y >> 2), ph);
             }
             __syncthreads();
             if (warp < ncand) {
@@ -238,31 +303,33 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             int chosen = 0, best_ref = 0, mvx = 0, mvy = 0, best_sub = 0;
             if (!skip_wins) {
                 // ---- phase 1: searches on four warp groups
+                const long long tg0 = (U.prof && gt == 0) ? clock64() : 0;
                 if (grp == 0) {
                     int mx, my;
-                    int sd = me_search_group<16>(S.cur, U.ref[0], bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9);
+                    int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
+                                                 U.prof ? &U.prof[PP_IT16] : nullptr);
                     if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
-                    mc16_group(U.ref[0], bx, by, mx, my, S.pr[0], gt);
+                    mc16_group(L0, bx, by, mx, my, S.pr[0], gt);
                 } else if (grp == 1) {
                     if (navail > 1) {
                         int mx, my;
-                        int sd = me_search_group<16>(S.cur, U.ref[1], bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10);
+                        int sd = me_search_group<16>(S.cur, L1, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10);
                         if (gt == 0) { S.mv[1][0] = mx; S.mv[1][1] = my; S.sad[1] = sd; }
-                        mc16_group(U.ref[1], bx, by, mx, my, S.pr[1], gt);
+                        mc16_group(L1, bx, by, mx, my, S.pr[1], gt);
                     }
                 } else if (grp == 2) {
                     int qpx = pmvx, qpy = pmvy, ssad = 0;
                     for (int q = 0; q < 4; ++q) {
                         const int qx = (q & 1) * 8, qy = (q >> 1) * 8;
                         int mx, my;
-                        ssad += me_search_group<8>(S.cur + qy * 16 + qx, R0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
-                                                   S.gsad[2], gw, lane, 11);
+                        ssad += me_search_group<8>(S.cur + qy * 16 + qx, L0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
+                                                   S.gsad[2], gw, lane, 11, U.prof ? &U.prof[PP_IT8] : nullptr);
                         if (gt == 0) { S.qmv[q][0] = mx; S.qmv[q][1] = my; }
                         qpx = mx; qpy = my;
                         if (gt < 16) {
                             const int r2 = gt >> 1, c2 = (gt & 1) * 4, ph = (my & 3) * 4 + (mx & 3);
                             reinterpret_cast<uint32_t *>(S.pred8[q])[gt] =
-                                mc_word(R0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
+                                mc_word(L0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
                         }
                     }
                     if (gt == 0) S.ssad = ssad;
@@ -288,6 +355,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     if (sel >= 0)
                         for (int p = gt; p < 256; p += 128) S.pr[2][p] = (uint8_t)nn_px(S.nn[sel], S.top, S.left, p & 15, p >> 4);
                 }
+                if (U.prof && gt == 0) atomicAdd(&U.prof[PP_G0 + grp], (unsigned long long)(clock64() - tg0));
                 __syncthreads();
                 pc.mark(PP_SEARCH);
                 // ---- phase 2: residuals of every candidate at once
