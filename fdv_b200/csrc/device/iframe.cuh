@@ -566,9 +566,11 @@ __device__ void chain_row(IShared *S, const IPlaneDev &P, int r, unsigned *err, 
             const int len = t < IS_NS ? C.out.slen[t] : C.out.c.len[t - IS_NS];
             reinterpret_cast<uint16_t *>(slot)[t] = (uint16_t)len;
         }
-        __threadfence();
-        cbar();
-        if (t == 0) atomicExch(&P.progress[r], col + 1);
+        cbar();   // orders the chain's writes before thread 0's fence and flag
+        if (t == 0) {
+            __threadfence();
+            atomicExch(&P.progress[r], col + 1);
+        }
         prof_add(c.prof, t, IP_CTU, tc);
         if (c.prof && t == 0) atomicAdd(&c.prof[IP_NCTU], 1ull);
     }

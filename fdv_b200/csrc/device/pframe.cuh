@@ -72,7 +72,7 @@ struct PShared {
     RegDec cdec[2];
     long long ce;
     int cb;
-    int task, row_ok;
+    int task, row_ok, amode;
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -188,7 +188,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         }
         const typename LumaOf<WIN>::T L0 = luma_src<WIN>(U.ref[0], win, 0, wy0, wrows);
         const typename LumaOf<WIN>::T L1 = luma_src<WIN>(U.ref[1], win, nref - 1, wy0, wrows);
-        int pmvx = 0, pmvy = 0;
+        int pmvx = 0, pmvy = 0, prev_mode = 0;
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
@@ -221,6 +221,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 S.ctop[pl][q] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q]) : 0;
                 S.cleft[pl][q] = cbx > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1]) : 0;
             } else if (tid == 128) {
+                // the above and above-right macroblock records (one 8-byte load
+                // each, issued together with the corner samples)
+                uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
+                for (int k = 0; k < 2; ++k)
+                    if (row > 0 && mbx + k < mbw)
+                        nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
                 S.ht = by > 0; S.hl = bx > 0;
                 S.tl = (by > 0 && bx > 0) ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
                 for (int pl = 0; pl < 2; ++pl)
@@ -229,12 +235,10 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 int n = 1;
                 S.cand[0].x = (int16_t)pmvx; S.cand[0].y = (int16_t)pmvy; S.cand[0].ref = 0; S.cand[0].inter = 1;
                 for (int k = 0; k < 2 && n < 3; ++k) {
-                    const int cx = mbx + k, cy = row - 1;
-                    if (cy < 0 || cx >= mbw) continue;
-                    const MBInfo *mp = &U.mbi[cy * mbw + cx];
+                    if (row == 0 || mbx + k >= mbw) continue;
                     MBInfo m;
-                    m.x = (int16_t)__ldcg(&mp->x); m.y = (int16_t)__ldcg(&mp->y);
-                    m.ref = ldcg8(&mp->ref); m.inter = ldcg8(&mp->inter);
+                    m.x = (int16_t)(nb[k].x & 0xffffu); m.y = (int16_t)(nb[k].x >> 16);
+                    m.ref = (uint8_t)(nb[k].y & 0xffu); m.inter = (uint8_t)((nb[k].y >> 8) & 0xffu);
                     if (!m.inter) continue;
                     bool dup = false;
                     for (int j2 = 0; j2 < n; ++j2)
@@ -242,14 +246,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     if (!dup) S.cand[n++] = m;
                 }
                 S.ncand = n;
+                S.amode = row > 0 ? (int)((nb[0].y >> 16) & 0xffu) : 0;
             }
             __syncthreads();
-            int ctx;   // mode context (fdv.h:4172): left / above macroblock skipped-ness
-            {
-                const int Lm = mbx > 0 ? ldcg8(&U.mbi[row * mbw + mbx - 1].mode) : 0;
-                const int Am = row > 0 ? ldcg8(&U.mbi[(row - 1) * mbw + mbx].mode) : 0;
-                ctx = (Lm != 0 ? 2 : 0) + (Am != 0 ? 1 : 0);
-            }
+            // mode context (fdv.h:4172): left / above macroblock skipped-ness;
+            // the left one is this block's previous macroblock
+            const int ctx = (prev_mode != 0 ? 2 : 0) + (S.amode != 0 ? 1 : 0);
             const RefPlanes &R0 = U.ref[0];
             if (U.force_skip) {
                 // A held frame: SKIP with the zero vector everywhere (fdv.h:5820-5836).
@@ -269,9 +271,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     U.mbi[row * mbw + mbx] = mi;
                 }
                 pmvx = 0; pmvy = 0;
-                __threadfence();
+                prev_mode = 0;
                 __syncthreads();
-                if (tid == 0) atomicExch(&U.progress[row], mbx + 1);
+                if (tid == 0) {
+                    __threadfence();
+                    atomicExch(&U.progress[row], mbx + 1);
+                }
                 continue;
             }
             pc.mark(PP_LOAD);
@@ -398,10 +403,19 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 }
                 __syncthreads();
                 pc.mark(PP_RESID);
-                for (int c = 0; c < 4; ++c) {
-                    if (!((pres >> (4 * c)) & 1u)) continue;
-                    decide_regions<PNT>(4, &S.blk[16 * c], &S.reg[4 * c], &S.dec[4 * c], lambda, false, &S.sink[c],
-                                        &S.cD[c], &S.cB[c], err);
+                {   // region decisions (fdv.h:5379-5411): candidate c on warp group c
+                    const int c = grp;
+                    if ((pres >> (4 * c)) & 1u) {
+                        if (gt < 4) region_choice(&S.blk[4 * (4 * c + gt)], S.reg[4 * c + gt], lambda, S.dec[4 * c + gt]);
+                        gbar(9 + grp, 128);
+                        if (gt == 0) {
+                            S.cD[c] = 0;
+                            S.cB[c] = 0;
+                            region_offsets(&S.dec[4 * c], 4, &S.sink[c], false, &S.cD[c], &S.cB[c], err);
+                        }
+                        gbar(9 + grp, 128);
+                        region_symbols(S.dec[4 * c + gw], &S.blk[4 * (4 * c + gw)], S.reg[4 * c + gw], &S.sink[c], false, lane);
+                    }
                 }
                 __syncthreads();
                 pc.mark(PP_DECIDE);
@@ -610,9 +624,14 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 }
             }
             if (tid == 0) U.mbi[row * mbw + mbx] = info;
-            __threadfence();
+            prev_mode = chosen;
+            // the block's writes are ordered before thread 0's fence by the
+            // barrier; the fence then orders them before the progress flag
             __syncthreads();
-            if (tid == 0) atomicExch(&U.progress[row], mbx + 1);
+            if (tid == 0) {
+                __threadfence();
+                atomicExch(&U.progress[row], mbx + 1);
+            }
             pc.mark(PP_OUT);
         }
         __syncthreads();
