@@ -58,8 +58,9 @@ struct PShared {
     Blk4 blk[64];
     uint8_t recA[16][64];
     Reg8 reg[16];
-    Reg8Scratch r8[8];
-    Blk4Scratch b4[16];
+    Reg8WScratch r8w[16];        // per warp: a region's 8x8 option
+    Reg8Scratch r8[2];           // chroma 8x8 options (64 threads each)
+    Blk4Scratch b4[32];          // per warp, two per warp for paired blocks
     RegDec dec[16];
     CoefSink sink[4];
     uint8_t sinkmem[4][kCsBytes];
@@ -372,22 +373,25 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const bool need8 = !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
                 const unsigned pres = 0xFu | (have1 ? 0xF0u : 0u) | (haveI ? 0xF00u : 0u) | (need8 ? 0xF000u : 0u);
                 if (tid < 4) cs_reset(&S.sink[tid]);
-                for (int b = warp; b < 64; b += 16) {
-                    const int g = b >> 2, s = b & 3;
+                // 32 block pairs (4x4 blocks 0-1 and 2-3 of region g, one per
+                // half-warp) and the 16 regions' 8x8 options: three warp tasks each
+                for (int pi = warp; pi < 32; pi += 16) {
+                    const int g = pi >> 1, s0 = (pi & 1) * 2, sy = (s0 >> 1) * 4;
                     if (!((pres >> g) & 1u)) continue;
-                    const int sx = (s & 1) * 4, sy = (s >> 1) * 4;
+                    const uint8_t *cp, *pp;
+                    int pstr;
                     if (g < 12) {
                         const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
-                        warp_block4(S.cur + (ry + sy) * 16 + rx + sx, 16, S.pr[c] + (ry + sy) * 16 + rx + sx, 16,
-                                    &S.recA[g][sy * 8 + sx], 8, S.q, lambda, true, &S.blk[b], &S.b4[warp], lane);
+                        cp = S.cur + (ry + sy) * 16 + rx; pp = S.pr[c] + (ry + sy) * 16 + rx; pstr = 16;
                     } else {
                         const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                        warp_block4(S.cur + (qy + sy) * 16 + qx + sx, 16, S.pred8[q] + sy * 8 + sx, 8,
-                                    &S.recA[g][sy * 8 + sx], 8, S.q, lambda, true, &S.blk[b], &S.b4[warp], lane);
+                        cp = S.cur + (qy + sy) * 16 + qx; pp = S.pred8[q] + sy * 8; pstr = 8;
                     }
+                    warp_block4x2(cp, cp + 4, 16, pp, pp + 4, pstr, &S.recA[g][sy * 8], &S.recA[g][sy * 8 + 4], 8, S.q,
+                                  lambda, true, &S.blk[4 * g + s0], &S.blk[4 * g + s0 + 1], &S.b4[2 * warp], lane);
                 }
-                for (int round = 0; round < 2; ++round) {
-                    const int g = round * 8 + (tid >> 6);
+                {
+                    const int g = warp;
                     if ((pres >> g) & 1u) {
                         const uint8_t *cp, *pp;
                         int pstr;
@@ -398,7 +402,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                             const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
                             cp = S.cur + qy * 16 + qx; pp = S.pred8[q]; pstr = 8;
                         }
-                        region8(cp, 16, pp, pstr, qp, &S.reg[g], &S.r8[tid >> 6], tid & 63, 1 + (tid >> 6));
+                        warp_region8(cp, 16, pp, pstr, qp, &S.reg[g], &S.r8w[warp], lane);
                     }
                 }
                 __syncthreads();

@@ -202,6 +202,147 @@ __device__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int
     __syncwarp();
 }
 
+// Sum of v over the 16 lanes of this lane's half-warp (two predicated warp
+// reductions, independent of each other).
+__device__ __forceinline__ int half_sum(int v, int lane) {
+    const int lo = __reduce_add_sync(FDVB_FULL, lane < 16 ? v : 0);
+    const int hi = __reduce_add_sync(FDVB_FULL, lane < 16 ? 0 : v);
+    return lane < 16 ? lo : hi;
+}
+
+// Two 4x4 blocks on one warp, block h on half-warp h (lanes 16h..16h+15),
+// with the same results as warp_block4 on each (fdv.h:5214-5278, RDOQ
+// fdv.h:2493-2536).  In a half, lane l owns raster position l and zigzag
+// position l; the RDOQ truncation candidates L = -1..14 sit on lanes 0..15 of
+// the half, the candidate that keeps every level (L = 15, possible only when
+// the last level is at 15) is scored from the half's lane-parallel inverse.
+// The reference's choice (bestJ < 0.0 || J < bestJ over L = last .. -1) is a
+// per-half minimum, ties to the highest L, when no cost is negative, and is
+// replayed step by step otherwise.  sc holds two scratch entries.
+__device__ void warp_block4x2(const uint8_t *cur0, const uint8_t *cur1, int cs, const uint8_t *pred0,
+                              const uint8_t *pred1, int ps, uint8_t *rec0, uint8_t *rec1, int rs, const QP4 &Q,
+                              double lambda, bool rdoq, Blk4 *out0, Blk4 *out1, Blk4Scratch *sc, int lane) {
+    const int h = lane >> 4, hb = lane & 16, l = lane & 15, i = l >> 2, j = l & 3;
+    const uint8_t *cur = h ? cur1 : cur0, *pred = h ? pred1 : pred0;
+    const int cv = cur[i * cs + j], pv = pred[i * ps + j];
+    const int res = cv - pv;
+    int x0 = __shfl_sync(FDVB_FULL, res, hb + i * 4 + 0), x1 = __shfl_sync(FDVB_FULL, res, hb + i * 4 + 1);
+    int x2 = __shfl_sync(FDVB_FULL, res, hb + i * 4 + 2), x3 = __shfl_sync(FDVB_FULL, res, hb + i * 4 + 3);
+    const int t = fwd1(x0, x1, x2, x3, j);
+    int y0 = __shfl_sync(FDVB_FULL, t, hb + 0 * 4 + j), y1 = __shfl_sync(FDVB_FULL, t, hb + 1 * 4 + j);
+    int y2 = __shfl_sync(FDVB_FULL, t, hb + 2 * 4 + j), y3 = __shfl_sync(FDVB_FULL, t, hb + 3 * 4 + j);
+    const int coef = fwd1(y0, y1, y2, y3, i);
+    int lev;
+    {
+        const int sign = coef < 0 ? -1 : 1;
+        const long long aw = coef < 0 ? -(long long)coef : (long long)coef;
+        lev = (int16_t)(sign * (int)((aw * Q.mf[l] + Q.f) >> Q.qbits));
+    }
+    int levz = __shfl_sync(FDVB_FULL, lev, hb + zz4(l));
+    const unsigned nzm = (__ballot_sync(FDVB_FULL, levz != 0) >> hb) & 0xffffu;
+    int last = nzm ? 31 - __clz(nzm) : -1;
+    // the inverse of the levels as quantised (also the L = 15 candidate)
+    auto inverse = [&](int lv) {
+        const int dq = lv * Q.dq[l];
+        const int d0 = __shfl_sync(FDVB_FULL, dq, hb + i * 4 + 0), d1 = __shfl_sync(FDVB_FULL, dq, hb + i * 4 + 1);
+        const int d2 = __shfl_sync(FDVB_FULL, dq, hb + i * 4 + 2), d3 = __shfl_sync(FDVB_FULL, dq, hb + i * 4 + 3);
+        const int u = inv1(d0, d1, d2, d3, j);
+        const int e0 = __shfl_sync(FDVB_FULL, u, hb + 0 * 4 + j), e1 = __shfl_sync(FDVB_FULL, u, hb + 1 * 4 + j);
+        const int e2 = __shfl_sync(FDVB_FULL, u, hb + 2 * 4 + j), e3 = __shfl_sync(FDVB_FULL, u, hb + 3 * 4 + j);
+        return (int)(int16_t)((inv1(e0, e1, e2, e3, i) + 32) >> 6);
+    };
+    if (rdoq && __any_sync(FDVB_FULL, last >= 0)) {
+        const uint32_t z = zz_enc(levz);
+        const bool in = l <= last;
+        const int bits0 = bits_val((uint32_t)(last + 1)) + half_sum(in ? bits_val(z) : 0, lane);
+        const int pre = scan16(in ? 8 * leb_size(z) : 0, lane);
+        const int tot = __shfl_sync(FDVB_FULL, pre, hb + 15);
+        const int L = l - 1;
+        int preL = __shfl_sync(FDVB_FULL, pre, hb + (L < 0 ? 0 : L));
+        if (L < 0) preL = 0;
+        const int bitsL = bits0 - (tot - preL);
+        const unsigned vmask = 1u | (nzm << 1);           // candidate c = L + 1, c = 0..16
+        const bool active = last >= 0;                      // this half truncates at all
+        const bool valid = active && ((vmask >> l) & 1u);
+        sc[h].res[l] = res;
+        sc[h].lev[l] = lev;
+        __syncwarp();
+        double J = 0.0;
+        if (valid) {
+            int d[16], r[16];
+#pragma unroll
+            for (int p = 0; p < 16; ++p) d[p] = (izz4(p) <= L ? sc[h].lev[p] : 0) * Q.dq[p];
+            idct4_thread(d, r);
+            int D = 0;
+#pragma unroll
+            for (int p = 0; p < 16; ++p) { const int e = sc[h].res[p] - r[p]; D += e * e; }
+            J = rd_cost((double)D, lambda, bitsL);
+        }
+        // candidate L = 15: every level kept
+        const bool v16 = active && ((vmask >> 16) & 1u);
+        double J16 = 0.0;
+        if (__any_sync(FDVB_FULL, v16)) {
+            const int e = res - inverse(lev);
+            const int D16 = half_sum(e * e, lane);
+            J16 = rd_cost((double)D16, lambda, bits0);
+        }
+        int bestL = last;
+        const bool neg = (valid && J < 0.0) || (v16 && J16 < 0.0);
+        if (!__any_sync(FDVB_FULL, neg)) {
+            // the minimum, ties to the highest candidate; non-negative doubles
+            // order like their bit patterns
+            const unsigned long long jb = (unsigned long long)__double_as_longlong(J);
+            const unsigned hi = valid ? (unsigned)(jb >> 32) : 0xffffffffu;
+            const unsigned mh0 = __reduce_min_sync(FDVB_FULL, h == 0 ? hi : 0xffffffffu);
+            const unsigned mh1 = __reduce_min_sync(FDVB_FULL, h == 1 ? hi : 0xffffffffu);
+            const unsigned mh = h ? mh1 : mh0;
+            const unsigned lo = (valid && hi == mh) ? (unsigned)jb : 0xffffffffu;
+            const unsigned ml0 = __reduce_min_sync(FDVB_FULL, h == 0 ? lo : 0xffffffffu);
+            const unsigned ml1 = __reduce_min_sync(FDVB_FULL, h == 1 ? lo : 0xffffffffu);
+            const unsigned ml = h ? ml1 : ml0;
+            const unsigned ck = (valid && hi == mh && lo == ml) ? (unsigned)l + 1u : 0u;
+            const unsigned bc0 = __reduce_max_sync(FDVB_FULL, h == 0 ? ck : 0u);
+            const unsigned bc1 = __reduce_max_sync(FDVB_FULL, h == 1 ? ck : 0u);
+            const unsigned bc = h ? bc1 : bc0;
+            const double jmin = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+            bestL = (int)bc - 2;
+            if (v16 && !(jmin < J16)) bestL = 15;
+        } else {
+            double bestJ = -1.0;
+            for (int c = 16; c >= 0; --c) {                 // uniform across the warp
+                const double Jc = c == 16 ? J16 : __shfl_sync(FDVB_FULL, J, hb + c);
+                const bool vc = c == 16 ? v16 : (active && ((vmask >> c) & 1u));
+                if (vc && (bestJ < 0.0 || Jc < bestJ)) { bestJ = Jc; bestL = c - 1; }
+            }
+        }
+        if (!active) bestL = last;
+        if (l > bestL) levz = 0;
+        if (izz4(l) > bestL) lev = 0;
+        last = bestL;
+        __syncwarp();
+    }
+    const int rr = inverse(lev);
+    const int r = clipb(pv + rr);
+    (h ? rec1 : rec0)[i * rs + j] = (uint8_t)r;
+    const int dd = cv - r;
+    const int ssd = half_sum(dd * dd, lane);
+    const uint32_t z = zz_enc(levz);
+    const bool in = l <= last;
+    const int bits = bits_val((uint32_t)(last + 1)) + half_sum(in ? bits_val(z) : 0, lane);
+    const int len = in ? leb_size(z) : 0;
+    const int end = scan16(len, lane);
+    Blk4 *out = h ? out1 : out0;
+    if (in) leb_write(out->bytes + (end - len), z);
+    const int nbytes = __shfl_sync(FDVB_FULL, end, hb + 15);
+    if (l == 0) {
+        out->count = last + 1;
+        out->nbytes = nbytes;
+        out->ssd = ssd;
+        out->bits = bits;
+    }
+    __syncwarp();
+}
+
 // ------------------------------------------------------ 8x8 transform --
 struct Reg8Scratch {
     int32_t X[64];
