@@ -35,7 +35,6 @@
 namespace fdvb {
 
 constexpr int PNT = 512;
-using PResid = ResidScratchT<PNT>;
 
 struct PShared {
     QP4 q;

@@ -1,7 +1,8 @@
 // Residual coding on the GPU: the 4x4 block coder with RDOQ (one warp per
-// block, one lane per truncation candidate), the 8x8 transform option (64
-// threads per region), the per-8x8-region transform-size decision, and the
-// chroma residual of SKIP/INTER macroblocks.
+// block, or two blocks per warp on half-warps; one lane per truncation
+// candidate), the 8x8 transform option (one warp, or 64 threads), the
+// per-8x8-region transform-size decision and its stream offsets, and the
+// team-level coder of whole n x n residuals.
 //
 //   code_block4        fdv.h:5214-5278   (+ fdv_rdoq4x4_inner fdv.h:2493-2536)
 //   8x8 option         fdv.h:5324-5377   (fdv_fdct8x8/quant8x8/dequant8x8/idct8x8 :2614-2685)
@@ -547,20 +548,6 @@ struct RegDec {
     int b;
 };
 
-// Scratch for one chunk of up to NT/64 8x8 regions of a code_residual call.
-template <int NT>
-struct ResidScratchT {
-    static constexpr int RMAX = NT / 64, NW = NT / 32;
-    Blk4 blk[4 * RMAX];
-    uint8_t recA[RMAX][64];
-    Reg8 reg[RMAX];
-    Reg8Scratch r8[RMAX];
-    Blk4Scratch b4[NW];
-    RegDec dec[RMAX];
-    long long e;
-    int b;
-};
-
 // The RD choice of one 8x8 region between its four 4x4 blocks (A) and its 8x8
 // transform (B), with the empty-region flag value 0 (fdv.h:5379-5411).
 __device__ __forceinline__ void region_choice(const Blk4 *b4, const Reg8 &R, double lambda, RegDec &D) {
@@ -644,50 +631,6 @@ __device__ void decide_regions(int nreg, Blk4 *blk, Reg8 *reg, RegDec *dec, doub
     __syncthreads();
     // one warp per region copies its flag, counts and level bytes
     for (int rg = warp; rg < nreg; rg += NT / 32) region_symbols(dec[rg], &blk[rg * 4], reg[rg], sink, chroma, lane);
-}
-
-// The whole block (NT threads) codes an n x n residual, n in {8, 16, 32, 64}:
-// per aligned 8x8 region, in raster order, the RD choice between four RDOQ'd
-// 4x4 transforms and one 8x8 transform, with the 3-valued region flag
-// (fdv.h:5300-5414).  Regions are processed NT/64 at a time: every 4x4 block
-// of the chunk on its own warp, every region's 8x8 option on 64 threads, then
-// the decisions.  cur has stride cs, pred ps, rec rs.  Appends to `sink`
-// (4x4 symbols to the chroma streams when `chroma`), returns the distortion
-// and adds the rate to *bits (uniform on return).
-template <int NT>
-__device__ long long code_residual_t(const uint8_t *cur, int cs, const uint8_t *pred, int ps, int n,
-                                     const QP4 &Q, int qp, double lambda, bool chroma, uint8_t *rec, int rs,
-                                     CoefSink *sink, int *bits, ResidScratchT<NT> *sc, unsigned *err) {
-    constexpr int RMAX = NT / 64, NW = NT / 32;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int rpl = n / 8, nreg_total = rpl * rpl;
-    long long etot = 0;
-    int btot = 0;
-    for (int r0 = 0; r0 < nreg_total; r0 += RMAX) {
-        const int nreg = min(RMAX, nreg_total - r0), nblk = nreg * 4;
-        for (int b = warp; b < nblk; b += NW) {
-            int rg = b >> 2, s = b & 3, gr = r0 + rg;
-            int rx = (gr % rpl) * 8, ry = (gr / rpl) * 8, sx = (s & 1) * 4, sy = (s >> 1) * 4;
-            warp_block4(cur + (ry + sy) * cs + rx + sx, cs, pred + (ry + sy) * ps + rx + sx, ps,
-                        &sc->recA[rg][sy * 8 + sx], 8, Q, lambda, true, &sc->blk[b], &sc->b4[warp], lane);
-        }
-        if (tid < nreg * 64) {
-            int rg = tid >> 6, gr = r0 + rg, rx = (gr % rpl) * 8, ry = (gr / rpl) * 8;
-            region8(cur + ry * cs + rx, cs, pred + ry * ps + rx, ps, qp, &sc->reg[rg], &sc->r8[rg], tid & 63, 1 + rg);
-        }
-        __syncthreads();
-        decide_regions<NT>(nreg, sc->blk, sc->reg, sc->dec, lambda, chroma, sink, &sc->e, &sc->b, err);
-        for (int p = tid; p < nreg * 64; p += NT) {
-            int rg = p >> 6, q = p & 63, gr = r0 + rg;
-            int y = (gr / rpl) * 8 + (q >> 3), x = (gr % rpl) * 8 + (q & 7);
-            rec[y * rs + x] = sc->dec[rg].choice ? sc->reg[rg].rec[q] : sc->recA[rg][q];
-        }
-        etot += sc->e;
-        btot += sc->b;
-        __syncthreads();
-    }
-    *bits += btot;
-    return etot;
 }
 
 // ---------------------------------------------- team residual coding --
