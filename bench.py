@@ -15,8 +15,9 @@ One step = encoding all 120 frames.
   host frames to the finished byte stream: host->device copies, the GPU loop,
   the symbol streams' device->host path and the host entropy coding.
 * ``cpu_baseline``: the reference's own tile-parallel encoder, compiled from its
-  sources (oracle/_ref), on one GOP of the workload with 8 threads (the band
-  count caps its parallelism).
+  sources (oracle/_ref), on one GOP of the workload: the faster of the
+  workload's 8-band layout (parallelism capped at 8 threads) and one macroblock
+  row per band (45 bands) on every host core.
 
 ``--impl reference`` times that reference encoder alone (rank 0).
 Under torchrun each rank encodes its own stream (weak scaling, no collective on
@@ -111,7 +112,7 @@ def band_layout():
     return [(b * bh_full, min(bh_full, H - b * bh_full)) for b in range(nb)]
 
 
-def reference_encode_seconds(frames, nthreads: int) -> float:
+def reference_encode_seconds(frames, nthreads: int, band_mbrows: int = BAND_MBROWS) -> float:
     """One fdv_vtile_encode of `frames` by the reference compiled from its sources."""
     import oracle as O
     L = O.ref(RANGE)
@@ -120,11 +121,32 @@ def reference_encode_seconds(frames, nthreads: int) -> float:
     cap = FSIZE * len(frames) + (1 << 20)
     out = np.empty(cap, np.uint8)
     t0 = time.perf_counter()
-    n = L.fdv_vtile_encode(arr, len(frames), W, H, QP, KEYINT, BAND_MBROWS, nthreads, out.ctypes.data_as(u8p), cap)
+    n = L.fdv_vtile_encode(arr, len(frames), W, H, QP, KEYINT, band_mbrows, nthreads, out.ctypes.data_as(u8p), cap)
     dt = time.perf_counter() - t0
     if n == 0:
         raise RuntimeError("reference encode failed")
     return dt
+
+
+def best_cpu(frames, repeats: int = 1) -> dict:
+    """The reference on the host cores, two ways: the workload's own 8-band
+    layout (its parallelism capped at 8 threads) and one macroblock row per band
+    (45 bands) on every core; the faster one is the baseline."""
+    ncpu = os.cpu_count() or 1
+    mpix = len(frames) * W * H / 1e6
+    nb8 = len(band_layout())
+    t8 = min(reference_encode_seconds(frames, ncpu) for _ in range(repeats))
+    t1 = min(reference_encode_seconds(frames, ncpu, 1) for _ in range(repeats))
+    v8, v1 = mpix / t8, mpix / t1
+    if v1 > v8:
+        return {"value": round(v1, 3), "cores": ncpu, "seconds": t1, "band_mbrows": 1,
+                "sample": f"frames 0-{len(frames) - 1} (1 key + {len(frames) - 1} P) of the workload, the reference's "
+                          f"fdv_vtile_encode with one macroblock row per band (45 bands) on {ncpu} threads "
+                          f"(faster than the workload's 8-band layout on {min(ncpu, nb8)} threads: {v8:.1f} Mpix/s)"}
+    return {"value": round(v8, 3), "cores": min(ncpu, nb8), "seconds": t8, "band_mbrows": BAND_MBROWS,
+            "sample": f"frames 0-{len(frames) - 1} (1 key + {len(frames) - 1} P) of the workload, the reference's "
+                      f"fdv_vtile_encode, 8 bands on {min(ncpu, nb8)} threads (faster than one macroblock row per "
+                      f"band on {ncpu} threads: {v1:.1f} Mpix/s)"}
 
 
 def run_reference(args) -> None:
@@ -137,13 +159,16 @@ def run_reference(args) -> None:
         return
     frames = render(1)[:KEYINT]              # one GOP: 1 key frame + 59 P-frames
     nthreads = os.cpu_count() or 1
+    # the faster of the two band layouts on the host cores, then timed alone
+    choice = best_cpu(frames)
+    bm = choice["band_mbrows"]
     for _ in range(args.warmup):
-        reference_encode_seconds(frames, nthreads)
-    ts = [reference_encode_seconds(frames, nthreads) for _ in range(args.steps)]
+        reference_encode_seconds(frames, nthreads, bm)
+    ts = [reference_encode_seconds(frames, nthreads, bm) for _ in range(args.steps)]
     mpix = len(frames) * W * H / 1e6
     value = mpix / statistics.mean(ts)
-    used = min(nthreads, len(band_layout()))
-    sample = f"frames 0-{KEYINT - 1} of the workload (1 key + {KEYINT - 1} P), fdv_vtile_encode, {used} threads"
+    used = choice["cores"]
+    sample = choice["sample"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpix/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -306,14 +331,9 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle as O
         if O.have_ref(RANGE):
-            sample = hframes[:KEYINT]
-            thr = os.cpu_count() or 1
-            dt = reference_encode_seconds(sample, thr)
-            used = min(thr, nb)
-            cpu = {"value": round(KEYINT * W * H / 1e6 / dt, 3), "unit": "Mpix/s", "cores": used,
-                   "kind": "reference",
-                   "sample": f"frames 0-{KEYINT - 1} (1 key + {KEYINT - 1} P) of the workload, the reference's "
-                             f"fdv_vtile_encode, {used} threads (its parallelism is capped by the 8 bands)"}
+            b = best_cpu(hframes[:KEYINT])
+            cpu = {"value": b["value"], "unit": "Mpix/s", "cores": b["cores"], "kind": "reference",
+                   "sample": b["sample"]}
 
     if rank == 0:
         print(json.dumps({

@@ -166,6 +166,11 @@ class Encoder:
         if lib().fdv_enc_repeat(self._e) != 0:
             raise FdvError(last_error() or "fdv_enc_repeat failed")
 
+    def set_bitrate(self, bits_per_second: int, fps: int = 30, bufsecs: float = 1.0) -> None:
+        """Average-bitrate control (fdv_enc_set_bitrate, fdv.h:1176); before the first frame."""
+        if lib().fdv_enc_set_bitrate(self._e, bits_per_second, fps, bufsecs) != 0:
+            raise FdvError(last_error() or "fdv_enc_set_bitrate failed")
+
     def count(self) -> int:
         return lib().fdv_enc_count(self._e)
 

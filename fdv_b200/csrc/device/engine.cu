@@ -152,6 +152,9 @@ struct fdvb_engine {
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
     int src_on_device = 0;
     int stall_unit = -1, stall_row = -1;
+    int defer_refs = 0;                     // leave the reference pool alone until commit
+    std::vector<int> pending_intra;         // frame types of the uncommitted step
+    bool pending = false;
     unsigned long long *d_prof = nullptr;   // phase profile accumulators (when enabled)
 };
 
@@ -486,14 +489,19 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
     launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
     CK(cudaGetLastError());
     E->launches += 1;
-    // 5. the new reference
-    std::vector<int> all(nu);
-    for (int i = 0; i < nu; ++i) all[i] = i;
-    if (prep_refs(E, all, stage) != 0) return -3;
-    E->launches += 2;
-    for (int i = 0; i < nu; ++i) {
-        Unit &u = E->units[i];
-        u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+    // 5. the new reference (deferred: the caller may code this frame again)
+    if (E->defer_refs) {
+        E->pending_intra.assign(is_intra, is_intra + nu);
+        E->pending = true;
+    } else {
+        std::vector<int> all(nu);
+        for (int i = 0; i < nu; ++i) all[i] = i;
+        if (prep_refs(E, all, stage) != 0) return -3;
+        E->launches += 2;
+        for (int i = 0; i < nu; ++i) {
+            Unit &u = E->units[i];
+            u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+        }
     }
     CK(cudaMemcpyAsync(SL.err_h, E->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
     CK(cudaEventRecord(SL.ev[5], E->st));
@@ -635,5 +643,30 @@ extern "C" int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long lon
         cudaMemset(E->d_prof, 0, 32 * sizeof(unsigned long long));
     }
     if (!enable && E->d_prof) { cudaFree(E->d_prof); E->d_prof = nullptr; }
+    return 0;
+}
+
+// Re-coding support (average-bitrate control codes a frame again, coarser,
+// when it overshoots): while deferral is on, a step leaves the reference pool
+// untouched, so the same frame can be stepped again against the same
+// references; commit then makes the last step's reconstruction the nearest
+// reference.  Only one frame may be in flight while deferring.
+extern "C" void fdvb_engine_defer_refs(fdvb_engine *E, int on) { if (E) E->defer_refs = on; }
+extern "C" int fdvb_engine_commit_refs(fdvb_engine *E) {
+    if (!E) return -1;
+    if (!E->pending) return 0;
+    if (E->inflight) { g_err = "a frame is still in flight"; return -1; }
+    CK(cudaSetDevice(E->device));
+    const int nu = (int)E->units.size();
+    std::vector<int> all(nu);
+    for (int i = 0; i < nu; ++i) all[i] = i;
+    if (prep_refs(E, all) != 0) return -3;
+    CK(cudaStreamSynchronize(E->st));
+    E->launches += 2;
+    for (int i = 0; i < nu; ++i) {
+        Unit &u = E->units[i];
+        u.nref = E->pending_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+    }
+    E->pending = false;
     return 0;
 }

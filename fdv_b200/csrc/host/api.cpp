@@ -12,6 +12,7 @@
 //   file head        "FDV1" [version u8][kind u8][fps u16][payload_len u32]
 //                                                                   fdv.h:7448-7464
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <condition_variable>
 #include <cstdlib>
@@ -56,9 +57,9 @@ void stream_header(std::vector<uint8_t> &b, int nframes, int w, int h, int qp, i
     b.insert(b.end(), hd, hd + o);
 }
 
-// Entropy-code unit u's analysis output of the engine's last step and append
-// [blob_len u32][blob] to its stream (the tail of fdv_video_encode's frame loop).
-int code_unit_frame(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp) {
+// Entropy-code unit u's analysis output of the engine's last step into
+// us.tmp; returns the blob length (0 on failure).
+size_t code_unit_blob(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp) {
     size_t blob = 0;
     if (us.tmp.size() < us.tmp_cap) us.tmp.resize(us.tmp_cap);
     if (is_intra) {
@@ -68,11 +69,11 @@ int code_unit_frame(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp)
         size_t o = 0;
         for (int p = 0; p < 3; ++p) {
             const fdvb_streams *s = fdvb_engine_istreams(E, u, p);
-            if (!s) return -1;
+            if (!s) return 0;
             size_t bcap = (size_t)pw[p] * ph[p] * 2 + 4096;
             std::vector<uint8_t> pb(bcap);
             size_t bl = fdvb_image_blob(s, pw[p], ph[p], qp, pb.data(), bcap, nullptr);
-            if (!bl || o + 4 + bl > us.tmp_cap) return -1;
+            if (!bl || o + 4 + bl > us.tmp_cap) return 0;
             o = fdvb_put32(us.tmp.data(), o, (uint32_t)bl);
             memcpy(us.tmp.data() + o, pb.data(), bl);
             o += bl;
@@ -80,14 +81,26 @@ int code_unit_frame(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp)
         blob = o;
     } else {
         const fdvb_streams *s = fdvb_engine_pstreams(E, u);
-        if (!s) return -1;
+        if (!s) return 0;
         blob = fdvb_pframe_blob(s, qp, us.tc.get(), us.tmp.data(), us.tmp_cap, nullptr);
-        if (!blob) return -1;
     }
+    return blob;
+}
+
+// Append [blob_len u32][blob] from us.tmp to the unit's stream.
+void append_blob(UnitStream &us, size_t blob) {
     uint8_t l4[4];
     fdvb_put32(l4, 0, (uint32_t)blob);
     us.bytes.insert(us.bytes.end(), l4, l4 + 4);
     us.bytes.insert(us.bytes.end(), us.tmp.begin(), us.tmp.begin() + (long)blob);
+}
+
+// Entropy-code unit u's output of the engine's last step and append it (the
+// tail of fdv_video_encode's frame loop).
+int code_unit_frame(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp) {
+    const size_t blob = code_unit_blob(E, u, us, is_intra, qp);
+    if (!blob) return -1;
+    append_blob(us, blob);
     return 0;
 }
 
@@ -226,6 +239,8 @@ struct fdv_encoder {
     fdvb_engine *E = nullptr;
     std::vector<UnitStream> us;
     std::vector<int> by0, bh;
+    int use_rc = 0;                                  // average-bitrate control on
+    fdv_rc rc{};
 };
 
 extern "C" {
@@ -413,13 +428,19 @@ size_t fdv_enc_bytes(const fdv_encoder *e) {
     return t;
 }
 int fdv_enc_set_bitrate(fdv_encoder *e, int bits_per_second, int fps, double bufsecs) {
-    (void)e; (void)bits_per_second; (void)fps; (void)bufsecs;
-    set_err("average-bitrate control is not provided by this library");
-    return -1;
+    if (!e || bits_per_second <= 0 || e->n != 0) { set_err("bitrate control must be set before the first frame"); return -1; }
+    fdv_rc_init(&e->rc, bits_per_second, fps, e->w, e->h, e->keyint, bufsecs, 0, 0);
+    e->use_rc = 1;
+    return 0;
 }
 
-// enc_push (fdv.h:8231-8377) for every band at once; a held frame re-emits
-// the reference as all-SKIP and carries a due key frame to the next real one.
+// enc_push (fdv.h:8231-8377): one frame for every band at once; a held frame
+// re-emits the reference as all-SKIP and carries a due key frame to the next
+// real one.  With bitrate control a single stream takes its QP and lambda
+// fraction from the controller and is coded again, coarser, while it lands
+// more than 1.5x over its allocation (at most three times, fdv.h:8281-8335);
+// a tiled stream gives every band the controller's whole QP (bands_push,
+// fdv.h:8066-8127).
 static int enc_push(fdv_encoder *e, const uint8_t *i420, int force_skip) {
     if (!e || (!i420 && !force_skip)) return -1;
     if (e->n >= 65535) { set_err("frame count limit"); return -1; }
@@ -429,7 +450,7 @@ static int enc_push(fdv_encoder *e, const uint8_t *i420, int force_skip) {
     else e->key_due = 0;
     const int nb = (int)e->us.size(), w = e->w, h = e->h, cw = w / 2, ch = h / 2;
     std::vector<const uint8_t *> planes(3 * nb, nullptr);
-    std::vector<int> intra(nb, is_intra), qps(nb, e->qp), fs(nb, force_skip);
+    std::vector<int> intra(nb, is_intra), fs(nb, force_skip);
     if (i420) {
         const uint8_t *fy = i420, *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
         for (int b = 0; b < nb; ++b) {
@@ -438,8 +459,59 @@ static int enc_push(fdv_encoder *e, const uint8_t *i420, int force_skip) {
             planes[3 * b + 2] = fv + (size_t)(e->by0[b] / 2) * cw;
         }
     }
-    if (fdvb_engine_step(e->E, planes.data(), intra.data(), qps.data(), nullptr, fs.data()) != 0) { set_engine_err(); return -1; }
-    if (code_all(e->E, e->us, is_intra, e->qp, e->nthreads) != 0) { set_err("entropy coding failed"); return -1; }
+    if (e->nbands > 0 || !e->use_rc) {
+        // fixed QP, or the tiled form of bitrate control: one whole QP per frame
+        int fqp = e->qp;
+        const size_t before = fdv_enc_bytes(e);
+        if (e->use_rc) fqp = force_skip ? e->rc.used_qp : fdv_rc_pick(&e->rc, is_intra);
+        std::vector<int> qps(nb, fqp);
+        if (fdvb_engine_step(e->E, planes.data(), intra.data(), qps.data(), nullptr, fs.data()) != 0) { set_engine_err(); return -1; }
+        if (code_all(e->E, e->us, is_intra, fqp, e->nthreads) != 0) { set_err("entropy coding failed"); return -1; }
+        ++e->n;
+        if (e->use_rc) {
+            const size_t used = fdv_enc_bytes(e) - before;
+            if (force_skip) fdv_rc_skip(&e->rc, used);
+            else fdv_rc_update(&e->rc, is_intra, used);
+        }
+        return 0;
+    }
+    // single stream under bitrate control
+    UnitStream &us = e->us[0];
+    int fqp = force_skip ? e->rc.used_qp : fdv_rc_pick(&e->rc, is_intra);
+    double lscale = e->rc.lscale;
+    double qreal = (double)fqp + log(lscale) / log(fdvb_rc_lfrac());
+    const fdvb_tabcache tc_before = *us.tc;   // a second coding starts from the same entropy state
+    fdvb_engine_defer_refs(e->E, 1);
+    auto code = [&](int q, double ls) -> size_t {
+        *us.tc = tc_before;
+        if (fdvb_engine_step(e->E, planes.data(), intra.data(), &q, &ls, fs.data()) != 0) return 0;
+        return code_unit_blob(e->E, 0, us, is_intra, q);
+    };
+    size_t blob = code(fqp, lscale);
+    if (blob > 0) {
+        for (int tries = 0; tries < 3 && qreal < (double)e->rc.qpmax; ++tries) {
+            const double alloc = e->rc.last_target > 1.0 ? e->rc.last_target : 1.0;
+            const double over = (double)blob * 8.0 / alloc;
+            if (over <= 1.5) break;
+            double step = 2.0 * log2(over);
+            if (step < 0.25) step = 0.25;
+            if (step > 4.0) step = 4.0;
+            double qn = qreal + step;
+            if (qn > (double)e->rc.qpmax) qn = (double)e->rc.qpmax;
+            int retry;
+            double rls;
+            fdv_rc_split(&e->rc, qn, &retry, &rls);
+            const size_t again = code(retry, rls);
+            if (!again) break;
+            blob = again; fqp = retry; qreal = qn; e->rc.used_qp = retry;
+        }
+        fdv_rc_adopt(&e->rc, is_intra, qreal);
+    }
+    fdvb_engine_defer_refs(e->E, 0);
+    if (blob == 0 || fdvb_engine_commit_refs(e->E) != 0) { set_engine_err(); return -1; }
+    append_blob(us, blob);
+    if (force_skip) fdv_rc_skip(&e->rc, blob);
+    else fdv_rc_update(&e->rc, is_intra, blob);
     ++e->n;
     return 0;
 }

@@ -15,6 +15,8 @@ int fdvb_engine_step(fdvb_engine *E, const uint8_t *const *planes, const int *is
 int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
                        const double *lscale, const int *force_skip);
 int fdvb_engine_collect(fdvb_engine *E);
+void fdvb_engine_defer_refs(fdvb_engine *E, int on);
+int fdvb_engine_commit_refs(fdvb_engine *E);
 const fdvb_streams *fdvb_engine_pstreams(fdvb_engine *E, int unit);
 const fdvb_streams *fdvb_engine_istreams(fdvb_engine *E, int unit, int plane);
 int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420);

@@ -63,6 +63,10 @@ int fdvb_leb_size(uint32_t u);
 // does (fdv.h:4870, :5804): lscale * 0.425 * 2^((qp - 12) / 3).
 double fdvb_lambda(int qp, double lscale);
 
+// The lambda multiplier spanning one quantiser step of the rate controller
+// (FDV_RC_LFRAC, fdv.h:7882-7884).
+extern "C" double fdvb_rc_lfrac(void);
+
 // The 8x8 DCT basis and quantiser steps (fdv.h:2597-2612), computed on the
 // host with the same libm calls and uploaded to the device.
 void fdvb_c8_tables(int32_t c8[64], int32_t qstep8[52]);

@@ -55,13 +55,41 @@ fdv_encoder *fdv_enc_open_tiled(int w, int h, int qp, int keyint, int band_mbrow
                                 int nthreads);                                     /* fdv.h:1186 */
 int fdv_enc_frame(fdv_encoder *e, const uint8_t *i420);                           /* fdv.h:1163 */
 int fdv_enc_repeat(fdv_encoder *e);                                                /* fdv.h:1169 */
-/* Average-bitrate control (fdv.h:1176) is not provided by this library: the
- * call returns -1 and the encoder keeps its fixed QP. */
+/* Switch an encoder to average-bitrate control before its first frame.
+ * Replaces fdv_enc_set_bitrate, fdv.h:1176 (implementation :8385-8392).  A
+ * single-stream encoder codes each P-frame at a real operating point (QP plus
+ * a lambda fraction) and codes a frame again, coarser, up to three times when
+ * it lands more than 1.5x over its allocation (fdv.h:8281-8335); a tiled
+ * encoder hands every band the same whole QP per frame (fdv.h:8076-8083).
+ * Returns -1 after the first frame or for a non-positive bitrate. */
 int fdv_enc_set_bitrate(fdv_encoder *e, int bits_per_second, int fps, double bufsecs);
 int fdv_enc_count(const fdv_encoder *e);                                           /* fdv.h:1189 */
 size_t fdv_enc_bytes(const fdv_encoder *e);                                        /* fdv.h:1190 */
 uint8_t *fdv_enc_finish(fdv_encoder *e, int fps, size_t *len);                    /* fdv.h:1195 */
 void fdv_enc_close(fdv_encoder *e);                                                /* fdv.h:1198 */
+
+/* The rate controller itself (fdv.h:1022-1053), for callers that drive
+ * fdv_video_encode-style loops themselves.  Same fields and semantics as the
+ * reference's fdv_rc. */
+typedef struct {
+    int bitrate;             /* bits per second, the average to hold */
+    int fps;
+    double bufbits;          /* bucket size */
+    int qpmin, qpmax, keyint;
+    double qp_p;             /* the P-frame operating point */
+    double ip_off;           /* how much finer a key frame is coded */
+    double last_target;      /* the last frame's allocation, bits */
+    double fill;             /* bucket fullness, bits */
+    int used_qp;
+    double lscale;           /* the operating point's fraction, as a lambda multiplier */
+} fdv_rc;
+void fdv_rc_init(fdv_rc *rc, int bitrate, int fps, int w, int h, int keyint, double bufsecs, int qpmin,
+                 int qpmax);                                                   /* fdv.h:1036 */
+int fdv_rc_pick(fdv_rc *rc, int is_intra);                                     /* fdv.h:1038 */
+void fdv_rc_update(fdv_rc *rc, int is_intra, size_t bytes);                    /* fdv.h:1039 */
+void fdv_rc_skip(fdv_rc *rc, size_t bytes);                                    /* fdv.h:1044 */
+void fdv_rc_adopt(fdv_rc *rc, int is_intra, double q);                         /* fdv.h:1051 */
+void fdv_rc_split(const fdv_rc *rc, double q, int *qp, double *lscale);        /* fdv.h:1053 */
 
 /* The 12-byte .fdv file head.  Replaces fdv_wrap, fdv.h:1094. */
 size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payload, size_t payload_len);

@@ -210,3 +210,40 @@ def ref_vtile_decode(stream: bytes, search_range: int = 16) -> np.ndarray:
     if L.fdv_vtile_decode(_ptr(buf), len(stream), _ptr(out), C.byref(a), C.byref(b), C.byref(c), 1) != 0:
         raise RuntimeError("reference tiled decode failed")
     return out.reshape(nf, -1)
+
+
+def ref_enc_stream(frames, w: int, h: int, qp: int, keyint: int, search_range: int = 16, bitrate: int = 0,
+                   fps: int = 30, bufsecs: float = 1.0, band_mbrows: int | None = None, nthreads: int = 1,
+                   repeat_after: tuple = ()) -> bytes:
+    """The reference's streaming encoder (fdv_enc_*, fdv.h:1157-1198) over
+    `frames`, optionally under its average-bitrate control
+    (fdv_enc_set_bitrate, :8385); after each frame index in repeat_after a
+    held frame (fdv_enc_repeat) is pushed.  Returns the finished .fdv file."""
+    L = ref(search_range)
+    vp = C.c_void_p
+    L.fdv_enc_open.restype = vp
+    L.fdv_enc_open.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    L.fdv_enc_open_tiled.restype = vp
+    L.fdv_enc_open_tiled.argtypes = [C.c_int] * 6
+    L.fdv_enc_set_bitrate.argtypes = [vp, C.c_int, C.c_int, C.c_double]
+    L.fdv_enc_frame.argtypes = [vp, u8p]
+    L.fdv_enc_repeat.argtypes = [vp]
+    L.fdv_enc_finish.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t)]
+    L.fdv_enc_finish.restype = vp
+    e = L.fdv_enc_open(w, h, qp, keyint) if band_mbrows is None else L.fdv_enc_open_tiled(w, h, qp, keyint,
+                                                                                         band_mbrows, nthreads)
+    if not e:
+        raise RuntimeError("reference fdv_enc_open failed")
+    if bitrate and L.fdv_enc_set_bitrate(e, bitrate, fps, bufsecs) != 0:
+        raise RuntimeError("reference fdv_enc_set_bitrate failed")
+    for i, f in enumerate(frames):
+        a = np.ascontiguousarray(f, dtype=np.uint8).reshape(-1)
+        if L.fdv_enc_frame(e, _ptr(a)) != 0:
+            raise RuntimeError("reference fdv_enc_frame failed")
+        if i in repeat_after and L.fdv_enc_repeat(e) != 0:
+            raise RuntimeError("reference fdv_enc_repeat failed")
+    n = C.c_size_t()
+    p = L.fdv_enc_finish(e, fps, C.byref(n))
+    if not p:
+        raise RuntimeError("reference fdv_enc_finish failed")
+    return C.string_at(p, n.value)

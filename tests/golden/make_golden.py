@@ -49,6 +49,25 @@ CASES = [
 ]
 
 
+# Streaming encodes (fdv_enc_*) under average-bitrate control: (name, scene
+# kwargs, encoder kwargs).  The low bitrates make frames overshoot their
+# allocation, so the reference codes them again, coarser (fdv.h:8281-8335).
+STREAMS = [
+    ("rc_single_low", dict(w=256, h=144, nframes=14, nrects=10, pan_qx=9, static_pct=40, seed=5),
+     dict(qp=24, keyint=6, search_range=16, bitrate=8000, fps=30, bufsecs=1.0, band_mbrows=None, nthreads=1,
+          repeat_after=[4])),
+    ("rc_single_cif", dict(w=352, h=288, nframes=12, nrects=6, seed=1),
+     dict(qp=28, keyint=0, search_range=16, bitrate=300000, fps=30, bufsecs=0.5, band_mbrows=None, nthreads=1,
+          repeat_after=[])),
+    ("rc_single_r32", dict(w=256, h=144, nframes=10, nrects=12, pan_qx=-7, pan_qy=2, static_pct=10, seed=11),
+     dict(qp=30, keyint=5, search_range=32, bitrate=60000, fps=25, bufsecs=2.0, band_mbrows=None, nthreads=1,
+          repeat_after=[6])),
+    ("rc_tiled", dict(w=192, h=160, nframes=10, nrects=8, pan_qx=-6, pan_qy=3, static_pct=20, seed=9),
+     dict(qp=20, keyint=4, search_range=16, bitrate=30000, fps=30, bufsecs=1.0, band_mbrows=3, nthreads=2,
+          repeat_after=[2])),
+]
+
+
 def scene(kw) -> list[np.ndarray]:
     kw = dict(kw)
     n = kw.pop("nframes")
@@ -72,6 +91,13 @@ def main() -> None:
             "frames_sha256": sha(b"".join(f.tobytes() for f in fr)),
             "decoded_sha256": sha(dec.tobytes()),
         }
+        print(name, len(s), flush=True)
+    out["streams"] = {}
+    for name, skw, ekw in STREAMS:
+        fr = scene(skw)
+        s = O.ref_enc_stream(fr, skw["w"], skw["h"], ekw["qp"], ekw["keyint"], ekw["search_range"], ekw["bitrate"],
+                             ekw["fps"], ekw["bufsecs"], ekw["band_mbrows"], ekw["nthreads"], tuple(ekw["repeat_after"]))
+        out["streams"][name] = {"scene": skw, "encode": ekw, "file_sha256": sha(s), "file_len": len(s)}
         print(name, len(s), flush=True)
     # known answers of the reference's kernels (its own tests pin the first two:
     # test_enc.c:466-476 flat block -> DC only; :817-826 motion search recovers
