@@ -67,6 +67,8 @@ def lib() -> C.CDLL:
         L.fdvg_frame.argtypes = [p, C.POINTER(u8p), C.POINTER(i), C.POINTER(i), C.POINTER(C.c_double), C.POINTER(i)]
         L.fdvg_pframe_streams.argtypes = [p, i, C.POINTER(u8p), C.POINTER(sz)]
         L.fdvg_iframe_streams.argtypes = [p, i, i, C.POINTER(u8p), C.POINTER(sz)]
+        L.fdvg_pframe_hist.argtypes = [p, i, C.POINTER(C.c_uint32)]
+        L.fdvg_iframe_hist.argtypes = [p, i, i, C.POINTER(C.c_uint32)]
         L.fdvg_recon.argtypes = [p, i, u8p]
         L.fdvg_set_refs.argtypes = [p, i, u8p, u8p]
         L.fdvb_tabcache_new.restype = p
@@ -244,6 +246,20 @@ class Engine:
         if lib().fdvg_iframe_streams(self._g, u, plane, s, n) != 0:
             raise FdvError(last_error())
         return [C.string_at(s[k], n[k]) if n[k] else b"" for k in range(12)]
+
+    def pframe_hist(self, u: int) -> np.ndarray:
+        """GPU symbol counts of the 16 P-frame streams, [16, 256]."""
+        h = np.zeros((16, 256), np.uint32)
+        if lib().fdvg_pframe_hist(self._g, u, h.ctypes.data_as(C.POINTER(C.c_uint32))) != 0:
+            raise FdvError(last_error())
+        return h
+
+    def iframe_hist(self, u: int, plane: int) -> np.ndarray:
+        """GPU symbol counts of a key-frame plane's 12 streams, [12, 256]."""
+        h = np.zeros((12, 256), np.uint32)
+        if lib().fdvg_iframe_hist(self._g, u, plane, h.ctypes.data_as(C.POINTER(C.c_uint32))) != 0:
+            raise FdvError(last_error())
+        return h
 
     def recon(self, u: int) -> np.ndarray:
         w, h = self.sizes[u]

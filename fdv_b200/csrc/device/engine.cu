@@ -91,6 +91,7 @@ struct CompactTaskH {
     const int *off;
     uint8_t *out;
     size_t cap;
+    uint32_t *hist;
 };
 
 struct RefSlot {
@@ -111,6 +112,9 @@ struct Unit {
     uint8_t *mmap[3] = {nullptr, nullptr, nullptr};
     int icols[3], irows[3], pw[3], ph[3];
     uint8_t *out_h[2] = {nullptr, nullptr}, *out_d[2] = {nullptr, nullptr};   // per in-flight slot
+    // per in-flight slot: the streams' symbol counts, [16][256] for a P-frame,
+    // [3][12][256] for a key frame (host-mapped, written by the compaction)
+    uint32_t *hist_h[2] = {nullptr, nullptr}, *hist_d[2] = {nullptr, nullptr};
     size_t out_cap = 0, out_off_i[3] = {0, 0, 0};
     int last_intra = 0, last_qp = 0;
     fdvb_streams ps{}, is[3]{};
@@ -206,6 +210,8 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     for (int k = 0; k < 2; ++k) {
         CK(cudaHostAlloc(&u.out_h[k], u.out_cap, cudaHostAllocMapped));
         CK(cudaHostGetDevicePointer(&u.out_d[k], u.out_h[k], 0));
+        CK(cudaHostAlloc(&u.hist_h[k], sizeof(uint32_t) * 36 * 256, cudaHostAllocMapped));
+        CK(cudaHostGetDevicePointer(&u.hist_d[k], u.hist_h[k], 0));
     }
     return 0;
 }
@@ -216,6 +222,7 @@ static void free_unit(Unit &u) {
     cudaFree(u.mbi); cudaFree(u.slots); cudaFree(u.progress);
     for (int p = 0; p < 3; ++p) { cudaFree(u.islots[p]); cudaFree(u.mmap[p]); }
     for (int k = 0; k < 2; ++k) if (u.out_h[k]) cudaFreeHost(u.out_h[k]);
+    for (int k = 0; k < 2; ++k) if (u.hist_h[k]) cudaFreeHost(u.hist_h[k]);
 }
 
 // Bytes of the descriptor area of a slot's staging buffer (each array 64-byte aligned).
@@ -415,7 +422,7 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         u.last_qp = qp[i];
         if (!is_intra[i]) {
             for (int r = 0; r < u.mbh; ++r) rows.push_back({i, r});
-            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[si], u.out_cap};
+            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[si], u.out_cap, u.hist_d[si]};
             cmp.push_back(c);
         } else {
             int prog = u.mbh;
@@ -429,7 +436,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
                 for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
                 prog += u.irows[p];
                 CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
-                               u.out_d[si] + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p]};
+                               u.out_d[si] + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p],
+                               u.hist_d[si] + p * 12 * 256};
                 cmp.push_back(c);
             }
         }
@@ -538,8 +546,15 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     for (int i = 0; i < (int)E->units.size(); ++i) {
         Unit &u = E->units[i];
         u.last_intra = SL.intra[i];
-        if (!u.last_intra) E->d2h += (long long)parse_streams(u.out_h[si], 16, &u.ps);
-        else for (int p = 0; p < 3; ++p) E->d2h += (long long)parse_streams(u.out_h[si] + u.out_off_i[p], 12, &u.is[p]);
+        if (!u.last_intra) {
+            E->d2h += (long long)parse_streams(u.out_h[si], 16, &u.ps) + 16 * 256 * 4;
+            u.ps.hist = u.hist_h[si];
+        } else {
+            for (int p = 0; p < 3; ++p) {
+                E->d2h += (long long)parse_streams(u.out_h[si] + u.out_off_i[p], 12, &u.is[p]) + 12 * 256 * 4;
+                u.is[p].hist = u.hist_h[si] + p * 12 * 256;
+            }
+        }
     }
     return 0;
 }

@@ -115,15 +115,21 @@ struct CompactTask {
     const int *off;        // device array [nstreams] of data offsets within a slot
     uint8_t *out;          // host-mapped: uint32 len[nstreams], then the streams back to back
     size_t cap;
+    uint32_t *hist;        // host-mapped [nstreams][256] symbol counts, or NULL
 };
 
 // One block per task, 1024 threads: 64 threads per stream scan the slot
-// lengths, then each thread copies its chunk of slots.
+// lengths, then each thread copies its chunk of slots and counts its bytes
+// into the stream's 256-bin histogram (the entropy tail's per-stream counts,
+// fdv.h:6228-6236 and :4899-4905), kept in shared memory and written out
+// beside the streams.
 __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks, unsigned *err) {
     const CompactTask &T = tasks[blockIdx.x];
     const int tid = threadIdx.x, k = tid >> 6, t = tid & 63;
     __shared__ unsigned s_tot[16][64];
     __shared__ unsigned s_base[17];
+    __shared__ unsigned s_hist[16][256];
+    for (int i = tid; i < 16 * 256; i += 1024) (&s_hist[0][0])[i] = 0u;
     const int nb = T.nslots, chunk = (nb + 63) / 64, b0 = t * chunk, b1 = min(nb, b0 + chunk);
     unsigned mine = 0;
     if (k < T.nstreams)
@@ -154,9 +160,17 @@ __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks,
             const uint8_t *slot = T.slots + (size_t)b * T.slot_bytes;
             int n = reinterpret_cast<const uint16_t *>(slot)[k];
             const uint8_t *src = slot + 32 + T.off[k];
-            for (int i = 0; i < n; ++i) dst[i] = src[i];
+            for (int i = 0; i < n; ++i) {
+                const uint8_t v = src[i];
+                dst[i] = v;
+                if (T.hist) atomicAdd(&s_hist[k][v], 1u);
+            }
             dst += n;
         }
+    }
+    if (T.hist) {
+        __syncthreads();
+        for (int i = tid; i < T.nstreams * 256; i += 1024) T.hist[i] = s_hist[i >> 8][i & 255];
     }
 }
 

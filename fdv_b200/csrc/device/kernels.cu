@@ -234,7 +234,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     for (int k = 0; k < 16; ++k) { int o = 0; for (int i = 0; i < k; ++i) o += kSlotCap[i]; poff[k] = o; }
     CompactTask cmp;
     cmp.slots = base + o_slots; cmp.nslots = nmb; cmp.slot_bytes = kSlotBytes; cmp.nstreams = 16;
-    cmp.off = reinterpret_cast<const int *>(base + o_off); cmp.out = out; cmp.cap = out_cap;
+    cmp.off = reinterpret_cast<const int *>(base + o_off); cmp.out = out; cmp.cap = out_cap; cmp.hist = nullptr;
 
     int *ticket = reinterpret_cast<int *>(base + o_misc);
     unsigned *err = reinterpret_cast<unsigned *>(base + o_misc + 8);

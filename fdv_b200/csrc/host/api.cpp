@@ -584,6 +584,18 @@ int fdvg_iframe_streams(fdvg_ctx *g, int u, int plane, const uint8_t **s12, size
     for (int k = 0; k < 12; ++k) { s12[k] = s->s[k]; n12[k] = s->n[k]; }
     return 0;
 }
+int fdvg_pframe_hist(fdvg_ctx *g, int u, uint32_t *hist) {
+    const fdvb_streams *s = fdvb_engine_pstreams(g, u);
+    if (!s || !s->hist || !hist) { set_err("no P-frame counts for this unit"); return -1; }
+    memcpy(hist, s->hist, sizeof(uint32_t) * 16 * 256);
+    return 0;
+}
+int fdvg_iframe_hist(fdvg_ctx *g, int u, int plane, uint32_t *hist) {
+    const fdvb_streams *s = fdvb_engine_istreams(g, u, plane);
+    if (!s || !s->hist || !hist) { set_err("no key-frame counts for this unit/plane"); return -1; }
+    memcpy(hist, s->hist, sizeof(uint32_t) * 12 * 256);
+    return 0;
+}
 int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420) {
     int rc = fdvb_engine_recon(g, u, i420);
     if (rc) set_engine_err();

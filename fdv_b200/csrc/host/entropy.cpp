@@ -242,20 +242,28 @@ size_t fdvb_pframe_blob(const fdvb_streams *st, int qp, fdvb_tabcache *tc,
         size_t o = 0;
         for (int k = 0; k < NS; ++k) { if (sn[k]) memcpy(all.data() + o, st->s[k], sn[k]); o += sn[k]; }
     }
+    // per-stream symbol counts (counted on the GPU when the streams came from
+    // the engine) and their sum, the one-model counts
+    static thread_local uint32_t ck[16][256];
+    for (int k = 0; k < NS; ++k) {
+        if (st->hist) memcpy(ck[k], st->hist + (size_t)k * 256, sizeof ck[k]);
+        else {
+            memset(ck[k], 0, sizeof ck[k]);
+            for (size_t i = 0; i < sn[k]; ++i) ck[k][st->s[k][i]]++;
+        }
+    }
     uint32_t c1[256] = {0};
-    for (size_t i = 0; i < total; ++i) c1[all[i]]++;
+    for (int k = 0; k < NS; ++k)
+        for (int v = 0; v < 256; ++v) c1[v] += ck[k][v];
     uint16_t f1[256];
     freqs_from_counts(c1, f1);
     std::vector<uint8_t> p1;
     size_t l1 = rans_encode(all.data(), total, f1, p1);
 
-    static thread_local uint32_t ck[16][256];
     uint16_t fk[16][256];
     std::vector<uint8_t> pay[16];
     size_t len[16];
     for (int k = 0; k < NS; ++k) {
-        memset(ck[k], 0, sizeof ck[k]);
-        for (size_t i = 0; i < sn[k]; ++i) ck[k][st->s[k][i]]++;
         freqs_from_counts(ck[k], fk[k]);
         len[k] = rans_encode(st->s[k], sn[k], fk[k], pay[k]);
     }
@@ -379,8 +387,17 @@ size_t fdvb_image_blob(const fdvb_streams *st, int w, int h, int qp,
         size_t o = 0;
         for (int k = 0; k < N; ++k) { if (sn[k]) memcpy(all.data() + o, st->s[k], sn[k]); o += sn[k]; }
     }
+    uint32_t ck[IS_N][256];
+    for (int k = 0; k < N; ++k) {
+        if (st->hist) memcpy(ck[k], st->hist + (size_t)k * 256, sizeof ck[k]);
+        else {
+            memset(ck[k], 0, sizeof ck[k]);
+            for (size_t i = 0; i < sn[k]; ++i) ck[k][st->s[k][i]]++;
+        }
+    }
     uint32_t c1[256] = {0};
-    for (size_t i = 0; i < total; ++i) c1[all[i]]++;
+    for (int k = 0; k < N; ++k)
+        for (int v = 0; v < 256; ++v) c1[v] += ck[k][v];
     uint16_t f1[256];
     freqs_from_counts(c1, f1);
     std::vector<uint8_t> p1;
@@ -389,9 +406,7 @@ size_t fdvb_image_blob(const fdvb_streams *st, int w, int h, int qp,
     std::vector<uint8_t> pay[IS_N];
     size_t len[IS_N];
     for (int k = 0; k < N; ++k) {
-        uint32_t ck[256] = {0};
-        for (size_t i = 0; i < sn[k]; ++i) ck[st->s[k][i]]++;
-        freqs_from_counts(ck, fk[k]);
+        freqs_from_counts(ck[k], fk[k]);
         len[k] = rans_encode(st->s[k], sn[k], fk[k], pay[k]);
     }
     size_t hdr = 0;

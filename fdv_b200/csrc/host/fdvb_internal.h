@@ -44,6 +44,7 @@ struct fdvb_tabcache {
 struct fdvb_streams {
     const uint8_t *s[16];
     size_t n[16];
+    const uint32_t *hist = nullptr;   // [16][256] symbol counts of the streams, when the GPU made them
 };
 
 // Entropy tail.  Each returns the blob length or 0 when `cap` is too small.

@@ -137,6 +137,13 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
  * Pointers stay valid until the next fdvg_frame. */
 int fdvg_pframe_streams(fdvg_ctx *g, int u, const uint8_t **s16, size_t *n16);
 int fdvg_iframe_streams(fdvg_ctx *g, int u, int plane, const uint8_t **s12, size_t *n12);
+/* The per-stream symbol counts of those streams, counted on the GPU while
+ * they are compacted: hist[k * 256 + v] is how often byte v occurs in stream
+ * k (16 streams for a P-frame, 12 per key-frame plane).  They are the counts
+ * the entropy tail builds its rANS tables from (fdv.h:6228-6236,
+ * :4899-4905); the library's own tail uses them instead of counting. */
+int fdvg_pframe_hist(fdvg_ctx *g, int u, uint32_t *hist);
+int fdvg_iframe_hist(fdvg_ctx *g, int u, int plane, uint32_t *hist);
 /* The last frame's deblocked reconstruction of unit u (tight I420). */
 int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420);
 /* Seed unit u's reference pool (nearest, and optionally the second). */

@@ -215,3 +215,31 @@ def test_bitrate_controlled_stream_matches_reference(built, golden, name):
         F.set_search_range(16)
     assert len(data) == case["file_len"]
     assert sha(data) == case["file_sha256"]
+
+
+def test_gpu_stream_counts_equal_host_counts(built):
+    """The symbol counts the compaction kernel makes equal a host count of the
+    streams it delivers, for P-frames and every key-frame plane (the counts
+    the entropy tail builds its tables from; the stream digests above show the
+    tail's output is unchanged when it uses them)."""
+    import fdv_b200 as F
+    w, h = 320, 176
+    fr = F.Scene(w, h, 3, nrects=8, pan_qx=9, static_pct=30, seed=12).frames(3)
+    eng = F.Engine([(w, 96), (w, 80)], 32)
+    def bands(f):
+        Y = f[:w * h].reshape(h, w); U = f[w * h:w * h * 5 // 4].reshape(h // 2, w // 2); V = f[w * h * 5 // 4:].reshape(h // 2, w // 2)
+        return [np.concatenate([Y[y0:y0 + bh].ravel(), U[y0 // 2:(y0 + bh) // 2].ravel(), V[y0 // 2:(y0 + bh) // 2].ravel()])
+                for y0, bh in ((0, 96), (96, 80))]
+    for f in range(3):
+        eng.step(bands(fr[f]), [int(f == 0)] * 2, [22, 30])
+        for u in range(2):
+            if f == 0:
+                for p in range(3):
+                    st, hg = eng.iframe_streams(u, p), eng.iframe_hist(u, p)
+                    for k in range(12):
+                        assert np.array_equal(hg[k], np.bincount(np.frombuffer(st[k], np.uint8), minlength=256)), (u, p, k)
+            else:
+                st, hg = eng.pframe_streams(u), eng.pframe_hist(u)
+                for k in range(16):
+                    assert np.array_equal(hg[k], np.bincount(np.frombuffer(st[k], np.uint8), minlength=256)), (u, k)
+    eng.close()
