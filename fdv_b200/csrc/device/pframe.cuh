@@ -153,6 +153,50 @@ __device__ __forceinline__ WindowLuma luma_src<true>(const RefPlanes &, const ui
     return WindowLuma{win + r * 4 * kWinPlane, wy0, wrows - 1};
 }
 
+// One residual warp task of region g (regions 4c..4c+3 belong to candidate c:
+// 0, 1 INTER16 on the two references, 2 INTRA16, 3 INTER8): j = 0, 1 the 4x4
+// block pairs 0-1 and 2-3 (one per half-warp), j = 2 the 8x8 option.
+__device__ __forceinline__ void resid_task(PShared &S, int g, int j, int qp, double lambda, int warp, int lane) {
+    const uint8_t *cp, *pp;
+    int pstr;
+    if (g < 12) {
+        const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
+        cp = S.cur + ry * 16 + rx; pp = S.pr[c] + ry * 16 + rx; pstr = 16;
+    } else {
+        const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
+        cp = S.cur + qy * 16 + qx; pp = S.pred8[q]; pstr = 8;
+    }
+    if (j < 2) {
+        const int s0 = 2 * j, sy = j * 4;
+        warp_block4x2(cp + sy * 16, cp + sy * 16 + 4, 16, pp + sy * pstr, pp + sy * pstr + 4, pstr, &S.recA[g][sy * 8],
+                      &S.recA[g][sy * 8 + 4], 8, S.q, lambda, true, &S.blk[4 * g + s0], &S.blk[4 * g + s0 + 1],
+                      &S.b4[2 * warp], lane);
+    } else {
+        warp_region8(cp, 16, pp, pstr, qp, &S.reg[g], &S.r8w[warp], lane);
+    }
+}
+
+// Candidate c's region decisions (fdv.h:5379-5411) on the four warps of a
+// group (barrier `bar`): transform choices, stream offsets in region order,
+// one warp per region copying its symbols; distortion and rate to cD/cB.
+__device__ __forceinline__ void group_decide(PShared &S, int c, double lambda, int gw, int gt, int lane, int bar,
+                                             unsigned *err) {
+    if (gt < 4) region_choice(&S.blk[4 * (4 * c + gt)], S.reg[4 * c + gt], lambda, S.dec[4 * c + gt]);
+    gbar(bar, 128);
+    if (gt == 0) {
+        S.cD[c] = 0;
+        S.cB[c] = 0;
+        region_offsets(&S.dec[4 * c], 4, &S.sink[c], false, &S.cD[c], &S.cB[c], err);
+    }
+    gbar(bar, 128);
+    region_symbols(S.dec[4 * c + gw], &S.blk[4 * (4 * c + gw)], S.reg[4 * c + gw], &S.sink[c], false, lane);
+}
+
+// Warp groups 0, 1 and 3 meet here after their searches (the pool of twelve
+// warps that codes the INTER16 and INTRA16 residuals while group 2 still
+// runs the INTER8 chain).
+constexpr int BAR_POOL = 13;
+
 template <bool WIN>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
@@ -309,6 +353,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             if (!skip_wins) {
                 // ---- phase 1: searches on four warp groups
                 const long long tg0 = (U.prof && gt == 0) ? clock64() : 0;
+                if (tid < 4) cs_reset(&S.sink[tid]);
                 if (grp == 0) {
                     int mx, my;
                     int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
@@ -360,67 +405,38 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     if (sel >= 0)
                         for (int p = gt; p < 256; p += 128) S.pr[2][p] = (uint8_t)nn_px(S.nn[sel], S.top, S.left, p & 15, p >> 4);
                 }
+                if (grp != 2) {
+                    // the pool: residuals of candidates 0 (INTER16 nearest), 1
+                    // (INTER16 second, with two references) and 2 (INTRA16, when
+                    // a sub-mode is allowed), three warp tasks per region
+                    team_bar(BAR_POOL, 384);
+                    const int pw = warp < 8 ? warp : warp - 4;      // 0..11
+                    const unsigned pmask = 0xFu | (navail > 1 ? 0xF0u : 0u) | (S.isel >= 0 ? 0xF00u : 0u);
+                    for (int t = pw; t < 36; t += 12) {
+                        const int g = t / 3, j = t - 3 * g;
+                        if ((pmask >> g) & 1u) resid_task(S, g, j, qp, lambda, warp, lane);
+                    }
+                    team_bar(BAR_POOL, 384);
+                    const int c = grp == 3 ? 2 : grp;
+                    if ((pmask >> (4 * c)) & 1u) group_decide(S, c, lambda, gw, gt, lane, 9 + grp, err);
+                }
                 if (U.prof && gt == 0) atomicAdd(&U.prof[PP_G0 + grp], (unsigned long long)(clock64() - tg0));
                 __syncthreads();
                 pc.mark(PP_SEARCH);
-                // ---- phase 2: residuals of every candidate at once
+                // ---- phase 2: the INTER8 residual, on every warp
                 const int isel = S.isel, ssad = S.ssad;
                 const bool have1 = navail > 1, haveI = isel >= 0;
-                // INTER8 residuals are needed unless the SAD gate rejects the
-                // split whichever INTER16 reference ends up chosen.
+                // needed unless the SAD gate rejects the split whichever INTER16
+                // reference ends up chosen
                 auto gate_skip = [&](int s16) { return s16 > 0 && ssad * 10 >= s16 * 9; };
                 const bool need8 = !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
-                const unsigned pres = 0xFu | (have1 ? 0xF0u : 0u) | (haveI ? 0xF00u : 0u) | (need8 ? 0xF000u : 0u);
-                if (tid < 4) cs_reset(&S.sink[tid]);
-                // 32 block pairs (4x4 blocks 0-1 and 2-3 of region g, one per
-                // half-warp) and the 16 regions' 8x8 options: three warp tasks each
-                for (int pi = warp; pi < 32; pi += 16) {
-                    const int g = pi >> 1, s0 = (pi & 1) * 2, sy = (s0 >> 1) * 4;
-                    if (!((pres >> g) & 1u)) continue;
-                    const uint8_t *cp, *pp;
-                    int pstr;
-                    if (g < 12) {
-                        const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
-                        cp = S.cur + (ry + sy) * 16 + rx; pp = S.pr[c] + (ry + sy) * 16 + rx; pstr = 16;
-                    } else {
-                        const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                        cp = S.cur + (qy + sy) * 16 + qx; pp = S.pred8[q] + sy * 8; pstr = 8;
-                    }
-                    warp_block4x2(cp, cp + 4, 16, pp, pp + 4, pstr, &S.recA[g][sy * 8], &S.recA[g][sy * 8 + 4], 8, S.q,
-                                  lambda, true, &S.blk[4 * g + s0], &S.blk[4 * g + s0 + 1], &S.b4[2 * warp], lane);
+                if (need8) {
+                    if (warp < 12) resid_task(S, 12 + warp / 3, warp % 3, qp, lambda, warp, lane);
+                    __syncthreads();
+                    pc.mark(PP_RESID);
+                    if (grp == 2) group_decide(S, 3, lambda, gw, gt, lane, 11, err);
+                    __syncthreads();
                 }
-                {
-                    const int g = warp;
-                    if ((pres >> g) & 1u) {
-                        const uint8_t *cp, *pp;
-                        int pstr;
-                        if (g < 12) {
-                            const int c = g >> 2, rr = g & 3, rx = (rr & 1) * 8, ry = (rr >> 1) * 8;
-                            cp = S.cur + ry * 16 + rx; pp = S.pr[c] + ry * 16 + rx; pstr = 16;
-                        } else {
-                            const int q = g - 12, qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                            cp = S.cur + qy * 16 + qx; pp = S.pred8[q]; pstr = 8;
-                        }
-                        warp_region8(cp, 16, pp, pstr, qp, &S.reg[g], &S.r8w[warp], lane);
-                    }
-                }
-                __syncthreads();
-                pc.mark(PP_RESID);
-                {   // region decisions (fdv.h:5379-5411): candidate c on warp group c
-                    const int c = grp;
-                    if ((pres >> (4 * c)) & 1u) {
-                        if (gt < 4) region_choice(&S.blk[4 * (4 * c + gt)], S.reg[4 * c + gt], lambda, S.dec[4 * c + gt]);
-                        gbar(9 + grp, 128);
-                        if (gt == 0) {
-                            S.cD[c] = 0;
-                            S.cB[c] = 0;
-                            region_offsets(&S.dec[4 * c], 4, &S.sink[c], false, &S.cD[c], &S.cB[c], err);
-                        }
-                        gbar(9 + grp, 128);
-                        region_symbols(S.dec[4 * c + gw], &S.blk[4 * (4 * c + gw)], S.reg[4 * c + gw], &S.sink[c], false, lane);
-                    }
-                }
-                __syncthreads();
                 pc.mark(PP_DECIDE);
                 // ---- phase 3: the reference's decision on these results
                 double Jbest = Js, Ji = 1e30, Jintra = 1e30, J8 = 1e30;
