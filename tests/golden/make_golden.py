@@ -46,7 +46,23 @@ CASES = [
      dict(qp=51, keyint=2, band_mbrows=None, search_range=64)),
     ("bands_q12", dict(w=192, h=160, nframes=6, nrects=8, pan_qx=-6, pan_qy=3, static_pct=20, seed=9),
      dict(qp=12, keyint=4, band_mbrows=3, search_range=16)),
+    # the 1080p stress shape: 1920x1088 (the format has no crop), 17 bands of 4
+    # macroblock rows, range +-64, QP 20, fast objects (up to 24 px/frame)
+    ("c3_1088_r64", dict(w=1920, h=1088, nframes=4, nrects=200, rect_min=8, rect_max=96, vmax_qpel=96, pan_qx=6,
+                         pan_qy=-3, static_pct=0, seed=3),
+     dict(qp=20, keyint=60, band_mbrows=4, search_range=64)),
 ]
+
+# Independent streams of mixed sizes and QPs coded together (one engine, one
+# launch per frame step): each must equal the reference's fdv_video_encode.
+BATCH = [
+    dict(w=320, h=240, nframes=5, nrects=6, seed=21, qp=18),
+    dict(w=640, h=368, nframes=5, nrects=12, pan_qx=5, seed=22, qp=27),
+    dict(w=1280, h=720, nframes=5, nrects=40, pan_qx=9, static_pct=40, seed=23, qp=36),
+    dict(w=1920, h=1088, nframes=5, nrects=60, pan_qx=-4, pan_qy=2, seed=24, qp=22),
+    dict(w=320, h=240, nframes=5, nrects=10, pan_qy=7, seed=25, qp=31),
+]
+BATCH_KEYINT = 3
 
 
 # Streaming encodes (fdv_enc_*) under average-bitrate control: (name, scene
@@ -92,6 +108,13 @@ def main() -> None:
             "decoded_sha256": sha(dec.tobytes()),
         }
         print(name, len(s), flush=True)
+    out["batch"] = {"keyint": BATCH_KEYINT, "search_range": 16, "streams": []}
+    for bk in BATCH:
+        skw = {k: v for k, v in bk.items() if k != "qp"}
+        fr = scene(skw)
+        s = O.ref_video_encode(fr, bk["w"], bk["h"], bk["qp"], BATCH_KEYINT, 16)
+        out["batch"]["streams"].append({"scene": skw, "qp": bk["qp"], "stream_sha256": sha(s), "stream_len": len(s)})
+        print("batch", bk["w"], bk["h"], len(s), flush=True)
     out["streams"] = {}
     for name, skw, ekw in STREAMS:
         fr = scene(skw)

@@ -77,7 +77,8 @@ def test_keyframe_matches_oracle(built, w, h, qp, seed):
     eng.close()
 
 
-@pytest.mark.parametrize("name", ["cif30", "pan256_k5", "tiny_q0", "tiny_q51_r64", "bands_q12", "hd720_g12"])
+@pytest.mark.parametrize("name", ["cif30", "pan256_k5", "tiny_q0", "tiny_q51_r64", "bands_q12", "hd720_g12",
+                                  "c3_1088_r64"])
 def test_stream_matches_reference(built, golden, name):
     import fdv_b200 as F
     case = golden["cases"][name]
@@ -243,3 +244,36 @@ def test_gpu_stream_counts_equal_host_counts(built):
                 for k in range(16):
                     assert np.array_equal(hg[k], np.bincount(np.frombuffer(st[k], np.uint8), minlength=256)), (u, k)
     eng.close()
+
+
+def test_batched_streams_match_reference(built, golden):
+    """Independent streams of mixed sizes (320x240 .. 1920x1088) and QPs coded
+    by one engine -- every frame step one P-frame launch (or one key-frame
+    launch) for all of them -- each equal to the reference's fdv_video_encode."""
+    import fdv_b200 as F
+    import oracle as O
+    B = golden["batch"]
+    K, specs = B["keyint"], B["streams"]
+    frames = [scene_frames(sp["scene"]) for sp in specs]
+    sizes = [(sp["scene"]["w"], sp["scene"]["h"]) for sp in specs]
+    nf = specs[0]["scene"]["nframes"]
+    eng = F.Engine(sizes, B["search_range"])
+    tcs = [F.TabCache() for _ in specs]
+    blobs = [[] for _ in specs]
+    for f in range(nf):
+        intra = int(f % K == 0)
+        eng.step([fr[f] for fr in frames], [intra] * len(specs), [sp["qp"] for sp in specs])
+        for u, sp in enumerate(specs):
+            (w, h), qp = sizes[u], sp["qp"]
+            if intra:
+                tcs[u].reset()
+                pw, ph = [w, w // 2, w // 2], [h, h // 2, h // 2]
+                blobs[u].append(O.iframe_blob([F.entropy_image(eng.iframe_streams(u, p), pw[p], ph[p], qp)
+                                               for p in range(3)]))
+            else:
+                blobs[u].append(F.entropy_pframe(eng.pframe_streams(u), qp, tcs[u]))
+    eng.close()
+    for u, sp in enumerate(specs):
+        st = O.compose_video(sizes[u][0], sizes[u][1], nf, sp["qp"], K, blobs[u])
+        assert len(st) == sp["stream_len"], u
+        assert sha(st) == sp["stream_sha256"], u
