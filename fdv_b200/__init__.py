@@ -68,6 +68,8 @@ def lib() -> C.CDLL:
         L.fdvg_pframe_streams.argtypes = [p, i, C.POINTER(u8p), C.POINTER(sz)]
         L.fdvg_iframe_streams.argtypes = [p, i, i, C.POINTER(u8p), C.POINTER(sz)]
         L.fdvg_pframe_hist.argtypes = [p, i, C.POINTER(C.c_uint32)]
+        L.fdvg_submit.argtypes = [p, C.POINTER(u8p), C.POINTER(i), C.POINTER(i), C.c_void_p, C.c_void_p]
+        L.fdvg_collect.argtypes = [p]
         L.fdvg_iframe_hist.argtypes = [p, i, i, C.POINTER(C.c_uint32)]
         L.fdvg_recon.argtypes = [p, i, u8p]
         L.fdvg_set_refs.argtypes = [p, i, u8p, u8p]
@@ -214,6 +216,18 @@ class Engine:
             raise FdvError(last_error() or "fdvg_create failed")
 
     def step(self, frames, is_intra, qp, lscale=None, force_skip=None) -> None:
+        """One frame for every unit (fdvg_frame)."""
+        self._call("fdvg_frame", frames, is_intra, qp, lscale, force_skip)
+
+    def submit(self, frames, is_intra, qp, lscale=None, force_skip=None) -> None:
+        """Queue one frame for every unit (fdvg_submit); collect() waits for the oldest."""
+        self._call("fdvg_submit", frames, is_intra, qp, lscale, force_skip)
+
+    def collect(self) -> None:
+        if lib().fdvg_collect(self._g) != 0:
+            raise FdvError(last_error())
+
+    def _call(self, fn, frames, is_intra, qp, lscale, force_skip) -> None:
         n = len(self.sizes)
         self._keep = []
         planes = (u8p * (3 * n))()
@@ -230,7 +244,7 @@ class Engine:
         qq = (C.c_int * n)(*[int(x) for x in qp])
         ls = (C.c_double * n)(*lscale) if lscale is not None else None
         fs = (C.c_int * n)(*[int(x) for x in force_skip]) if force_skip is not None else None
-        if lib().fdvg_frame(self._g, planes, ii, qq, ls, fs) != 0:
+        if getattr(lib(), fn)(self._g, planes, ii, qq, ls, fs) != 0:
             raise FdvError(last_error())
 
     def pframe_streams(self, u: int) -> list[bytes]:

@@ -572,6 +572,17 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
     if (rc) set_engine_err();
     return rc;
 }
+int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                const double *lscale, const int *force_skip) {
+    int rc = fdvb_engine_submit(g, planes, is_intra, qp, lscale, force_skip);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_collect(fdvg_ctx *g) {
+    int rc = fdvb_engine_collect(g);
+    if (rc) set_engine_err();
+    return rc;
+}
 int fdvg_pframe_streams(fdvg_ctx *g, int u, const uint8_t **s16, size_t *n16) {
     const fdvb_streams *s = fdvb_engine_pstreams(g, u);
     if (!s || !s16 || !n16) { set_err("no P-frame streams for this unit"); return -1; }

@@ -129,6 +129,16 @@ void fdvg_destroy(fdvg_ctx *g);
  * lscale may be NULL (1.0: the fractional-lambda multiplier of fdv.h:5804). */
 int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
                const double *lscale, const int *force_skip);
+/* fdvg_frame in two halves, so a host can entropy-code one frame while the GPU
+ * analyses the next: fdvg_submit copies the sources (through pinned staging;
+ * the caller may reuse its buffers on return) and queues the frame; at most
+ * two frames are in flight.  fdvg_collect waits for the oldest one, after which
+ * the stream and count accessors describe it until the next fdvg_collect.  A
+ * caller keeps the streams of collected frame f only until it submits frame
+ * f + 2. */
+int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                const double *lscale, const int *force_skip);
+int fdvg_collect(fdvg_ctx *g);
 /* The last frame's symbol streams of unit u.  P-frame: 16 streams in the
  * blob's order (9 structure streams by model, then 4x4 counts, 4x4 levels,
  * 8x8 counts, 8x8 levels, region flags, chroma counts, chroma levels).  Key

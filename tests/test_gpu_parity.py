@@ -277,3 +277,27 @@ def test_batched_streams_match_reference(built, golden):
         st = O.compose_video(sizes[u][0], sizes[u][1], nf, sp["qp"], K, blobs[u])
         assert len(st) == sp["stream_len"], u
         assert sha(st) == sp["stream_sha256"], u
+
+
+def test_submit_collect_pipeline_equals_step(built):
+    """fdvg_submit / fdvg_collect with two frames in flight give every frame
+    the same streams and reconstruction as fdvg_frame one at a time."""
+    import fdv_b200 as F
+    w, h = 160, 96
+    fr = F.Scene(w, h, 5, nrects=5, pan_qx=7, seed=31).frames(5)
+    ref = F.Engine([(w, h)], 16)
+    want = []
+    for f in range(5):
+        ref.step([fr[f]], [int(f == 0)], [26])
+        want.append([ref.iframe_streams(0, p) for p in range(3)] if f == 0 else ref.pframe_streams(0))
+    ref.close()
+    eng = F.Engine([(w, h)], 16)
+    got = []
+    for f in range(6):
+        if f < 5:
+            eng.submit([fr[f]], [int(f == 0)], [26])
+        if f > 0:
+            eng.collect()
+            got.append([eng.iframe_streams(0, p) for p in range(3)] if f == 1 else eng.pframe_streams(0))
+    eng.close()
+    assert got == want
