@@ -72,6 +72,16 @@ def lib() -> C.CDLL:
         L.fdvg_collect.argtypes = [p]
         L.fdvg_iframe_hist.argtypes = [p, i, i, C.POINTER(C.c_uint32)]
         L.fdvg_recon.argtypes = [p, i, u8p]
+        L.fdvg_set_learned.argtypes = [p, C.POINTER(C.c_float), C.c_float]
+        L.fdvg_set_records.argtypes = [p, i]
+        L.fdvg_set_learned_conf.argtypes = [p, C.POINTER(C.c_float)]
+        L.fdvg_mb_records.argtypes = [p, i, u8p, C.POINTER(C.c_int16), u8p, C.POINTER(C.c_float)]
+        L.fdvb_set_learned.argtypes = [C.POINTER(C.c_float), C.c_float]
+        dd, ll = C.c_double, C.c_longlong
+        L.fdvg_stats.argtypes = [p] + [C.POINTER(t) for t in (dd, dd, ll, dd, ll, ll, ll, ll)]
+        L.fdvg_stats.restype = None
+        L.fdvg_stats_reset.argtypes = [p]
+        L.fdvg_stats_reset.restype = None
         L.fdvg_set_refs.argtypes = [p, i, u8p, u8p]
         L.fdvb_tabcache_new.restype = p
         L.fdvb_tabcache_reset.argtypes = [p]
@@ -126,6 +136,13 @@ def set_search_range(r: int) -> int:
 
 def get_search_range() -> int:
     return lib().fdvb_get_search_range()
+
+
+def set_learned(params, conf: float = 0.8) -> None:
+    """Learned proposals for the fdv_* encoders from the next call on (fdvb_set_learned); None: off."""
+    a = None if params is None else np.ascontiguousarray(params, np.float32)
+    if lib().fdvb_set_learned(a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None, conf) != 0:
+        raise FdvError(last_error())
 
 
 def video_encode(frames, w: int, h: int, qp: int, keyint: int) -> bytes:
@@ -274,6 +291,47 @@ class Engine:
         if lib().fdvg_iframe_hist(self._g, u, plane, h.ctypes.data_as(C.POINTER(C.c_uint32))) != 0:
             raise FdvError(last_error())
         return h
+
+    def set_learned(self, params, conf: float = 0.8) -> None:
+        """Learned proposals for later P-frames (fdvg_set_learned); None: off."""
+        a = None if params is None else np.ascontiguousarray(params, np.float32)
+        ptr = a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+        if lib().fdvg_set_learned(self._g, ptr, conf) != 0:
+            raise FdvError(last_error())
+
+    def set_learned_conf(self, conf3) -> None:
+        """Per-class thresholds (SKIP, inter, intra); above 1 keeps a class on the full search."""
+        a = (C.c_float * 3)(*[float(c) for c in conf3])
+        if lib().fdvg_set_learned_conf(self._g, a) != 0:
+            raise FdvError(last_error())
+
+    def stats(self) -> dict:
+        """Device-timed totals since creation or stats_reset() (fdvg_stats)."""
+        v = [C.c_double(), C.c_double(), C.c_longlong(), C.c_double(), C.c_longlong(), C.c_longlong(),
+             C.c_longlong(), C.c_longlong()]
+        lib().fdvg_stats(self._g, *[C.byref(x) for x in v])
+        k = ["step_ms", "p_ms", "p_launches", "i_ms", "i_launches", "launches", "steps", "d2h_bytes"]
+        return {n: x.value for n, x in zip(k, v)}
+
+    def stats_reset(self) -> None:
+        lib().fdvg_stats_reset(self._g)
+
+    def set_records(self, on: bool) -> None:
+        if lib().fdvg_set_records(self._g, int(on)) != 0:
+            raise FdvError(last_error())
+
+    def mb_records(self, u: int, cost: bool = True) -> dict:
+        """The last P-frame's per-macroblock mode, MV, reference (and RD cost)."""
+        w, h = self.sizes[u]
+        n = (w // 16) * (h // 16)
+        mode = np.empty(n, np.uint8)
+        mv = np.empty((n, 2), np.int16)
+        ref = np.empty(n, np.uint8)
+        c = np.empty(n, np.float32) if cost else None
+        if lib().fdvg_mb_records(self._g, u, _ptr(mode), mv.ctypes.data_as(C.POINTER(C.c_int16)), _ptr(ref),
+                                 c.ctypes.data_as(C.POINTER(C.c_float)) if cost else None) != 0:
+            raise FdvError(last_error())
+        return {"mode": mode, "mv": mv, "ref": ref, "cost": c}
 
     def recon(self, u: int) -> np.ndarray:
         w, h = self.sizes[u]

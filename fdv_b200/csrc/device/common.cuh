@@ -150,6 +150,7 @@ __device__ __forceinline__ uint8_t *slot_data(uint8_t *slot, int k) { return slo
 enum : unsigned {
     kErrWaitTimeout = 1u,    // a wavefront wait gave up
     kErrSlotOverflow = 2u,   // a symbol stream exceeded its per-block slot
+    kErrMmaTimeout = 4u,     // a tensor-core completion wait gave up
 };
 
 // Bounded spin until *flag >= need.  Gives up after `limit_ns` of wall time

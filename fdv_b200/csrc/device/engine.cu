@@ -117,6 +117,7 @@ struct Unit {
     uint32_t *hist_h[2] = {nullptr, nullptr}, *hist_d[2] = {nullptr, nullptr};
     size_t out_cap = 0, out_off_i[3] = {0, 0, 0};
     int last_intra = 0, last_qp = 0;
+    int mb_off = 0;               // first macroblock of this unit in engine-wide per-macroblock arrays
     fdvb_streams ps{}, is[3]{};
 };
 
@@ -160,6 +161,14 @@ struct fdvb_engine {
     std::vector<int> pending_intra;         // frame types of the uncommitted step
     bool pending = false;
     unsigned long long *d_prof = nullptr;   // phase profile accumulators (when enabled)
+    // learned proposals: a private inference network, its per-macroblock
+    // hints and the P units of the current step ({unit, first macroblock})
+    fdvl_net *lnet = nullptr;
+    float3 lconf = {0.8f, 0.8f, 0.8f};       // per class: SKIP, inter, intra (> 1: never)
+    lrn::Hint *d_hints = nullptr;
+    int2 *d_pu = nullptr;
+    int total_mbs = 0;
+    float *d_mbcost = nullptr;              // per-macroblock RD cost records (when enabled)
 };
 
 static int round_up(int v, int a) { return (v + a - 1) / a * a; }
@@ -230,7 +239,7 @@ static size_t stage_desc_bytes(int nu, int maxrows, int maxitasks) {
     auto a = [](size_t n) { return (n + 63) / 64 * 64; };
     return a(sizeof(UnitDev) * nu) + a(sizeof(RowTask) * maxrows) + a(sizeof(IPlaneDevH) * 3 * nu) +
            a(sizeof(ITaskH) * maxitasks) + a(sizeof(PrepTaskH) * nu) + a(sizeof(DbTaskH) * 3 * nu) +
-           a(sizeof(CompactTaskH) * 3 * nu);
+           a(sizeof(CompactTaskH) * 3 * nu) + a(sizeof(int2) * nu);
 }
 
 extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
@@ -260,6 +269,7 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
         for (int p = 0; p < 3; ++p) maxitasks += E->units[i].irows[p];
     }
     E->maxrows = maxrows; E->maxitasks = maxitasks;
+    for (auto &u : E->units) { u.mb_off = E->total_mbs; E->total_mbs += u.mbw * u.mbh; }
     bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_rows, sizeof(RowTask) * maxrows) == cudaSuccess &&
               cudaMalloc(&E->d_planes, sizeof(IPlaneDevH) * 3 * nunits) == cudaSuccess &&
@@ -302,6 +312,8 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
     if (E->d_prof) cudaFree(E->d_prof);
+    if (E->lnet) fdvl_destroy(E->lnet);
+    cudaFree(E->d_hints); cudaFree(E->d_pu); cudaFree(E->d_mbcost);
     for (auto &sl : E->slot) {
         for (auto &e : sl.ev) if (e) cudaEventDestroy(e);
         if (sl.stage) cudaFreeHost(sl.stage);
@@ -404,6 +416,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
     std::vector<ITaskH> itasks;
     std::vector<CompactTaskH> cmp;
     std::vector<DbTaskH> db;
+    std::vector<int2> pu;   // P units and their first macroblock in the hint array
+    int nhint = 0;
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         UnitDev &d = ud[i];
@@ -418,6 +432,13 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
         d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
         d.prof = E->d_prof;
+        d.hint = nullptr;
+        d.mbcost = E->d_mbcost ? E->d_mbcost + u.mb_off : nullptr;
+        if (!is_intra[i] && E->lnet) {
+            pu.push_back(make_int2(i, nhint));
+            d.hint = E->d_hints + nhint;
+            nhint += u.mbw * u.mbh;
+        }
         SL.intra[i] = is_intra[i];
         u.last_qp = qp[i];
         if (!is_intra[i]) {
@@ -469,7 +490,18 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         CK(cudaMemcpyAsync(E->d_rows, staged(rows.data(), sizeof(RowTask) * rows.size()), sizeof(RowTask) * rows.size(),
                            cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)rows.size(), E->nsm);
+        if (!pu.empty())
+            CK(cudaMemcpyAsync(E->d_pu, staged(pu.data(), sizeof(int2) * pu.size()), sizeof(int2) * pu.size(),
+                               cudaMemcpyHostToDevice, E->st));
         CK(cudaEventRecord(SL.ev[1], E->st));
+        if (!pu.empty()) {
+            if (lrn_infer_units(E->lnet, E->d_units, E->d_pu, (int)pu.size(), nhint, E->lconf, 4 * E->range,
+                                E->d_hints, E->d_err, E->st) != 0) {
+                g_err = std::string("learned inference: ") + fdvl_last_error();
+                return -3;
+            }
+            E->launches += 1;
+        }
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range, E->st);
         CK(cudaGetLastError());
         CK(cudaEventRecord(SL.ev[2], E->st));
@@ -540,7 +572,8 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     }
     const unsigned err = *SL.err_h;
     if (err) {
-        g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out" : "symbol slot overflow";
+        g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out"
+                : (err & kErrMmaTimeout) ? "tensor-core completion wait timed out" : "symbol slot overflow";
         return -4;
     }
     for (int i = 0; i < (int)E->units.size(); ++i) {
@@ -683,5 +716,72 @@ extern "C" int fdvb_engine_commit_refs(fdvb_engine *E) {
         u.nref = E->pending_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
     }
     E->pending = false;
+    return 0;
+}
+
+// Learned proposals for every later P-frame (params: fdvl_nparams() floats;
+// NULL turns them off).  The engine owns a private inference network.
+extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, float conf) {
+    if (!E) return -1;
+    CK(cudaSetDevice(E->device));
+    if (!params) {
+        if (E->lnet) { cudaStreamSynchronize(E->st); fdvl_destroy(E->lnet); E->lnet = nullptr; }
+        return 0;
+    }
+    if (!E->lnet) {
+        E->lnet = lrn_create(E->device, E->total_mbs, 0, 16, 16);
+        if (!E->lnet) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
+        if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * E->total_mbs));
+        if (!E->d_pu) CK(cudaMalloc(&E->d_pu, sizeof(int2) * E->units.size()));
+    }
+    CK(cudaStreamSynchronize(E->st));
+    if (fdvl_set_params(E->lnet, params) != 0) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
+    E->lconf = make_float3(conf, conf, conf);
+    return 0;
+}
+
+// Per-class confidence thresholds of the learned proposals (SKIP, inter,
+// intra); a threshold above 1 turns that class's narrowed analysis off.
+extern "C" int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf3) {
+    if (!E || !conf3) return -1;
+    E->lconf = make_float3(conf3[0], conf3[1], conf3[2]);
+    return 0;
+}
+
+// Per-macroblock decision records of the last collected P-frame: mode
+// (0 SKIP, 1 INTER16, 2 INTRA16, 3 INTER8), MV (the neighbour-prediction
+// vector: INTER8 keeps its last quadrant's), reference and RD cost (when
+// enabled before the frame).  Any output may be NULL.
+extern "C" int fdvb_engine_records(fdvb_engine *E, int enable) {
+    if (!E) return -1;
+    CK(cudaSetDevice(E->device));
+    if (enable && !E->d_mbcost) {
+        CK(cudaMalloc(&E->d_mbcost, sizeof(float) * E->total_mbs));
+        CK(cudaMemset(E->d_mbcost, 0, sizeof(float) * E->total_mbs));
+    } else if (!enable && E->d_mbcost) {
+        cudaStreamSynchronize(E->st);
+        cudaFree(E->d_mbcost);
+        E->d_mbcost = nullptr;
+    }
+    return 0;
+}
+
+extern "C" int fdvb_engine_mb_records(fdvb_engine *E, int unit, uint8_t *mode, int16_t *mv, uint8_t *ref, float *cost) {
+    if (!E || unit < 0 || unit >= (int)E->units.size()) { g_err = "bad unit"; return -1; }
+    CK(cudaSetDevice(E->device));
+    CK(cudaStreamSynchronize(E->st));
+    Unit &u = E->units[unit];
+    const int n = u.mbw * u.mbh;
+    std::vector<MBInfo> mi(n);
+    CK(cudaMemcpy(mi.data(), u.mbi, sizeof(MBInfo) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+        if (mode) mode[i] = mi[i].mode;
+        if (mv) { mv[2 * i] = mi[i].x; mv[2 * i + 1] = mi[i].y; }
+        if (ref) ref[i] = mi[i].ref;
+    }
+    if (cost) {
+        if (!E->d_mbcost) { g_err = "cost records are off"; return -1; }
+        CK(cudaMemcpy(cost, E->d_mbcost + u.mb_off, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
     return 0;
 }

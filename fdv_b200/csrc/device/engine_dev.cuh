@@ -1,6 +1,7 @@
 // Device-side descriptors of the batched encoder engine.
 #pragma once
 #include "common.cuh"
+#include "learned.cuh"
 
 namespace fdvb {
 
@@ -18,6 +19,8 @@ struct UnitDev {
     int qp, navail, force_skip, range;
     int stall_row;              // test hook: this row never runs (-1: none)
     unsigned long long *prof;   // optional per-phase cycle accumulators (NULL: off)
+    const lrn::Hint *hint;      // learned proposals per macroblock (NULL: the plain search)
+    float *mbcost;              // per macroblock: RD cost of the chosen mode (NULL: off)
 };
 
 // Phases of a macroblock, for the optional cycle profile.

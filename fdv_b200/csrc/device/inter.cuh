@@ -148,7 +148,8 @@ __device__ __forceinline__ int sad_packed(uint32_t c0, uint32_t c1, const Src &R
 template <int BS, class Src>
 __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by, int range, int pmx, int pmy,
                                int *mvx, int *mvy, int *s_sad, int gw, int lane, int bar,
-                               unsigned long long *iters = nullptr) {
+                               unsigned long long *iters = nullptr, const short2 *cands = nullptr, int ncands = 0,
+                               int max_ld = 64) {
     constexpr bool DB = BS == 8;
     const int lim = range * 4;
     uint32_t c0, c1 = 0;
@@ -168,11 +169,24 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
     py = py < -lim ? -lim : (py > lim ? lim : py);
     const bool seed = px != 0 || py != 0;
     int best, bxv = 0, byv = 0;
-    {   // the zero vector (k = 0) and the seed (k = 1)
+    // extra starting points (16x16 only): whole-pel positions of the proposals
+    auto cand_at = [&](int k, int &x, int &y) {
+        x = (cands[k].x >> 2) * 4;
+        y = (cands[k].y >> 2) * 4;
+        x = x < -lim ? -lim : (x > lim ? lim : x);
+        y = y < -lim ? -lim : (y > lim ? lim : y);
+    };
+    {   // the zero vector (k = 0), the seed (k = 1) and any proposals (k = 2..)
         int *s = scores();
         if (BS == 16) {
             if (gw == 0) { int v = sad_packed<16>(c0, c1, R, bx, by, 0, 0, lane); if (lane == 0) s[0] = v; }
             if (gw == 1 && seed) { int v = sad_packed<16>(c0, c1, R, bx, by, px, py, lane); if (lane == 0) s[1] = v; }
+            for (int k = 2 + gw; k < 2 + ncands; k += 4) {
+                int x, y;
+                cand_at(k - 2, x, y);
+                int v = sad_packed<16>(c0, c1, R, bx, by, x, y, lane);
+                if (lane == 0) s[k] = v;
+            }
         } else if (gw == 0) {
             const int hk = lane >> 4;
             int v = sad_packed<8>(c0, c1, R, bx, by, hk ? px : 0, hk ? py : 0, lane);
@@ -181,9 +195,14 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
         gbar(bar, 128);
         best = s[0];
         if (seed && s[1] < best) { best = s[1]; bxv = px; byv = py; }
+        for (int k = 0; k < ncands; ++k) {
+            int x, y;
+            cand_at(k, x, y);
+            if (s[2 + k] < best) { best = s[2 + k]; bxv = x; byv = y; }
+        }
         end_step();
     }
-    for (int it = 0; it < 64; ++it) {   // large diamond
+    for (int it = 0; it < max_ld; ++it) {   // large diamond
         const int cx = bxv, cy = byv;
         int *s = scores();
         if (BS == 16) {

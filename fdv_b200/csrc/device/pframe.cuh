@@ -43,6 +43,8 @@ struct PShared {
     int tl, ht, hl, ctl[2];
     MBInfo cand[3];
     int ncand, ssd3[3];
+    short2 lmv[lrn::kMvHyp];     // learned proposals of this macroblock
+    int lcls;                    // their confident class, -1: none
     uint8_t predS[3][256];
     // phase 1
     uint8_t pr[3][256];          // 16x16 predictions: nearest ref, second ref, selected intra
@@ -197,6 +199,9 @@ __device__ __forceinline__ void group_decide(PShared &S, int c, double lambda, i
 // runs the INTER8 chain).
 constexpr int BAR_POOL = 13;
 
+// Large-diamond steps of the 16x16 search when it starts from learned proposals.
+constexpr int kLearnLd = 4;
+
 template <bool WIN>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
@@ -291,6 +296,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 }
                 S.ncand = n;
                 S.amode = row > 0 ? (int)((nb[0].y >> 16) & 0xffu) : 0;
+                S.lcls = -1;
+                if (U.hint) {
+                    const lrn::Hint hh = U.hint[row * mbw + mbx];
+                    S.lcls = hh.cls;
+                    for (int k = 0; k < lrn::kMvHyp; ++k) S.lmv[k] = hh.mv[k];
+                }
             }
             __syncthreads();
             // mode context (fdv.h:4172): left / above macroblock skipped-ness;
@@ -313,6 +324,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     write_slot_structs(slot, ctx, &m0, 1, err);
                     MBInfo mi = {0, 0, 0, 1, 0, 0};
                     U.mbi[row * mbw + mbx] = mi;
+                    if (U.mbcost) U.mbcost[row * mbw + mbx] = 0.f;
                 }
                 pmvx = 0; pmvy = 0;
                 prev_mode = 0;
@@ -345,7 +357,17 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             for (int mi = 1; mi < ncand; ++mi) if (S.ssd3[mi] < Ds) { Ds = S.ssd3[mi]; best_mi = mi; }
             const int midx_bits = ncand > 1 ? kBitsMode : 0;
             const double Js = rd_cost((double)Ds, lambda, kBitsMode + midx_bits);
-            const bool skip_wins = Js <= lam14;
+            // A confident learned proposal narrows the analysis: SKIP takes the
+            // best merge candidate; inter searches only the nearest reference's
+            // 16x16 vector, from the proposed vectors (a few diamond steps and
+            // the sub-pel refinement), without the INTER8 chain and intra;
+            // intra skips the motion searches.  Without a confident class the
+            // full analysis runs, its nearest-reference 16x16 search seeded
+            // with the proposed vectors as well.
+            const int lcls = S.lcls;
+            const bool lfast = lcls >= 0, l_intra = lcls == 2;
+            const bool skip_wins = Js <= lam14 || lcls == 0;
+            double Jc = Js;   // RD cost of the chosen mode
             pc.mark(PP_SKIP);
             if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); if (skip_wins) atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
 
@@ -355,55 +377,66 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const long long tg0 = (U.prof && gt == 0) ? clock64() : 0;
                 if (tid < 4) cs_reset(&S.sink[tid]);
                 if (grp == 0) {
-                    int mx, my;
-                    int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
-                                                 U.prof ? &U.prof[PP_IT16] : nullptr);
-                    if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
-                    mc16_group(L0, bx, by, mx, my, S.pr[0], gt);
+                    if (!l_intra) {
+                        int mx, my;
+                        // with proposals the search also starts from them; a full
+                        // search (not confident) still runs the diamond to the end
+                        int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
+                                                     U.prof ? &U.prof[PP_IT16] : nullptr, U.hint ? S.lmv : nullptr,
+                                                     U.hint ? lrn::kMvHyp : 0, lfast ? kLearnLd : 64);
+                        if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
+                        mc16_group(L0, bx, by, mx, my, S.pr[0], gt);
+                    }
                 } else if (grp == 1) {
-                    if (navail > 1) {
+                    if (navail > 1 && !lfast) {
                         int mx, my;
                         int sd = me_search_group<16>(S.cur, L1, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10);
                         if (gt == 0) { S.mv[1][0] = mx; S.mv[1][1] = my; S.sad[1] = sd; }
                         mc16_group(L1, bx, by, mx, my, S.pr[1], gt);
                     }
                 } else if (grp == 2) {
-                    int qpx = pmvx, qpy = pmvy, ssad = 0;
-                    for (int q = 0; q < 4; ++q) {
-                        const int qx = (q & 1) * 8, qy = (q >> 1) * 8;
-                        int mx, my;
-                        ssad += me_search_group<8>(S.cur + qy * 16 + qx, L0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
-                                                   S.gsad[2], gw, lane, 11, U.prof ? &U.prof[PP_IT8] : nullptr);
-                        if (gt == 0) { S.qmv[q][0] = mx; S.qmv[q][1] = my; }
-                        qpx = mx; qpy = my;
-                        if (gt < 16) {
-                            const int r2 = gt >> 1, c2 = (gt & 1) * 4, ph = (my & 3) * 4 + (mx & 3);
-                            reinterpret_cast<uint32_t *>(S.pred8[q])[gt] =
-                                mc_word(L0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
+                    if (!lfast) {
+                        int qpx = pmvx, qpy = pmvy, ssad = 0;
+                        for (int q = 0; q < 4; ++q) {
+                            const int qx = (q & 1) * 8, qy = (q >> 1) * 8;
+                            int mx, my;
+                            ssad += me_search_group<8>(S.cur + qy * 16 + qx, L0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
+                                                       S.gsad[2], gw, lane, 11, U.prof ? &U.prof[PP_IT8] : nullptr);
+                            if (gt == 0) { S.qmv[q][0] = mx; S.qmv[q][1] = my; }
+                            qpx = mx; qpy = my;
+                            if (gt < 16) {
+                                const int r2 = gt >> 1, c2 = (gt & 1) * 4, ph = (my & 3) * 4 + (mx & 3);
+                                reinterpret_cast<uint32_t *>(S.pred8[q])[gt] =
+                                    mc_word(L0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
+                            }
                         }
+                        if (gt == 0) S.ssad = ssad;
                     }
-                    if (gt == 0) S.ssad = ssad;
                 } else {
-                    // intra 16x16 sub-modes, SATD-screened (fdv.h:5961-5970)
-                    if (gt < 4) S.nn[gt] = nn_setup(gt, S.top, S.left, S.tl, 16, S.ht, S.hl);
-                    gbar(12, 128);
-                    if (gt < 64) {
-                        const int m = gt >> 4, b = gt & 15, oy = (b >> 2) * 4, ox = (b & 3) * 4;
-                        uint8_t pk[16];
-                        for (int p = 0; p < 16; ++p) pk[p] = (uint8_t)nn_px(S.nn[m], S.top, S.left, ox + (p & 3), oy + (p >> 2));
-                        S.satd[gt] = satd4(S.cur + oy * 16 + ox, 16, pk, 4);
+                    if (lfast && !l_intra) {
+                        if (gt == 0) S.isel = -1;
+                    } else {
+                        // intra 16x16 sub-modes, SATD-screened (fdv.h:5961-5970)
+                        if (gt < 4) S.nn[gt] = nn_setup(gt, S.top, S.left, S.tl, 16, S.ht, S.hl);
+                        gbar(12, 128);
+                        if (gt < 64) {
+                            const int m = gt >> 4, b = gt & 15, oy = (b >> 2) * 4, ox = (b & 3) * 4;
+                            uint8_t pk[16];
+                            for (int p = 0; p < 16; ++p) pk[p] = (uint8_t)nn_px(S.nn[m], S.top, S.left, ox + (p & 3), oy + (p >> 2));
+                            S.satd[gt] = satd4(S.cur + oy * 16 + ox, 16, pk, 4);
+                        }
+                        gbar(12, 128);
+                        int sel = -1, sbest = 0;
+                        for (int m = 0; m < 4; ++m) {
+                            if (!nn_mode_ok(m, 16, S.ht, S.hl)) continue;
+                            int sa = 0;
+                            for (int b = 0; b < 16; ++b) sa += S.satd[m * 16 + b];
+                            if (sel < 0 || sa < sbest) { sbest = sa; sel = m; }
+                        }
+                        if (gt == 0) S.isel = sel;
+                        if (sel >= 0)
+                            for (int p = gt; p < 256; p += 128) S.pr[2][p] = (uint8_t)nn_px(S.nn[sel], S.top, S.left, p & 15, p >> 4);
                     }
-                    gbar(12, 128);
-                    int sel = -1, sbest = 0;
-                    for (int m = 0; m < 4; ++m) {
-                        if (!nn_mode_ok(m, 16, S.ht, S.hl)) continue;
-                        int sa = 0;
-                        for (int b = 0; b < 16; ++b) sa += S.satd[m * 16 + b];
-                        if (sel < 0 || sa < sbest) { sbest = sa; sel = m; }
-                    }
-                    if (gt == 0) S.isel = sel;
-                    if (sel >= 0)
-                        for (int p = gt; p < 256; p += 128) S.pr[2][p] = (uint8_t)nn_px(S.nn[sel], S.top, S.left, p & 15, p >> 4);
                 }
                 if (grp != 2) {
                     // the pool: residuals of candidates 0 (INTER16 nearest), 1
@@ -411,7 +444,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     // a sub-mode is allowed), three warp tasks per region
                     team_bar(BAR_POOL, 384);
                     const int pw = warp < 8 ? warp : warp - 4;      // 0..11
-                    const unsigned pmask = 0xFu | (navail > 1 ? 0xF0u : 0u) | (S.isel >= 0 ? 0xF00u : 0u);
+                    const unsigned pmask = (l_intra ? 0u : 0xFu) | (navail > 1 && !lfast ? 0xF0u : 0u) |
+                                           (S.isel >= 0 ? 0xF00u : 0u);
                     for (int t = pw; t < 36; t += 12) {
                         const int g = t / 3, j = t - 3 * g;
                         if ((pmask >> g) & 1u) resid_task(S, g, j, qp, lambda, warp, lane);
@@ -429,7 +463,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 // needed unless the SAD gate rejects the split whichever INTER16
                 // reference ends up chosen
                 auto gate_skip = [&](int s16) { return s16 > 0 && ssad * 10 >= s16 * 9; };
-                const bool need8 = !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
+                const bool need8 = !lfast && !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
                 if (need8) {
                     if (warp < 12) resid_task(S, 12 + warp / 3, warp % 3, qp, lambda, warp, lane);
                     __syncthreads();
@@ -441,7 +475,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 // ---- phase 3: the reference's decision on these results
                 double Jbest = Js, Ji = 1e30, Jintra = 1e30, J8 = 1e30;
                 int sad16 = 0;
-                for (int r = 0; r < navail; ++r) {
+                const int nsearch = l_intra ? 0 : (lfast ? 1 : navail);
+                for (int r = 0; r < nsearch; ++r) {
                     if (r > 0 && Jbest <= lam16) break;
                     const int rmx = S.mv[r][0], rmy = S.mv[r][1];
                     const int bb = 2 * kBitsMode + bits_val(zz_enc(rmx - pmvx)) + bits_val(zz_enc(rmy - pmvy)) + S.cB[r];
@@ -454,7 +489,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     best_sub = isel;
                     if (Jintra < Jbest) Jbest = Jintra;
                 }
-                if (Jbest > lam19 && !gate_skip(sad16)) {
+                if (!lfast && Jbest > lam19 && !gate_skip(sad16)) {
                     int b8 = kBitsMode, px = pmvx, py = pmvy;
                     for (int q = 0; q < 4; ++q) {
                         b8 += bits_val(zz_enc(S.qmv[q][0] - px)) + bits_val(zz_enc(S.qmv[q][1] - py));
@@ -466,6 +501,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 if (Ji < Jmin) { Jmin = Ji; chosen = 1; }
                 if (Jintra < Jmin) { Jmin = Jintra; chosen = 2; }
                 if (J8 < Jmin) { Jmin = J8; chosen = 3; }
+                Jc = Jmin;
             }
 
             // ---- commit (fdv.h:6049-6160)
@@ -642,7 +678,10 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     if (tid == 0) slot_len(slot)[PS_CN + k] = (uint16_t)n;
                 }
             }
-            if (tid == 0) U.mbi[row * mbw + mbx] = info;
+            if (tid == 0) {
+                U.mbi[row * mbw + mbx] = info;
+                if (U.mbcost) U.mbcost[row * mbw + mbx] = (float)Jc;
+            }
             prev_mode = chosen;
             // the block's writes are ordered before thread 0's fence by the
             // barrier; the fence then orders them before the progress flag

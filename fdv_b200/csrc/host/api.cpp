@@ -19,6 +19,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -198,34 +199,71 @@ struct CachedEngine {
     int device, range;
     std::vector<int> w, h;
     fdvb_engine *E;
+    int lver;   // version of the learned-proposal setting the engine carries (0: plain)
 };
 constexpr size_t kCacheMax = 4;
 std::mutex g_cache_mu;
 std::vector<CachedEngine> *g_cache = new std::vector<CachedEngine>();   // never destroyed: outlives the CUDA runtime
 
+// The process-wide learned-proposal setting of the fdv_* encoders
+// (fdvb_set_learned): parameters, confidence threshold, and a version that
+// engines compare against the one they carry.
+std::mutex g_learn_mu;
+std::vector<float> *g_learn_params = new std::vector<float>();
+float g_learn_conf = 0.8f;
+int g_learn_ver = 0;       // bumped on every change; 0 never reused
+int g_learn_on = 0;
+std::map<fdvb_engine *, int> *g_engine_lver = new std::map<fdvb_engine *, int>();
+
 fdvb_engine *engine_acquire(int n, const int *w, const int *h, int range, int device) {
+    fdvb_engine *E = nullptr;
+    int ver = 0;
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
         for (size_t i = 0; i < g_cache->size(); ++i) {
             CachedEngine &c = (*g_cache)[i];
             if (c.device == device && c.range == range && (int)c.w.size() == n &&
                 std::equal(c.w.begin(), c.w.end(), w) && std::equal(c.h.begin(), c.h.end(), h)) {
-                fdvb_engine *E = c.E;
+                E = c.E;
+                ver = c.lver;
                 g_cache->erase(g_cache->begin() + (long)i);
-                return E;
+                break;
             }
         }
     }
-    return fdvb_engine_create(n, w, h, range, device);
+    if (!E) E = fdvb_engine_create(n, w, h, range, device);
+    if (!E) return nullptr;
+    std::vector<float> params;
+    float conf;
+    int want, on;
+    {
+        std::lock_guard<std::mutex> lk(g_learn_mu);
+        want = g_learn_ver;
+        on = g_learn_on;
+        conf = g_learn_conf;
+        if (on && want != ver) params = *g_learn_params;
+    }
+    if (want != ver) {
+        if (fdvb_engine_set_learned(E, on ? params.data() : nullptr, conf) != 0) {
+            fdvb_engine_destroy(E);
+            return nullptr;
+        }
+        ver = want;
+    }
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    (*g_engine_lver)[E] = ver;
+    return E;
 }
 void engine_release(fdvb_engine *E, int n, const int *w, const int *h, int range, int device) {
     fdvb_engine *evict = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
-        g_cache->push_back({device, range, std::vector<int>(w, w + n), std::vector<int>(h, h + n), E});
+        const int ver = (*g_engine_lver)[E];
+        g_cache->push_back({device, range, std::vector<int>(w, w + n), std::vector<int>(h, h + n), E, ver});
         if (g_cache->size() > kCacheMax) {
             evict = g_cache->front().E;
             g_cache->erase(g_cache->begin());
+            g_engine_lver->erase(evict);
         }
     }
     if (evict) fdvb_engine_destroy(evict);
@@ -252,6 +290,7 @@ void fdvb_release_engines(void) {
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
         v.swap(*g_cache);
+        for (auto &c : v) g_engine_lver->erase(c.E);
     }
     for (auto &c : v) fdvb_engine_destroy(c.E);
 }
@@ -636,6 +675,38 @@ void fdvg_stats_reset(fdvg_ctx *g) { fdvb_engine_stats_reset(g); }
 void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns) { fdvb_engine_set_wait_ns(g, ns); }
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row) { fdvb_engine_inject_stall(g, u, row); }
 int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out32) { return fdvb_engine_profile(g, enable, out32); }
+
+int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf) {
+    if (!g) { set_err("null context"); return -1; }
+    const int rc = fdvb_engine_set_learned(g, params, conf);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf3) {
+    if (!g || !conf3) { set_err("null argument"); return -1; }
+    return fdvb_engine_learned_conf(g, conf3);
+}
+int fdvg_set_records(fdvg_ctx *g, int enable) {
+    const int rc = fdvb_engine_records(g, enable);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_mb_records(fdvg_ctx *g, int u, uint8_t *mode, int16_t *mv, uint8_t *ref, float *cost) {
+    const int rc = fdvb_engine_mb_records(g, u, mode, mv, ref, cost);
+    if (rc) set_engine_err();
+    return rc;
+}
+
+int fdvb_set_learned(const float *params, float conf) {
+    if (params && !(conf > 0.f && conf <= 1.f)) { set_err("confidence threshold must be in (0, 1]"); return -1; }
+    std::lock_guard<std::mutex> lk(g_learn_mu);
+    if (params) g_learn_params->assign(params, params + fdvl_nparams());
+    else g_learn_params->clear();
+    g_learn_on = params != nullptr;
+    g_learn_conf = conf;
+    ++g_learn_ver;
+    return 0;
+}
 
 // ---------------------------------------------------- entropy tail ABI --
 fdvb_tabcache *fdvb_tabcache_new(void) { return new fdvb_tabcache(); }

@@ -250,6 +250,76 @@ fdvb_scene_state *fdvb_scene_open(const fdvb_scene_params *params);
 int fdvb_scene_frame(const fdvb_scene_state *s, int f, uint8_t *i420);
 void fdvb_scene_close(fdvb_scene_state *s);
 
+
+/* ---- Learned proposal network (no counterpart in the reference) ----------
+ * A 4-layer convolutional network (141,323 parameters; bf16 on the tensor
+ * cores, fp32 master weights and accumulation) that proposes four motion
+ * vectors and a SKIP / inter / intra prior per macroblock.  It is trained on
+ * (macroblock, chosen MV, chosen mode, RD cost) tuples of the plain encoder.
+ * Training samples index a bank of luma planes on the device.  All functions
+ * return 0 or -1 (fdvl_last_error() says why). */
+typedef struct fdvl_net fdvl_net;
+typedef struct {
+    int cur, ref;        /* bank slots of the current and the nearest reference luma */
+    int mbx, mby;        /* macroblock */
+    int cls;             /* 0 SKIP, 1 inter (INTER16 / INTER8), 2 intra */
+    int has_mv;          /* mvx/mvy is a target (inter on the nearest reference) */
+    int mvx, mvy;        /* quarter-pel */
+    int qp;              /* the frame's quantiser (an input of the network) */
+    float weight;
+} fdvl_sample;
+int fdvl_nparams(void);
+fdvl_net *fdvl_create(int device, int max_batch, int bank_frames, int w, int h);
+void fdvl_destroy(fdvl_net *n);
+int fdvl_set_params(fdvl_net *n, const float *p);   /* also resets the Adam state */
+int fdvl_get_params(fdvl_net *n, float *p);
+int fdvl_bank_put(fdvl_net *n, int slot, const uint8_t *y);
+/* Input features (n x 32 x 32 x 4) and outputs (n x 16: 8 MV coordinates in
+ * units of 16 quarter-pels, 3 mode logits, 5 zero) of n samples. */
+int fdvl_features(fdvl_net *n, const fdvl_sample *s, int nb, float *x);
+int fdvl_forward(fdvl_net *n, const fdvl_sample *s, int nb, float *out);
+/* The same through the fused per-frame inference kernel the encoder uses,
+ * plus its per-macroblock proposals (20 bytes each: four quarter-pel vectors
+ * as int16 x/y pairs clamped to +-lim, then the confident class as int32,
+ * -1 when the mode softmax stays below conf). */
+int fdvl_forward_fused(fdvl_net *n, const fdvl_sample *s, int nb, float conf, int lim, float *out, void *hints);
+/* Gradient of the batch-mean loss (nb a multiple of 64); loss[3] = total, mode, MV. */
+int fdvl_grads(fdvl_net *n, const fdvl_sample *s, int nb, float *grad, float *loss);
+int fdvl_train_step(fdvl_net *n, const fdvl_sample *s, int nb, float lr, float *loss);
+/* Adam over shuffled batches with a cosine-decayed rate; curve[2*epochs]
+ * (mode, MV loss per epoch, sampled) may be NULL. */
+int fdvl_train(fdvl_net *n, const fdvl_sample *s, int ns, int batch, int epochs, float lr, unsigned long long seed,
+               float *curve);
+const char *fdvl_last_error(void);
+/* One D[M][N] = A[M][K] * B[N][K]^T through the network's tcgen05 GEMM
+ * (A, B bf16 bit patterns, row-major; K a multiple of 64*nsplit). */
+int fdvl_gemm(int device, int M, int N, int K, const uint16_t *A, const uint16_t *B, float *D, int nsplit);
+
+/* The learned-proposal form of the encoder.  With proposals on, every P-frame
+ * first runs the network over all its macroblocks (one inference per frame
+ * step); where the mode prior's softmax reaches `conf`, the macroblock's
+ * analysis is narrowed: SKIP / inter search the nearest reference's 16x16
+ * vector from the four proposed vectors (a few diamond steps, then the
+ * sub-pel refinement) and skip the second reference, the INTER8 chain and
+ * intra; intra skips the motion searches.  Elsewhere the full search runs.
+ * The streams stay valid fdv streams (the decoder does not care how a mode
+ * was chosen) but are no longer byte-identical to the reference encoder's.
+ * params: fdvl_nparams() floats; NULL turns proposals off. */
+int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf);
+/* Per-class thresholds (SKIP, inter, intra) in place of the single one; a
+ * value above 1 keeps that class on the full search. */
+int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf3);
+/* The process-wide setting used by fdv_video_encode / fdv_vtile_encode /
+ * fdv_enc_* from the next call on. */
+int fdvb_set_learned(const float *params, float conf);
+/* Per-macroblock decision records of the last collected P-frame (for
+ * building training tuples): mode (0 SKIP, 1 INTER16, 2 INTRA16, 3 INTER8),
+ * MV (quarter-pel, the vector neighbours predict from), reference, and RD
+ * cost of the chosen mode (fdvg_set_records(g, 1) before the frame).  Any
+ * output may be NULL. */
+int fdvg_set_records(fdvg_ctx *g, int enable);
+int fdvg_mb_records(fdvg_ctx *g, int u, uint8_t *mode, int16_t *mv, uint8_t *ref, float *cost);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,205 @@
+"""The learned network on the GPU against its CPU oracle (oracle/learned_ref.py):
+the tcgen05 GEMM, the input features, the forward pass, the gradients of every
+layer and the Adam step.  Tolerances: the GEMM sums exact bf16 products in fp32
+(relative 1e-5 of the row scale); forward and gradients differ from the
+oracle only by fp32 summation order and the bf16 roundings it flips
+(relative L2 error 2e-2 per layer)."""
+import numpy as np
+import pytest
+
+import oracle.learned_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    import fdv_b200.learned as L
+    return L
+
+
+def _bits(x):
+    return R.to_bf16_bits(x)
+
+
+@pytest.mark.parametrize("m,n,k,split", [(300, 48, 128, 1), (128, 256, 64, 1), (1000, 160, 576, 1),
+                                         (77, 2560, 64, 1), (256, 32, 1024, 4), (64, 16, 2560, 8)])
+def test_gemm_matches_fp64(L, m, n, k, split):
+    rng = np.random.default_rng(m + n + k)
+    a = R.bf16(rng.standard_normal((m, k)).astype(np.float32))
+    b = R.bf16(rng.standard_normal((n, k)).astype(np.float32))
+    d = L.gemm(_bits(a), _bits(b), split)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    scale = np.sqrt((a.astype(np.float64) ** 2).sum(1))[:, None] * np.sqrt((b.astype(np.float64) ** 2).sum(1))[None]
+    assert np.all(np.abs(d - ref) <= 1e-5 * scale + 1e-6)
+
+
+def _bank(L, w=96, h=64, nslots=3, seed=0):
+    rng = np.random.default_rng(seed)
+    planes = []
+    base = rng.integers(0, 256, (h + 8, w + 8)).astype(np.float32)
+    for s in range(nslots):
+        # smooth-ish moving content
+        p = base[s:s + h, 2 * s:2 * s + w]
+        planes.append(np.clip(p * 0.5 + 64 + rng.integers(-4, 5, (h, w)), 0, 255).astype(np.uint8))
+    net = L.Net(w, h, nslots, max_batch=256)
+    for s, p in enumerate(planes):
+        net.bank_put(s, p)
+    return net, planes
+
+
+def _samples(L, n, w, h, seed=1):
+    rng = np.random.default_rng(seed)
+    s = L.samples(n)
+    s["cur"] = rng.integers(1, 3, n)
+    s["ref"] = s["cur"] - 1
+    s["mbx"] = rng.integers(0, w // 16, n)
+    s["mby"] = rng.integers(0, h // 16, n)
+    s["cls"] = rng.integers(0, 3, n)
+    s["has_mv"] = (s["cls"] == 1).astype(np.int32)
+    s["mvx"] = rng.integers(-64, 65, n)
+    s["mvy"] = rng.integers(-64, 65, n)
+    s["weight"] = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    s["qp"] = rng.integers(12, 40, n)
+    return s
+
+
+def _oracle_x(planes, s):
+    return np.stack([R.features(planes[c], planes[r], bx * 16, by * 16, qp)
+                     for c, r, bx, by, qp in zip(s["cur"], s["ref"], s["mbx"], s["mby"], s["qp"])])
+
+
+def _targets(s):
+    return (s["cls"], s["has_mv"].astype(np.float64), s["mvx"] / 16.0, s["mvy"] / 16.0, s["weight"].astype(np.float64))
+
+
+def test_features_exact(L):
+    net, planes = _bank(L)
+    s = _samples(L, 40, net.w, net.h)
+    assert np.array_equal(net.features(s), _oracle_x(planes, s))
+
+
+def test_forward_and_gradients_match_oracle(L):
+    net, planes = _bank(L)
+    p = R.init_params(7)
+    p[R.OFFS[0][1]:R.OFFS[0][1] + 32] = 0.02
+    net.set_params(p)
+    s = _samples(L, 128, net.w, net.h, seed=4)
+    x = _oracle_x(planes, s)
+    out_ref, cache = R.forward(p, x)
+    out = net.forward(s)
+    err = np.linalg.norm(out[:, :11] - out_ref) / np.linalg.norm(out_ref)
+    assert err < 2e-2, err
+    assert np.all(out[:, 11:] == 0)
+    g, loss = net.grads(s)
+    ce, mv, gout = R.loss_grad(out_ref, *_targets(s))
+    assert abs(loss[1] - ce.mean()) < 2e-2 * max(1.0, ce.mean())
+    assert abs(loss[2] - mv.mean()) < 2e-2 * max(1.0, mv.mean())
+    gref = R.backward(p, cache, gout)
+    for l in range(4):
+        wo, bo = R.OFFS[l]
+        cout = R.GEO[l][2]
+        for name, a, b in (("W", g[wo:bo], gref[wo:bo]), ("b", g[bo:bo + cout], gref[bo:bo + cout])):
+            e = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+            assert e < 2e-2, (l, name, e)
+
+
+def test_fused_inference_matches_layered_forward(L):
+    """The encoder's fused inference kernel computes what the layer-by-layer
+    training forward does (same bf16 rounding points), and its proposals
+    follow from those outputs."""
+    net, planes = _bank(L)
+    p = L.init_params(13)
+    net.set_params(p)
+    for n in (8, 61, 200):   # whole and partial groups of eight
+        s = _samples(L, n, net.w, net.h, seed=n)
+        ref = net.forward(s)
+        out, hs = net.forward_fused(s, conf=0.5, lim=64)
+        err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+        assert err < 2e-3, err
+        o = out.astype(np.float64)
+        mv = np.clip(np.rint(o[:, :8] * 16), -64, 64).reshape(n, 4, 2)
+        assert np.abs(hs["mv"] - mv).max() <= 1
+        lg = o[:, 8:11]
+        pr = np.exp(lg - lg.max(1, keepdims=True))
+        pr /= pr.sum(1, keepdims=True)
+        cls = np.where(pr.max(1) >= 0.5, pr.argmax(1), -1)
+        near = np.abs(pr.max(1) - 0.5) < 1e-3
+        assert np.all((hs["cls"] == cls) | near)
+
+
+def test_adam_step_matches_oracle(L):
+    net, planes = _bank(L)
+    p = R.init_params(9)
+    net.set_params(p)
+    s = _samples(L, 64, net.w, net.h, seed=6)
+    g, _ = net.grads(s)
+    net.train_step(s, 1e-3)
+    p1 = net.params()
+    q, _, _ = R.adam(p, np.zeros_like(p), np.zeros_like(p), g.astype(np.float32), 1, 1e-3)
+    assert np.max(np.abs(p1 - q)) < 1e-6
+
+
+def test_training_lowers_loss(L):
+    net, planes = _bank(L)
+    net.set_params(R.init_params(11))
+    s = _samples(L, 1024, net.w, net.h, seed=8)
+    # labels that are a function of the macroblock, so there is something to learn
+    s["cls"] = (s["mbx"] + 2 * s["mby"] + s["cur"]) % 3
+    s["has_mv"] = (s["cls"] == 1).astype(np.int32)
+    s["mvx"] = s["mbx"] * 16 - 40
+    s["mvy"] = s["mby"] * 16 - 24
+    s["weight"] = 1.0
+    curve = net.train(s, 128, 6, 2e-3, seed=3)
+    assert np.isfinite(curve).all()
+    assert curve[-1].sum() < 0.7 * curve[0].sum(), curve
+
+
+def test_mb_records_match_oracle(built):
+    """The decision records the training tuples come from equal the CPU
+    restatement's per-macroblock modes and vectors."""
+    import fdv_b200 as F
+    import oracle as O
+    w, h, qp = 160, 96, 26
+    frames = F.Scene(w, h, 4, nrects=4, rect_min=8, rect_max=32, pan_qx=5, seed=3).frames(4)
+    eng = F.Engine([(w, h)], 16, 0)
+    eng.set_records(True)
+    ref = O.OracleUnit(w, h, 16)
+    for f, fr in enumerate(frames):
+        eng.step([fr], [int(f == 0)], [qp])
+        ref.frame(fr, int(f == 0), qp)
+        if f:
+            r = eng.mb_records(0)
+            m, mv = ref.mb_info()
+            assert np.array_equal(r["mode"], m)
+            assert np.array_equal(r["mv"], mv)
+            assert np.all(r["cost"] >= 0)
+    eng.close()
+
+
+def _forcing_params(L, cls, seed=5):
+    """A random network whose mode logits always pick `cls`."""
+    p = L.init_params(seed)
+    b4 = R.OFFS[3][1]
+    p[b4 + 8:b4 + 11] = -20.0
+    p[b4 + 8 + cls] = 20.0
+    return p
+
+
+@pytest.mark.parametrize("cls", [0, 1, 2, -1])
+def test_learned_stream_decodes_to_gpu_reconstruction(built, cls):
+    """Streams of the learned form stay valid: the reference decoder
+    reconstructs every frame exactly as the GPU encoder did, with every
+    macroblock sent down one learned path (cls 0/1/2) or a mixture (-1)."""
+    import fdv_b200 as F
+    import fdv_b200.learned as L
+    import oracle as O
+    w, h, qp = 320, 192, 26
+    frames = F.Scene(w, h, 6, nrects=8, rect_min=8, rect_max=48, vmax_qpel=20, pan_qx=3, seed=11).frames(6)
+    p = _forcing_params(L, cls) if cls >= 0 else L.init_params(3)
+    stream, recs, _ = L.encode_engine(frames, w, h, qp, 0, params=p, conf=0.5 if cls >= 0 else 0.34)
+    dec = O.ref_video_decode(stream, 16)
+    for f in range(len(frames)):
+        assert np.array_equal(dec[f], recs[f]), f
+    plain, _, _ = L.encode_engine(frames, w, h, qp, 0)
+    assert plain == O.ref_video_encode(frames, w, h, qp, 0)
