@@ -19,6 +19,13 @@ One step = encoding all 120 frames.
   workload's 8-band layout (parallelism capped at 8 threads) and one macroblock
   row per band (45 bands) on every host core.
 
+* ``learned``: the learned-proposal form against the plain form on the
+  learned workload (the small workload's content generator at 1280x720: noise
+  background and 6 moving rectangles, QP 23, range 16, 60 frames, one key
+  frame): whole-step Mpix/s of both (device-timed, per-frame inference
+  included), the P-frame analysis speed-up, and the BD-rate / PSNR of the
+  learned form against the plain form over QP 18/23/28/32 (20 frames).
+
 ``--impl reference`` times that reference encoder alone (rank 0).
 Under torchrun each rank encodes its own stream (weak scaling, no collective on
 the data path); timings are reduced with MAX over ranks.
@@ -342,6 +349,72 @@ def run_reference(args) -> None:
     }))
 
 
+LEARN_NF, LEARN_QP, LEARN_CONF = 60, 23, 0.8
+
+
+def run_learned(local: int) -> dict:
+    """The learned-proposal form against the plain form on the learned workload."""
+    import torch
+    import fdv_b200 as F
+    import fdv_b200.learned as LN
+    L = F.lib()
+    p = LN.load_params(LN.DEFAULT_WEIGHTS)
+    sc = F.Scene(W, H, LEARN_NF, seed=1, **LN.CONTENT)
+    frames = np.stack([sc.frame(f) for f in range(LEARN_NF)])
+    dev = torch.from_numpy(frames).to(f"cuda:{local}")
+    torch.cuda.synchronize()
+    cw = W // 2
+    sets = []
+    for f in range(LEARN_NF):
+        fb = dev.data_ptr() + f * FSIZE
+        ps = (F.u8p * 3)(C.cast(fb, F.u8p), C.cast(fb + W * H, F.u8p), C.cast(fb + W * H + (H // 2) * cw, F.u8p))
+        sets.append(ps)
+    qp = (C.c_int * 1)(LEARN_QP)
+    intra = [(C.c_int * 1)(1 if f == 0 else 0) for f in range(LEARN_NF)]
+
+    def run(params, conf4=None):
+        g = F.Engine([(W, H)], LN.RANGE, local)
+        if params is not None:
+            g.set_learned(params, LEARN_CONF)
+            if conf4 is not None:
+                g.set_learned_conf(conf4[:3], conf4[3], bool(conf4[4]) if len(conf4) > 4 else False)
+
+        def step():
+            for f in range(LEARN_NF):
+                if L.fdvg_frame_device(g._g, sets[f], intra[f], qp, None, None) != 0:
+                    raise RuntimeError(F.last_error())
+        step()
+        g.stats_reset()
+        step()
+        st = g.stats()
+        g.close()
+        return st
+
+    plain = run(None)
+    learned = run(p)
+    seeded = run(p, (2.0, 2.0, 2.0, 0.0))   # inference and seeded searches, no narrowing
+    ev = LN.evaluate(p, LEARN_CONF, nframes=20, seeds=(1,))
+    mpix = LEARN_NF * W * H / 1e6
+    pf = lambda st: st["p_ms"] / max(1, st["p_launches"])
+    return {
+        "metric": "720p encode Mpix/s on 1 B200 (learned-proposal form)",
+        "value": round(mpix / (learned["step_ms"] / 1e3), 3), "unit": "Mpix/s",
+        "plain_value": round(mpix / (plain["step_ms"] / 1e3), 3),
+        "speedup": round(plain["step_ms"] / learned["step_ms"], 4),
+        "p_frame_ms": {"plain": round(pf(plain), 4), "learned": round(pf(learned), 4),
+                       "inference_and_seeding_only": round(pf(seeded), 4)},
+        "p_frame_speedup": round(pf(plain) / pf(learned), 4),
+        "bd_rate_pct": None if ev["bd_rate_pct"] is None else round(ev["bd_rate_pct"], 4),
+        "rd_points": ev["points"],
+        "setting": {"skip_conf": LEARN_CONF, "skip_gate_lambda": 400,
+                    "inter_conf": 0.9, "inter_path": "nearest-reference 16x16 and INTER8, seeded, 4 diamond steps",
+                    "intra": "full search", "other_mbs": "full search seeded with the proposals"},
+        "workload": f"learned: 1280x720, {LEARN_NF} frames (1 key), QP {LEARN_QP}, range 16, 6 moving rectangles "
+                    f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, 20 frames",
+        "weights": "fdv_b200/proposal_c4.f32",
+    }
+
+
 def main() -> None:
     global NF
     ap = argparse.ArgumentParser()
@@ -352,6 +425,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI end-to-end leg (profiling runs)")
     ap.add_argument("--frames", type=int, default=NF, help="frames per step (profiling runs use a few)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--workload", default="hd720", choices=["hd720", "batch48"],
                     help="batch48: the 48-stream batched workload (timed steps = P-frame steps)")
     args = ap.parse_args()
@@ -505,6 +579,10 @@ def main() -> None:
             cpu = {"value": b["value"], "unit": "Mpix/s", "cores": b["cores"], "kind": "reference",
                    "sample": b["sample"]}
 
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = run_learned(local)
+
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": round(value, 3), "unit": "Mpix/s", "n_gpus": world,
@@ -528,6 +606,7 @@ def main() -> None:
                 "d2h_bytes_per_step": int(d2h // max(1, args.steps))},
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "learned": learned,
         }))
     g.close()
     if dist is not None:

@@ -299,9 +299,11 @@ class Engine:
         if lib().fdvg_set_learned(self._g, ptr, conf) != 0:
             raise FdvError(last_error())
 
-    def set_learned_conf(self, conf3) -> None:
-        """Per-class thresholds (SKIP, inter, intra); above 1 keeps a class on the full search."""
-        a = (C.c_float * 3)(*[float(c) for c in conf3])
+    def set_learned_conf(self, conf3, skip_gate: float = 0.0, inter8: bool = False) -> None:
+        """Per-class thresholds (SKIP, inter, intra; above 1 keeps a class on the
+        full search), the SKIP gate in units of lambda (0: none), and INTER8 in
+        the confident-inter path."""
+        a = (C.c_float * 5)(*[float(c) for c in conf3], float(skip_gate), float(bool(inter8)))
         if lib().fdvg_set_learned_conf(self._g, a) != 0:
             raise FdvError(last_error())
 

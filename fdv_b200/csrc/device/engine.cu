@@ -35,7 +35,7 @@
 namespace fdvb {
 // kernels (pframe.cu, iframe.cu, frame_ops.cu)
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, int range, cudaStream_t st);
+                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st);
 struct IPlaneDev;
 struct ITask;
 size_t iframe_smem_bytes();
@@ -165,6 +165,8 @@ struct fdvb_engine {
     // hints and the P units of the current step ({unit, first macroblock})
     fdvl_net *lnet = nullptr;
     float3 lconf = {0.8f, 0.8f, 0.8f};       // per class: SKIP, inter, intra (> 1: never)
+    double lgate = 0.0;                      // confident SKIP needs J <= lgate * lambda (0: always)
+    int linter8 = 0;                         // confident inter also tries INTER8
     lrn::Hint *d_hints = nullptr;
     int2 *d_pu = nullptr;
     int total_mbs = 0;
@@ -433,6 +435,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
         d.prof = E->d_prof;
         d.hint = nullptr;
+        d.skip_gate = E->lgate;
+        d.inter8 = E->linter8;
         d.mbcost = E->d_mbcost ? E->d_mbcost + u.mb_off : nullptr;
         if (!is_intra[i] && E->lnet) {
             pu.push_back(make_int2(i, nhint));
@@ -502,7 +506,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
             }
             E->launches += 1;
         }
-        launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range, E->st);
+        launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range,
+                      !pu.empty(), E->st);
         CK(cudaGetLastError());
         CK(cudaEventRecord(SL.ev[2], E->st));
         E->launches += 1;
@@ -721,6 +726,11 @@ extern "C" int fdvb_engine_commit_refs(fdvb_engine *E) {
 
 // Learned proposals for every later P-frame (params: fdvl_nparams() floats;
 // NULL turns them off).  The engine owns a private inference network.
+// Default SKIP gate, in units of lambda: static macroblocks' best merge
+// candidate costs around 100-300 lambda, a wrongly predicted SKIP over moving
+// content far more.
+constexpr double kLearnSkipGate = 400.0;
+constexpr float kLearnInterConf = 0.9f;
 extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, float conf) {
     if (!E) return -1;
     CK(cudaSetDevice(E->device));
@@ -736,15 +746,25 @@ extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, floa
     }
     CK(cudaStreamSynchronize(E->st));
     if (fdvl_set_params(E->lnet, params) != 0) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
-    E->lconf = make_float3(conf, conf, conf);
+    // the product setting: SKIP narrowing at `conf` behind the RD-cost gate;
+    // inter narrowing at kLearnInterConf, INTER8 kept; intra keeps the full
+    // search (every full search seeded with the proposals)
+    E->lconf = make_float3(conf, kLearnInterConf, 2.f);
+    E->lgate = kLearnSkipGate;
+    E->linter8 = 1;
     return 0;
 }
 
 // Per-class confidence thresholds of the learned proposals (SKIP, inter,
-// intra); a threshold above 1 turns that class's narrowed analysis off.
-extern "C" int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf3) {
-    if (!E || !conf3) return -1;
-    E->lconf = make_float3(conf3[0], conf3[1], conf3[2]);
+// intra; a threshold above 1 turns that class's narrowed analysis off), the
+// SKIP gate (a confident SKIP is taken only when the best merge candidate's
+// RD cost is at most gate * lambda; gate <= 0: always) and whether the
+// confident-inter path also tries INTER8.
+extern "C" int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf5) {
+    if (!E || !conf5) return -1;
+    E->lconf = make_float3(conf5[0], conf5[1], conf5[2]);
+    E->lgate = conf5[3];
+    E->linter8 = conf5[4] != 0.f;
     return 0;
 }
 

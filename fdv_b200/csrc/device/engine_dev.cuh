@@ -20,6 +20,8 @@ struct UnitDev {
     int stall_row;              // test hook: this row never runs (-1: none)
     unsigned long long *prof;   // optional per-phase cycle accumulators (NULL: off)
     const lrn::Hint *hint;      // learned proposals per macroblock (NULL: the plain search)
+    double skip_gate;           // a confident SKIP needs its RD cost <= skip_gate * lambda (<= 0: no gate)
+    int inter8;                 // the confident-inter path also tries INTER8 (seeded, short searches)
     float *mbcost;              // per macroblock: RD cost of the chosen mode (NULL: off)
 };
 

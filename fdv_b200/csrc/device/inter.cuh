@@ -169,7 +169,7 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
     py = py < -lim ? -lim : (py > lim ? lim : py);
     const bool seed = px != 0 || py != 0;
     int best, bxv = 0, byv = 0;
-    // extra starting points (16x16 only): whole-pel positions of the proposals
+    // extra starting points: whole-pel positions of the proposals
     auto cand_at = [&](int k, int &x, int &y) {
         x = (cands[k].x >> 2) * 4;
         y = (cands[k].y >> 2) * 4;
@@ -191,6 +191,13 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
             const int hk = lane >> 4;
             int v = sad_packed<8>(c0, c1, R, bx, by, hk ? px : 0, hk ? py : 0, lane);
             if ((lane & 15) == 0 && (hk == 0 || seed)) s[hk] = v;
+        } else if (gw <= 2 && ncands > 0) {
+            // up to four proposals on the half-warps of warps 1 and 2
+            const int ci = 2 * (gw - 1) + (lane >> 4);
+            int x, y;
+            cand_at(ci < ncands ? ci : 0, x, y);
+            int v = sad_packed<8>(c0, c1, R, bx, by, x, y, lane);
+            if ((lane & 15) == 0 && ci < ncands) s[2 + ci] = v;
         }
         gbar(bar, 128);
         best = s[0];

@@ -43,23 +43,24 @@ void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticke
 // search range allows it (up to 32); a range of 64 reads them from global
 // memory.  All units of one launch share the range.
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, int range, cudaStream_t st) {
+                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st) {
     static std::mutex mu;
-    static bool attr[64][2] = {};
+    static bool attr[64][4] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const bool win = range <= 32;
+    const int v = (win ? 1 : 0) + (learned ? 2 : 0);
     const size_t smem = win ? (size_t)kPWinOff + kPWinBytes : sizeof(PShared);
+    void (*const k[4])(const UnitDev *, const RowTask *, int, int *, unsigned *, unsigned long long) = {
+        pframe_kernel<false, false>, pframe_kernel<true, false>, pframe_kernel<false, true>, pframe_kernel<true, true>};
     {
         std::lock_guard<std::mutex> lk(mu);
-        if (dev >= 0 && dev < 64 && !attr[dev][win]) {
-            if (win) cudaFuncSetAttribute(pframe_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            else cudaFuncSetAttribute(pframe_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr[dev][win] = true;
+        if (dev >= 0 && dev < 64 && !attr[dev][v]) {
+            cudaFuncSetAttribute(k[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr[dev][v] = true;
         }
     }
-    if (win) pframe_kernel<true><<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
-    else pframe_kernel<false><<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
+    k[v]<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
 }
 
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st) {
@@ -227,7 +228,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     u.slots = base + o_slots;
     u.lambda = fdvb_lambda(qp, lscale);
     u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1; u.prof = nullptr;
-    u.hint = nullptr; u.mbcost = nullptr;
+    u.hint = nullptr; u.mbcost = nullptr; u.skip_gate = 0.0; u.inter8 = 0;
     RowTask rows[8192 / 16];
     for (int r = 0; r < mbh; ++r) rows[r] = {0, r};
     DbTask db[3] = {{rec, w, h, qp}, {rec + (size_t)w * h, cw, ch, qp}, {rec + (size_t)w * h + (size_t)cw * ch, cw, ch, qp}};
@@ -251,7 +252,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     if (!ok) return static_fail("descriptor upload failed");
     launch_refprep(base + o_prep, far_ref ? 2 : 1, w, h, B, st);
     launch_pframe(reinterpret_cast<const UnitDev *>(base + o_unit), reinterpret_cast<const RowTask *>(base + o_rows),
-                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, range, st);
+                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, range, false, st);
     launch_deblock(base + o_db, 3, st);
     launch_compact(base + o_cmp, 1, err, st);
     if (cudaGetLastError() != cudaSuccess) return static_fail("kernel launch failed");

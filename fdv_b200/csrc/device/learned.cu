@@ -175,7 +175,7 @@ __device__ __forceinline__ bf16 qp_feat(int qp) { return __float2bfloat16_rn((fl
 __global__ void features_kernel(const Sample *__restrict__ S, int n, bf16 *__restrict__ X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n * kPatch * kPatch) return;
-    const int s = i >> 10, y = (i >> 5) & 31, x = i & 31;   // X[s][y][x][8]
+    const int s = i >> 10, y = (i >> 5) & 31, x = i & 31;   // X[s][y][x][4]
     const Sample &q = S[s];
     const int c0 = px_at(q.cur, q.cs, q.w, q.h, q.bx - 8 + x, q.by - 8 + y);
     const int c1 = px_at(q.ref, q.rs, q.w, q.h, q.bx - 8 + x, q.by - 8 + y);
@@ -184,14 +184,15 @@ __global__ void features_kernel(const Sample *__restrict__ S, int n, bf16 *__res
                     px_at(q.cur, q.cs, q.w, q.h, gx, gy + 1) + px_at(q.cur, q.cs, q.w, q.h, gx + 1, gy + 1) + 2) >> 2;
     const int c3 = (px_at(q.ref, q.rs, q.w, q.h, gx, gy) + px_at(q.ref, q.rs, q.w, q.h, gx + 1, gy) +
                     px_at(q.ref, q.rs, q.w, q.h, gx, gy + 1) + px_at(q.ref, q.rs, q.w, q.h, gx + 1, gy + 1) + 2) >> 2;
-    const bf16 z = __float2bfloat16_rn(0.f);
-    __align__(16) bf16 o[8] = {feat(c0), feat(c1), feat(c2), feat(c3), qp_feat(q.qp), z, z, z};
-    *reinterpret_cast<uint4 *>(X + (size_t)i * 8) = *reinterpret_cast<const uint4 *>(o);
+    __align__(8) bf16 o[4] = {feat(c0), feat(c1), feat(c2), feat(c3)};
+    *reinterpret_cast<uint2 *>(X + (size_t)i * 4) = *reinterpret_cast<const uint2 *>(o);
 }
 
 // col[(b*So + oy)*So + ox][k] for a 3x3 stride-2 pad-1 convolution of
 // X[b][Si][Si][Cin]; k >= 9*Cin is zero.  One thread per 8-element chunk.
-__global__ void im2col_kernel(const bf16 *__restrict__ X, int nb, int si, int cin, int kp, bf16 *__restrict__ col) {
+// (With S: the first convolution, whose column kQpCol is the sample's quantiser.)
+__global__ void im2col_kernel(const bf16 *__restrict__ X, int nb, int si, int cin, int kp, bf16 *__restrict__ col,
+                              const Sample *__restrict__ S) {
     const int so = si / 2, kc8 = kp / 8;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)nb * so * so * kc8) return;
@@ -207,6 +208,8 @@ __global__ void im2col_kernel(const bf16 *__restrict__ X, int nb, int si, int ci
             const int tap = k / cin, c = k - tap * cin, ky = tap / 3, kx = tap - ky * 3;
             const int y = 2 * oy - 1 + ky, x = 2 * ox - 1 + kx;
             if (y >= 0 && y < si && x >= 0 && x < si) v = X[(((size_t)b * si + y) * si + x) * cin + c];
+        } else if (S && k == kQpCol) {
+            v = qp_feat(S[b].qp);
         }
         o[j] = v;
     }
@@ -499,7 +502,8 @@ int forward(fdvl_net *n, const Sample *S, int nb, cudaStream_t st) {
         const LayerGeo &G = kGeo[l];
         const int so = G.sin / 2, rows = nb * so * so;
         const long long chunks = (long long)rows * (G.kp / 8);
-        im2col_kernel<<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(x, nb, G.sin, G.cin, G.kp, n->col[l]);
+        im2col_kernel<<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(x, nb, G.sin, G.cin, G.kp, n->col[l],
+                                                                        l == 0 ? S : nullptr);
         if (gemm(n, st, n->col[l], G.kp, n->Wb[l], G.kp, rows, G.gn, G.kp, EPI_BIAS_RELU_BF16, nullptr, n->Y[l],
                  G.gn, n->w + b_off(l), G.cout))
             return -1;
@@ -655,8 +659,7 @@ int fused_infer(fdvl_net *n, const Sample *S, int nb, float3 conf, int lim, Hint
     InferW W;
     W.img = n->wimg;
     for (int l = 0; l < 4; ++l) W.b[l] = n->w + b_off(l);
-    const int groups = (nb + IMB - 1) / IMB;
-    infer_kernel<<<std::min(groups, n->nsm), INT, kInferSmem, st>>>(S, nb, W, conf, lim, hints, out, err);
+    infer_kernel<<<std::min(nb, n->nsm), INT, kInferSmem, st>>>(S, nb, W, conf, lim, hints, out, err);
     return cu_ok(cudaGetLastError(), "fused inference") ? 0 : -1;
 }
 

@@ -1,18 +1,18 @@
 // The learned motion/mode proposal network: geometry shared by the training
 // kernels, the fused inference kernel and the host driver.
 //
-// Input per macroblock: 32x32 positions x 8 channels (bf16; pixels as (v-128)/64):
+// Input per macroblock: 32x32 positions x 4 channels (bf16, (v-128)/64):
 //   0  current luma, the macroblock and 8 pixels around it (clamped at the edges)
 //   1  nearest reference luma at the same place
 //   2  current luma over 64x64 around the macroblock, 2x2-averaged
 //   3  nearest reference luma over the same 64x64, 2x2-averaged
-//   4  the quantiser, (qp-26)/8, everywhere (whether a residual is worth its
-//      bits depends on it)
-//   5-7 zero (one 16-byte vector per position)
-// Three 3x3 stride-2 convolutions with ReLU (8->32, 32->64, 64->160 channels;
+// and the quantiser, (qp-26)/8, as a 37th reduction column of the first
+// convolution (a per-macroblock term of every output: whether a residual is
+// worth its bits depends on it).
+// Three 3x3 stride-2 convolutions with ReLU (4->32, 32->64, 64->160 channels;
 // 32x32 -> 16x16 -> 8x8 -> 4x4) and one fully connected layer (2560 -> 11):
 // four motion-vector hypotheses (x, y in units of 16 quarter-pels) and three
-// mode logits (SKIP, inter, intra).  141,323 parameters.
+// mode logits (SKIP, inter, intra).  140,203 parameters.
 //
 // Activations are NHWC.  A convolution's reduction index is
 // k = (ky*3 + kx)*Cin + ci, so an im2col row gathers nine contiguous channel
@@ -26,7 +26,8 @@
 namespace fdvb {
 namespace lrn {
 
-constexpr int kPatch = 32, kChan = 8;
+constexpr int kPatch = 32, kChan = 4;
+constexpr int kQpCol = 36;   // the first convolution's quantiser column
 constexpr int kOut = 11, kOutPad = 16;
 constexpr int kMvHyp = 4;
 
@@ -38,7 +39,7 @@ struct LayerGeo {
 };
 // conv1, conv2, conv3, fc
 constexpr LayerGeo kGeo[4] = {
-    {32, 8, 32, 72, 128, 32, 64},
+    {32, 4, 32, 37, 64, 32, 64},
     {16, 32, 64, 288, 320, 64, 64},
     {8, 64, 160, 576, 576, 160, 192},
     {4, 160, 11, 2560, 2560, 16, 64},
@@ -46,7 +47,7 @@ constexpr LayerGeo kGeo[4] = {
 constexpr int sout(int l) { return kGeo[l].sin / 2; }
 constexpr int pos_per_mb(int l) { return l < 3 ? sout(l) * sout(l) : 1; }
 
-// fp32 master parameters, flat: W1[32][72] b1[32] W2[64][288] b2[64]
+// fp32 master parameters, flat: W1[32][37] b1[32] W2[64][288] b2[64]
 // W3[160][576] b3[160] W4[11][2560] b4[11]
 constexpr int w_off(int l) {
     int o = 0;
@@ -57,8 +58,8 @@ constexpr int b_off(int l) { return w_off(l) + kGeo[l].cout * kGeo[l].k; }
 constexpr int kNParams = w_off(4);
 constexpr int kWOff[4] = {w_off(0), w_off(1), w_off(2), w_off(3)};
 constexpr int kBOff[4] = {b_off(0), b_off(1), b_off(2), b_off(3)};
-static_assert(kWOff[1] == 2336 && kWOff[2] == 20832 && kWOff[3] == 113152, "offsets");
-static_assert(kNParams == 141323, "parameter count");
+static_assert(kWOff[1] == 1216 && kWOff[2] == 19712 && kWOff[3] == 112032, "offsets");
+static_assert(kNParams == 140203, "parameter count");
 
 // One training or inference sample: where its patch comes from, and (training)
 // the encoder's decision it is taught.

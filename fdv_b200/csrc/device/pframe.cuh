@@ -43,8 +43,6 @@ struct PShared {
     int tl, ht, hl, ctl[2];
     MBInfo cand[3];
     int ncand, ssd3[3];
-    short2 lmv[lrn::kMvHyp];     // learned proposals of this macroblock
-    int lcls;                    // their confident class, -1: none
     uint8_t predS[3][256];
     // phase 1
     uint8_t pr[3][256];          // 16x16 predictions: nearest ref, second ref, selected intra
@@ -75,6 +73,12 @@ struct PShared {
     long long ce;
     int cb;
     int task, row_ok, amode;
+    // (appended last, so the members above keep their offsets)
+    alignas(16) uint8_t pre[256];   // the next macroblock's source, prefetched by cp.async
+    alignas(8) uint8_t prec[2][64];
+    short2 lmv[lrn::kMvHyp];     // learned proposals of this macroblock
+    short2 lmv2[lrn::kMvHyp];    // the same doubled, for the second reference (two frames back)
+    int lcls;                    // their confident class, -1: none
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -120,6 +124,10 @@ constexpr int kPWinBytes = 8 * kWinPlane;   // 2 references x 4 planes
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
@@ -202,7 +210,9 @@ constexpr int BAR_POOL = 13;
 // Large-diamond steps of the 16x16 search when it starts from learned proposals.
 constexpr int kLearnLd = 4;
 
-template <bool WIN>
+// LRN: the learned-proposal form (units carry hints); the plain instance has
+// none of its code.
+template <bool WIN, bool LRN>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
               int *ticket, unsigned *err, unsigned long long wait_ns) {
@@ -219,7 +229,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const int t = S.task;
         __syncthreads();
         if (t >= nrows) {
-            if (WIN) cp_async_wait_all();
+            cp_async_wait_all();
             return;
         }
         const UnitDev &U = units[rows[t].unit];
@@ -230,11 +240,24 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const double lam14 = __dmul_rn(lambda, 14.0), lam16 = __dmul_rn(lambda, 16.0), lam19 = __dmul_rn(lambda, 19.0);
         qp4_setup(&S.q, qp, tid);
         const int nref = navail > 1 ? 2 : 1, wy0 = row * 16 - R - 3, wrows = 2 * R + 23;
-        if (WIN) {
-            cp_async_wait_all();   // this block's copies for an earlier row have landed
-            __syncthreads();
-            win_fill(win, U, nref, -3, 4, wy0, wrows, tid);   // macroblock 0's strips and macroblock 1's
-        }
+        cp_async_wait_all();   // this block's copies for an earlier row have landed
+        __syncthreads();
+        if (WIN) win_fill(win, U, nref, -3, 4, wy0, wrows, tid);   // macroblock 0's strips and macroblock 1's
+        // source prefetch: each macroblock's luma and chroma are copied into
+        // S.pre while the one before it is analysed (aligned planes only)
+        const bool pf = ((reinterpret_cast<uintptr_t>(U.cur[0]) | (uintptr_t)w) & 15) == 0 &&
+                        ((reinterpret_cast<uintptr_t>(U.cur[1]) | reinterpret_cast<uintptr_t>(U.cur[2]) |
+                          (uintptr_t)cw) & 7) == 0;
+        auto prefetch = [&](int pbx, int pby) {
+            if (tid < 16) {
+                cp_async16(&S.pre[tid * 16], U.cur[0] + (size_t)(pby + tid) * w + pbx);
+            } else if (tid < 32) {
+                const int k = tid - 16, pl = k >> 3, r = k & 7;
+                cp_async8(&S.prec[pl][r * 8], U.cur[1 + pl] + (size_t)(pby / 2 + r) * cw + pbx / 2);
+            }
+            cp_async_commit();
+        };
+        if (pf) prefetch(0, row * 16);
         const typename LumaOf<WIN>::T L0 = luma_src<WIN>(U.ref[0], win, 0, wy0, wrows);
         const typename LumaOf<WIN>::T L1 = luma_src<WIN>(U.ref[1], win, nref - 1, wy0, wrows);
         int pmvx = 0, pmvy = 0, prev_mode = 0;
@@ -242,7 +265,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
             pc.start();
-            if (WIN) cp_async_wait_all();   // this thread's strip copies; the barrier below publishes them
+            cp_async_wait_all();   // this thread's strip and source copies; the barrier below publishes them
             if (row > 0) {
                 if (tid == 0) S.row_ok = wait_at_least(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
             } else if (tid == 0) S.row_ok = 1;
@@ -256,7 +279,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             if (tid < 64) {
                 const int r2 = tid >> 2, c2 = (tid & 3) * 4;
                 *reinterpret_cast<uint32_t *>(&S.cur[tid * 4]) =
-                    *reinterpret_cast<const uint32_t *>(&U.cur[0][(size_t)(by + r2) * w + bx + c2]);
+                    pf ? *reinterpret_cast<const uint32_t *>(&S.pre[tid * 4])
+                       : *reinterpret_cast<const uint32_t *>(&U.cur[0][(size_t)(by + r2) * w + bx + c2]);
+            } else if (tid < 96 && pf) {
+                const int k = tid - 64, pl = k >> 4;
+                *reinterpret_cast<uint32_t *>(&S.curc[pl][(k & 15) * 4]) =
+                    *reinterpret_cast<const uint32_t *>(&S.prec[pl][(k & 15) * 4]);
             } else if (tid < 96) {
                 const int k = tid - 64, pl = k >> 4, r2 = (k & 15) >> 1, c2 = (k & 1) * 4;
                 *reinterpret_cast<uint32_t *>(&S.curc[pl][(k & 15) * 4]) =
@@ -297,13 +325,17 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 S.ncand = n;
                 S.amode = row > 0 ? (int)((nb[0].y >> 16) & 0xffu) : 0;
                 S.lcls = -1;
-                if (U.hint) {
+                if (LRN && U.hint) {
                     const lrn::Hint hh = U.hint[row * mbw + mbx];
                     S.lcls = hh.cls;
-                    for (int k = 0; k < lrn::kMvHyp; ++k) S.lmv[k] = hh.mv[k];
+                    for (int k = 0; k < lrn::kMvHyp; ++k) {
+                        S.lmv[k] = hh.mv[k];
+                        S.lmv2[k] = make_short2((short)(2 * hh.mv[k].x), (short)(2 * hh.mv[k].y));
+                    }
                 }
             }
             __syncthreads();
+            if (pf && mbx + 1 < mbw) prefetch(bx + 16, by);   // S.pre is consumed
             // mode context (fdv.h:4172): left / above macroblock skipped-ness;
             // the left one is this block's previous macroblock
             const int ctx = (prev_mode != 0 ? 2 : 0) + (S.amode != 0 ? 1 : 0);
@@ -364,9 +396,13 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             // intra skips the motion searches.  Without a confident class the
             // full analysis runs, its nearest-reference 16x16 search seeded
             // with the proposed vectors as well.
-            const int lcls = S.lcls;
+            // (a SKIP the gate turns down was predicted wrongly: full analysis)
+            const int lcls0 = LRN ? S.lcls : -1;
+            const bool gate_ok = !LRN || U.skip_gate <= 0.0 || Js <= __dmul_rn(U.skip_gate, lambda);
+            const int lcls = (lcls0 == 0 && !gate_ok) ? -1 : lcls0;
             const bool lfast = lcls >= 0, l_intra = lcls == 2;
-            const bool skip_wins = Js <= lam14 || lcls == 0;
+            const bool l8 = !lfast || (LRN && lcls == 1 && U.inter8);   // INTER8 analysed
+            const bool skip_wins = Js <= lam14 || (LRN && lcls == 0);
             double Jc = Js;   // RD cost of the chosen mode
             pc.mark(PP_SKIP);
             if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); if (skip_wins) atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
@@ -382,26 +418,30 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                         // with proposals the search also starts from them; a full
                         // search (not confident) still runs the diamond to the end
                         int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
-                                                     U.prof ? &U.prof[PP_IT16] : nullptr, U.hint ? S.lmv : nullptr,
-                                                     U.hint ? lrn::kMvHyp : 0, lfast ? kLearnLd : 64);
+                                                     U.prof ? &U.prof[PP_IT16] : nullptr, (LRN && U.hint) ? S.lmv : nullptr,
+                                                     (LRN && U.hint) ? lrn::kMvHyp : 0, lfast ? kLearnLd : 64);
                         if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
                         mc16_group(L0, bx, by, mx, my, S.pr[0], gt);
                     }
                 } else if (grp == 1) {
                     if (navail > 1 && !lfast) {
                         int mx, my;
-                        int sd = me_search_group<16>(S.cur, L1, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10);
+                        int sd = me_search_group<16>(S.cur, L1, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10,
+                                                     nullptr, (LRN && U.hint) ? S.lmv2 : nullptr,
+                                                     (LRN && U.hint) ? lrn::kMvHyp : 0);
                         if (gt == 0) { S.mv[1][0] = mx; S.mv[1][1] = my; S.sad[1] = sd; }
                         mc16_group(L1, bx, by, mx, my, S.pr[1], gt);
                     }
                 } else if (grp == 2) {
-                    if (!lfast) {
+                    if (l8) {
                         int qpx = pmvx, qpy = pmvy, ssad = 0;
                         for (int q = 0; q < 4; ++q) {
                             const int qx = (q & 1) * 8, qy = (q >> 1) * 8;
                             int mx, my;
                             ssad += me_search_group<8>(S.cur + qy * 16 + qx, L0, bx + qx, by + qy, R, qpx, qpy, &mx, &my,
-                                                       S.gsad[2], gw, lane, 11, U.prof ? &U.prof[PP_IT8] : nullptr);
+                                                       S.gsad[2], gw, lane, 11, U.prof ? &U.prof[PP_IT8] : nullptr,
+                                                       (LRN && U.hint) ? S.lmv : nullptr,
+                                                       (LRN && U.hint) ? lrn::kMvHyp : 0, lfast ? kLearnLd : 64);
                             if (gt == 0) { S.qmv[q][0] = mx; S.qmv[q][1] = my; }
                             qpx = mx; qpy = my;
                             if (gt < 16) {
@@ -459,11 +499,11 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 pc.mark(PP_SEARCH);
                 // ---- phase 2: the INTER8 residual, on every warp
                 const int isel = S.isel, ssad = S.ssad;
-                const bool have1 = navail > 1, haveI = isel >= 0;
+                const bool have1 = navail > 1 && !lfast, haveI = isel >= 0;
                 // needed unless the SAD gate rejects the split whichever INTER16
                 // reference ends up chosen
                 auto gate_skip = [&](int s16) { return s16 > 0 && ssad * 10 >= s16 * 9; };
-                const bool need8 = !lfast && !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
+                const bool need8 = l8 && !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
                 if (need8) {
                     if (warp < 12) resid_task(S, 12 + warp / 3, warp % 3, qp, lambda, warp, lane);
                     __syncthreads();
@@ -489,7 +529,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     best_sub = isel;
                     if (Jintra < Jbest) Jbest = Jintra;
                 }
-                if (!lfast && Jbest > lam19 && !gate_skip(sad16)) {
+                if (l8 && Jbest > lam19 && !gate_skip(sad16)) {
                     int b8 = kBitsMode, px = pmvx, py = pmvy;
                     for (int q = 0; q < 4; ++q) {
                         b8 += bits_val(zz_enc(S.qmv[q][0] - px)) + bits_val(zz_enc(S.qmv[q][1] - py));

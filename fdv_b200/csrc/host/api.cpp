@@ -682,9 +682,9 @@ int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf) {
     if (rc) set_engine_err();
     return rc;
 }
-int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf3) {
-    if (!g || !conf3) { set_err("null argument"); return -1; }
-    return fdvb_engine_learned_conf(g, conf3);
+int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf5) {
+    if (!g || !conf5) { set_err("null argument"); return -1; }
+    return fdvb_engine_learned_conf(g, conf5);
 }
 int fdvg_set_records(fdvg_ctx *g, int enable) {
     const int rc = fdvb_engine_records(g, enable);

@@ -31,6 +31,6 @@ void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row);
 int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out32);
 int fdvb_engine_set_learned(fdvb_engine *E, const float *params, float conf);
 int fdvb_engine_records(fdvb_engine *E, int enable);
-int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf3);
+int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf5);
 int fdvb_engine_mb_records(fdvb_engine *E, int unit, uint8_t *mode, int16_t *mv, uint8_t *ref, float *cost);
 }

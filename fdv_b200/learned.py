@@ -113,7 +113,7 @@ class Net:
 
     def features(self, s: np.ndarray) -> np.ndarray:
         s = np.ascontiguousarray(s, SAMPLE)
-        x = np.empty((len(s), 32, 32, 8), np.float32)
+        x = np.empty((len(s), 32, 32, 4), np.float32)
         _check(lib().fdvl_features(self._n, s.ctypes.data, len(s), _f(x)), "features")
         return x
 
@@ -221,7 +221,7 @@ def collect(nframes: int = 2000, clip: int = 50, qps=QPS, seed0: int = 1000, ski
 
 
 # fp32 parameter layout (fdv_b200/csrc/device/learned.cuh): per layer W[cout][k] then b[cout]
-GEO = [(8, 32, 72), (32, 64, 288), (64, 160, 576), (160, 11, 2560)]   # cin, cout, k
+GEO = [(4, 32, 37), (32, 64, 288), (64, 160, 576), (160, 11, 2560)]   # cin, cout, k
 
 
 def init_params(seed: int = 1) -> np.ndarray:
@@ -276,7 +276,7 @@ def encode_engine(frames, w: int, h: int, qp: int, keyint: int = 0, params=None,
     if params is not None:
         if np.ndim(conf):
             eng.set_learned(params, 0.8)
-            eng.set_learned_conf(conf)
+            eng.set_learned_conf(conf[:3], conf[3] if len(conf) > 3 else 0.0, bool(conf[4]) if len(conf) > 4 else False)
         else:
             eng.set_learned(params, conf)
     tc = TabCache()

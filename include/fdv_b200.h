@@ -252,7 +252,7 @@ void fdvb_scene_close(fdvb_scene_state *s);
 
 
 /* ---- Learned proposal network (no counterpart in the reference) ----------
- * A 4-layer convolutional network (141,323 parameters; bf16 on the tensor
+ * A 4-layer convolutional network (140,203 parameters; bf16 on the tensor
  * cores, fp32 master weights and accumulation) that proposes four motion
  * vectors and a SKIP / inter / intra prior per macroblock.  It is trained on
  * (macroblock, chosen MV, chosen mode, RD cost) tuples of the plain encoder.
@@ -304,11 +304,21 @@ int fdvl_gemm(int device, int M, int N, int K, const uint16_t *A, const uint16_t
  * intra; intra skips the motion searches.  Elsewhere the full search runs.
  * The streams stay valid fdv streams (the decoder does not care how a mode
  * was chosen) but are no longer byte-identical to the reference encoder's.
- * params: fdvl_nparams() floats; NULL turns proposals off. */
+ * params: fdvl_nparams() floats; NULL turns proposals off.  This call sets
+ * the product configuration: the SKIP class at threshold `conf`, taken only
+ * while the best merge candidate's RD cost is at most 400 lambda; the inter
+ * class at 0.9, its narrowed analysis keeping INTER8 (four seeded, shortened
+ * 8x8 searches); intra always on the full search.  Every full search starts
+ * its motion searches from the proposed vectors too (doubled for the second
+ * reference).  fdvg_set_learned_conf changes it. */
 int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf);
-/* Per-class thresholds (SKIP, inter, intra) in place of the single one; a
- * value above 1 keeps that class on the full search. */
-int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf3);
+/* conf5: per-class thresholds (SKIP, inter, intra) in place of the single
+ * one -- a value above 1 keeps that class on the full search --, a SKIP gate
+ * (a confident SKIP is taken only while the best merge candidate's RD cost
+ * is at most gate * lambda; gate <= 0: no gate) and, when nonzero, INTER8 in
+ * the confident-inter path (its four searches seeded with the proposals and
+ * cut to a few diamond steps). */
+int fdvg_set_learned_conf(fdvg_ctx *g, const float *conf5);
 /* The process-wide setting used by fdv_video_encode / fdv_vtile_encode /
  * fdv_enc_* from the next call on. */
 int fdvb_set_learned(const float *params, float conf);

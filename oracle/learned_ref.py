@@ -9,17 +9,17 @@ GPU sums in fp32, so the two agree to fp32 accumulation-order noise.  With
 ``use_bf16=False`` it is a plain float64 model, used for finite-difference
 checks of the backward pass itself.
 
-Geometry (fdv_b200/csrc/device/learned.cuh): 32 x 32 x 8 input (four luma
-channels, the quantiser, three zeros), three 3x3 stride-2 pad-1 convolutions
-with ReLU (8->32->64->160), a 2560->11 fully connected layer; NHWC, reduction
-index (ky*3+kx)*Cin + ci.
+Geometry (fdv_b200/csrc/device/learned.cuh): 32 x 32 x 4 luma input, three
+3x3 stride-2 pad-1 convolutions with ReLU (4->32->64->160; the first has a
+37th reduction column holding the quantiser, (qp-26)/8), a 2560->11 fully
+connected layer; NHWC, reduction index (ky*3+kx)*Cin + ci.
 """
 from __future__ import annotations
 
 import numpy as np
 
 GEO = [  # sin, cin, cout, k
-    (32, 8, 32, 72),
+    (32, 4, 32, 37),
     (16, 32, 64, 288),
     (8, 64, 160, 576),
     (4, 160, 11, 2560),
@@ -71,8 +71,8 @@ def init_params(seed: int = 1) -> np.ndarray:
     return p
 
 
-def features(cur: np.ndarray, ref: np.ndarray, bx: int, by: int, qp: int) -> np.ndarray:
-    """32 x 32 x 8 input of the macroblock at (bx, by); planes are h x w luma."""
+def features(cur: np.ndarray, ref: np.ndarray, bx: int, by: int) -> np.ndarray:
+    """32 x 32 x 4 input of the macroblock at (bx, by); planes are h x w luma."""
     h, w = cur.shape
     ys = np.clip(np.arange(32) + by - 8, 0, h - 1)
     xs = np.clip(np.arange(32) + bx - 8, 0, w - 1)
@@ -89,10 +89,7 @@ def features(cur: np.ndarray, ref: np.ndarray, bx: int, by: int, qp: int) -> np.
         return (s + 2) >> 2
 
     x = np.stack([c0, c1, avg(cur), avg(ref)], axis=-1).astype(np.float32)
-    out = np.zeros((32, 32, 8), np.float32)
-    out[..., :4] = bf16((x - 128.0) / 64.0)
-    out[..., 4] = (qp - 26) / 8.0
-    return out
+    return bf16((x - 128.0) / 64.0)
 
 
 def im2col(x: np.ndarray) -> np.ndarray:
@@ -118,8 +115,8 @@ def col2im(dcol: np.ndarray, b: int, s: int, c: int) -> np.ndarray:
     return dxp[:, 1:s + 1, 1:s + 1, :]
 
 
-def forward(p: np.ndarray, x: np.ndarray, use_bf16: bool = True):
-    """x [B][32][32][8] -> (out [B][11], cache)."""
+def forward(p: np.ndarray, x: np.ndarray, qp, use_bf16: bool = True):
+    """x [B][32][32][4], qp [B] -> (out [B][11], cache)."""
     r = bf16 if use_bf16 else (lambda a: a)
     acc = np.float64
     ft = np.float32 if use_bf16 else np.float64
@@ -130,6 +127,8 @@ def forward(p: np.ndarray, x: np.ndarray, use_bf16: bool = True):
     for l in range(3):
         w, bias = layers[l]
         col = im2col(a)
+        if l == 0:   # the quantiser column
+            col = np.concatenate([col, np.repeat((np.asarray(qp, np.float64) - 26) / 8.0, 256)[:, None]], axis=1)
         z = col.astype(acc) @ r(w).astype(acc).T + bias.astype(acc)
         y = r(np.maximum(z, 0.0).astype(ft))
         cache["cols"].append(col)

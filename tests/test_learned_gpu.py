@@ -65,8 +65,8 @@ def _samples(L, n, w, h, seed=1):
 
 
 def _oracle_x(planes, s):
-    return np.stack([R.features(planes[c], planes[r], bx * 16, by * 16, qp)
-                     for c, r, bx, by, qp in zip(s["cur"], s["ref"], s["mbx"], s["mby"], s["qp"])])
+    return np.stack([R.features(planes[c], planes[r], bx * 16, by * 16)
+                     for c, r, bx, by in zip(s["cur"], s["ref"], s["mbx"], s["mby"])])
 
 
 def _targets(s):
@@ -86,7 +86,7 @@ def test_forward_and_gradients_match_oracle(L):
     net.set_params(p)
     s = _samples(L, 128, net.w, net.h, seed=4)
     x = _oracle_x(planes, s)
-    out_ref, cache = R.forward(p, x)
+    out_ref, cache = R.forward(p, x, s["qp"])
     out = net.forward(s)
     err = np.linalg.norm(out[:, :11] - out_ref) / np.linalg.norm(out_ref)
     assert err < 2e-2, err
@@ -197,9 +197,26 @@ def test_learned_stream_decodes_to_gpu_reconstruction(built, cls):
     w, h, qp = 320, 192, 26
     frames = F.Scene(w, h, 6, nrects=8, rect_min=8, rect_max=48, vmax_qpel=20, pan_qx=3, seed=11).frames(6)
     p = _forcing_params(L, cls) if cls >= 0 else L.init_params(3)
-    stream, recs, _ = L.encode_engine(frames, w, h, qp, 0, params=p, conf=0.5 if cls >= 0 else 0.34)
+    conf = (0.5, 0.5, 0.5, 0.0) if cls >= 0 else (0.34, 0.34, 0.34, 0.0)
+    stream, recs, _ = L.encode_engine(frames, w, h, qp, 0, params=p, conf=conf)
     dec = O.ref_video_decode(stream, 16)
     for f in range(len(frames)):
         assert np.array_equal(dec[f], recs[f]), f
     plain, _, _ = L.encode_engine(frames, w, h, qp, 0)
     assert plain == O.ref_video_encode(frames, w, h, qp, 0)
+
+
+def test_trained_weights_product_setting(built):
+    """The committed network in the product setting: valid streams whose
+    reconstruction the reference decoder reproduces, on held-out content."""
+    import fdv_b200 as F
+    import fdv_b200.learned as L
+    import oracle as O
+    w, h, qp = 320, 192, 23
+    frames = F.Scene(w, h, 8, seed=77, **L.CONTENT).frames(8)
+    p = L.load_params(L.DEFAULT_WEIGHTS)
+    stream, recs, st = L.encode_engine(frames, w, h, qp, 0, params=p, conf=0.8)
+    dec = O.ref_video_decode(stream, 16)
+    for f in range(len(frames)):
+        assert np.array_equal(dec[f], recs[f]), f
+    assert L.psnr_y(frames, recs, w, h) > 40.0
