@@ -472,6 +472,7 @@ struct fdvl_net {
     float *dWT[4] = {}, *db[4] = {}, *dY[3] = {}, *dcol[2] = {};
     unsigned *err = nullptr;
     uint8_t *wimg = nullptr;      // canonical weight images of the fused inference kernel
+    unsigned long long *iprof = nullptr;   // fused-inference phase profile (when enabled)
     float *outf = nullptr;        // fused-inference outputs (tests)
     Hint *hints = nullptr;        // fused-inference hints (tests)
     int nsm = 148;
@@ -567,6 +568,7 @@ void net_free(fdvl_net *n) {
     cudaSetDevice(n->device);
     if (n->st) cudaStreamSynchronize(n->st);
     for (void *p : n->owned) cudaFree(p);
+    if (n->iprof) cudaFree(n->iprof);
     for (int i = 0; i < 2; ++i) {
         if (n->S_h[i]) cudaFreeHost(n->S_h[i]);
         if (n->S_ev[i]) cudaEventDestroy(n->S_ev[i]);
@@ -659,6 +661,7 @@ int fused_infer(fdvl_net *n, const Sample *S, int nb, float3 conf, int lim, Hint
     InferW W;
     W.img = n->wimg;
     for (int l = 0; l < 4; ++l) W.b[l] = n->w + b_off(l);
+    W.prof = n->iprof;
     infer_kernel<<<std::min(nb, n->nsm), INT, kInferSmem, st>>>(S, nb, W, conf, lim, hints, out, err);
     return cu_ok(cudaGetLastError(), "fused inference") ? 0 : -1;
 }
@@ -857,6 +860,22 @@ int fdvl_forward(fdvl_net *n, const fdvl_sample *s, int nb, float *out) {
     if (load_batch(n, s, nb, tmp) || forward(n, n->S, nb, n->st)) return -1;
     LCK(cudaMemcpyAsync(out, n->O, sizeof(float) * kOutPad * nb, cudaMemcpyDeviceToHost, n->st));
     return check_err(n);
+}
+
+int fdvl_infer_profile(fdvl_net *n, int enable, unsigned long long *out16) {
+    if (!n) return -1;
+    cudaSetDevice(n->device);
+    if (enable && !n->iprof) {
+        LCK(cudaMalloc(&n->iprof, 16 * sizeof(unsigned long long)));
+        LCK(cudaMemset(n->iprof, 0, 16 * sizeof(unsigned long long)));
+    }
+    if (out16 && n->iprof) {
+        LCK(cudaStreamSynchronize(n->st));
+        LCK(cudaMemcpy(out16, n->iprof, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        LCK(cudaMemset(n->iprof, 0, 16 * sizeof(unsigned long long)));
+    }
+    if (!enable && n->iprof) { cudaFree(n->iprof); n->iprof = nullptr; }
+    return 0;
 }
 
 int fdvl_forward_fused(fdvl_net *n, const fdvl_sample *s, int nb, float conf, int lim, float *out, void *hints) {

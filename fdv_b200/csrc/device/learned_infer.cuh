@@ -42,22 +42,28 @@ constexpr int kWImage = kW1c + kW2c + kW3c + kW4c;
 // shared memory
 constexpr int kAbuf = 128 * 128;            // one 128-row x 64-K operand tile
 constexpr int kWin = 65 * 72;               // one 64x64(+1) luma window, 72-byte rows
-constexpr int O_W1 = 0, O_W2 = O_W1 + kW1c, O_A = O_W2 + kW2c, O_R1 = O_A + 2 * kAbuf;
-// R1: X0[2] (16 KB) + Y1[2] (32 KB); conv1's tiles 2-3 sit in the Y1 half until
-// its epilogue; then conv3 weight chunks; then the fc operand
+// A: four operand tiles (conv1's four tiles; conv2's chunks 0-3, chunk 4 in
+// X0; conv3's chunks three at a time, their weights in A3 + R1); before that
+// the staged luma windows, at the end the fc outputs.
+constexpr int O_W1 = 0, O_W2 = O_W1 + kW1c, O_A = O_W2 + kW2c, O_R1 = O_A + 4 * kAbuf;
+// R1: X0[2] (16 KB) + Y1[2] (32 KB); then conv3 weight chunks; then the fc operand
 constexpr int kR1 = 16384 + 2 * 16384;
 constexpr int O_X0 = O_R1, O_Y1 = O_R1 + 16384;
+constexpr int O_W3 = O_A + 3 * kAbuf;       // three conv3 weight chunks (A3 + R1)
 constexpr int O_Y2 = O_R1 + kR1, O_BAR = O_Y2 + IMB * 8192, O_SMP = O_BAR + 64;
 constexpr int kInferSmem = O_SMP + IMB * (int)sizeof(Sample);
 // the weight offsets below are the flat parameter layout's
 static_assert(kWOff[1] == 1216 && kWOff[2] == 19712 && kWOff[3] == 112032, "parameter layout");
-static_assert(2 * kW3chunk <= kR1 && 3 * kAbuf <= kR1 && 2 * kW4chunk <= IMB * 8192 && 4 * kWin <= 2 * kAbuf,
+static_assert(O_W3 + 3 * kW3chunk <= O_R1 + kR1 && 3 * kAbuf <= kR1 && 2 * kW4chunk <= IMB * 8192 &&
+                  4 * kWin <= 4 * kAbuf && kInferSmem <= 232448,
               "region reuse");
 
 struct InferW {
     const uint8_t *img;                     // kWImage bytes: W1c | W2c | W3c | W4c
     const float *b[4];                      // fp32 biases
+    unsigned long long *prof;               // optional per-phase cycle sums (thread 0 of each CTA)
 };
+enum { IP_STAGE = 0, IP_FEAT, IP_C1, IP_C1E, IP_C2, IP_C2E, IP_C3, IP_FC, IP_NGROUP, IP_N = 16 };
 
 // Canonical operand images of the current bf16-rounded weights.
 __global__ void prep_infer_weights(const float *__restrict__ w, uint8_t *__restrict__ img) {
@@ -165,13 +171,21 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
         if (b) ++iss1; else ++iss0;
     };
     const uint32_t a0 = smem_u32(sm + O_A), a1 = a0 + kAbuf, w1s = smem_u32(sm + O_W1), w2s = smem_u32(sm + O_W2);
-    // conv1's four tiles: the two operand buffers, then the Y1 half of R1
-    const uint32_t t1s[4] = {a0, a1, smem_u32(sm + O_Y1), smem_u32(sm + O_Y1) + kAbuf};
+    const uint32_t t1s[4] = {a0, a0 + kAbuf, a0 + 2 * kAbuf, a0 + 3 * kAbuf};
     const int mb0 = (int)((long long)blockIdx.x * n / gridDim.x), mb1 = (int)((long long)(blockIdx.x + 1) * n / gridDim.x);
+    long long tmark = clock64();
+    auto mark = [&](int ph) {
+        if (W.prof && tid == 0) {
+            const long long t = clock64();
+            atomicAdd(&W.prof[ph], (unsigned long long)(t - tmark));
+            tmark = t;
+        }
+    };
     for (int g0 = mb0; g0 < mb1; g0 += IMB) {
         const int cnt = min(IMB, mb1 - g0);
         if (tid < cnt) smp[tid] = S[g0 + tid];
         __syncthreads();
+        if (W.prof && tid == 0) atomicAdd(&W.prof[IP_NGROUP], 1ull);
         for (int pair = 0; 2 * pair < cnt; ++pair) {
             // the two macroblocks' 64x64 (+1) windows of the current and the
             // reference luma: 8-byte loads where the window is inside the
@@ -187,7 +201,8 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
                     const bool inner = x0 >= 0 && x0 + 8 <= sp.w && y >= 0 && y < sp.h &&
                                        ((reinterpret_cast<uintptr_t>(P) | (uintptr_t)st) & 7) == 0;
                     if (inner) {
-                        v = __ldg(reinterpret_cast<const uint2 *>(P + (size_t)y * st + x0));
+                        cpa8(win + (j * 2 + pl) * kWin + row * 72 + 8 * q, P + (size_t)y * st + x0);
+                        continue;
                     } else {
                         const int yy = min(max(y, 0), sp.h - 1);
                         uint32_t b[8];
@@ -199,7 +214,10 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
                 }
                 *reinterpret_cast<uint2 *>(win + (j * 2 + pl) * kWin + row * 72 + 8 * q) = v;
             }
+            cpa_commit();
+            cpa_wait<0>();
             __syncthreads();
+            mark(IP_STAGE);
             // features: full-resolution 32x32 at window offset 16, 2x2 means of the 64x64
 #pragma unroll
             for (int e = tid; e < 2 * 1024; e += INT) {
@@ -216,6 +234,7 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
                 reinterpret_cast<uint2 *>(X0)[e] = *reinterpret_cast<const uint2 *>(o);
             }
             __syncthreads();
+            mark(IP_FEAT);
             // conv1: four tiles t = (macroblock j, half h) built at once, rows =
             // output positions h*128 .., K = 9 taps x 4 channels + the quantiser
             {
@@ -224,7 +243,7 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
                 for (int t = 0; t < 4; ++t) {
                     const int j = t >> 1, p = (t & 1) * 128 + rr, oy = p >> 4, ox = p & 15;
                     const uint2 *xj = reinterpret_cast<const uint2 *>(X0) + j * 1024;
-                    uint8_t *tile = sm + (t < 2 ? O_A + t * kAbuf : O_Y1 + (t - 2) * kAbuf);
+                    uint8_t *tile = sm + O_A + t * kAbuf;
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int kc = rk + 2 * u;   // 8 K values: taps 2kc, 2kc+1
@@ -260,6 +279,7 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
             ++iss1;
             wait_buf(1);
             tc_after_sync();
+            mark(IP_C1);
             // conv1 epilogue: warps 0-3 macroblock 0, warps 4-7 macroblock 1
             for (int hh = 0; hh < 2; ++hh) {
                 const int t = 2 * half + hh, p = hh * 128 + q4 * 32 + lane;
@@ -271,13 +291,15 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
             }
             tc_before_sync();
             __syncthreads();
-            // conv2: rows = (macroblock r>>6, position r&63), K chunks of 64
+            mark(IP_C1E);
+            // conv2: rows = (macroblock r>>6, position r&63); all five 64-wide K
+            // chunks built at once (A0-A3, then X0), one MMA batch
             {
                 const int j = rr >> 6, p = rr & 63, oy = p >> 3, ox = p & 7;
                 const bf16 *yj = Y1 + j * 256 * 32;
+#pragma unroll
                 for (int c = 0; c < 5; ++c) {
-                    const int b = c & 1;
-                    wait_buf(b);
+                    uint8_t *chunk = sm + (c < 4 ? O_A + c * kAbuf : O_X0);
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int kc = rk + 2 * u, k0 = c * 64 + kc * 8, tap = k0 >> 5, ci = k0 & 31;
@@ -285,16 +307,29 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
                         uint4 v = make_uint4(0, 0, 0, 0);
                         if (tap < 9 && y >= 0 && y < 16 && x >= 0 && x < 16)
                             v = *reinterpret_cast<const uint4 *>(yj + (y * 16 + x) * 32 + ci);
-                        *reinterpret_cast<uint4 *>(sm + O_A + b * kAbuf + umma_off(rr, kc * 8)) = v;
+                        *reinterpret_cast<uint4 *>(chunk + umma_off(rr, kc * 8)) = v;
                     }
-                    fence_async_smem();
-                    __syncthreads();
-                    mma4(b ? a1 : a0, w2s + c * kW2chunk, tmem + 128, 64, c > 0, b);
                 }
+                fence_async_smem();
+                __syncthreads();
+                if (tid == 0) {
+                    tc_after_sync();
+                    const uint32_t id = umma_idesc_bf16(128, 64);
+                    const uint32_t x0s = smem_u32(sm + O_X0);
+#pragma unroll
+                    for (int c = 0; c < 5; ++c)
+#pragma unroll
+                        for (int ks = 0; ks < 4; ++ks)
+                            umma_bf16(tmem + 128, umma_desc((c < 4 ? a0 + c * kAbuf : x0s) + ks * 256, 128, 1024),
+                                      umma_desc(w2s + c * kW2chunk + ks * 256, 128, 1024), id, (c | ks) ? 1u : 0u);
+                    umma_commit(&bar[1]);
+                }
+                ++iss1;
             }
             wait_buf(0);
             wait_buf(1);
             tc_after_sync();
+            mark(IP_C2);
             {
                 const int r = q4 * 32 + lane, j = r >> 6, p = r & 63, c0 = half * 32;
                 float v[16];
@@ -306,41 +341,53 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
             }
             tc_before_sync();
             __syncthreads();
+            mark(IP_C2E);
         }
-        // conv3: rows = (macroblock r>>4, position r&15), K chunks of 64; each
-        // weight chunk is copied one step ahead
+        // conv3: rows = (macroblock r>>4, position r&15); nine 64-wide K chunks
+        // in three rounds of three (operands in A0-A2, weights in A3 + R1)
         {
             const uint8_t *w3 = W.img + kW1c + kW2c;
             const int m = rr >> 4, p = rr & 15, oy = p >> 2, ox = p & 3;
-            for (int e = tid; e < kW3chunk / 16; e += INT) cpa16(sm + O_R1 + e * 16, w3 + e * 16, 16);
-            cpa_commit();
-            for (int c = 0; c < 9; ++c) {
-                const int b = c & 1;
-                wait_buf(b);   // MMA c-2 read operand buffer b and weight buffer b
+            for (int rnd = 0; rnd < 3; ++rnd) {
+                wait_buf(1);   // the previous round's MMAs are done with these buffers
+                for (int e = tid; e < 3 * kW3chunk / 16; e += INT)
+                    cpa16(sm + O_W3 + e * 16, w3 + rnd * 3 * kW3chunk + e * 16, 16);
+                cpa_commit();
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int kc = rk + 2 * u, k0 = c * 64 + kc * 8, tap = k0 >> 6, ci = k0 & 63;
-                    const int ky = (tap * 11) >> 5, kx = tap - 3 * ky, y = 2 * oy - 1 + ky, x = 2 * ox - 1 + kx;
-                    uint4 v = make_uint4(0, 0, 0, 0);
-                    if (y >= 0 && y < 8 && x >= 0 && x < 8 && (m < cnt))
-                        v = *reinterpret_cast<const uint4 *>(Y2 + (m * 64 + y * 8 + x) * 64 + ci);
-                    *reinterpret_cast<uint4 *>(sm + O_A + b * kAbuf + umma_off(rr, kc * 8)) = v;
+                for (int cc = 0; cc < 3; ++cc) {
+                    const int c = rnd * 3 + cc;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int kc = rk + 2 * u, k0 = c * 64 + kc * 8, tap = k0 >> 6, ci = k0 & 63;
+                        const int ky = (tap * 11) >> 5, kx = tap - 3 * ky, y = 2 * oy - 1 + ky, x = 2 * ox - 1 + kx;
+                        uint4 v = make_uint4(0, 0, 0, 0);
+                        if (y >= 0 && y < 8 && x >= 0 && x < 8 && (m < cnt))
+                            v = *reinterpret_cast<const uint4 *>(Y2 + (m * 64 + y * 8 + x) * 64 + ci);
+                        *reinterpret_cast<uint4 *>(sm + O_A + cc * kAbuf + umma_off(rr, kc * 8)) = v;
+                    }
                 }
                 cpa_wait<0>();
                 fence_async_smem();
                 __syncthreads();
-                mma4(b ? a1 : a0, smem_u32(sm + O_R1 + b * kW3chunk), tmem + 256, 160, c > 0, b);
-                if (c + 1 < 9) {   // next weight chunk into the other buffer, once MMA c-1 is done with it
-                    wait_buf(b ^ 1);
-                    for (int e = tid; e < kW3chunk / 16; e += INT)
-                        cpa16(sm + O_R1 + (b ^ 1) * kW3chunk + e * 16, w3 + (c + 1) * kW3chunk + e * 16, 16);
-                    cpa_commit();
+                if (tid == 0) {
+                    tc_after_sync();
+                    const uint32_t id = umma_idesc_bf16(128, 160), w3s = smem_u32(sm + O_W3);
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                        for (int ks = 0; ks < 4; ++ks)
+                            umma_bf16(tmem + 256, umma_desc(a0 + cc * kAbuf + ks * 256, 128, 1024),
+                                      umma_desc(w3s + cc * kW3chunk + ks * 256, 128, 1024), id,
+                                      (rnd | cc | ks) ? 1u : 0u);
+                    umma_commit(&bar[1]);
                 }
+                ++iss1;
             }
         }
         wait_buf(0);
         wait_buf(1);
         tc_after_sync();
+        mark(IP_C3);
         // fc weight chunks 0 and 1 (the conv2 output region is free now)
         const uint8_t *w4 = W.img + kW1c + kW2c + kW3c;
         for (int e = tid; e < 2 * kW4chunk / 16; e += INT) cpa16(sm + O_Y2 + e * 16, w4 + e * 16, 16);
@@ -410,6 +457,7 @@ infer_kernel(const Sample *__restrict__ S, int n, InferW W, float3 conf, int lim
             if (hints) hints[i] = make_hint(o, conf, lim);
         }
         __syncthreads();
+        mark(IP_FC);
     }
     tc_before_sync();
     __syncthreads();

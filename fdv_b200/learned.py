@@ -383,7 +383,9 @@ def main(argv=None) -> None:
     import json
     import time
     ap = argparse.ArgumentParser(description="train / evaluate the learned proposal network")
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "eval", "infer-demo", "encode-demo"],
+                    help="infer-demo / encode-demo: fixed small runs for profiling (fused inference over one "
+                         "1280x720 frame three times plus one 512-sample training step; an 8-frame learned encode)")
     ap.add_argument("--frames", type=int, default=2000)
     ap.add_argument("--clip", type=int, default=50)
     ap.add_argument("--epochs", type=int, default=3)
@@ -406,8 +408,31 @@ def main(argv=None) -> None:
         info.update({"collect_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "curve": curve.tolist(),
                      "samples_per_s": round(len(smp) * a.epochs / max(t2 - t1, 1e-9))})
         print(json.dumps(info))
-    else:
+    elif a.cmd == "eval":
         print(json.dumps(evaluate(load_params(a.weights), a.conf, nframes=a.eval_frames)))
+    elif a.cmd == "infer-demo":
+        net = Net(W, H, 2, max_batch=3648)
+        rng = np.random.default_rng(0)
+        for s in range(2):
+            net.bank_put(s, rng.integers(0, 256, W * H, dtype=np.uint8))
+        net.set_params(load_params(a.weights))
+        s = samples((W // 16) * (H // 16))
+        s["cur"], s["ref"], s["qp"] = 0, 1, 23
+        s["mbx"] = np.tile(np.arange(W // 16), H // 16)
+        s["mby"] = np.repeat(np.arange(H // 16), W // 16)
+        for _ in range(3):
+            net.forward_fused(s, a.conf, 64)
+        t = samples(512)
+        t["cur"], t["ref"], t["qp"], t["weight"], t["has_mv"] = 0, 1, 23, 1.0, 1
+        t["mbx"], t["mby"] = rng.integers(0, W // 16, 512), rng.integers(0, H // 16, 512)
+        t["cls"] = rng.integers(0, 3, 512)
+        net.train_step(t, 1e-3)
+        print("ok")
+    else:
+        from . import Scene
+        frames = Scene(W, H, 8, seed=1, **CONTENT).frames(8)
+        st, _, _ = encode_engine(frames, W, H, 23, 0, params=load_params(a.weights), conf=a.conf)
+        print("ok", len(st))
 
 
 if __name__ == "__main__":

@@ -283,6 +283,10 @@ int fdvl_forward(fdvl_net *n, const fdvl_sample *s, int nb, float *out);
  * as int16 x/y pairs clamped to +-lim, then the confident class as int32,
  * -1 when the mode softmax stays below conf). */
 int fdvl_forward_fused(fdvl_net *n, const fdvl_sample *s, int nb, float conf, int lim, float *out, void *hints);
+/* Per-phase cycle sums of the fused inference kernel, for tuning (enable
+ * turns the counters on; out16 receives and clears them): staging, features,
+ * conv1, its epilogue, conv2, its epilogue, conv3, fc, then the group count. */
+int fdvl_infer_profile(fdvl_net *n, int enable, unsigned long long *out16);
 /* Gradient of the batch-mean loss (nb a multiple of 64); loss[3] = total, mode, MV. */
 int fdvl_grads(fdvl_net *n, const fdvl_sample *s, int nb, float *grad, float *loss);
 int fdvl_train_step(fdvl_net *n, const fdvl_sample *s, int nb, float lr, float *loss);
