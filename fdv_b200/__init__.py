@@ -97,6 +97,10 @@ def lib() -> C.CDLL:
         L.fdvb_scene_frame.argtypes = [p, i, u8p]
         L.fdvb_scene_close.argtypes = [p]
         L.fdvb_scene_close.restype = None
+        ip = C.POINTER(i)
+        L.fdv_video_decode.argtypes = [u8p, sz, u8p, ip, ip, ip]
+        L.fdv_vtile_decode.argtypes = [u8p, sz, u8p, ip, ip, ip, i]
+        L.fdvd_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -165,6 +169,33 @@ def vtile_encode(frames, w: int, h: int, qp: int, keyint: int, band_mbrows: int,
     if n == 0:
         raise FdvError(last_error() or "fdv_vtile_encode failed")
     return out[:n].tobytes()
+
+
+def _decode(fn, stream: bytes, nf: int, w: int, h: int, *extra) -> np.ndarray:
+    if nf <= 0 or w <= 0 or h <= 0 or w % 16 or h % 16:
+        raise FdvError("bad stream header")
+    src = np.frombuffer(stream, np.uint8)
+    out = np.empty(nf * w * h * 3 // 2, np.uint8)
+    n, ww, hh = C.c_int(), C.c_int(), C.c_int()
+    if fn(_ptr(src), src.size, _ptr(out), C.byref(n), C.byref(ww), C.byref(hh), *extra) != 0:
+        raise FdvError((lib().fdvd_last_error() or b"").decode() or "decode failed")
+    return out.reshape(n.value, -1)
+
+
+def video_decode(stream: bytes) -> np.ndarray:
+    """fdv_video_decode (fdv.h:907): [nframes][w*h*3/2] I420 frames."""
+    if len(stream) < 8:
+        raise FdvError("bad stream header")
+    nf, w, h = np.frombuffer(stream[:6], "<u2")
+    return _decode(lib().fdv_video_decode, stream, int(nf), int(w), int(h))
+
+
+def vtile_decode(stream: bytes, nthreads: int = 8) -> np.ndarray:
+    """fdv_vtile_decode (fdv.h:980): [nframes][w*h*3/2] I420 frames."""
+    if len(stream) < 12:
+        raise FdvError("bad stream header")
+    w, h, nf = np.frombuffer(stream[:6], "<u2")
+    return _decode(lib().fdv_vtile_decode, stream, int(nf), int(w), int(h), nthreads)
 
 
 class Encoder:

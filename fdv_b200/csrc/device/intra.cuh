@@ -21,7 +21,7 @@ struct NNPred {
     int kind;     // 0 = flat (dc), 1 = vertical, 2 = horizontal, 3 = plane
     int dc, a, b, c, c0;
 };
-__device__ NNPred nn_setup(int mode, const uint8_t *top, const uint8_t *left, int tl, int n, int ht, int hl) {
+__device__ inline NNPred nn_setup(int mode, const uint8_t *top, const uint8_t *left, int tl, int n, int ht, int hl) {
     NNPred P = {0, 0, 0, 0, 0, 0};
     if (mode == 3 && nn_mode_ok(3, n, ht, hl)) {
         int half = n / 2, H = 0, V = 0;
@@ -61,7 +61,7 @@ __device__ __forceinline__ int nn_px(const NNPred &P, const uint8_t *top, const 
 
 // 4x4 directional prediction of pixel (x, y) from Tn = T(-1..7) and
 // Ln = L(-1..3), T(-1) = L(-1) = the corner.
-__device__ int pred4_px(int mode, const int *Tn, const int *Ln, int ht, int hl, int x, int y) {
+__device__ inline int pred4_px(int mode, const int *Tn, const int *Ln, int ht, int hl, int x, int y) {
 #define T(i) Tn[(i) + 1]
 #define L(i) Ln[(i) + 1]
     switch (mode) {
@@ -109,7 +109,7 @@ __device__ int pred4_px(int mode, const int *Tn, const int *Ln, int ht, int hl, 
 }
 
 // SATD of one 4x4 block on one thread: cur stride cs, pred stride ps.
-__device__ int satd4(const uint8_t *cur, int cs, const uint8_t *pred, int ps) {
+__device__ inline int satd4(const uint8_t *cur, int cs, const uint8_t *pred, int ps) {
     int d[16];
 #pragma unroll
     for (int i = 0; i < 4; ++i)

@@ -18,7 +18,7 @@ def header_functions():
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = re.findall(r"\b([a-z_0-9]+)\s*\(", text)
     skip = {"if", "sizeof"}
-    return sorted({n for n in names if n.startswith(("fdv_", "fdvb_", "fdvg_")) and n not in skip})
+    return sorted({n for n in names if n.startswith(("fdv_", "fdvb_", "fdvg_", "fdvd_")) and n not in skip})
 
 
 def test_library_exports_every_declared_symbol(built):
@@ -34,7 +34,8 @@ def test_reference_api_names_present(built):
     import fdv_b200 as F
     L = F.lib()
     for n in ["fdv_video_encode", "fdv_vtile_encode", "fdv_enc_open", "fdv_enc_open_tiled", "fdv_enc_frame",
-              "fdv_enc_repeat", "fdv_enc_count", "fdv_enc_bytes", "fdv_enc_finish", "fdv_enc_close", "fdv_wrap"]:
+              "fdv_enc_repeat", "fdv_enc_count", "fdv_enc_bytes", "fdv_enc_finish", "fdv_enc_close", "fdv_wrap",
+              "fdv_video_decode", "fdv_vtile_decode"]:
         assert hasattr(L, n)
 
 
@@ -70,6 +71,32 @@ def test_no_cpu_fallback(built):
         F.video_encode(fr, 32, 32, 20, 0)
     L = F.lib()
     assert L.fdv_enc_open(32, 32, 20, 0) is None
+
+
+def test_decoder_header_checks_and_no_cpu_fallback(built):
+    """Malformed headers are rejected before any device work; a well-formed
+    stream without a device fails loudly instead of decoding on the CPU."""
+    import torch
+    import fdv_b200 as F
+    import oracle as O
+    L = F.lib()
+    u8p = C.POINTER(C.c_uint8)
+    out = np.empty(1 << 16, np.uint8)
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    def dec(buf, tiled=False):
+        src = np.frombuffer(buf, np.uint8).copy() if buf else np.zeros(1, np.uint8)
+        args = (src.ctypes.data_as(u8p), len(buf), out.ctypes.data_as(u8p), C.byref(a), C.byref(b), C.byref(c))
+        return L.fdv_vtile_decode(*args, 1) if tiled else L.fdv_video_decode(*args)
+    assert dec(b"") == -1 and "header" in F.lib().fdvd_last_error().decode()
+    assert dec(struct.pack("<HHHBB", 1, 40, 32, 20, 0) + b"\0" * 8) == -1          # width not a multiple of 16
+    assert dec(struct.pack("<HHHBB", 1, 32, 32, 60, 0) + b"\0" * 8) == -1          # qp > 51
+    assert dec(struct.pack("<HHHBBHH", 32, 32, 1, 20, 0, 3, 1) + b"\0" * 8, True) == -1   # 3 bands of 16 rows for 32
+    assert "band" in F.lib().fdvd_last_error().decode()
+    if not torch.cuda.is_available():
+        fr = scene_frames(dict(w=32, h=32, nframes=1, nrects=1, rect_max=16, seed=1))
+        s = O.ref_video_encode(fr, 32, 32, 20, 0)
+        with pytest.raises(F.FdvError):
+            F.video_decode(s)
 
 
 def test_wrap_matches_reference(built):
