@@ -70,7 +70,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                     print("compiled", os.path.relpath(futs[f], ROOT))
     objs = [_obj(s) for s in sources()]
     if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lpthread", "-ldl", "-lrt"]
+        # -z defs: an unresolved symbol fails the link instead of the first call
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lpthread", "-ldl", "-lrt",
+               "-Xlinker", "-z", "-Xlinker", "defs"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

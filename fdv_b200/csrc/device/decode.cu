@@ -21,8 +21,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -359,9 +361,24 @@ void launch_deblock(const void *tasks, int ntasks, cudaStream_t st);
 
 }  // namespace fdvb
 
+
 // ---------------------------------------------------------------------------
 // Host side: the decoder engine and the fdv_video_decode / fdv_vtile_decode
 // entry points.
+//
+// A decode runs as a pipeline over the frames:
+//   parse workers  each owns a fixed set of units (bands) and, frame by frame,
+//                  entropy-decodes and parses their blobs and packs each one
+//                  into a pinned slot (kSlots per unit, so parsing runs up to
+//                  kSlots frames ahead of the GPU);
+//   the submitter  (the calling thread) uploads a frame's slots and its
+//                  launch descriptors, launches the reconstruction, deblocking,
+//                  the download of every unit's frame into a pinned output
+//                  slot and the reference preparation, all on one stream;
+//   copiers        wait for a frame's download and scatter it into the
+//                  caller's buffer.
+// Frame f+1's reconstruction reads frame f's references, so the GPU work is
+// in stream order; parsing never depends on pixels, so it overlaps freely.
 // ---------------------------------------------------------------------------
 using namespace fdvb;
 
@@ -369,14 +386,18 @@ namespace {
 
 thread_local std::string g_derr;
 
-struct PrepTaskD {
+struct PrepTaskD {   // frame_ops.cuh PrepTask
     const uint8_t *rec[3];
     uint8_t *G, *B, *H, *J, *U, *V;
     int w, h, ys, cs, border;
 };
-struct DbTaskD { uint8_t *p; int w, h, qp; };
+struct DbTaskD { uint8_t *p; int w, h, qp; };   // frame_ops.cuh DbTask
+
+constexpr int kSlots = 3;      // parse slots per unit
+constexpr int kOutSlots = 4;   // output frames in flight
 
 int round_up(int v, int a) { return (v + a - 1) / a * a; }
+size_t al256(size_t v) { return (v + 255) & ~size_t(255); }
 
 template <class T>
 T *dmalloc(size_t n, std::vector<void *> &own) {
@@ -391,61 +412,69 @@ struct RefBuf {
     uint8_t *G = nullptr, *B = nullptr, *H = nullptr, *J = nullptr, *U = nullptr, *V = nullptr;
 };
 
+// One frame of one unit, parsed and packed for a single upload: a P-frame's
+// macroblocks, coefficient blocks and INTRA16 list, or per plane of a key
+// frame its leaves, CTU leaf ranges, coefficients and region flags.
+struct PSlot {
+    uint8_t *pin = nullptr;   // pinned, the unit's pay_cap bytes
+    size_t used = 0;
+    int intra = 0, qp = 0, nintra = 0;
+    size_t o_mbs = 0, o_coef = 0, o_intra = 0;
+    size_t o_leaves[3] = {}, o_ctu[3] = {}, o_icoef[3] = {}, o_flags[3] = {};
+    int pqp[3] = {};
+};
+
 struct DUnit {
     int w = 0, h = 0, mbw = 0, mbh = 0, cw = 0, ch = 0;
-    uint8_t *rec = nullptr;           // tight I420
+    size_t rec_off = 0, fs = 0;   // the unit's tight I420 frame in the engine's reconstruction buffer
     RefBuf ref[2];
     int near_i = 0, nref = 0;
     fdvb_tabcache tc{};
-    // device copies of the parse
-    dec::PMB *d_mbs = nullptr;
-    int16_t *d_coef = nullptr;
-    int32_t *d_intra = nullptr;
-    dec::Leaf *d_leaves[3] = {};
-    int32_t *d_ctu[3] = {};
-    int16_t *d_icoef[3] = {};
-    uint8_t *d_flags[3] = {};
-    int *d_prog = nullptr;            // key-frame row progress, three planes
-    int pw[3], ph[3], cols[3], rows[3];
-    // this frame
-    const uint8_t *blob = nullptr;
-    size_t blen = 0;
-    int intra = 0, rc = 0;
-    dec::PFrame pf;
+    uint8_t *d_pay = nullptr;     // the current frame's payload on the device
+    size_t pay_cap = 0;
+    int *d_prog = nullptr;        // key-frame CTU-row progress, three planes
+    int pw[3] = {}, ph[3] = {}, cols[3] = {}, rows[3] = {};
+    PSlot slot[kSlots];
+    dec::PFrame pf;               // parse scratch, capacity kept between frames
     dec::IPlane ip[3];
 };
 
 struct DecEngine {
     int device = 0, border = 32, nsm = 148;
+    std::vector<std::pair<int, int>> sizes;
     cudaStream_t st = nullptr;
     std::vector<DUnit> units;
-    std::vector<void *> own;
-    dk::PUnit *d_pu = nullptr;
-    int *d_uoff = nullptr;
-    dk::IPlaneD *d_planes = nullptr;
-    dk::ITask *d_tasks = nullptr;
-    PrepTaskD *d_prep = nullptr;
-    DbTaskD *d_db = nullptr;
+    std::vector<void *> own;      // device allocations
+    std::vector<void *> pinned;   // host allocations
+    uint8_t *d_rec = nullptr;     // every unit's reconstruction, back to back
+    size_t rec_bytes = 0;
+    uint8_t *out_pin[kOutSlots] = {};
+    uint8_t *desc_pin[kOutSlots] = {};
+    uint8_t *d_desc = nullptr;
+    size_t desc_cap = 0;
     int *d_ticket = nullptr;
     unsigned *d_err = nullptr;
-    uint8_t *stage = nullptr;         // pinned
-    size_t stage_cap = 0;
+    cudaEvent_t ev_in[kSlots] = {}, ev_out[kOutSlots] = {};
+    int ntask_max = 0;
     ~DecEngine() {
+        cudaSetDevice(device);
         if (st) cudaStreamSynchronize(st);
+        for (auto e : ev_in) if (e) cudaEventDestroy(e);
+        for (auto e : ev_out) if (e) cudaEventDestroy(e);
         for (void *p : own) cudaFree(p);
-        if (stage) cudaFreeHost(stage);
+        for (void *p : pinned) cudaFreeHost(p);
         if (st) cudaStreamDestroy(st);
     }
 };
 
-bool ck(cudaError_t e, const char *what) {
+bool ck(cudaError_t e, const char *what, std::string &err) {
     if (e == cudaSuccess) return true;
-    g_derr = std::string(what) + ": " + cudaGetErrorString(e);
+    err = std::string(what) + ": " + cudaGetErrorString(e);
     return false;
 }
-#define DCK(x)                          \
-    do {                                \
-        if (!ck((x), #x)) return -1;    \
+#define DCK(x)                               \
+    do {                                     \
+        if (!ck((x), #x, g_derr)) return -1; \
     } while (0)
 
 // The transform tables of this translation unit's kernels.
@@ -468,29 +497,56 @@ int reference_border() {
     return r <= 16 ? 32 : (r <= 32 ? 64 : 96);
 }
 
-int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes) {
-    DCK(cudaGetDevice(&E.device));
-    cudaDeviceGetAttribute(&E.nsm, cudaDevAttrMultiProcessorCount, E.device);
+// Byte sizes of one frame's launch descriptors (the largest frame: every unit
+// a P-frame and a key frame at once).
+struct DescLayout {
+    size_t pu, uoff, planes, tasks, db, prep, total;
+    DescLayout(int nu, int ntasks) {
+        pu = 0;
+        uoff = pu + al256(sizeof(dk::PUnit) * nu);
+        planes = uoff + al256(sizeof(int) * (nu + 1));
+        tasks = planes + al256(sizeof(dk::IPlaneD) * 3 * nu);
+        db = tasks + al256(sizeof(dk::ITask) * std::max(ntasks, 1));
+        prep = db + al256(sizeof(DbTaskD) * 3 * nu);
+        total = prep + al256(sizeof(PrepTaskD) * nu);
+    }
+};
+
+int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes, int device, int border) {
+    E.device = device;
+    E.border = border;
+    E.sizes = sizes;
+    DCK(cudaSetDevice(device));
+    cudaDeviceGetAttribute(&E.nsm, cudaDevAttrMultiProcessorCount, device);
     DCK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    for (auto &e : E.ev_in) DCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : E.ev_out) DCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (upload_dec_tables()) return -1;
-    E.border = reference_border();
-    const int Bp = E.border + 16;   // allocated border: the checked one plus the filter taps
+    const int Bp = border + 16;   // allocated border: the checked one plus the filter taps
     const int nu = (int)sizes.size();
     E.units.resize(nu);
-    size_t stage = 0;
+    auto fail_alloc = [&]() { g_derr = "device or pinned allocation failed"; return -1; };
+    auto pin = [&](size_t n) -> uint8_t * {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, std::max<size_t>(n, 1), cudaHostAllocDefault) != cudaSuccess) return nullptr;
+        E.pinned.push_back(p);
+        return static_cast<uint8_t *>(p);
+    };
     int ntasks = 0;
     for (int i = 0; i < nu; ++i) {
         DUnit &u = E.units[i];
         u.w = sizes[i].first;
         u.h = sizes[i].second;
         u.mbw = u.w / 16; u.mbh = u.h / 16; u.cw = u.w / 2; u.ch = u.h / 2;
-        const size_t fs = (size_t)u.w * u.h * 3 / 2, nmb = (size_t)u.mbw * u.mbh;
-        u.rec = dmalloc<uint8_t>(fs, E.own);
+        u.fs = (size_t)u.w * u.h * 3 / 2;
+        u.rec_off = E.rec_bytes;
+        E.rec_bytes += u.fs;
+        const size_t nmb = (size_t)u.mbw * u.mbh;
         const int ys = round_up(u.w + 2 * Bp, 64), cs = round_up(u.cw + 2 * Bp, 64);
         const size_t lsz = (size_t)ys * (u.h + 2 * Bp), csz = (size_t)cs * (u.ch + 2 * Bp);
         for (int r = 0; r < 2; ++r) {
             uint8_t *m = dmalloc<uint8_t>(4 * lsz + 2 * csz, E.own);
-            if (!m) { g_derr = "device allocation failed"; return -1; }
+            if (!m) return fail_alloc();
             DCK(cudaMemset(m, 0, 4 * lsz + 2 * csz));
             RefBuf &s = u.ref[r];
             s.G = m + (size_t)Bp * ys + Bp; m += lsz;
@@ -502,206 +558,79 @@ int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes) {
             s.rp.G = s.G; s.rp.B = s.B; s.rp.H = s.H; s.rp.J = s.J; s.rp.U = s.U; s.rp.V = s.V;
             s.rp.ys = ys; s.rp.cs = cs;
         }
-        u.d_mbs = dmalloc<dec::PMB>(nmb, E.own);
-        u.d_coef = dmalloc<int16_t>(nmb * 384, E.own);
-        u.d_intra = dmalloc<int32_t>(nmb, E.own);
         u.pw[0] = u.w; u.ph[0] = u.h; u.pw[1] = u.pw[2] = u.cw; u.ph[1] = u.ph[2] = u.ch;
         int nprog = 0;
-        size_t istage = 0;
+        size_t ipay = 0;
         for (int p = 0; p < 3; ++p) {
             u.cols[p] = (u.pw[p] + 63) / 64;
             u.rows[p] = (u.ph[p] + 63) / 64;
             nprog += u.rows[p];
             ntasks += u.rows[p];
             const size_t px = (size_t)u.pw[p] * u.ph[p];
-            u.d_leaves[p] = dmalloc<dec::Leaf>(px / 16, E.own);
-            u.d_ctu[p] = dmalloc<int32_t>((size_t)u.cols[p] * u.rows[p] + 1, E.own);
-            u.d_icoef[p] = dmalloc<int16_t>(px, E.own);
-            u.d_flags[p] = dmalloc<uint8_t>(px / 64 + 1, E.own);
-            if (!u.d_leaves[p] || !u.d_ctu[p] || !u.d_icoef[p] || !u.d_flags[p]) {
-                g_derr = "device allocation failed";
-                return -1;
-            }
-            istage += px / 16 * sizeof(dec::Leaf) + ((size_t)u.cols[p] * u.rows[p] + 1) * 4 + px * 2 + px / 64 + 1024;
+            // at most one leaf per 4x4 cell, one coefficient per sample, one flag per 8x8 region
+            ipay += al256(px / 16 * sizeof(dec::Leaf)) + al256(((size_t)u.cols[p] * u.rows[p] + 1) * 4) +
+                    al256(px * 2) + al256(px / 64 + 1);
         }
+        const size_t ppay = al256(nmb * sizeof(dec::PMB)) + al256(nmb * 384 * 2) + al256(nmb * 4);
+        u.pay_cap = std::max(ppay, ipay);
+        u.d_pay = dmalloc<uint8_t>(u.pay_cap, E.own);
         u.d_prog = dmalloc<int>(nprog, E.own);
-        const size_t pstage = nmb * sizeof(dec::PMB) + nmb * 384 * 2 + nmb * 4 + 1024;
-        stage += std::max(pstage, istage) + fs + 256;
-        if (!u.rec || !u.d_mbs || !u.d_coef || !u.d_intra || !u.d_prog) { g_derr = "device allocation failed"; return -1; }
+        if (!u.d_pay || !u.d_prog) return fail_alloc();
+        for (auto &sl : u.slot)
+            if (!(sl.pin = pin(u.pay_cap))) return fail_alloc();
     }
-    E.d_pu = dmalloc<dk::PUnit>(nu, E.own);
-    E.d_uoff = dmalloc<int>(nu + 1, E.own);
-    E.d_planes = dmalloc<dk::IPlaneD>(3 * nu, E.own);
-    E.d_tasks = dmalloc<dk::ITask>(ntasks, E.own);
-    E.d_prep = dmalloc<PrepTaskD>(nu, E.own);
-    E.d_db = dmalloc<DbTaskD>(3 * nu, E.own);
+    E.ntask_max = ntasks;
+    const DescLayout D(nu, ntasks);
+    E.desc_cap = D.total;
+    E.d_desc = dmalloc<uint8_t>(D.total, E.own);
+    E.d_rec = dmalloc<uint8_t>(E.rec_bytes, E.own);
     E.d_ticket = dmalloc<int>(1, E.own);
     E.d_err = dmalloc<unsigned>(1, E.own);
-    E.stage_cap = stage + 8192 + (size_t)nu * (sizeof(dk::PUnit) + 3 * sizeof(dk::IPlaneD) + sizeof(PrepTaskD) +
-                                               3 * sizeof(DbTaskD) + 8 * 256) + (size_t)ntasks * sizeof(dk::ITask);
-    if (!E.d_pu || !E.d_uoff || !E.d_planes || !E.d_tasks || !E.d_prep || !E.d_db || !E.d_ticket || !E.d_err ||
-        !ck(cudaHostAlloc(reinterpret_cast<void **>(&E.stage), E.stage_cap, cudaHostAllocDefault), "pinned staging")) {
-        if (g_derr.empty()) g_derr = "device allocation failed";
-        return -1;
-    }
+    if (!E.d_desc || !E.d_rec || !E.d_ticket || !E.d_err) return fail_alloc();
+    for (int o = 0; o < kOutSlots; ++o)
+        if (!(E.out_pin[o] = pin(E.rec_bytes)) || !(E.desc_pin[o] = pin(D.total))) return fail_alloc();
     return 0;
 }
 
-// One frame of every unit: parse (a host thread per unit), upload, reconstruct,
-// deblock, download into the unit's planes of the output frame (strides
-// ostride and ostride / 2), then the decoded frame becomes the reference.
-int engine_frame(DecEngine &E, uint8_t *const *outY, uint8_t *const *outU, uint8_t *const *outV, int ostride) {
-    const int nu = (int)E.units.size();
-    auto parse = [&](int i) {
-        DUnit &u = E.units[i];
-        if (u.intra) {
-            memset(&u.tc, 0, sizeof u.tc);   // tables and history restart at a key frame
-            size_t p = 0;
-            u.rc = 0;
-            for (int pl = 0; pl < 3 && u.rc == 0; ++pl) {
-                if (p + 4 > u.blen) { u.rc = -1; break; }
-                uint32_t n = 0;
-                for (int k = 0; k < 4; ++k) n |= (uint32_t)u.blob[p + k] << (8 * k);
-                p += 4;
-                if (p + n > u.blen || n < 4) { u.rc = -1; break; }
-                u.rc = dec::parse_iplane(u.blob + p, n, u.pw[pl], u.ph[pl], u.ip[pl]);
-                p += n;
-            }
-        } else {
-            u.rc = dec::parse_pframe(u.blob, u.blen, u.w, u.h, E.border, &u.tc, u.pf);
-        }
-    };
-    if (nu == 1) {
-        parse(0);
-    } else {
-        std::vector<std::thread> th;
-        for (int i = 0; i < nu; ++i) th.emplace_back(parse, i);
-        for (auto &t : th) t.join();
-    }
-    for (int i = 0; i < nu; ++i)
-        if (E.units[i].rc) { g_derr = "malformed frame blob"; return -1; }
+// Engines kept between calls, keyed by device, border and unit sizes; taken
+// out while in use.
+constexpr size_t kCacheMax = 4;
+std::mutex g_dcache_mu;
+std::vector<DecEngine *> *g_dcache = new std::vector<DecEngine *>();   // never destroyed: outlives the CUDA runtime
 
-    uint8_t *sp = E.stage, *const send = E.stage + E.stage_cap;
-    bool room = true;
-    auto put = [&](const void *src, size_t n) -> const uint8_t * {
-        const size_t a = (n + 255) / 256 * 256;
-        if (sp + a > send) { room = false; return nullptr; }
-        memcpy(sp, src, n);
-        const uint8_t *r = sp;
-        sp += a;
-        return r;
-    };
-    auto up = [&](void *dst, const void *src, size_t n) -> int {
-        if (!n) return 0;
-        const uint8_t *s = put(src, n);
-        if (!s) { g_derr = "staging buffer too small"; return -1; }
-        DCK(cudaMemcpyAsync(dst, s, n, cudaMemcpyHostToDevice, E.st));
-        return 0;
-    };
-    std::vector<dk::PUnit> pu;
-    std::vector<int> uoff{0};
-    std::vector<dk::IPlaneD> ipl;
-    std::vector<dk::ITask> tasks;
-    std::vector<DbTaskD> db;
-    std::vector<PrepTaskD> prep;
-    for (int i = 0; i < nu; ++i) {
-        DUnit &u = E.units[i];
-        uint8_t *rec[3] = {u.rec, u.rec + (size_t)u.w * u.h, u.rec + (size_t)u.w * u.h + (size_t)u.cw * u.ch};
-        if (!u.intra) {
-            dec::PFrame &f = u.pf;
-            if (up(u.d_mbs, f.mbs.data(), f.mbs.size() * sizeof(dec::PMB)) ||
-                up(u.d_coef, f.coef.data(), f.coef.size() * 2) || up(u.d_intra, f.intra.data(), f.intra.size() * 4))
-                return -1;
-            dk::PUnit d{};
-            d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh; d.qp = f.qp;
-            for (int p = 0; p < 3; ++p) d.rec[p] = rec[p];
-            d.ref[0] = u.ref[u.near_i].rp;
-            d.ref[1] = u.nref >= 2 ? u.ref[1 - u.near_i].rp : u.ref[u.near_i].rp;
-            d.mbs = u.d_mbs; d.coef = u.d_coef; d.intra = u.d_intra; d.nintra = (int)f.intra.size();
-            pu.push_back(d);
-            uoff.push_back(uoff.back() + u.mbw * u.mbh);
-            for (int p = 0; p < 3; ++p) db.push_back({rec[p], u.pw[p], u.ph[p], f.qp});
-        } else {
-            int prog = 0;
-            for (int p = 0; p < 3; ++p) {
-                dec::IPlane &P = u.ip[p];
-                if (up(u.d_leaves[p], P.leaves.data(), P.leaves.size() * sizeof(dec::Leaf)) ||
-                    up(u.d_ctu[p], P.ctu_first.data(), P.ctu_first.size() * 4) ||
-                    up(u.d_icoef[p], P.coef.data(), P.coef.size() * 2) ||
-                    up(u.d_flags[p], P.flags.data(), P.flags.size()))
-                    return -1;
-                dk::IPlaneD d{};
-                d.rec = rec[p]; d.w = u.pw[p]; d.h = u.ph[p]; d.cols = u.cols[p]; d.rows = u.rows[p];
-                d.leaves = u.d_leaves[p]; d.ctu_first = u.d_ctu[p]; d.coef = u.d_icoef[p]; d.flags = u.d_flags[p];
-                d.progress = u.d_prog + prog; d.qp = P.qp;
-                prog += u.rows[p];
-                ipl.push_back(d);
-                db.push_back({rec[p], u.pw[p], u.ph[p], P.qp});
+DecEngine *engine_acquire(const std::vector<std::pair<int, int>> &sizes) {
+    const int device = fdvb_device_setting(), border = reference_border();
+    {
+        std::lock_guard<std::mutex> lk(g_dcache_mu);
+        for (size_t i = 0; i < g_dcache->size(); ++i) {
+            DecEngine *E = (*g_dcache)[i];
+            if (E->device == device && E->border == border && E->sizes == sizes) {
+                g_dcache->erase(g_dcache->begin() + (long)i);
+                return E;
             }
-            DCK(cudaMemsetAsync(u.d_prog, 0, sizeof(int) * prog, E.st));
         }
     }
-    // key-frame rows in (row, plane) order, so every plane's early rows start first
+    DecEngine *E = new DecEngine();
+    if (engine_init(*E, sizes, device, border)) {
+        const std::string e = g_derr;
+        delete E;
+        g_derr = e;
+        return nullptr;
+    }
+    return E;
+}
+
+void engine_release(DecEngine *E) {
+    DecEngine *evict = nullptr;
     {
-        int maxr = 0;
-        for (auto &p : ipl) maxr = std::max(maxr, p.rows);
-        for (int r = 0; r < maxr; ++r)
-            for (int p = 0; p < (int)ipl.size(); ++p)
-                if (r < ipl[p].rows) tasks.push_back({p, r});
+        std::lock_guard<std::mutex> lk(g_dcache_mu);
+        g_dcache->push_back(E);
+        if (g_dcache->size() > kCacheMax) {
+            evict = g_dcache->front();
+            g_dcache->erase(g_dcache->begin());
+        }
     }
-    DCK(cudaMemsetAsync(E.d_err, 0, sizeof(unsigned), E.st));
-    if (!pu.empty()) {
-        if (up(E.d_pu, pu.data(), pu.size() * sizeof(dk::PUnit)) || up(E.d_uoff, uoff.data(), uoff.size() * 4))
-            return -1;
-        dk::pdec_inter_kernel<<<uoff.back(), 64, 0, E.st>>>(E.d_pu, E.d_uoff, (int)pu.size());
-        dk::pdec_intra_kernel<<<(int)pu.size(), 64, 0, E.st>>>(E.d_pu);
-    }
-    if (!tasks.empty()) {
-        if (up(E.d_planes, ipl.data(), ipl.size() * sizeof(dk::IPlaneD)) ||
-            up(E.d_tasks, tasks.data(), tasks.size() * sizeof(dk::ITask)))
-            return -1;
-        DCK(cudaMemsetAsync(E.d_ticket, 0, sizeof(int), E.st));
-        dk::idec_kernel<<<std::min((int)tasks.size(), E.nsm), dk::kINT, 0, E.st>>>(
-            E.d_planes, E.d_tasks, (int)tasks.size(), E.d_ticket, E.d_err, 4000000000ull);
-    }
-    DCK(cudaGetLastError());
-    if (up(E.d_db, db.data(), db.size() * sizeof(DbTaskD))) return -1;
-    launch_deblock(E.d_db, (int)db.size(), E.st);
-    // download, and the decoded frame becomes the nearest reference (load_ref, fdv.h:5183)
-    std::vector<uint8_t *> hostbuf(nu);
-    for (int i = 0; i < nu; ++i) {
-        DUnit &u = E.units[i];
-        const size_t fs = (size_t)u.w * u.h * 3 / 2, a = (fs + 255) / 256 * 256;
-        if (sp + a > send) { g_derr = "staging buffer too small"; return -1; }
-        hostbuf[i] = sp;
-        sp += a;
-        DCK(cudaMemcpyAsync(hostbuf[i], u.rec, fs, cudaMemcpyDeviceToHost, E.st));
-        RefBuf &far = u.ref[1 - u.near_i];
-        uint8_t *rec[3] = {u.rec, u.rec + (size_t)u.w * u.h, u.rec + (size_t)u.w * u.h + (size_t)u.cw * u.ch};
-        prep.push_back({{rec[0], rec[1], rec[2]}, far.G, far.B, far.H, far.J, far.U, far.V, u.w, u.h, far.rp.ys,
-                        far.rp.cs, E.border + 16});
-    }
-    int maxw = 0, maxh = 0;
-    for (auto &u : E.units) { maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h); }
-    if (up(E.d_prep, prep.data(), prep.size() * sizeof(PrepTaskD))) return -1;
-    launch_refprep(E.d_prep, (int)prep.size(), maxw, maxh, E.border + 16, E.st);
-    DCK(cudaGetLastError());
-    unsigned herr = 0;
-    DCK(cudaMemcpyAsync(&herr, E.d_err, sizeof herr, cudaMemcpyDeviceToHost, E.st));
-    DCK(cudaStreamSynchronize(E.st));
-    if (herr) { g_derr = "key-frame wavefront wait timed out"; return -1; }
-    for (int i = 0; i < nu; ++i) {
-        DUnit &u = E.units[i];
-        const uint8_t *s = hostbuf[i];
-        for (int y = 0; y < u.h; ++y) memcpy(outY[i] + (size_t)y * ostride, s + (size_t)y * u.w, u.w);
-        s += (size_t)u.w * u.h;
-        for (int y = 0; y < u.ch; ++y) memcpy(outU[i] + (size_t)y * (ostride / 2), s + (size_t)y * u.cw, u.cw);
-        s += (size_t)u.cw * u.ch;
-        for (int y = 0; y < u.ch; ++y) memcpy(outV[i] + (size_t)y * (ostride / 2), s + (size_t)y * u.cw, u.cw);
-        u.near_i = 1 - u.near_i;
-        u.nref = u.intra ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
-    }
-    return 0;
+    delete evict;
 }
 
 struct Stream {   // one fdv_video_encode container
@@ -732,31 +661,280 @@ bool next_blob(Stream &s, const uint8_t **b, size_t *n) {
     return true;
 }
 
+// Parse one blob of unit u and pack it into slot S.  0, or -1 for a
+// malformed blob.
+int parse_pack(DUnit &u, const uint8_t *blob, size_t blen, int intra, int border, PSlot &S) {
+    size_t off = 0;
+    bool room = true;
+    auto put = [&](const void *src, size_t n) -> size_t {
+        const size_t at = off;
+        if (off + n > u.pay_cap) { room = false; return 0; }
+        if (n) memcpy(S.pin + off, src, n);
+        off = al256(off + n);
+        return at;
+    };
+    S.intra = intra;
+    if (intra) {
+        memset(&u.tc, 0, sizeof u.tc);   // tables and history restart at a key frame
+        size_t p = 0;
+        for (int pl = 0; pl < 3; ++pl) {
+            if (p + 4 > blen) return -1;
+            uint32_t n = 0;
+            for (int k = 0; k < 4; ++k) n |= (uint32_t)blob[p + k] << (8 * k);
+            p += 4;
+            if (p + n > blen || n < 4) return -1;
+            dec::IPlane &P = u.ip[pl];
+            if (dec::parse_iplane(blob + p, n, u.pw[pl], u.ph[pl], P)) return -1;
+            p += n;
+            S.o_leaves[pl] = put(P.leaves.data(), P.leaves.size() * sizeof(dec::Leaf));
+            S.o_ctu[pl] = put(P.ctu_first.data(), P.ctu_first.size() * 4);
+            S.o_icoef[pl] = put(P.coef.data(), P.coef.size() * 2);
+            S.o_flags[pl] = put(P.flags.data(), P.flags.size());
+            S.pqp[pl] = P.qp;
+        }
+    } else {
+        dec::PFrame &f = u.pf;
+        if (dec::parse_pframe(blob, blen, u.w, u.h, border, &u.tc, f)) return -1;
+        S.qp = f.qp;
+        S.nintra = (int)f.intra.size();
+        S.o_mbs = put(f.mbs.data(), f.mbs.size() * sizeof(dec::PMB));
+        S.o_coef = put(f.coef.data(), f.coef.size() * 2);
+        S.o_intra = put(f.intra.data(), f.intra.size() * 4);
+    }
+    S.used = off;
+    return room ? 0 : -1;
+}
+
+// Progress shared by the pipeline's threads.
+struct Pipe {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<int> parsed;   // units parsed, per frame
+    std::vector<char> copied;  // frame scattered into the output
+    int submitted = 0;         // frames whose GPU work is enqueued
+    bool abort = false;
+    std::string err;
+    void fail(const std::string &e) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!abort) err = e;
+            abort = true;
+        }
+        cv.notify_all();
+    }
+    template <class P>
+    bool wait(P pred) {   // false when the pipeline was aborted
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return abort || pred(); });
+        return !abort;
+    }
+};
+
 // Decode one stream per band (band b at rows y0[b]) into full W x H frames.
-int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int H, int nf, uint8_t *out) {
+int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int H, int nf, uint8_t *out,
+                 int nthreads) {
     std::vector<std::pair<int, int>> sizes;
     for (auto &s : bs) sizes.push_back({s.w, s.h});
-    DecEngine E;
-    if (engine_init(E, sizes)) return -1;
+    DecEngine *Ep = engine_acquire(sizes);
+    if (!Ep) return -1;
+    DecEngine &E = *Ep;
+    DCK(cudaSetDevice(E.device));
     const int nu = (int)bs.size(), cw = W / 2, ch = H / 2;
     const size_t fsize = (size_t)W * H + 2 * (size_t)cw * ch;
-    std::vector<uint8_t *> oy(nu), ou(nu), ov(nu);
-    for (int f = 0; f < nf; ++f) {
-        uint8_t *fy = out + (size_t)f * fsize, *fu = fy + (size_t)W * H, *fv = fu + (size_t)cw * ch;
+    for (auto &u : E.units) { u.near_i = 0; u.nref = 0; }
+    DCK(cudaMemsetAsync(E.d_err, 0, sizeof(unsigned), E.st));
+
+    Pipe P;
+    P.parsed.assign(nf, 0);
+    P.copied.assign(nf, 0);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nwk = std::max(1, std::min({nthreads, nu, (int)hw}));
+    const int ncopy = std::max(1, std::min(4, (int)hw - nwk - 1));
+    const int border = E.border, device = E.device;
+
+    auto parse_worker = [&](int wk) {
+        cudaSetDevice(device);
+        for (int f = 0; f < nf; ++f) {
+            const int s = f % kSlots;
+            if (f >= kSlots) {   // slot s last held frame f - kSlots: its upload must be done
+                if (!P.wait([&] { return P.submitted >= f - kSlots + 1; })) return;
+                std::string e;
+                if (!ck(cudaEventSynchronize(E.ev_in[s]), "upload", e)) { P.fail(e); return; }
+            }
+            int n = 0;
+            for (int i = wk; i < nu; i += nwk, ++n) {
+                DUnit &u = E.units[i];
+                const uint8_t *blob;
+                size_t blen;
+                if (!next_blob(bs[i], &blob, &blen)) { P.fail("truncated stream"); return; }
+                const int intra = f == 0 || (bs[i].keyint > 0 && f % bs[i].keyint == 0);
+                if (parse_pack(u, blob, blen, intra, border, u.slot[s])) { P.fail("malformed frame blob"); return; }
+            }
+            {
+                std::lock_guard<std::mutex> lk(P.mu);
+                P.parsed[f] += n;
+            }
+            P.cv.notify_all();
+        }
+    };
+    auto copier = [&](int c) {
+        cudaSetDevice(device);
+        for (int f = c; f < nf; f += ncopy) {
+            if (!P.wait([&] { return P.submitted > f; })) return;
+            std::string e;
+            if (!ck(cudaEventSynchronize(E.ev_out[f % kOutSlots]), "download", e)) { P.fail(e); return; }
+            const uint8_t *src = E.out_pin[f % kOutSlots];
+            uint8_t *fy = out + (size_t)f * fsize, *fu = fy + (size_t)W * H, *fv = fu + (size_t)cw * ch;
+            for (int i = 0; i < nu; ++i) {
+                const DUnit &u = E.units[i];
+                const uint8_t *s = src + u.rec_off;
+                memcpy(fy + (size_t)y0[i] * W, s, (size_t)u.w * u.h);
+                memcpy(fu + (size_t)(y0[i] / 2) * cw, s + (size_t)u.w * u.h, (size_t)u.cw * u.ch);
+                memcpy(fv + (size_t)(y0[i] / 2) * cw, s + (size_t)u.w * u.h + (size_t)u.cw * u.ch,
+                       (size_t)u.cw * u.ch);
+            }
+            {
+                std::lock_guard<std::mutex> lk(P.mu);
+                P.copied[f] = 1;
+            }
+            P.cv.notify_all();
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 0; k < nwk; ++k) th.emplace_back(parse_worker, k);
+    for (int c = 0; c < ncopy; ++c) th.emplace_back(copier, c);
+
+    const DescLayout D(nu, E.ntask_max);
+    std::vector<dk::PUnit> pu;
+    std::vector<int> uoff;
+    std::vector<dk::IPlaneD> ipl;
+    std::vector<dk::ITask> tasks;
+    std::vector<DbTaskD> db;
+    std::vector<PrepTaskD> prep;
+    auto submit = [&](int f) -> int {
+        const int s = f % kSlots, o = f % kOutSlots;
+        pu.clear(); uoff.assign(1, 0); ipl.clear(); tasks.clear(); db.clear(); prep.clear();
         for (int i = 0; i < nu; ++i) {
             DUnit &u = E.units[i];
-            if (!next_blob(bs[i], &u.blob, &u.blen)) { g_derr = "truncated stream"; return -1; }
-            u.intra = f == 0 || (bs[i].keyint > 0 && f % bs[i].keyint == 0);
-            oy[i] = fy + (size_t)y0[i] * W;
-            ou[i] = fu + (size_t)(y0[i] / 2) * cw;
-            ov[i] = fv + (size_t)(y0[i] / 2) * cw;
+            const PSlot &S = u.slot[s];
+            DCK(cudaMemcpyAsync(u.d_pay, S.pin, S.used, cudaMemcpyHostToDevice, E.st));
+            uint8_t *rec[3] = {E.d_rec + u.rec_off, E.d_rec + u.rec_off + (size_t)u.w * u.h,
+                               E.d_rec + u.rec_off + (size_t)u.w * u.h + (size_t)u.cw * u.ch};
+            if (!S.intra) {
+                dk::PUnit d{};
+                d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh; d.qp = S.qp;
+                for (int p = 0; p < 3; ++p) d.rec[p] = rec[p];
+                d.ref[0] = u.ref[u.near_i].rp;
+                d.ref[1] = u.nref >= 2 ? u.ref[1 - u.near_i].rp : u.ref[u.near_i].rp;
+                d.mbs = reinterpret_cast<const dec::PMB *>(u.d_pay + S.o_mbs);
+                d.coef = reinterpret_cast<const int16_t *>(u.d_pay + S.o_coef);
+                d.intra = reinterpret_cast<const int32_t *>(u.d_pay + S.o_intra);
+                d.nintra = S.nintra;
+                pu.push_back(d);
+                uoff.push_back(uoff.back() + u.mbw * u.mbh);
+                for (int p = 0; p < 3; ++p) db.push_back({rec[p], u.pw[p], u.ph[p], S.qp});
+            } else {
+                int prog = 0;
+                for (int p = 0; p < 3; ++p) {
+                    dk::IPlaneD d{};
+                    d.rec = rec[p]; d.w = u.pw[p]; d.h = u.ph[p]; d.cols = u.cols[p]; d.rows = u.rows[p];
+                    d.leaves = reinterpret_cast<const dec::Leaf *>(u.d_pay + S.o_leaves[p]);
+                    d.ctu_first = reinterpret_cast<const int32_t *>(u.d_pay + S.o_ctu[p]);
+                    d.coef = reinterpret_cast<const int16_t *>(u.d_pay + S.o_icoef[p]);
+                    d.flags = u.d_pay + S.o_flags[p];
+                    d.progress = u.d_prog + prog;
+                    d.qp = S.pqp[p];
+                    prog += u.rows[p];
+                    ipl.push_back(d);
+                    db.push_back({rec[p], u.pw[p], u.ph[p], S.pqp[p]});
+                }
+                DCK(cudaMemsetAsync(u.d_prog, 0, sizeof(int) * prog, E.st));
+            }
+            RefBuf &far = u.ref[1 - u.near_i];
+            prep.push_back({{rec[0], rec[1], rec[2]}, far.G, far.B, far.H, far.J, far.U, far.V, u.w, u.h, far.rp.ys,
+                            far.rp.cs, border + 16});
         }
-        if (engine_frame(E, oy.data(), ou.data(), ov.data(), W)) return -1;
+        // key-frame rows in (row, plane) order, so every plane's early rows start first
+        int maxr = 0;
+        for (auto &p : ipl) maxr = std::max(maxr, p.rows);
+        for (int r = 0; r < maxr; ++r)
+            for (int p = 0; p < (int)ipl.size(); ++p)
+                if (r < ipl[p].rows) tasks.push_back({p, r});
+        uint8_t *h = E.desc_pin[o];
+        memcpy(h + D.pu, pu.data(), pu.size() * sizeof(dk::PUnit));
+        memcpy(h + D.uoff, uoff.data(), uoff.size() * sizeof(int));
+        memcpy(h + D.planes, ipl.data(), ipl.size() * sizeof(dk::IPlaneD));
+        memcpy(h + D.tasks, tasks.data(), tasks.size() * sizeof(dk::ITask));
+        memcpy(h + D.db, db.data(), db.size() * sizeof(DbTaskD));
+        memcpy(h + D.prep, prep.data(), prep.size() * sizeof(PrepTaskD));
+        DCK(cudaMemcpyAsync(E.d_desc, h, D.total, cudaMemcpyHostToDevice, E.st));
+        DCK(cudaEventRecord(E.ev_in[s], E.st));
+        const auto *d_pu = reinterpret_cast<const dk::PUnit *>(E.d_desc + D.pu);
+        if (!pu.empty()) {
+            dk::pdec_inter_kernel<<<uoff.back(), 64, 0, E.st>>>(d_pu, reinterpret_cast<const int *>(E.d_desc + D.uoff),
+                                                                 (int)pu.size());
+            int nintra = 0;
+            for (auto &d : pu) nintra += d.nintra;
+            if (nintra) dk::pdec_intra_kernel<<<(int)pu.size(), 64, 0, E.st>>>(d_pu);
+        }
+        if (!tasks.empty()) {
+            DCK(cudaMemsetAsync(E.d_ticket, 0, sizeof(int), E.st));
+            dk::idec_kernel<<<std::min((int)tasks.size(), E.nsm), dk::kINT, 0, E.st>>>(
+                reinterpret_cast<const dk::IPlaneD *>(E.d_desc + D.planes),
+                reinterpret_cast<const dk::ITask *>(E.d_desc + D.tasks), (int)tasks.size(), E.d_ticket, E.d_err,
+                4000000000ull);
+        }
+        DCK(cudaGetLastError());
+        launch_deblock(E.d_desc + D.db, (int)db.size(), E.st);
+        DCK(cudaMemcpyAsync(E.out_pin[o], E.d_rec, E.rec_bytes, cudaMemcpyDeviceToHost, E.st));
+        // the decoded frame becomes the nearest reference (load_ref, fdv.h:5183)
+        int maxw = 0, maxh = 0;
+        for (auto &u : E.units) { maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h); }
+        launch_refprep(E.d_desc + D.prep, (int)prep.size(), maxw, maxh, border + 16, E.st);
+        DCK(cudaGetLastError());
+        DCK(cudaEventRecord(E.ev_out[o], E.st));
+        for (int i = 0; i < nu; ++i) {
+            DUnit &u = E.units[i];
+            u.near_i = 1 - u.near_i;
+            u.nref = u.slot[s].intra ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+        }
+        return 0;
+    };
+    for (int f = 0; f < nf; ++f) {
+        if (!P.wait([&] { return P.parsed[f] == nu && (f < kOutSlots || P.copied[f - kOutSlots]); })) break;
+        if (submit(f)) { P.fail(g_derr); break; }
+        {
+            std::lock_guard<std::mutex> lk(P.mu);
+            P.submitted = f + 1;
+        }
+        P.cv.notify_all();
     }
+    for (auto &t : th) t.join();
+    unsigned herr = 0;
+    std::string e;
+    const bool ok = ck(cudaMemcpyAsync(&herr, E.d_err, sizeof herr, cudaMemcpyDeviceToHost, E.st), "error word", e) &&
+                    ck(cudaStreamSynchronize(E.st), "decode", e);
+    if (!ok) {   // the context may be unusable: drop the engine
+        delete Ep;
+        g_derr = e;
+        return -1;
+    }
+    engine_release(Ep);
+    if (P.abort) { g_derr = P.err; return -1; }
+    if (herr) { g_derr = "key-frame wavefront wait timed out"; return -1; }
     return 0;
 }
 
 }  // namespace
+
+void fdvd_release_cached(void) {
+    std::vector<DecEngine *> v;
+    {
+        std::lock_guard<std::mutex> lk(g_dcache_mu);
+        v.swap(*g_dcache);
+    }
+    for (DecEngine *E : v) delete E;
+}
 
 extern "C" {
 
@@ -767,7 +945,7 @@ int fdv_video_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, 
     Stream s;
     if (!out || !open_stream(in, len, s)) { g_derr = "bad stream header"; return -1; }
     std::vector<Stream> bs{s};
-    if (decode_bands(bs, {0}, s.w, s.h, s.nf, out)) return -1;
+    if (decode_bands(bs, {0}, s.w, s.h, s.nf, out, 1)) return -1;
     if (nframes) *nframes = s.nf;
     if (w) *w = s.w;
     if (h) *h = s.h;
@@ -775,7 +953,6 @@ int fdv_video_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, 
 }
 
 int fdv_vtile_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, int *w, int *h, int nthreads) {
-    (void)nthreads;   // the bands are reconstructed together on the GPU, parsed on a host thread each
     g_derr.clear();
     if (!in || !out || len < 12) { g_derr = "bad stream header"; return -1; }
     size_t p = 0;
@@ -805,7 +982,7 @@ int fdv_vtile_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, 
         }
         p += n;
     }
-    if (decode_bands(bs, y0, W, H, nf, out)) return -1;
+    if (decode_bands(bs, y0, W, H, nf, out, nthreads)) return -1;
     if (nframes) *nframes = nf;
     if (w) *w = W;
     if (h) *h = H;

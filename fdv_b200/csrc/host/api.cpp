@@ -286,6 +286,7 @@ extern "C" {
 const char *fdvb_last_error(void) { return g_api_err.c_str(); }
 
 void fdvb_release_engines(void) {
+    fdvd_release_cached();
     std::vector<CachedEngine> v;
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -302,6 +303,9 @@ int fdvb_set_search_range(int range) {
     return old;
 }
 int fdvb_get_search_range(void) { return g_range; }
+}  // extern "C"
+int fdvb_device_setting(void) { return g_device; }
+extern "C" {
 int fdvb_set_device(int device) {
     if (device < 0) return -1;
     int old = g_device;

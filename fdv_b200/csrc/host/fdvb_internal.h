@@ -71,3 +71,8 @@ extern "C" double fdvb_rc_lfrac(void);
 // The 8x8 DCT basis and quantiser steps (fdv.h:2597-2612), computed on the
 // host with the same libm calls and uploaded to the device.
 void fdvb_c8_tables(int32_t c8[64], int32_t qstep8[52]);
+
+// The CUDA device the library's engines open on (fdvb_set_device).
+int fdvb_device_setting(void);
+// Frees the decoders' cached engines (part of fdvb_release_engines).
+void fdvd_release_cached(void);

@@ -123,9 +123,10 @@ int fdvb_get_search_range(void);
 int fdvb_set_device(int device);
 /* Description of the last failure on the calling thread. */
 const char *fdvb_last_error(void);
-/* fdv_video_encode and fdv_vtile_encode keep up to four GPU engines (device
- * and pinned memory for one frame geometry) between calls so that repeated
- * calls skip the set-up; this frees them.  No counterpart in the reference. */
+/* fdv_video_encode and fdv_vtile_encode, and the two decoders, each keep up to
+ * four GPU engines (device and pinned memory for one frame geometry) between
+ * calls so that repeated calls skip the set-up; this frees them.  No
+ * counterpart in the reference. */
 void fdvb_release_engines(void);
 
 /* -------------------------------------------- the inner engine ABI -- */

@@ -201,13 +201,14 @@ def ref_video_decode(stream: bytes, search_range: int = 16) -> np.ndarray:
     return out.reshape(nf, -1)
 
 
-def ref_vtile_decode(stream: bytes, search_range: int = 16) -> np.ndarray:
+def ref_vtile_decode(stream: bytes, search_range: int = 16, nthreads: int = 1) -> np.ndarray:
+    """Decoded frames of a tiled stream, by the reference's fdv_vtile_decode on nthreads threads."""
     L = ref(search_range)
     w, h, nf = struct.unpack_from("<HHH", stream, 0)
     buf = np.frombuffer(stream, np.uint8).copy()
     out = np.empty(nf * w * h * 3 // 2, np.uint8)
     a, b, c = C.c_int(), C.c_int(), C.c_int()
-    if L.fdv_vtile_decode(_ptr(buf), len(stream), _ptr(out), C.byref(a), C.byref(b), C.byref(c), 1) != 0:
+    if L.fdv_vtile_decode(_ptr(buf), len(stream), _ptr(out), C.byref(a), C.byref(b), C.byref(c), nthreads) != 0:
         raise RuntimeError("reference tiled decode failed")
     return out.reshape(nf, -1)
 
