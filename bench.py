@@ -26,6 +26,13 @@ One step = encoding all 120 frames.
   included), the P-frame analysis speed-up, and the BD-rate / PSNR of the
   learned form against the plain form over QP 18/23/28/32 (20 frames).
 
+* ``decode``: the GPU decoder (``fdv_vtile_decode`` through the C ABI: the
+  coded stream in host memory, the decoded frames into a host buffer) on the
+  workload's own coded stream, against the reference's ``fdv_vtile_decode`` on
+  every host core writing into the same buffer; the frames must be identical.
+  Its roofline is the P-frame reconstruction kernel's, timed by the decoder's
+  own CUDA events.  ``--workload decode`` runs this leg alone.
+
 ``--impl reference`` times that reference encoder alone (rank 0).
 Under torchrun each rank encodes its own stream (weak scaling, no collective on
 the data path); timings are reduced with MAX over ranks.
@@ -352,6 +359,81 @@ def run_reference(args) -> None:
 LEARN_NF, LEARN_QP, LEARN_CONF = 60, 23, 0.8
 
 
+# --------------------------------------------------------------- decode --
+DECODE_METRIC = "720p decode Mpix/s on 1 B200 (fdv_vtile_decode, bit-exact)"
+
+
+def run_decode(stream: bytes, steps: int, warmup: int, ref_range: int = RANGE) -> dict:
+    """The GPU decoder on `stream` (the workload's tiled stream) against the
+    reference decoder on every host core, both through fdv_vtile_decode into
+    one pre-faulted host buffer."""
+    import fdv_b200 as F
+    import oracle as O
+    L = F.lib()
+    u8p = F.u8p
+    w, h, nf = (int(x) for x in np.frombuffer(stream[:6], "<u2"))
+    fs = w * h * 3 // 2
+    src = np.frombuffer(stream, np.uint8)
+    out = np.ones(nf * fs, np.uint8)   # touched once: page faults stay out of both timings
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    ncpu = os.cpu_count() or 1
+
+    def dec(lib):
+        if lib.fdv_vtile_decode(src.ctypes.data_as(u8p), len(stream), out.ctypes.data_as(u8p), C.byref(a),
+                                C.byref(b), C.byref(c), ncpu) != 0:
+            raise RuntimeError("decode failed")
+
+    for _ in range(max(1, warmup)):
+        dec(L)
+    L.fdvd_timing(1)
+    F.decode_stats(reset=True)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dec(L)
+    dt = (time.perf_counter() - t0) / steps
+    L.fdvd_timing(0)
+    st = F.decode_stats(reset=True)
+    ours = out.copy()
+    mpix = nf * w * h / 1e6
+    res = {"metric": DECODE_METRIC, "value": round(mpix / dt, 3), "unit": "Mpix/s", "ms_per_step": round(dt * 1e3, 3),
+           "steps": steps, "frames_per_step": int(nf), "host_threads": ncpu,
+           "h2d_bytes_per_step": len(stream), "d2h_bytes_per_step": int(nf * fs),
+           "kernels": {k: {"launches_per_step": v[1] // max(1, steps),
+                           "avg_launch_ms": round(v[0] / v[1], 4) if v[1] else None}
+                       for k, v in st.items()}}
+    # roofline: P-frame reconstruction, all bands in one launch; algorithmic
+    # bytes = the reference samples read and the reconstruction written (one
+    # byte each per I420 sample) plus the 32-byte macroblock records
+    ni, ti = st["inter"][1], st["inter"][0]
+    if ni:
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except OSError:
+            pass
+        peak = peaks.get("hbm_gbs") or 6650.0
+        alg = 2 * fs + 32 * (w // 16) * (h // 16)
+        ach = alg / (ti / ni / 1e3) / 1e9
+        res["roofline"] = {"bound": "hbm", "kernel": "pdec_inter_kernel", "achieved": round(ach, 3), "peak": peak,
+                           "unit": "GB/s", "frac": round(ach / peak, 6), "algorithmic_bytes_per_launch": alg,
+                           "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                           "note": "one frame per launch (the next frame predicts from it): latency-bound"}
+    if O.have_ref(ref_range):
+        R = O.ref(ref_range)
+        dec(R)
+        same = bool(np.array_equal(out, ours))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            dec(R)
+        rt = (time.perf_counter() - t0) / steps
+        res["reference"] = {"value": round(mpix / rt, 3), "unit": "Mpix/s", "cores": ncpu, "kind": "reference",
+                            "sample": f"the same {nf}-frame stream, the reference's fdv_vtile_decode on {ncpu} "
+                                      f"threads (oracle/_ref), mean of {steps}"}
+        res["identical_to_reference"] = same
+    return res
+
+
 def run_learned(local: int) -> dict:
     """The learned-proposal form against the plain form on the learned workload."""
     import torch
@@ -426,8 +508,10 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the C-ABI end-to-end leg (profiling runs)")
     ap.add_argument("--frames", type=int, default=NF, help="frames per step (profiling runs use a few)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
-    ap.add_argument("--workload", default="hd720", choices=["hd720", "batch48"],
-                    help="batch48: the 48-stream batched workload (timed steps = P-frame steps)")
+    ap.add_argument("--no-decode", action="store_true", help="skip the decoder leg")
+    ap.add_argument("--workload", default="hd720", choices=["hd720", "batch48", "decode"],
+                    help="batch48: the 48-stream batched workload (timed steps = P-frame steps); "
+                         "decode: the decoder leg alone")
     args = ap.parse_args()
     if args.workload == "batch48":
         if args.impl == "reference":
@@ -439,6 +523,19 @@ def main() -> None:
     NF = max(1, min(args.frames, 120))
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "decode":
+        import fdv_b200 as F
+        import oracle as O
+        F.set_search_range(RANGE)
+        fr = render(1)[:NF]
+        if O.have_ref(RANGE):   # the same bytes as ours; keeps the process's GPU launches the decoder's alone
+            stream = O.ref_vtile_encode(fr, W, H, QP, KEYINT, BAND_MBROWS, os.cpu_count() or 1, RANGE)
+        else:
+            stream = F.vtile_encode(fr, W, H, QP, KEYINT, BAND_MBROWS, os.cpu_count() or 1)
+        r = run_decode(stream, args.steps, args.warmup)
+        r["config"] = {"workload": "decode of " + (WORKLOAD if NF == 120 else WORKLOAD + f" (first {NF} frames)")}
+        print(json.dumps(r))
         return
 
     rank = int(os.environ.get("RANK", "0"))
@@ -583,6 +680,12 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_learned:
         learned = run_learned(local)
 
+    decode = None
+    if rank == 0 and world == 1 and not args.no_decode:
+        if args.no_e2e:
+            n = L.fdv_vtile_encode(arr, NF, W, H, QP, KEYINT, BAND_MBROWS, nthreads, out.ctypes.data_as(u8p), cap)
+        decode = run_decode(out[:n].tobytes(), max(3, args.steps), 2)
+
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": round(value, 3), "unit": "Mpix/s", "n_gpus": world,
@@ -607,6 +710,7 @@ def main() -> None:
             "gpu_launches": int(launches),
             "clocks": clocks,
             "learned": learned,
+            "decode": decode,
         }))
     g.close()
     if dist is not None:

@@ -101,6 +101,10 @@ def lib() -> C.CDLL:
         L.fdv_video_decode.argtypes = [u8p, sz, u8p, ip, ip, ip]
         L.fdv_vtile_decode.argtypes = [u8p, sz, u8p, ip, ip, ip, i]
         L.fdvd_last_error.restype = C.c_char_p
+        L.fdvd_timing.argtypes = [i]
+        L.fdvd_timing.restype = None
+        L.fdvd_stats.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_longlong), i]
+        L.fdvd_stats.restype = None
         _lib = L
     return _lib
 
@@ -196,6 +200,15 @@ def vtile_decode(stream: bytes, nthreads: int = 8) -> np.ndarray:
         raise FdvError("bad stream header")
     w, h, nf = np.frombuffer(stream[:6], "<u2")
     return _decode(lib().fdv_vtile_decode, stream, int(nf), int(w), int(h), nthreads)
+
+
+def decode_stats(reset: bool = True) -> dict:
+    """Decoder kernel timing accumulated while fdvd_timing was on (fdvd_stats)."""
+    ms = (C.c_double * 5)()
+    n = (C.c_longlong * 5)()
+    lib().fdvd_stats(ms, n, int(reset))
+    keys = ("inter", "intra16", "key", "frame_ops", "frame")
+    return {k: (ms[j], n[j]) for j, k in enumerate(keys)}
 
 
 class Encoder:

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -456,9 +457,11 @@ struct DecEngine {
     unsigned *d_err = nullptr;
     cudaEvent_t ev_in[kSlots] = {}, ev_out[kOutSlots] = {};
     int ntask_max = 0;
+    std::vector<cudaEvent_t> tev;   // timing events (fdvd_timing), reused between calls
     ~DecEngine() {
         cudaSetDevice(device);
         if (st) cudaStreamSynchronize(st);
+        for (auto e : tev) cudaEventDestroy(e);
         for (auto e : ev_in) if (e) cudaEventDestroy(e);
         for (auto e : ev_out) if (e) cudaEventDestroy(e);
         for (void *p : own) cudaFree(p);
@@ -591,6 +594,15 @@ int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes, int
         if (!(E.out_pin[o] = pin(E.rec_bytes)) || !(E.desc_pin[o] = pin(D.total))) return fail_alloc();
     return 0;
 }
+
+// Kernel timing (fdvd_timing / fdvd_stats): kinds 0 P-frame inter
+// reconstruction, 1 INTRA16 reconstruction, 2 key-frame reconstruction,
+// 3 deblocking + reference preparation, 4 the whole frame step on the GPU.
+constexpr int kTimeKinds = 5;
+std::atomic<int> g_dtiming{0};
+std::mutex g_dstat_mu;
+double g_dms[kTimeKinds];
+long long g_dn[kTimeKinds];
 
 // Engines kept between calls, keyed by device, border and unit sizes; taken
 // out while in use.
@@ -805,6 +817,25 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     for (int c = 0; c < ncopy; ++c) th.emplace_back(copier, c);
 
     const DescLayout D(nu, E.ntask_max);
+    const bool timing = g_dtiming.load() != 0;
+    struct TMark { int kind, a, b; };
+    std::vector<TMark> marks;
+    int nev = 0;
+    auto tev = [&]() -> int {   // record the next timing event on the stream
+        if (nev == (int)E.tev.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            E.tev.push_back(e);
+        }
+        if (cudaEventRecord(E.tev[nev], E.st) != cudaSuccess) return -1;
+        return nev++;
+    };
+    auto mark = [&](int kind, int a) {
+        if (a >= 0) {
+            const int b = tev();
+            if (b >= 0) marks.push_back({kind, a, b});
+        }
+    };
     std::vector<dk::PUnit> pu;
     std::vector<int> uoff;
     std::vector<dk::IPlaneD> ipl;
@@ -813,6 +844,7 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     std::vector<PrepTaskD> prep;
     auto submit = [&](int f) -> int {
         const int s = f % kSlots, o = f % kOutSlots;
+        const int t_frame = timing ? tev() : -1;
         pu.clear(); uoff.assign(1, 0); ipl.clear(); tasks.clear(); db.clear(); prep.clear();
         for (int i = 0; i < nu; ++i) {
             DUnit &u = E.units[i];
@@ -871,20 +903,29 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
         DCK(cudaEventRecord(E.ev_in[s], E.st));
         const auto *d_pu = reinterpret_cast<const dk::PUnit *>(E.d_desc + D.pu);
         if (!pu.empty()) {
+            int t0 = timing ? tev() : -1;
             dk::pdec_inter_kernel<<<uoff.back(), 64, 0, E.st>>>(d_pu, reinterpret_cast<const int *>(E.d_desc + D.uoff),
                                                                  (int)pu.size());
+            mark(0, t0);
             int nintra = 0;
             for (auto &d : pu) nintra += d.nintra;
-            if (nintra) dk::pdec_intra_kernel<<<(int)pu.size(), 64, 0, E.st>>>(d_pu);
+            if (nintra) {
+                t0 = timing ? tev() : -1;
+                dk::pdec_intra_kernel<<<(int)pu.size(), 64, 0, E.st>>>(d_pu);
+                mark(1, t0);
+            }
         }
         if (!tasks.empty()) {
             DCK(cudaMemsetAsync(E.d_ticket, 0, sizeof(int), E.st));
+            const int t0 = timing ? tev() : -1;
             dk::idec_kernel<<<std::min((int)tasks.size(), E.nsm), dk::kINT, 0, E.st>>>(
                 reinterpret_cast<const dk::IPlaneD *>(E.d_desc + D.planes),
                 reinterpret_cast<const dk::ITask *>(E.d_desc + D.tasks), (int)tasks.size(), E.d_ticket, E.d_err,
                 4000000000ull);
+            mark(2, t0);
         }
         DCK(cudaGetLastError());
+        const int t_ops = timing ? tev() : -1;
         launch_deblock(E.d_desc + D.db, (int)db.size(), E.st);
         DCK(cudaMemcpyAsync(E.out_pin[o], E.d_rec, E.rec_bytes, cudaMemcpyDeviceToHost, E.st));
         // the decoded frame becomes the nearest reference (load_ref, fdv.h:5183)
@@ -892,6 +933,8 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
         for (auto &u : E.units) { maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h); }
         launch_refprep(E.d_desc + D.prep, (int)prep.size(), maxw, maxh, border + 16, E.st);
         DCK(cudaGetLastError());
+        mark(3, t_ops);   // includes the download between the two
+        mark(4, t_frame);
         DCK(cudaEventRecord(E.ev_out[o], E.st));
         for (int i = 0; i < nu; ++i) {
             DUnit &u = E.units[i];
@@ -919,6 +962,16 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
         g_derr = e;
         return -1;
     }
+    if (timing && !P.abort) {
+        double ms[kTimeKinds] = {};
+        long long n[kTimeKinds] = {};
+        for (auto &m : marks) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, E.tev[m.a], E.tev[m.b]) == cudaSuccess) { ms[m.kind] += t; ++n[m.kind]; }
+        }
+        std::lock_guard<std::mutex> lk(g_dstat_mu);
+        for (int k = 0; k < kTimeKinds; ++k) { g_dms[k] += ms[k]; g_dn[k] += n[k]; }
+    }
     engine_release(Ep);
     if (P.abort) { g_derr = P.err; return -1; }
     if (herr) { g_derr = "key-frame wavefront wait timed out"; return -1; }
@@ -939,6 +992,17 @@ void fdvd_release_cached(void) {
 extern "C" {
 
 const char *fdvd_last_error(void) { return g_derr.c_str(); }
+
+void fdvd_timing(int on) { g_dtiming.store(on ? 1 : 0); }
+
+void fdvd_stats(double *ms, long long *n, int reset) {
+    std::lock_guard<std::mutex> lk(g_dstat_mu);
+    for (int k = 0; k < kTimeKinds; ++k) {
+        if (ms) ms[k] = g_dms[k];
+        if (n) n[k] = g_dn[k];
+        if (reset) { g_dms[k] = 0; g_dn[k] = 0; }
+    }
+}
 
 int fdv_video_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, int *w, int *h) {
     g_derr.clear();

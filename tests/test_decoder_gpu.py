@@ -160,3 +160,24 @@ def test_corrupted_blobs_match_reference_verdict(built):
                 F.video_decode(b)
         else:
             assert np.array_equal(F.video_decode(b), ref), pos
+
+
+def test_decoder_timing_counts_launches(built):
+    """fdvd_timing brackets every launch: one inter launch per P-frame step,
+    one key-frame launch per key step, one frame step per frame."""
+    import fdv_b200 as F
+    w, h = 128, 96
+    fr = F.Scene(w, h, 7, nrects=4, pan_qx=5, seed=3).frames(7)
+    s = F.vtile_encode(fr, w, h, 24, 3, 2, 4)
+    L = F.lib()
+    F.decode_stats(reset=True)
+    L.fdvd_timing(1)
+    try:
+        F.vtile_decode(s)
+    finally:
+        L.fdvd_timing(0)
+    st = F.decode_stats(reset=True)
+    assert st["frame"][1] == 7 and st["key"][1] == 3 and st["inter"][1] == 4 and st["frame_ops"][1] == 7
+    assert all(v[0] > 0 for k, v in st.items() if v[1])
+    F.vtile_decode(s)
+    assert F.decode_stats()["frame"][1] == 0
