@@ -400,7 +400,8 @@ def run_decode(stream: bytes, steps: int, warmup: int, ref_range: int = RANGE) -
            "h2d_bytes_per_step": len(stream), "d2h_bytes_per_step": int(nf * fs),
            "kernels": {k: {"launches_per_step": v[1] // max(1, steps),
                            "avg_launch_ms": round(v[0] / v[1], 4) if v[1] else None}
-                       for k, v in st.items()}}
+                       for k, v in st.items() if not k.startswith("host_")},
+           "host_ms_per_step": {k[5:]: round(v[0] / max(1, steps), 3) for k, v in st.items() if k.startswith("host_")}}
     # roofline: P-frame reconstruction, all bands in one launch; algorithmic
     # bytes = the reference samples read and the reconstruction written (one
     # byte each per I420 sample) plus the 32-byte macroblock records

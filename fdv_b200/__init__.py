@@ -204,10 +204,11 @@ def vtile_decode(stream: bytes, nthreads: int = 8) -> np.ndarray:
 
 def decode_stats(reset: bool = True) -> dict:
     """Decoder kernel timing accumulated while fdvd_timing was on (fdvd_stats)."""
-    ms = (C.c_double * 5)()
-    n = (C.c_longlong * 5)()
+    ms = (C.c_double * 9)()
+    n = (C.c_longlong * 9)()
     lib().fdvd_stats(ms, n, int(reset))
-    keys = ("inter", "intra16", "key", "frame_ops", "frame")
+    keys = ("inter", "intra16", "key", "frame_ops", "frame", "host_symbols", "host_scatter", "host_submit_wait",
+            "host_records")
     return {k: (ms[j], n[j]) for j, k in enumerate(keys)}
 
 

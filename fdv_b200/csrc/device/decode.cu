@@ -22,7 +22,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
+#include <deque>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -51,6 +53,9 @@ struct PUnit {
     const int16_t *coef;
     const int32_t *intra;
     int nintra;
+    int ibase;     // first INTRA16 ticket of this unit
+    int epoch;     // this frame step's value of a finished macroblock's flag
+    int *done;     // per-macroblock flags (INTRA16 macroblocks)
 };
 
 struct IPlaneD {
@@ -183,49 +188,78 @@ __global__ void __launch_bounds__(64) pdec_inter_kernel(const PUnit *__restrict_
     }
 }
 
-// INTRA16 macroblocks of one unit, raster order (fdv.h:6624-6645).
-__global__ void __launch_bounds__(64) pdec_intra_kernel(const PUnit *__restrict__ units) {
+// INTRA16 macroblocks (fdv.h:6624-6645) of every unit.  Blocks take tickets
+// in raster order over the units' INTRA16 lists; a macroblock predicts from
+// its left, top and top-left neighbours, so it waits (bounded) only for those
+// of them that are INTRA16 themselves -- they hold earlier tickets, so they
+// are running or done.  Inter neighbours were finished by pdec_inter_kernel.
+__global__ void __launch_bounds__(64) pdec_intra_kernel(const PUnit *__restrict__ units, int nu, int total,
+                                                         int *ticket, unsigned *err, unsigned long long wait_ns) {
     __shared__ uint8_t top[16], left[16], pred[256], cpred[2][64], ctop[2][8], cleft[2][8];
     __shared__ int res[256], cres[2][64], tl, ctl[2];
     __shared__ NNPred nn[3];
     __shared__ int32_t Y[64];
     __shared__ long long B[64];
+    __shared__ int s_k, s_ok;
     const int t = threadIdx.x;
-    const PUnit &U = units[blockIdx.x];
-    const int w = U.w, cw = w / 2;
-    for (int i = 0; i < U.nintra; ++i) {
-        const int m = U.intra[i];
+    for (;;) {
+        if (t == 0) s_k = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int k = s_k;
+        if (k >= total) return;
+        int ui = 0;
+        while (ui + 1 < nu && k >= units[ui + 1].ibase) ++ui;
+        const PUnit &U = units[ui];
+        const int m = U.intra[k - U.ibase];
         const PMB mb = U.mbs[m];
-        const int bx = (m % U.mbw) * 16, by = (m / U.mbw) * 16, cbx = bx / 2, cby = by / 2;
+        const int mbx = m % U.mbw, mby = m / U.mbw;
+        const int bx = mbx * 16, by = mby * 16, cbx = bx / 2, cby = by / 2;
         const int ht = by > 0, hl = bx > 0;
+        const int w = U.w, cw = w / 2;
+        if (t == 0) {
+            bool ok = true;
+            if (hl && U.mbs[m - 1].mode == 2) ok = ok && wait_at_least(&U.done[m - 1], U.epoch, err, wait_ns);
+            if (ht && U.mbs[m - U.mbw].mode == 2) ok = ok && wait_at_least(&U.done[m - U.mbw], U.epoch, err, wait_ns);
+            if (ht && hl && U.mbs[m - U.mbw - 1].mode == 2)
+                ok = ok && wait_at_least(&U.done[m - U.mbw - 1], U.epoch, err, wait_ns);
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) continue;   // the error word is set; the frame is abandoned
+        // neighbours through L2: other blocks of this launch wrote some of them
         if (t < 16) {
-            top[t] = ht ? U.rec[0][(size_t)(by - 1) * w + bx + t] : 0;
-            left[t] = hl ? U.rec[0][(size_t)(by + t) * w + bx - 1] : 0;
+            top[t] = ht ? __ldcg(&U.rec[0][(size_t)(by - 1) * w + bx + t]) : 0;
+            left[t] = hl ? __ldcg(&U.rec[0][(size_t)(by + t) * w + bx - 1]) : 0;
         } else if (t < 32) {
-            const int k = t - 16, pl = k >> 3, q = k & 7;
-            ctop[pl][q] = ht ? U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q] : 0;
-            cleft[pl][q] = hl ? U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1] : 0;
+            const int q = t - 16, pl = q >> 3, i = q & 7;
+            ctop[pl][i] = ht ? __ldcg(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + i]) : 0;
+            cleft[pl][i] = hl ? __ldcg(&U.rec[1 + pl][(size_t)(cby + i) * cw + cbx - 1]) : 0;
         } else if (t == 32) {
-            tl = (ht && hl) ? U.rec[0][(size_t)(by - 1) * w + bx - 1] : 128;
-            for (int pl = 0; pl < 2; ++pl) ctl[pl] = (ht && hl) ? U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1] : 128;
+            tl = (ht && hl) ? __ldcg(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
+            for (int pl = 0; pl < 2; ++pl)
+                ctl[pl] = (ht && hl) ? __ldcg(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
         }
         __syncthreads();
         if (t == 0) nn[0] = nn_setup(mb.sub, top, left, tl, 16, ht, hl);
         else if (t < 3) nn[t] = nn_setup(mb.sub, ctop[t - 1], cleft[t - 1], ctl[t - 1], 8, ht, hl);
         __syncthreads();
-        for (int k = t; k < 256; k += 64) pred[k] = (uint8_t)nn_px(nn[0], top, left, k & 15, k >> 4);
-        for (int k = t; k < 128; k += 64) {
-            const int pl = k >> 6, p = k & 63;
+        for (int i = t; i < 256; i += 64) pred[i] = (uint8_t)nn_px(nn[0], top, left, i & 15, i >> 4);
+        for (int i = t; i < 128; i += 64) {
+            const int pl = i >> 6, p = i & 63;
             cpred[pl][p] = (uint8_t)nn_px(nn[1 + pl], ctop[pl], cleft[pl], p & 7, p >> 3);
         }
         mb_residual(mb, U.coef + mb.coef, U.qp, res, cres, Y, B, t, true);
-        for (int k = t; k < 256; k += 64)
-            U.rec[0][(size_t)(by + (k >> 4)) * w + bx + (k & 15)] = (uint8_t)clipb(pred[k] + res[k]);
-        for (int k = t; k < 128; k += 64) {
-            const int pl = k >> 6, p = k & 63;
+        for (int i = t; i < 256; i += 64)
+            U.rec[0][(size_t)(by + (i >> 4)) * w + bx + (i & 15)] = (uint8_t)clipb(pred[i] + res[i]);
+        for (int i = t; i < 128; i += 64) {
+            const int pl = i >> 6, p = i & 63;
             U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = (uint8_t)clipb(cpred[pl][p] + cres[pl][p]);
         }
         __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            atomicExch(&U.done[m], U.epoch);
+        }
     }
 }
 
@@ -417,6 +451,7 @@ struct RefBuf {
 // macroblocks, coefficient blocks and INTRA16 list, or per plane of a key
 // frame its leaves, CTU leaf ranges, coefficients and region flags.
 struct PSlot {
+    dec::Syms sy[3];          // entropy-decoded streams (a key frame: one per plane)
     uint8_t *pin = nullptr;   // pinned, the unit's pay_cap bytes
     size_t used = 0;
     int intra = 0, qp = 0, nintra = 0;
@@ -431,42 +466,49 @@ struct DUnit {
     RefBuf ref[2];
     int near_i = 0, nref = 0;
     fdvb_tabcache tc{};
-    uint8_t *d_pay = nullptr;     // the current frame's payload on the device
+    uint8_t *d_pay[2] = {};       // payload on the device, by frame-step parity
     size_t pay_cap = 0;
     int *d_prog = nullptr;        // key-frame CTU-row progress, three planes
+    int *d_done = nullptr;        // INTRA16 macroblocks' finished flags (frame-step epochs)
     int pw[3] = {}, ph[3] = {}, cols[3] = {}, rows[3] = {};
     PSlot slot[kSlots];
-    dec::PFrame pf;               // parse scratch, capacity kept between frames
-    dec::IPlane ip[3];
 };
 
 struct DecEngine {
     int device = 0, border = 32, nsm = 148;
     std::vector<std::pair<int, int>> sizes;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;      // reconstruction, deblocking, reference preparation
+    cudaStream_t st_in = nullptr;   // uploads
+    cudaStream_t st_out = nullptr;  // downloads
     std::vector<DUnit> units;
     std::vector<void *> own;      // device allocations
     std::vector<void *> pinned;   // host allocations
-    uint8_t *d_rec = nullptr;     // every unit's reconstruction, back to back
+    uint8_t *d_rec[2] = {};       // every unit's reconstruction, back to back, by frame-step parity
     size_t rec_bytes = 0;
     uint8_t *out_pin[kOutSlots] = {};
     uint8_t *desc_pin[kOutSlots] = {};
-    uint8_t *d_desc = nullptr;
+    uint8_t *d_desc[2] = {};      // launch descriptors, by frame-step parity
     size_t desc_cap = 0;
-    int *d_ticket = nullptr;
+    int *d_ticket = nullptr;      // [0] key-frame rows, [1] INTRA16 macroblocks
     unsigned *d_err = nullptr;
+    int epoch = 0;                // frame steps run by this engine
     cudaEvent_t ev_in[kSlots] = {}, ev_out[kOutSlots] = {};
+    // per parity b: uploads done, kernels done with the payload and
+    // descriptors, frame deblocked, frame downloaded
+    cudaEvent_t ev_up[2] = {}, ev_used[2] = {}, ev_dbk[2] = {}, ev_d2h[2] = {};
     int ntask_max = 0;
     std::vector<cudaEvent_t> tev;   // timing events (fdvd_timing), reused between calls
     ~DecEngine() {
         cudaSetDevice(device);
-        if (st) cudaStreamSynchronize(st);
+        for (auto q : {st, st_in, st_out}) if (q) cudaStreamSynchronize(q);
         for (auto e : tev) cudaEventDestroy(e);
         for (auto e : ev_in) if (e) cudaEventDestroy(e);
         for (auto e : ev_out) if (e) cudaEventDestroy(e);
+        for (int b = 0; b < 2; ++b)
+            for (auto e : {ev_up[b], ev_used[b], ev_dbk[b], ev_d2h[b]}) if (e) cudaEventDestroy(e);
         for (void *p : own) cudaFree(p);
         for (void *p : pinned) cudaFreeHost(p);
-        if (st) cudaStreamDestroy(st);
+        for (auto q : {st, st_in, st_out}) if (q) cudaStreamDestroy(q);
     }
 };
 
@@ -521,9 +563,12 @@ int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes, int
     E.sizes = sizes;
     DCK(cudaSetDevice(device));
     cudaDeviceGetAttribute(&E.nsm, cudaDevAttrMultiProcessorCount, device);
-    DCK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    for (auto q : {&E.st, &E.st_in, &E.st_out}) DCK(cudaStreamCreateWithFlags(q, cudaStreamNonBlocking));
     for (auto &e : E.ev_in) DCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : E.ev_out) DCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (int b = 0; b < 2; ++b)
+        for (auto e : {&E.ev_up[b], &E.ev_used[b], &E.ev_dbk[b], &E.ev_d2h[b]})
+            DCK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     if (upload_dec_tables()) return -1;
     const int Bp = border + 16;   // allocated border: the checked one plus the filter taps
     const int nu = (int)sizes.size();
@@ -576,29 +621,36 @@ int engine_init(DecEngine &E, const std::vector<std::pair<int, int>> &sizes, int
         }
         const size_t ppay = al256(nmb * sizeof(dec::PMB)) + al256(nmb * 384 * 2) + al256(nmb * 4);
         u.pay_cap = std::max(ppay, ipay);
-        u.d_pay = dmalloc<uint8_t>(u.pay_cap, E.own);
+        for (auto &dp : u.d_pay)
+            if (!(dp = dmalloc<uint8_t>(u.pay_cap, E.own))) return fail_alloc();
         u.d_prog = dmalloc<int>(nprog, E.own);
-        if (!u.d_pay || !u.d_prog) return fail_alloc();
+        u.d_done = dmalloc<int>(nmb, E.own);
+        if (!u.d_prog || !u.d_done) return fail_alloc();
+        DCK(cudaMemset(u.d_done, 0, nmb * sizeof(int)));
         for (auto &sl : u.slot)
             if (!(sl.pin = pin(u.pay_cap))) return fail_alloc();
     }
     E.ntask_max = ntasks;
     const DescLayout D(nu, ntasks);
     E.desc_cap = D.total;
-    E.d_desc = dmalloc<uint8_t>(D.total, E.own);
-    E.d_rec = dmalloc<uint8_t>(E.rec_bytes, E.own);
-    E.d_ticket = dmalloc<int>(1, E.own);
+    for (int b = 0; b < 2; ++b)
+        if (!(E.d_desc[b] = dmalloc<uint8_t>(D.total, E.own)) || !(E.d_rec[b] = dmalloc<uint8_t>(E.rec_bytes, E.own)))
+            return fail_alloc();
+    E.d_ticket = dmalloc<int>(2, E.own);
     E.d_err = dmalloc<unsigned>(1, E.own);
-    if (!E.d_desc || !E.d_rec || !E.d_ticket || !E.d_err) return fail_alloc();
+    if (!E.d_ticket || !E.d_err) return fail_alloc();
     for (int o = 0; o < kOutSlots; ++o)
         if (!(E.out_pin[o] = pin(E.rec_bytes)) || !(E.desc_pin[o] = pin(D.total))) return fail_alloc();
     return 0;
 }
 
-// Kernel timing (fdvd_timing / fdvd_stats): kinds 0 P-frame inter
-// reconstruction, 1 INTRA16 reconstruction, 2 key-frame reconstruction,
-// 3 deblocking + reference preparation, 4 the whole frame step on the GPU.
-constexpr int kTimeKinds = 5;
+// Timing (fdvd_timing / fdvd_stats): kinds 0 P-frame inter reconstruction,
+// 1 INTRA16 reconstruction, 2 key-frame reconstruction, 3 deblocking +
+// reference preparation, 4 the whole frame step on the GPU (CUDA events);
+// host wall time of 5 symbol decoding (summed over the chains), 6 scattering
+// decoded frames (summed over copiers), 7 the submitter waiting for parsed
+// frames, 8 building records (summed over the record workers).
+constexpr int kTimeKinds = 9;
 std::atomic<int> g_dtiming{0};
 std::mutex g_dstat_mu;
 double g_dms[kTimeKinds];
@@ -673,9 +725,35 @@ bool next_blob(Stream &s, const uint8_t **b, size_t *n) {
     return true;
 }
 
-// Parse one blob of unit u and pack it into slot S.  0, or -1 for a
-// malformed blob.
-int parse_pack(DUnit &u, const uint8_t *blob, size_t blen, int intra, int border, PSlot &S) {
+// The sequential half of parsing one blob of unit u into slot S: its symbol
+// streams (the P-frame table cache carries from frame to frame).  0, or -1
+// for a malformed blob.
+int parse_symbols(DUnit &u, const uint8_t *blob, size_t blen, int intra, PSlot &S) {
+    S.intra = intra;
+    if (!intra) return dec::pframe_symbols(blob, blen, u.w, u.h, &u.tc, S.sy[0]);
+    memset(&u.tc, 0, sizeof u.tc);   // tables and history restart at a key frame
+    size_t p = 0;
+    for (int pl = 0; pl < 3; ++pl) {
+        if (p + 4 > blen) return -1;
+        uint32_t n = 0;
+        for (int k = 0; k < 4; ++k) n |= (uint32_t)blob[p + k] << (8 * k);
+        p += 4;
+        if (p + n > blen || n < 4) return -1;
+        if (dec::iplane_symbols(blob + p, n, u.pw[pl], u.ph[pl], S.sy[pl])) return -1;
+        p += n;
+    }
+    return 0;
+}
+
+// Record scratch of one worker thread (capacity kept between frames).
+struct RecScratch {
+    dec::PFrame pf;
+    dec::IPlane ip;
+};
+
+// The independent half: slot S's symbols into records, packed into its
+// pinned payload.
+int parse_records(const DUnit &u, int border, PSlot &S, RecScratch &R) {
     size_t off = 0;
     bool room = true;
     auto put = [&](const void *src, size_t n) -> size_t {
@@ -685,19 +763,10 @@ int parse_pack(DUnit &u, const uint8_t *blob, size_t blen, int intra, int border
         off = al256(off + n);
         return at;
     };
-    S.intra = intra;
-    if (intra) {
-        memset(&u.tc, 0, sizeof u.tc);   // tables and history restart at a key frame
-        size_t p = 0;
+    if (S.intra) {
         for (int pl = 0; pl < 3; ++pl) {
-            if (p + 4 > blen) return -1;
-            uint32_t n = 0;
-            for (int k = 0; k < 4; ++k) n |= (uint32_t)blob[p + k] << (8 * k);
-            p += 4;
-            if (p + n > blen || n < 4) return -1;
-            dec::IPlane &P = u.ip[pl];
-            if (dec::parse_iplane(blob + p, n, u.pw[pl], u.ph[pl], P)) return -1;
-            p += n;
+            dec::IPlane &P = R.ip;
+            if (dec::iplane_records(S.sy[pl], P)) return -1;
             S.o_leaves[pl] = put(P.leaves.data(), P.leaves.size() * sizeof(dec::Leaf));
             S.o_ctu[pl] = put(P.ctu_first.data(), P.ctu_first.size() * 4);
             S.o_icoef[pl] = put(P.coef.data(), P.coef.size() * 2);
@@ -705,8 +774,8 @@ int parse_pack(DUnit &u, const uint8_t *blob, size_t blen, int intra, int border
             S.pqp[pl] = P.qp;
         }
     } else {
-        dec::PFrame &f = u.pf;
-        if (dec::parse_pframe(blob, blen, u.w, u.h, border, &u.tc, f)) return -1;
+        dec::PFrame &f = R.pf;
+        if (dec::pframe_records(S.sy[0], u.w, u.h, border, f)) return -1;
         S.qp = f.qp;
         S.nintra = (int)f.intra.size();
         S.o_mbs = put(f.mbs.data(), f.mbs.size() * sizeof(dec::PMB));
@@ -721,6 +790,7 @@ int parse_pack(DUnit &u, const uint8_t *blob, size_t blen, int intra, int border
 struct Pipe {
     std::mutex mu;
     std::condition_variable cv;
+    std::deque<std::pair<int, int>> jobs;   // (frame, unit) with symbols, awaiting records
     std::vector<int> parsed;   // units parsed, per frame
     std::vector<char> copied;  // frame scattered into the output
     int submitted = 0;         // frames whose GPU work is enqueued
@@ -759,11 +829,21 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     Pipe P;
     P.parsed.assign(nf, 0);
     P.copied.assign(nf, 0);
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int nwk = std::max(1, std::min({nthreads, nu, (int)hw}));
-    const int ncopy = std::max(1, std::min(4, (int)hw - nwk - 1));
+    // threads: nwk symbol chains (units split among them), nrec record
+    // workers, ncopy copiers, and this one; nthreads bounds the parsing ones
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int ncopy = hw >= 8 ? 2 : 1;
+    const int nparse = std::max(2, std::min(nthreads, hw - ncopy - 1));
+    const int nwk = std::max(1, std::min(nu, nparse - 1));
+    const int nrec = std::max(1, nparse - nwk);
     const int border = E.border, device = E.device;
 
+    const bool timing = g_dtiming.load() != 0;
+    std::atomic<long long> host_ns[4] = {{0}, {0}, {0}, {0}};   // symbols, scatter, submit wait, records
+    auto now_ns = [] {
+        return std::chrono::duration_cast<std::chrono::nanoseconds>(
+                   std::chrono::steady_clock::now().time_since_epoch()).count();
+    };
     auto parse_worker = [&](int wk) {
         cudaSetDevice(device);
         for (int f = 0; f < nf; ++f) {
@@ -773,18 +853,45 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
                 std::string e;
                 if (!ck(cudaEventSynchronize(E.ev_in[s]), "upload", e)) { P.fail(e); return; }
             }
-            int n = 0;
-            for (int i = wk; i < nu; i += nwk, ++n) {
+            for (int i = wk; i < nu; i += nwk) {
                 DUnit &u = E.units[i];
                 const uint8_t *blob;
                 size_t blen;
+                const long long t0 = timing ? now_ns() : 0;
                 if (!next_blob(bs[i], &blob, &blen)) { P.fail("truncated stream"); return; }
                 const int intra = f == 0 || (bs[i].keyint > 0 && f % bs[i].keyint == 0);
-                if (parse_pack(u, blob, blen, intra, border, u.slot[s])) { P.fail("malformed frame blob"); return; }
+                if (parse_symbols(u, blob, blen, intra, u.slot[s])) { P.fail("malformed frame blob"); return; }
+                if (timing) host_ns[0] += now_ns() - t0;
+                {
+                    std::lock_guard<std::mutex> lk(P.mu);
+                    P.jobs.push_back({f, i});
+                }
+                P.cv.notify_all();
             }
+        }
+    };
+    const long long njobs = (long long)nf * nu;
+    long long taken = 0;   // jobs handed to record workers (under P.mu)
+    auto rec_worker = [&]() {
+        RecScratch R;
+        for (;;) {
+            std::pair<int, int> job;
+            {
+                std::unique_lock<std::mutex> lk(P.mu);
+                P.cv.wait(lk, [&] { return P.abort || taken == njobs || !P.jobs.empty(); });
+                if (P.abort || (taken == njobs && P.jobs.empty())) return;
+                job = P.jobs.front();
+                P.jobs.pop_front();
+                ++taken;
+            }
+            const long long t0 = timing ? now_ns() : 0;
+            DUnit &u = E.units[job.second];
+            if (parse_records(u, border, u.slot[job.first % kSlots], R)) { P.fail("malformed frame blob"); return; }
+            if (timing) host_ns[3] += now_ns() - t0;
             {
                 std::lock_guard<std::mutex> lk(P.mu);
-                P.parsed[f] += n;
+                P.parsed[job.first] += 1;
+                if (taken == njobs) P.cv.notify_all();   // idle workers can leave
             }
             P.cv.notify_all();
         }
@@ -795,6 +902,7 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
             if (!P.wait([&] { return P.submitted > f; })) return;
             std::string e;
             if (!ck(cudaEventSynchronize(E.ev_out[f % kOutSlots]), "download", e)) { P.fail(e); return; }
+            const long long t0 = timing ? now_ns() : 0;
             const uint8_t *src = E.out_pin[f % kOutSlots];
             uint8_t *fy = out + (size_t)f * fsize, *fu = fy + (size_t)W * H, *fv = fu + (size_t)cw * ch;
             for (int i = 0; i < nu; ++i) {
@@ -805,6 +913,7 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
                 memcpy(fv + (size_t)(y0[i] / 2) * cw, s + (size_t)u.w * u.h + (size_t)u.cw * u.ch,
                        (size_t)u.cw * u.ch);
             }
+            if (timing) host_ns[1] += now_ns() - t0;
             {
                 std::lock_guard<std::mutex> lk(P.mu);
                 P.copied[f] = 1;
@@ -814,10 +923,10 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     };
     std::vector<std::thread> th;
     for (int k = 0; k < nwk; ++k) th.emplace_back(parse_worker, k);
+    for (int k = 0; k < nrec; ++k) th.emplace_back(rec_worker);
     for (int c = 0; c < ncopy; ++c) th.emplace_back(copier, c);
 
     const DescLayout D(nu, E.ntask_max);
-    const bool timing = g_dtiming.load() != 0;
     struct TMark { int kind, a, b; };
     std::vector<TMark> marks;
     int nev = 0;
@@ -842,26 +951,38 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     std::vector<dk::ITask> tasks;
     std::vector<DbTaskD> db;
     std::vector<PrepTaskD> prep;
+    // Frame step f uses the device buffers of parity b = f & 1: its uploads
+    // (st_in) wait until step f-2's kernels are done with them, its kernels
+    // (st) wait for the uploads and for step f-2's download of the same
+    // reconstruction buffer, its download (st_out) waits for the deblocking.
     auto submit = [&](int f) -> int {
-        const int s = f % kSlots, o = f % kOutSlots;
-        const int t_frame = timing ? tev() : -1;
+        const int s = f % kSlots, o = f % kOutSlots, b = f & 1;
+        const int epoch = ++E.epoch;
+        uint8_t *const drec = E.d_rec[b], *const ddesc = E.d_desc[b];
+        int nintra = 0;
         pu.clear(); uoff.assign(1, 0); ipl.clear(); tasks.clear(); db.clear(); prep.clear();
+        if (f >= 2) DCK(cudaStreamWaitEvent(E.st_in, E.ev_used[b], 0));
         for (int i = 0; i < nu; ++i) {
             DUnit &u = E.units[i];
             const PSlot &S = u.slot[s];
-            DCK(cudaMemcpyAsync(u.d_pay, S.pin, S.used, cudaMemcpyHostToDevice, E.st));
-            uint8_t *rec[3] = {E.d_rec + u.rec_off, E.d_rec + u.rec_off + (size_t)u.w * u.h,
-                               E.d_rec + u.rec_off + (size_t)u.w * u.h + (size_t)u.cw * u.ch};
+            uint8_t *const pay = u.d_pay[b];
+            DCK(cudaMemcpyAsync(pay, S.pin, S.used, cudaMemcpyHostToDevice, E.st_in));
+            uint8_t *rec[3] = {drec + u.rec_off, drec + u.rec_off + (size_t)u.w * u.h,
+                               drec + u.rec_off + (size_t)u.w * u.h + (size_t)u.cw * u.ch};
             if (!S.intra) {
                 dk::PUnit d{};
                 d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh; d.qp = S.qp;
                 for (int p = 0; p < 3; ++p) d.rec[p] = rec[p];
                 d.ref[0] = u.ref[u.near_i].rp;
                 d.ref[1] = u.nref >= 2 ? u.ref[1 - u.near_i].rp : u.ref[u.near_i].rp;
-                d.mbs = reinterpret_cast<const dec::PMB *>(u.d_pay + S.o_mbs);
-                d.coef = reinterpret_cast<const int16_t *>(u.d_pay + S.o_coef);
-                d.intra = reinterpret_cast<const int32_t *>(u.d_pay + S.o_intra);
+                d.mbs = reinterpret_cast<const dec::PMB *>(pay + S.o_mbs);
+                d.coef = reinterpret_cast<const int16_t *>(pay + S.o_coef);
+                d.intra = reinterpret_cast<const int32_t *>(pay + S.o_intra);
                 d.nintra = S.nintra;
+                d.ibase = nintra;
+                d.epoch = epoch;
+                d.done = u.d_done;
+                nintra += S.nintra;
                 pu.push_back(d);
                 uoff.push_back(uoff.back() + u.mbw * u.mbh);
                 for (int p = 0; p < 3; ++p) db.push_back({rec[p], u.pw[p], u.ph[p], S.qp});
@@ -870,17 +991,16 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
                 for (int p = 0; p < 3; ++p) {
                     dk::IPlaneD d{};
                     d.rec = rec[p]; d.w = u.pw[p]; d.h = u.ph[p]; d.cols = u.cols[p]; d.rows = u.rows[p];
-                    d.leaves = reinterpret_cast<const dec::Leaf *>(u.d_pay + S.o_leaves[p]);
-                    d.ctu_first = reinterpret_cast<const int32_t *>(u.d_pay + S.o_ctu[p]);
-                    d.coef = reinterpret_cast<const int16_t *>(u.d_pay + S.o_icoef[p]);
-                    d.flags = u.d_pay + S.o_flags[p];
+                    d.leaves = reinterpret_cast<const dec::Leaf *>(pay + S.o_leaves[p]);
+                    d.ctu_first = reinterpret_cast<const int32_t *>(pay + S.o_ctu[p]);
+                    d.coef = reinterpret_cast<const int16_t *>(pay + S.o_icoef[p]);
+                    d.flags = pay + S.o_flags[p];
                     d.progress = u.d_prog + prog;
                     d.qp = S.pqp[p];
                     prog += u.rows[p];
                     ipl.push_back(d);
                     db.push_back({rec[p], u.pw[p], u.ph[p], S.pqp[p]});
                 }
-                DCK(cudaMemsetAsync(u.d_prog, 0, sizeof(int) * prog, E.st));
             }
             RefBuf &far = u.ref[1 - u.near_i];
             prep.push_back({{rec[0], rec[1], rec[2]}, far.G, far.B, far.H, far.J, far.U, far.V, u.w, u.h, far.rp.ys,
@@ -899,19 +1019,30 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
         memcpy(h + D.tasks, tasks.data(), tasks.size() * sizeof(dk::ITask));
         memcpy(h + D.db, db.data(), db.size() * sizeof(DbTaskD));
         memcpy(h + D.prep, prep.data(), prep.size() * sizeof(PrepTaskD));
-        DCK(cudaMemcpyAsync(E.d_desc, h, D.total, cudaMemcpyHostToDevice, E.st));
-        DCK(cudaEventRecord(E.ev_in[s], E.st));
-        const auto *d_pu = reinterpret_cast<const dk::PUnit *>(E.d_desc + D.pu);
+        DCK(cudaMemcpyAsync(ddesc, h, D.total, cudaMemcpyHostToDevice, E.st_in));
+        DCK(cudaEventRecord(E.ev_in[s], E.st_in));
+        DCK(cudaEventRecord(E.ev_up[b], E.st_in));
+
+        DCK(cudaStreamWaitEvent(E.st, E.ev_up[b], 0));
+        if (f >= 2) DCK(cudaStreamWaitEvent(E.st, E.ev_d2h[b], 0));
+        const int t_frame = timing ? tev() : -1;
+        for (int i = 0; i < nu; ++i)
+            if (E.units[i].slot[s].intra) {
+                const DUnit &u = E.units[i];
+                DCK(cudaMemsetAsync(u.d_prog, 0, sizeof(int) * (u.rows[0] + u.rows[1] + u.rows[2]), E.st));
+            }
+        const auto *d_pu = reinterpret_cast<const dk::PUnit *>(ddesc + D.pu);
         if (!pu.empty()) {
             int t0 = timing ? tev() : -1;
-            dk::pdec_inter_kernel<<<uoff.back(), 64, 0, E.st>>>(d_pu, reinterpret_cast<const int *>(E.d_desc + D.uoff),
+            dk::pdec_inter_kernel<<<uoff.back(), 64, 0, E.st>>>(d_pu, reinterpret_cast<const int *>(ddesc + D.uoff),
                                                                  (int)pu.size());
             mark(0, t0);
-            int nintra = 0;
-            for (auto &d : pu) nintra += d.nintra;
             if (nintra) {
+                DCK(cudaMemsetAsync(E.d_ticket + 1, 0, sizeof(int), E.st));
                 t0 = timing ? tev() : -1;
-                dk::pdec_intra_kernel<<<(int)pu.size(), 64, 0, E.st>>>(d_pu);
+                dk::pdec_intra_kernel<<<std::min(nintra, 8 * E.nsm), 64, 0, E.st>>>(d_pu, (int)pu.size(), nintra,
+                                                                                  E.d_ticket + 1, E.d_err,
+                                                                                  4000000000ull);
                 mark(1, t0);
             }
         }
@@ -919,23 +1050,27 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
             DCK(cudaMemsetAsync(E.d_ticket, 0, sizeof(int), E.st));
             const int t0 = timing ? tev() : -1;
             dk::idec_kernel<<<std::min((int)tasks.size(), E.nsm), dk::kINT, 0, E.st>>>(
-                reinterpret_cast<const dk::IPlaneD *>(E.d_desc + D.planes),
-                reinterpret_cast<const dk::ITask *>(E.d_desc + D.tasks), (int)tasks.size(), E.d_ticket, E.d_err,
+                reinterpret_cast<const dk::IPlaneD *>(ddesc + D.planes),
+                reinterpret_cast<const dk::ITask *>(ddesc + D.tasks), (int)tasks.size(), E.d_ticket, E.d_err,
                 4000000000ull);
             mark(2, t0);
         }
         DCK(cudaGetLastError());
         const int t_ops = timing ? tev() : -1;
-        launch_deblock(E.d_desc + D.db, (int)db.size(), E.st);
-        DCK(cudaMemcpyAsync(E.out_pin[o], E.d_rec, E.rec_bytes, cudaMemcpyDeviceToHost, E.st));
+        launch_deblock(ddesc + D.db, (int)db.size(), E.st);
+        DCK(cudaEventRecord(E.ev_dbk[b], E.st));
+        DCK(cudaStreamWaitEvent(E.st_out, E.ev_dbk[b], 0));
+        DCK(cudaMemcpyAsync(E.out_pin[o], drec, E.rec_bytes, cudaMemcpyDeviceToHost, E.st_out));
+        DCK(cudaEventRecord(E.ev_d2h[b], E.st_out));
+        DCK(cudaEventRecord(E.ev_out[o], E.st_out));
         // the decoded frame becomes the nearest reference (load_ref, fdv.h:5183)
         int maxw = 0, maxh = 0;
         for (auto &u : E.units) { maxw = std::max(maxw, u.w); maxh = std::max(maxh, u.h); }
-        launch_refprep(E.d_desc + D.prep, (int)prep.size(), maxw, maxh, border + 16, E.st);
+        launch_refprep(ddesc + D.prep, (int)prep.size(), maxw, maxh, border + 16, E.st);
         DCK(cudaGetLastError());
-        mark(3, t_ops);   // includes the download between the two
+        mark(3, t_ops);
         mark(4, t_frame);
-        DCK(cudaEventRecord(E.ev_out[o], E.st));
+        DCK(cudaEventRecord(E.ev_used[b], E.st));
         for (int i = 0; i < nu; ++i) {
             DUnit &u = E.units[i];
             u.near_i = 1 - u.near_i;
@@ -944,7 +1079,9 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
         return 0;
     };
     for (int f = 0; f < nf; ++f) {
+        const long long t0 = timing ? now_ns() : 0;
         if (!P.wait([&] { return P.parsed[f] == nu && (f < kOutSlots || P.copied[f - kOutSlots]); })) break;
+        if (timing) host_ns[2] += now_ns() - t0;
         if (submit(f)) { P.fail(g_derr); break; }
         {
             std::lock_guard<std::mutex> lk(P.mu);
@@ -956,7 +1093,8 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
     unsigned herr = 0;
     std::string e;
     const bool ok = ck(cudaMemcpyAsync(&herr, E.d_err, sizeof herr, cudaMemcpyDeviceToHost, E.st), "error word", e) &&
-                    ck(cudaStreamSynchronize(E.st), "decode", e);
+                    ck(cudaStreamSynchronize(E.st), "decode", e) && ck(cudaStreamSynchronize(E.st_in), "upload", e) &&
+                    ck(cudaStreamSynchronize(E.st_out), "download", e);
     if (!ok) {   // the context may be unusable: drop the engine
         delete Ep;
         g_derr = e;
@@ -969,6 +1107,7 @@ int decode_bands(std::vector<Stream> &bs, const std::vector<int> &y0, int W, int
             float t = 0.f;
             if (cudaEventElapsedTime(&t, E.tev[m.a], E.tev[m.b]) == cudaSuccess) { ms[m.kind] += t; ++n[m.kind]; }
         }
+        for (int k = 0; k < 4; ++k) { ms[5 + k] = host_ns[k] * 1e-6; n[5 + k] = nf; }
         std::lock_guard<std::mutex> lk(g_dstat_mu);
         for (int k = 0; k < kTimeKinds; ++k) { g_dms[k] += ms[k]; g_dn[k] += n[k]; }
     }
@@ -1009,7 +1148,7 @@ int fdv_video_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, 
     Stream s;
     if (!out || !open_stream(in, len, s)) { g_derr = "bad stream header"; return -1; }
     std::vector<Stream> bs{s};
-    if (decode_bands(bs, {0}, s.w, s.h, s.nf, out, 1)) return -1;
+    if (decode_bands(bs, {0}, s.w, s.h, s.nf, out, 1 << 16)) return -1;   // one chain, records on every core
     if (nframes) *nframes = s.nf;
     if (w) *w = s.w;
     if (h) *h = s.h;

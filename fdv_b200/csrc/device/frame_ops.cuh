@@ -36,35 +36,73 @@ __device__ __forceinline__ int hfr(const uint8_t *p, int w, int h, int x, int y)
                 rpx(p, w, h, x + 1, y), rpx(p, w, h, x + 2, y), rpx(p, w, h, x + 3, y));
 }
 
-// Grid: x over padded columns, y over padded rows, z = task.  Luma planes.
-__global__ void refprep_luma_kernel(const PrepTask *tasks) {
+// Luma planes.  A block makes a 128 x 16 tile of the padded plane (32 x 8
+// threads, 4 adjacent samples per thread and row, stored as one 32-bit word:
+// padded widths and row starts are multiples of 4).  The clamped source tile
+// with a 2/3-sample halo is staged in shared memory once, then its horizontal
+// 6-tap sums; b, h and j come from those.  Grid: x over 128-column tiles, y over
+// 16-row tiles, z = task.
+constexpr int kRpTW = 128, kRpTH = 16;
+__global__ void __launch_bounds__(256) refprep_luma_kernel(const PrepTask *tasks) {
+    __shared__ uint8_t S[kRpTH + 5][kRpTW + 8];   // rows y0-2 .. y0+TH+2, columns x0-2 .. x0+TW+2
+    __shared__ int16_t Hs[kRpTH + 5][kRpTW];      // 6-tap horizontal sums at x0 .. x0+TW-1
     const PrepTask &T = tasks[blockIdx.z];
     const int B = T.border, pw = T.w + 2 * B, ph = T.h + 2 * B;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
-    if (px >= pw || py >= ph) return;
-    const int x = px - B, y = py - B;
+    const int px0 = blockIdx.x * kRpTW, py0 = blockIdx.y * kRpTH;
+    if (px0 >= pw || py0 >= ph) return;
+    const int x0 = px0 - B, y0 = py0 - B, w = T.w, h = T.h;
     const uint8_t *r = T.rec[0];
-    const int w = T.w, h = T.h;
-    const long o = (long)y * T.ys + x;
-    T.G[o] = (uint8_t)rpx(r, w, h, x, y);
-    T.B[o] = (uint8_t)clipb((hfr(r, w, h, x, y) + 16) >> 5);
-    int v = tap6(rpx(r, w, h, x, y - 2), rpx(r, w, h, x, y - 1), rpx(r, w, h, x, y),
-                 rpx(r, w, h, x, y + 1), rpx(r, w, h, x, y + 2), rpx(r, w, h, x, y + 3));
-    T.H[o] = (uint8_t)clipb((v + 16) >> 5);
-    int jj = tap6(hfr(r, w, h, x, y - 2), hfr(r, w, h, x, y - 1), hfr(r, w, h, x, y),
-                  hfr(r, w, h, x, y + 1), hfr(r, w, h, x, y + 2), hfr(r, w, h, x, y + 3));
-    T.J[o] = (uint8_t)clipb((jj + 512) >> 10);
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int k = tid; k < (kRpTH + 5) * (kRpTW + 5); k += 256) {
+        const int i = k / (kRpTW + 5), j = k - i * (kRpTW + 5);
+        S[i][j] = (uint8_t)rpx(r, w, h, x0 - 2 + j, y0 - 2 + i);
+    }
+    __syncthreads();
+    for (int k = tid; k < (kRpTH + 5) * kRpTW; k += 256) {
+        const int i = k / kRpTW, j = k - i * kRpTW;
+        Hs[i][j] = (int16_t)tap6(S[i][j], S[i][j + 1], S[i][j + 2], S[i][j + 3], S[i][j + 4], S[i][j + 5]);
+    }
+    __syncthreads();
+    const int tx = threadIdx.x * 4;
+    if (px0 + tx >= pw) return;
+    for (int rr = threadIdx.y; rr < kRpTH && py0 + rr < ph; rr += 8) {
+        uint32_t g = 0, b = 0, hv = 0, jv = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = tx + q;
+            const int v = tap6(S[rr][j + 2], S[rr + 1][j + 2], S[rr + 2][j + 2], S[rr + 3][j + 2], S[rr + 4][j + 2],
+                               S[rr + 5][j + 2]);
+            const int jj = tap6(Hs[rr][j], Hs[rr + 1][j], Hs[rr + 2][j], Hs[rr + 3][j], Hs[rr + 4][j], Hs[rr + 5][j]);
+            g |= (uint32_t)S[rr + 2][j + 2] << (8 * q);
+            b |= (uint32_t)clipb((Hs[rr + 2][j] + 16) >> 5) << (8 * q);
+            hv |= (uint32_t)clipb((v + 16) >> 5) << (8 * q);
+            jv |= (uint32_t)clipb((jj + 512) >> 10) << (8 * q);
+        }
+        const long o = (long)(y0 + rr) * T.ys + x0 + tx;
+        *reinterpret_cast<uint32_t *>(T.G + o) = g;
+        *reinterpret_cast<uint32_t *>(T.B + o) = b;
+        *reinterpret_cast<uint32_t *>(T.H + o) = hv;
+        *reinterpret_cast<uint32_t *>(T.J + o) = jv;
+    }
 }
 
-__global__ void refprep_chroma_kernel(const PrepTask *tasks) {
+// Chroma planes: the border replicated, 4 adjacent samples per thread (32 x 8
+// threads make a 128 x 8 tile).
+__global__ void __launch_bounds__(256) refprep_chroma_kernel(const PrepTask *tasks) {
     const PrepTask &T = tasks[blockIdx.z];
     const int B = T.border, cw = T.w / 2, ch = T.h / 2, pw = cw + 2 * B, ph = ch + 2 * B;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    const int px = (blockIdx.x * blockDim.x + threadIdx.x) * 4, py = blockIdx.y * blockDim.y + threadIdx.y;
     if (px >= pw || py >= ph) return;
     const int x = px - B, y = py - B;
+    uint32_t u = 0, v = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        u |= (uint32_t)rpx(T.rec[1], cw, ch, x + q, y) << (8 * q);
+        v |= (uint32_t)rpx(T.rec[2], cw, ch, x + q, y) << (8 * q);
+    }
     const long o = (long)y * T.cs + x;
-    T.U[o] = (uint8_t)rpx(T.rec[1], cw, ch, x, y);
-    T.V[o] = (uint8_t)rpx(T.rec[2], cw, ch, x, y);
+    *reinterpret_cast<uint32_t *>(T.U + o) = u;
+    *reinterpret_cast<uint32_t *>(T.V + o) = v;
 }
 
 // ------------------------------------------------------------- deblock --

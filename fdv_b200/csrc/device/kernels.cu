@@ -64,10 +64,11 @@ void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ti
 }
 
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st) {
+    if (border & 3) return;   // the kernels store 4 samples at a time from padded column 0
     dim3 blk(32, 8);
-    dim3 gl((maxw + 2 * border + 31) / 32, (maxh + 2 * border + 7) / 8, ntasks);
+    dim3 gl((maxw + 2 * border + kRpTW - 1) / kRpTW, (maxh + 2 * border + kRpTH - 1) / kRpTH, ntasks);
     refprep_luma_kernel<<<gl, blk, 0, st>>>(static_cast<const PrepTask *>(tasks));
-    dim3 gc((maxw / 2 + 2 * border + 31) / 32, (maxh / 2 + 2 * border + 7) / 8, ntasks);
+    dim3 gc((maxw / 2 + 2 * border + 127) / 128, (maxh / 2 + 2 * border + 7) / 8, ntasks);
     refprep_chroma_kernel<<<gc, blk, 0, st>>>(static_cast<const PrepTask *>(tasks));
 }
 

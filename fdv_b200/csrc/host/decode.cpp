@@ -103,7 +103,7 @@ struct RansDec {
         for (int s = 0; s < 256; ++s) {
             freq[s] = f[s];
             cum[s] = c;
-            for (uint16_t k = 0; k < f[s]; ++k) slot[c + k] = (uint8_t)s;
+            if (f[s]) memset(slot + c, s, f[s]);
             c = (uint16_t)(c + f[s]);
         }
     }
@@ -124,16 +124,37 @@ struct RansDec {
 };
 
 // ------------------------------------------------------ adaptive decoder --
-unsigned am_find(const AModel &m, uint32_t v, uint32_t *cum) {
-    unsigned pos = 0;
-    uint32_t rem = v;
-    for (unsigned pw = 128; pw; pw >>= 1) {
-        const unsigned np = pos + pw;
-        if (np <= 256 && m.t[np] <= rem) { pos = np; rem -= m.t[np]; }
+// The adaptive model as the decoder keeps it: the frequencies alone.  The
+// encoder's Fenwick tree serves its cumulative lookups; the decoder finds a
+// symbol by a linear scan from symbol 0 instead -- the models are skewed
+// towards small symbols, so the scan mostly stops after a few steps, and an
+// increment is then a single add.  Same arithmetic as AModel (init, add,
+// halving at kAdMax).
+struct DModel {
+    uint32_t f[256];
+    uint32_t tot;
+    void init(const uint32_t hist[256]) {   // AModel::init without the tree
+        uint64_t s = 0;
+        for (int i = 0; i < 256; ++i) s += hist[i];
+        uint32_t t = 0;
+        if (s <= kAdScale) {
+            for (int i = 0; i < 256; ++i) t += (f[i] = kAdBase + hist[i]);
+        } else {
+            for (int i = 0; i < 256; ++i)   // a zero count scales to zero: no division
+                t += (f[i] = kAdBase + (hist[i] ? (uint32_t)(((uint64_t)hist[i] * kAdScale + s / 2) / s) : 0));
+        }
+        tot = t;
     }
-    *cum = v - rem;
-    return pos;
-}
+    void add(unsigned s, uint32_t d) {
+        f[s] += d;
+        tot += d;
+        if (tot > kAdMax) {
+            uint32_t t = 0;
+            for (int i = 0; i < 256; ++i) t += (f[i] = (f[i] + 1) >> 1);
+            tot = t;
+        }
+    }
+};
 
 struct ADec {
     const uint8_t *in;
@@ -142,12 +163,13 @@ struct ADec {
     ADec(const uint8_t *i, size_t l) : in(i), len(l) {
         for (int k = 0; k < 4; ++k) { code = (code << 8) | (p < len ? in[p] : 0); ++p; }
     }
-    unsigned sym(AModel &m) {
+    unsigned sym(DModel &m) {
         const uint32_t r = range / m.tot;
         uint32_t v = code / r;
         if (v >= m.tot) v = m.tot - 1;
-        uint32_t cum;
-        const unsigned s = am_find(m, v, &cum);
+        unsigned s = 0;
+        uint32_t cum = 0;
+        while (cum + m.f[s] <= v) cum += m.f[s++];   // ends by 255: v < tot
         code -= r * cum;
         range = r * m.f[s];
         while (range < (1u << 24)) {
@@ -215,7 +237,7 @@ bool mv_in_bounds(int w, int h, int border, int x, int y, int bw, int bh, int mv
 
 }  // namespace
 
-int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_tabcache *tc, PFrame &out) {
+int pframe_symbols(const uint8_t *in, size_t len, int w, int h, fdvb_tabcache *tc, Syms &out) {
     if (len < 2) return -1;
     size_t p = 0;
     const int qp = in[p++];
@@ -236,7 +258,10 @@ int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_t
         if (total > maxsyms) return -1;
     }
     for (size_t k = 0, o = 0; k < kNS; ++k) { base[k] = o; o += sn[k]; }
-    std::vector<uint8_t> syms(total ? total : 1);
+    out.qp = qp;
+    std::vector<uint8_t> &syms = out.buf;
+    syms.resize(total ? total : 1);
+    for (int k = 0; k < kNS; ++k) { out.sn[k] = sn[k]; out.base[k] = base[k]; }
     if (!(emode & 1)) {   // one shared model
         uint16_t freq[256];
         bool ok = true;
@@ -279,7 +304,7 @@ int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_t
             ADec ad(in + p, n);
             for (int k = 0; k < kNS; ++k) {
                 if (!((am >> k) & 1)) continue;
-                AModel m;
+                DModel m;
                 m.init(tc->hist[k]);
                 for (size_t i = 0; i < sn[k]; ++i) syms[base[k] + i] = (uint8_t)ad.sym(m);
             }
@@ -295,10 +320,14 @@ int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_t
         }
         if (tc->hn < (1 << 20)) ++tc->hn;
     }
+    return 0;
+}
 
+int pframe_records(const Syms &sy, int w, int h, int border, PFrame &out) {
+    const int qp = sy.qp;
     bool ok = true;
     Rd S[kNS];
-    for (int k = 0; k < kNS; ++k) S[k] = Rd{syms.data(), base[k], base[k] + sn[k], &ok};
+    for (int k = 0; k < kNS; ++k) S[k] = Rd{sy.buf.data(), sy.base[k], sy.base[k] + sy.sn[k], &ok};
     Coef R{S[9], S[10], S[11], S[12], S[13], S[14], S[15]};
     const int mbw = w / 16, mbh = h / 16;
     out.qp = qp;
@@ -439,6 +468,12 @@ int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_t
     return ok ? 0 : -1;
 }
 
+int parse_pframe(const uint8_t *in, size_t len, int w, int h, int border, fdvb_tabcache *tc, PFrame &out) {
+    Syms sy;
+    if (pframe_symbols(in, len, w, h, tc, sy)) return -1;
+    return pframe_records(sy, w, h, border, out);
+}
+
 namespace {
 constexpr int kIsModeB = 4, kIsMode0 = 5, kIsMode1 = 6, kIsN = 12;
 
@@ -493,7 +528,7 @@ struct IParse {
 };
 }  // namespace
 
-int parse_iplane(const uint8_t *in, size_t len, int ew, int eh, IPlane &out) {
+int iplane_symbols(const uint8_t *in, size_t len, int ew, int eh, Syms &out) {
     if (len < 6) return -1;
     size_t p = 0;
     const int w = (int)get16(in, &p), h = (int)get16(in, &p);
@@ -519,7 +554,12 @@ int parse_iplane(const uint8_t *in, size_t len, int ew, int eh, IPlane &out) {
             total += v;
         }
     }
-    std::vector<uint8_t> syms(total ? total : 1);
+    out.qp = qp;
+    out.w = w;
+    out.h = h;
+    for (int k = 0; k < kIsN; ++k) { out.sn[k] = sn[k]; out.base[k] = off[k]; }
+    std::vector<uint8_t> &syms = out.buf;
+    syms.resize(total ? total : 1);
     if (imode == 2) {   // one adaptive blob, every model starting flat
         bool ok = true;
         const uint32_t la = rd_count32(in, &p, len, &ok);
@@ -527,7 +567,7 @@ int parse_iplane(const uint8_t *in, size_t len, int ew, int eh, IPlane &out) {
         const uint32_t flat[256] = {0};
         ADec ad(in + p, la);
         for (int k = 0; k < kIsN; ++k) {
-            AModel m;
+            DModel m;
             m.init(flat);
             for (size_t i = 0; i < sn[k]; ++i) syms[off[k] + i] = (uint8_t)ad.sym(m);
         }
@@ -554,10 +594,15 @@ int parse_iplane(const uint8_t *in, size_t len, int ew, int eh, IPlane &out) {
             p += lk;
         }
     }
+    return 0;
+}
+
+int iplane_records(const Syms &sy, IPlane &out) {
+    const int w = sy.w, h = sy.h, qp = sy.qp;
     bool ok = true;
     Rd S[kIsN];
-    for (int k = 0; k < kIsN; ++k) S[k] = Rd{syms.data(), off[k], off[k] + sn[k], &ok};
-    Rd empty{syms.data(), 0, 0, &ok};
+    for (int k = 0; k < kIsN; ++k) S[k] = Rd{sy.buf.data(), sy.base[k], sy.base[k] + sy.sn[k], &ok};
+    Rd empty{sy.buf.data(), 0, 0, &ok};
     Coef R{S[7], S[8], S[9], S[10], S[11], empty, empty};
     out.w = w;
     out.h = h;
@@ -574,6 +619,12 @@ int parse_iplane(const uint8_t *in, size_t len, int ew, int eh, IPlane &out) {
         }
     out.ctu_first.push_back((int32_t)out.leaves.size());
     return ok ? 0 : -1;
+}
+
+int parse_iplane(const uint8_t *in, size_t len, int w, int h, IPlane &out) {
+    Syms sy;
+    if (iplane_symbols(in, len, w, h, sy)) return -1;
+    return iplane_records(sy, out);
 }
 
 }  // namespace dec

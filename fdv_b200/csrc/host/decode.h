@@ -56,6 +56,20 @@ struct IPlane {
     std::vector<uint8_t> flags;
 };
 
+// The entropy-decoded symbol streams of one blob: stream k is
+// buf[base[k] .. base[k] + sn[k]).  Decoding them is the part of the parse
+// that is sequential over frames (the P-frame table cache); turning symbols
+// into records depends on nothing but the symbols.
+struct Syms {
+    int qp = 0, w = 0, h = 0;   // w, h: a key-frame plane's dimensions
+    std::vector<uint8_t> buf;
+    size_t sn[16] = {}, base[16] = {};
+};
+int pframe_symbols(const uint8_t *in, size_t len, int w, int h, fdvb_tabcache *tc, Syms &out);
+int pframe_records(const Syms &s, int w, int h, int border, PFrame &out);
+int iplane_symbols(const uint8_t *in, size_t len, int w, int h, Syms &out);
+int iplane_records(const Syms &s, IPlane &out);
+
 // A P-frame blob of a w x h unit against references with a `border`-sample
 // border (the reference's FDV_BORDER: motion vectors reaching past it are
 // rejected, fdv.h:6480).  tc carries the entropy tables between frames.

@@ -49,8 +49,9 @@ size_t fdv_vtile_encode(const uint8_t *const *frames, int nframes, int w, int h,
  * fdv.h:6856-6930) and fdv_vtile_decode, fdv.h:980 (implementation
  * fdv.h:7245-7370), same signatures: nframes consecutive I420 frames into out,
  * which must hold them.  The frame blobs are entropy-decoded and parsed on the
- * host, by up to nthreads workers (one for fdv_video_decode) running up to
- * three frames ahead of the GPU; prediction, inverse transforms, deblocking
+ * host -- entropy decoding by one chain per band, records by a worker pool,
+ * nthreads threads in all at most -- running up to three frames ahead of the
+ * GPU; prediction, inverse transforms, deblocking
  * and reference preparation run on the GPU, bit-exact with the reference
  * decoder.
  * Returns 0, or -1 for a malformed stream or a device failure (the reason:
@@ -63,13 +64,18 @@ int fdv_vtile_decode(const uint8_t *in, size_t len, uint8_t *out, int *nframes, 
 /* The reason the last fdv_*_decode call on this thread failed ("" if none). */
 const char *fdvd_last_error(void);
 /* Decoder timing, off by default (no counterpart in the reference): with it on,
- * CUDA events on the decoder's stream bracket each launch.  fdvd_stats reads
- * the milliseconds ms[k] and launches n[k] accumulated since the last reset,
- * k = 0 P-frame inter reconstruction, 1 INTRA16 reconstruction, 2 key-frame
- * reconstruction, 3 deblocking + download + reference preparation, 4 whole
- * frame steps on the GPU (upload to download); reset != 0 clears them. */
+ * CUDA events on the decoder's compute stream bracket each launch and the host
+ * stages are clocked.  fdvd_stats reads the milliseconds ms[k] and counts n[k]
+ * accumulated since the last reset, k = 0 P-frame inter reconstruction,
+ * 1 INTRA16 reconstruction, 2 key-frame reconstruction, 3 deblocking +
+ * reference preparation, 4 whole frame steps on the compute stream (launches);
+ * host wall time of 5 entropy decoding (summed over the per-band chains),
+ * 6 scattering decoded frames into the output (summed over the copier
+ * threads), 7 the submitting thread waiting for parsed frames, 8 building
+ * records from symbols (summed over the record workers) (counts: frames);
+ * reset != 0 clears them. */
 void fdvd_timing(int on);
-void fdvd_stats(double ms[5], long long n[5], int reset);
+void fdvd_stats(double ms[9], long long n[9], int reset);
 
 /* Streaming encoder.  Replaces the fdv_enc_* family, fdv.h:1157-1198
  * (implementation fdv.h:8129-8459).  Output is byte-identical to
