@@ -172,4 +172,34 @@ __device__ __forceinline__ bool wait_at_least(const int *flag, int need, unsigne
     }
 }
 
+// Progress flags between blocks with release/acquire at GPU scope (lighter
+// than a full fence plus an atomic exchange).  The publisher's block writes
+// are ordered before its release by the block barrier that precedes it; the
+// waiter's acquire orders its later loads, and the barrier after the wait
+// extends that to its block.
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Bounded wait until *flag >= need: spins without sleeping at first (the
+// flag usually arrives within a few microseconds), checks the error word
+// every 16 polls, then backs off.
+__device__ __forceinline__ bool wait_progress(const int *flag, int need, unsigned *err,
+                                              unsigned long long limit_ns) {
+    if (ld_acquire_gpu(flag) >= need) return true;
+    const unsigned long long t0 = globaltimer();
+    for (unsigned i = 1;; ++i) {
+        if (ld_acquire_gpu(flag) >= need) return true;
+        if (!(i & 15)) {
+            if (*(volatile unsigned *)err) return false;
+            if (globaltimer() - t0 > limit_ns) { atomicOr(err, kErrWaitTimeout); return false; }
+        }
+        if (i > 256) __nanosleep(64);
+    }
+}
+
 }  // namespace fdvb

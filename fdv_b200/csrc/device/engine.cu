@@ -34,6 +34,7 @@
 
 namespace fdvb {
 // kernels (pframe.cu, iframe.cu, frame_ops.cu)
+void launch_lrn_preskip(const UnitDev *units, const int2 *pu, int np, int total, cudaStream_t st);
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
                    unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st);
 struct IPlaneDev;
@@ -161,6 +162,7 @@ struct fdvb_engine {
     std::vector<int> pending_intra;         // frame types of the uncommitted step
     bool pending = false;
     unsigned long long *d_prof = nullptr;   // phase profile accumulators (when enabled)
+    unsigned long long *d_tl = nullptr;     // per-macroblock timeline (with the phase profile)
     // learned proposals: a private inference network, its per-macroblock
     // hints and the P units of the current step ({unit, first macroblock})
     fdvl_net *lnet = nullptr;
@@ -168,6 +170,7 @@ struct fdvb_engine {
     double lgate = 0.0;                      // confident SKIP needs J <= lgate * lambda (0: always)
     int linter8 = 0;                         // confident inter also tries INTER8
     lrn::Hint *d_hints = nullptr;
+    float *d_prejs = nullptr;                // per hinted macroblock: the SKIP pre-analysis (lrn_preskip_kernel)
     int2 *d_pu = nullptr;
     int total_mbs = 0;
     float *d_mbcost = nullptr;              // per-macroblock RD cost records (when enabled)
@@ -314,8 +317,9 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
     if (E->d_prof) cudaFree(E->d_prof);
+    if (E->d_tl) cudaFree(E->d_tl);
     if (E->lnet) fdvl_destroy(E->lnet);
-    cudaFree(E->d_hints); cudaFree(E->d_pu); cudaFree(E->d_mbcost);
+    cudaFree(E->d_hints); cudaFree(E->d_prejs); cudaFree(E->d_pu); cudaFree(E->d_mbcost);
     for (auto &sl : E->slot) {
         for (auto &e : sl.ev) if (e) cudaEventDestroy(e);
         if (sl.stage) cudaFreeHost(sl.stage);
@@ -438,9 +442,11 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         d.skip_gate = E->lgate;
         d.inter8 = E->linter8;
         d.mbcost = E->d_mbcost ? E->d_mbcost + u.mb_off : nullptr;
+        d.tl = E->d_tl ? E->d_tl + 2 * (size_t)u.mb_off : nullptr;
         if (!is_intra[i] && E->lnet) {
             pu.push_back(make_int2(i, nhint));
             d.hint = E->d_hints + nhint;
+            d.prejs = E->d_prejs + nhint;
             nhint += u.mbw * u.mbh;
         }
         SL.intra[i] = is_intra[i];
@@ -504,7 +510,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
                 g_err = std::string("learned inference: ") + fdvl_last_error();
                 return -3;
             }
-            E->launches += 1;
+            launch_lrn_preskip(E->d_units, E->d_pu, (int)pu.size(), nhint, E->st);
+            E->launches += 2;
         }
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range,
                       !pu.empty(), E->st);
@@ -690,13 +697,29 @@ extern "C" int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long lon
     if (enable && !E->d_prof) {
         if (cudaMalloc(&E->d_prof, 32 * sizeof(unsigned long long)) != cudaSuccess) return -3;
         cudaMemset(E->d_prof, 0, 32 * sizeof(unsigned long long));
+        if (cudaMalloc(&E->d_tl, 2 * sizeof(unsigned long long) * E->total_mbs) != cudaSuccess) return -3;
+        cudaMemset(E->d_tl, 0, 2 * sizeof(unsigned long long) * E->total_mbs);
     }
     if (out32 && E->d_prof) {
         cudaMemcpy(out32, E->d_prof, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
         cudaMemset(E->d_prof, 0, 32 * sizeof(unsigned long long));
     }
-    if (!enable && E->d_prof) { cudaFree(E->d_prof); E->d_prof = nullptr; }
+    if (!enable && E->d_prof) {
+        cudaFree(E->d_prof); E->d_prof = nullptr;
+        cudaFree(E->d_tl); E->d_tl = nullptr;
+    }
     return 0;
+}
+
+// The last P-frame's per-macroblock timeline of unit u (phase profile on):
+// out[2 m] the end of macroblock m's wait, out[2 m + 1] its publication,
+// %globaltimer nanoseconds.
+extern "C" int fdvb_engine_timeline(fdvb_engine *E, int u, unsigned long long *out) {
+    if (!E || !E->d_tl || u < 0 || u >= (int)E->units.size() || !out) return -1;
+    const Unit &U = E->units[u];
+    if (cudaStreamSynchronize(E->st) != cudaSuccess) return -3;
+    return cudaMemcpy(out, E->d_tl + 2 * (size_t)U.mb_off, 2 * sizeof(unsigned long long) * U.mbw * U.mbh,
+                      cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : -3;
 }
 
 // Re-coding support (average-bitrate control codes a frame again, coarser,
@@ -742,6 +765,7 @@ extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, floa
         E->lnet = lrn_create(E->device, E->total_mbs, 0, 16, 16);
         if (!E->lnet) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
         if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * E->total_mbs));
+        if (!E->d_prejs) CK(cudaMalloc(&E->d_prejs, sizeof(float) * E->total_mbs));
         if (!E->d_pu) CK(cudaMalloc(&E->d_pu, sizeof(int2) * E->units.size()));
     }
     CK(cudaStreamSynchronize(E->st));

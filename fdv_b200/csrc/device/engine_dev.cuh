@@ -23,6 +23,13 @@ struct UnitDev {
     double skip_gate;           // a confident SKIP needs its RD cost <= skip_gate * lambda (<= 0: no gate)
     int inter8;                 // the confident-inter path also tries INTER8 (seeded, short searches)
     float *mbcost;              // per macroblock: RD cost of the chosen mode (NULL: off)
+    // per macroblock, from lrn_preskip_kernel (NULL: none): the RD cost of a
+    // confident SKIP with the zero vector that passed the gate, its
+    // reconstruction already written; -1 otherwise
+    const float *prejs;
+    // per macroblock, with the phase profile on (NULL: off): %globaltimer when
+    // its wait for the row above ended and when it published its progress
+    unsigned long long *tl;
 };
 
 // Phases of a macroblock, for the optional cycle profile.

@@ -63,6 +63,62 @@ void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ti
     k[v]<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
 }
 
+// The learned form's SKIP pre-analysis, one warp per macroblock of the P
+// units (pu: {unit, first macroblock}), between the inference and the
+// wavefront: a macroblock the network calls SKIP confidently gets the zero
+// vector's SKIP analysed here -- prediction, SSD, RD cost, the gate -- and,
+// when the gate passes, its reconstruction written and its cost kept in
+// prejs; the wavefront commits it without analysis when its merge list turns
+// out to be {zero vector on reference 0}, which gives the same SKIP
+// (pframe_kernel).  Otherwise prejs is -1.
+__global__ void __launch_bounds__(128) lrn_preskip_kernel(const UnitDev *__restrict__ units, const int2 *__restrict__ pu,
+                                                          int np, int total) {
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (gw >= total) return;
+    int k = 0;
+    while (k + 1 < np && gw >= pu[k + 1].y) ++k;
+    const UnitDev &U = units[pu[k].x];
+    const int m = gw - pu[k].y;
+    float *pj = const_cast<float *>(U.prejs) + m;
+    if (U.hint[m].cls != 0) {
+        if (lane == 0) *pj = -1.f;
+        return;
+    }
+    const int w = U.w, bx = (m % U.mbw) * 16, by = (m / U.mbw) * 16;
+    const RefPlanes &R = U.ref[0];
+    const int r = lane >> 1, c = (lane & 1) * 8;   // a lane: 8 samples of one row
+    const uint8_t *cp = U.cur[0] + (size_t)(by + r) * w + bx + c;
+    const uint8_t *rp = R.G + (long)(by + r) * R.ys + bx + c;
+    uint8_t pv[8];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        pv[i] = rp[i];
+        const int d = (int)cp[i] - (int)pv[i];
+        s += d * d;
+    }
+    s = __reduce_add_sync(FDVB_FULL, s);
+    const double Js = rd_cost((double)s, U.lambda, kBitsMode);   // one merge candidate: no index bits
+    if (!(U.skip_gate <= 0.0 || Js <= __dmul_rn(U.skip_gate, U.lambda))) {
+        if (lane == 0) *pj = -1.f;
+        return;
+    }
+    uint8_t *dr = U.rec[0] + (size_t)(by + r) * w + bx + c;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dr[i] = pv[i];
+    const int cw = w / 2, cbx = bx / 2, cby = by / 2;
+    for (int q = lane; q < 128; q += 32) {
+        const int pl = q >> 6, p = q & 63;
+        U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] =
+            (uint8_t)mc_cpx(pl ? R.V : R.U, R.cs, cbx + (p & 7), cby + (p >> 3), 0, 0);
+    }
+    if (lane == 0) *pj = (float)Js;
+}
+
+void launch_lrn_preskip(const UnitDev *units, const int2 *pu, int np, int total, cudaStream_t st) {
+    lrn_preskip_kernel<<<(total + 3) / 4, 128, 0, st>>>(units, pu, np, total);
+}
+
 void launch_refprep(const void *tasks, int ntasks, int maxw, int maxh, int border, cudaStream_t st) {
     if (border & 3) return;   // the kernels store 4 samples at a time from padded column 0
     dim3 blk(32, 8);
@@ -229,7 +285,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     u.slots = base + o_slots;
     u.lambda = fdvb_lambda(qp, lscale);
     u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1; u.prof = nullptr;
-    u.hint = nullptr; u.mbcost = nullptr; u.skip_gate = 0.0; u.inter8 = 0;
+    u.hint = nullptr; u.mbcost = nullptr; u.skip_gate = 0.0; u.inter8 = 0; u.prejs = nullptr; u.tl = nullptr;
     RowTask rows[8192 / 16];
     for (int r = 0; r < mbh; ++r) rows[r] = {0, r};
     DbTask db[3] = {{rec, w, h, qp}, {rec + (size_t)w * h, cw, ch, qp}, {rec + (size_t)w * h + (size_t)cw * ch, cw, ch, qp}};

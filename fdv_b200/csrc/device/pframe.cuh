@@ -79,6 +79,12 @@ struct PShared {
     short2 lmv[lrn::kMvHyp];     // learned proposals of this macroblock
     short2 lmv2[lrn::kMvHyp];    // the same doubled, for the second reference (two frames back)
     int lcls;                    // their confident class, -1: none
+    // learned form, indexed by macroblock parity (a fast macroblock has no
+    // barrier after its reads, so thread 0 may already write the next one's)
+    uint2 nbi[2][2];             // the above and above-right macroblock records
+    float pjs[2];                // prejs of the macroblock
+    int fast[2];                 // a pre-analysed zero-vector SKIP whose merge list is {0}
+    int rok[2];                  // row_ok
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -266,15 +272,66 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
             pc.start();
             cp_async_wait_all();   // this thread's strip and source copies; the barrier below publishes them
-            if (row > 0) {
-                if (tid == 0) S.row_ok = wait_at_least(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
-            } else if (tid == 0) S.row_ok = 1;
-            __syncthreads();
-            if (!S.row_ok) break;
-            if (WIN && mbx >= 1) win_fill(win, U, nref, mbx + 4, mbx + 4, wy0, wrows, tid);
+            const int par = mbx & 1;
+            if (LRN && U.prejs) {
+                if (tid == 0) {
+                    // The learned form's pre-analysed SKIPs: the zero vector is
+                    // what the merge list offers iff the left vector is zero
+                    // and the above / above-right macroblocks are not inter or
+                    // carry the zero vector on reference 0 (fdv.h:5711-5729).
+                    const float pjs = __ldcg(&U.prejs[row * mbw + mbx]);
+                    const int ok = row > 0 ? wait_progress(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns) : 1;
+                    uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
+                    for (int k = 0; k < 2; ++k)
+                        if (row > 0 && mbx + k < mbw)
+                            nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
+                    bool zero = pmvx == 0 && pmvy == 0;
+                    for (int k = 0; k < 2; ++k)
+                        if (((nb[k].y >> 8) & 0xffu) && (nb[k].x != 0 || (nb[k].y & 0xffu) != 0)) zero = false;
+                    S.nbi[par][0] = nb[0]; S.nbi[par][1] = nb[1];
+                    S.pjs[par] = pjs;
+                    S.fast[par] = pjs >= 0.f && zero;
+                    S.rok[par] = ok;
+                }
+                __syncthreads();
+            } else {
+                if (row > 0) {
+                    if (tid == 0) S.row_ok = wait_progress(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
+                } else if (tid == 0) S.row_ok = 1;
+                __syncthreads();
+            }
+            if (LRN && U.prejs ? !S.rok[par] : !S.row_ok) break;
+            const bool fast = LRN && U.prejs && S.fast[par];
+            if (WIN && mbx >= 1 && !fast) win_fill(win, U, nref, mbx + 4, mbx + 4, wy0, wrows, tid);
             pc.mark(PP_WAIT);
+            if (U.tl && tid == 0) U.tl[2 * (row * mbw + mbx)] = globaltimer();
             uint8_t *slot = U.slots + (size_t)(row * mbw + mbx) * kSlotBytes;
             if (tid < 16) slot_len(slot)[tid] = 0;
+            if (fast) {
+                // SKIP with the zero vector: reconstruction written ahead,
+                // the symbols and the record here (as the commit below)
+                __syncwarp();
+                if (tid == 0) {
+                    const int amode = row > 0 ? (int)((S.nbi[par][0].y >> 16) & 0xffu) : 0;
+                    uint8_t m0 = 0;
+                    write_slot_structs(slot, (prev_mode != 0 ? 2 : 0) + (amode != 0 ? 1 : 0), &m0, 1, err);
+                    MBInfo mi = {0, 0, 0, 1, 0, 0};
+                    U.mbi[row * mbw + mbx] = mi;
+                    if (U.mbcost) U.mbcost[row * mbw + mbx] = S.pjs[par];
+                    if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
+                    st_release_gpu(&U.progress[row], mbx + 1);
+                    if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
+                }
+                pmvx = 0; pmvy = 0;
+                prev_mode = 0;
+                // the reference window's next strip, after the publication
+                if (WIN && mbx >= 1) win_fill(win, U, nref, mbx + 4, mbx + 4, wy0, wrows, tid);
+                // this macroblock's source (landed: waited at the top) is not
+                // needed; the next one's goes into the same buffer
+                if (pf && mbx + 1 < mbw) prefetch(bx + 16, by);
+                pc.mark(PP_OUT);
+                continue;
+            }
             // ---- the macroblock, its current-frame neighbours, merge candidates
             if (tid < 64) {
                 const int r2 = tid >> 2, c2 = (tid & 3) * 4;
@@ -301,9 +358,13 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 // the above and above-right macroblock records (one 8-byte load
                 // each, issued together with the corner samples)
                 uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
-                for (int k = 0; k < 2; ++k)
-                    if (row > 0 && mbx + k < mbw)
-                        nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
+                if (LRN && U.prejs) {
+                    nb[0] = S.nbi[par][0]; nb[1] = S.nbi[par][1];
+                } else {
+                    for (int k = 0; k < 2; ++k)
+                        if (row > 0 && mbx + k < mbw)
+                            nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
+                }
                 S.ht = by > 0; S.hl = bx > 0;
                 S.tl = (by > 0 && bx > 0) ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
                 for (int pl = 0; pl < 2; ++pl)
@@ -362,8 +423,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 prev_mode = 0;
                 __syncthreads();
                 if (tid == 0) {
-                    __threadfence();
-                    atomicExch(&U.progress[row], mbx + 1);
+                    st_release_gpu(&U.progress[row], mbx + 1);
                 }
                 continue;
             }
@@ -727,8 +787,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             // barrier; the fence then orders them before the progress flag
             __syncthreads();
             if (tid == 0) {
-                __threadfence();
-                atomicExch(&U.progress[row], mbx + 1);
+                st_release_gpu(&U.progress[row], mbx + 1);
+                if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
             }
             pc.mark(PP_OUT);
         }

@@ -679,6 +679,7 @@ void fdvg_stats_reset(fdvg_ctx *g) { fdvb_engine_stats_reset(g); }
 void fdvg_set_wait_timeout_ns(fdvg_ctx *g, unsigned long long ns) { fdvb_engine_set_wait_ns(g, ns); }
 void fdvg_inject_stall(fdvg_ctx *g, int u, int row) { fdvb_engine_inject_stall(g, u, row); }
 int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out32) { return fdvb_engine_profile(g, enable, out32); }
+int fdvg_mb_timeline(fdvg_ctx *g, int u, unsigned long long *out) { return fdvb_engine_timeline(g, u, out); }
 
 int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf) {
     if (!g) { set_err("null context"); return -1; }

@@ -29,6 +29,7 @@ void fdvb_engine_stats_reset(fdvb_engine *E);
 void fdvb_engine_set_wait_ns(fdvb_engine *E, unsigned long long ns);
 void fdvb_engine_inject_stall(fdvb_engine *E, int unit, int row);
 int fdvb_engine_profile(fdvb_engine *E, int enable, unsigned long long *out32);
+int fdvb_engine_timeline(fdvb_engine *E, int u, unsigned long long *out);
 int fdvb_engine_set_learned(fdvb_engine *E, const float *params, float conf);
 int fdvb_engine_records(fdvb_engine *E, int enable);
 int fdvb_engine_learned_conf(fdvb_engine *E, const float *conf5);

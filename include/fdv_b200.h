@@ -219,6 +219,10 @@ void fdvg_inject_stall(fdvg_ctx *g, int u, int row);
  * 4x4 leaves, 8x8/16x16/32x32/64x64 leaves, CTU total, CTU count, 4x4 leaf
  * count). */
 int fdvg_phase_profile(fdvg_ctx *g, int enable, unsigned long long *out32);
+/* With the phase profile on: the last P-frame's timeline of unit u, two
+ * %globaltimer stamps (ns) per macroblock in raster order -- the end of its
+ * wait for the row above and its progress publication. */
+int fdvg_mb_timeline(fdvg_ctx *g, int u, unsigned long long *out);
 
 /* Allocation-free P-frame analysis of one unit.  No counterpart in the
  * reference.  For callers that cannot allocate device memory while they
