@@ -202,4 +202,22 @@ __device__ __forceinline__ bool wait_progress(const int *flag, int need, unsigne
     }
 }
 
+// A progress word with the count in bits 8 and up (and a payload below):
+// waits until the count reaches need and returns the observed word, or -1
+// after the limit or when another block has raised an error.
+__device__ __forceinline__ int wait_count(const int *flag, int need, unsigned *err, unsigned long long limit_ns) {
+    int v = ld_acquire_gpu(flag);
+    if ((v >> 8) >= need) return v;
+    const unsigned long long t0 = globaltimer();
+    for (unsigned i = 1;; ++i) {
+        v = ld_acquire_gpu(flag);
+        if ((v >> 8) >= need) return v;
+        if (!(i & 15)) {
+            if (*(volatile unsigned *)err) return -1;
+            if (globaltimer() - t0 > limit_ns) { atomicOr(err, kErrWaitTimeout); return -1; }
+        }
+        if (i > 256) __nanosleep(64);
+    }
+}
+
 }  // namespace fdvb

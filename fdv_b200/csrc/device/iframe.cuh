@@ -25,11 +25,14 @@
 #include <cooperative_groups.h>
 #include "common.cuh"
 #include "intra.cuh"
+#include "pred4_table.h"
 #include "residual.cuh"
 
 namespace fdvb {
 
 namespace cg = cooperative_groups;
+
+__device__ const P4Tab g_p4tab = make_p4tab();
 
 constexpr int INT = 512;              // threads per block
 constexpr int ICL = 4;                // blocks per cluster
@@ -135,6 +138,8 @@ struct ChainArea {
     double res_J[4];                      // per leaf size: the team's result (written by the team)
     int res_idx[4], res_mode[4];
     int abort, task, row_ok;
+    uint16_t p4[9 * 16];                  // the 4x4 prediction table (pred4_table.h)
+    int N4[3][14];                        // per screening warp: the neighbour vector
 };
 struct IShared {
     QP4 q;
@@ -278,35 +283,54 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     const int tx = bx - c.bx0, ty = by - c.by0;
     const int ht = by > 0, hl = bx > 0, htl = ht && hl;
     const int htr = ht && (bx + 4 < c.w) && cell_done(bx + 4, by - 1, bx, by);
-    // neighbours (gather_neighbors fdv.h:3689-3706), one copy per warp
-    int *T9 = C.T9w[w], *L5 = C.L5w[w];
-    if (lane < 8) T9[lane + 1] = ht ? ((lane < 4 || htr) ? TL(C, ty - 1, tx + lane) : TL(C, ty - 1, tx + 3)) : 0;
-    else if (lane < 12) L5[lane - 7] = hl ? TL(C, ty + lane - 8, tx - 1) : 0;
-    else if (lane == 12) { const int v = htl ? TL(C, ty - 1, tx - 1) : 128; T9[0] = v; L5[0] = v; }
-    __syncwarp();
-    {   // predictions and SATD (fdv.h:3803-3823)
-        const int l = lane & 15, i = l >> 2, j = l & 3, rb = lane & ~3, cb = (lane & 16) + j;
-        const int sv = C.src[(ty + i) * 64 + tx + j];
-        for (int pass = 0; pass < 2; ++pass) {
-            if (pass && w != 0) break;
-            const int m = pass ? 8 : 2 * w + (lane >> 4);
-            const int pv = mode_ok4(m, ht, htr, hl, htl) ? pred4_px(m, T9, L5, ht, hl, j, i) : 0;
-            C.cp[m][l] = (uint8_t)pv;
-            const int d = sv - pv;
-            const int x0 = __shfl_sync(FDVB_FULL, d, rb), x1 = __shfl_sync(FDVB_FULL, d, rb + 1);
-            const int x2 = __shfl_sync(FDVB_FULL, d, rb + 2), x3 = __shfl_sync(FDVB_FULL, d, rb + 3);
-            const int a0 = x0 + x1, a1 = x0 - x1, a2 = x2 + x3, a3 = x2 - x3;
-            const int hv = j == 0 ? a0 + a2 : (j == 1 ? a1 + a3 : (j == 2 ? a0 - a2 : a1 - a3));
-            const int y0 = __shfl_sync(FDVB_FULL, hv, cb), y1 = __shfl_sync(FDVB_FULL, hv, cb + 4);
-            const int y2 = __shfl_sync(FDVB_FULL, hv, cb + 8), y3 = __shfl_sync(FDVB_FULL, hv, cb + 12);
-            const int b0 = y0 + y1, b1 = y0 - y1, b2 = y2 + y3, b3 = y2 - y3;
-            int sa = abs(i == 0 ? b0 + b2 : (i == 1 ? b1 + b3 : (i == 2 ? b0 - b2 : b1 - b3)));
-            sa += __shfl_xor_sync(FDVB_FULL, sa, 8);
-            sa += __shfl_xor_sync(FDVB_FULL, sa, 4);
-            sa += __shfl_xor_sync(FDVB_FULL, sa, 2);
-            sa += __shfl_xor_sync(FDVB_FULL, sa, 1);
-            if (l == 0) C.csat[m] = sa;
+    // neighbours (gather_neighbors fdv.h:3689-3706), one copy per screening
+    // warp: N = L(3..0) T(-1) T(0..7) DC (pred4_table.h)
+    if (w < 3) {
+        int *N = C.N4[w];
+        int v = 0;
+        if (lane < 8) v = ht ? ((lane < 4 || htr) ? TL(C, ty - 1, tx + lane) : TL(C, ty - 1, tx + 3)) : 0;
+        else if (lane < 12) v = hl ? TL(C, ty + lane - 8, tx - 1) : 0;
+        else if (lane == 12) v = htl ? TL(C, ty - 1, tx - 1) : 128;
+        const int sT = __reduce_add_sync(FDVB_FULL, lane < 4 ? v : 0);
+        const int sL = __reduce_add_sync(FDVB_FULL, (lane >= 8 && lane < 12) ? v : 0);
+        if (lane < 8) N[5 + lane] = v;
+        else if (lane < 12) N[3 - (lane - 8)] = v;
+        else if (lane == 12) N[4] = v;
+        else if (lane == 13)
+            N[13] = (ht && hl) ? (sT + sL + 4) >> 3 : (ht ? (sT + 2) >> 2 : (hl ? (sL + 2) >> 2 : 128));
+        __syncwarp();
+        // predictions and SATD (fdv.h:3803-3823): 8 lanes per mode, modes
+        // 0-3 on warp 0, 4-7 on warp 1, 8 on warp 2; a lane holds two
+        // samples (row i, columns 2h and 2h + 1)
+        const int m = w < 2 ? 4 * w + (lane >> 3) : 8;
+        const int q = lane & 7, i = q >> 1, h = q & 1, x0 = 2 * h;
+        const uint16_t *op = &C.p4[m * 16 + i * 4 + x0];
+        const int p0 = p4_eval(op[0], N), p1 = p4_eval(op[1], N);
+        if (w < 2 || lane < 8) {
+            C.cp[m][i * 4 + x0] = (uint8_t)p0;
+            C.cp[m][i * 4 + x0 + 1] = (uint8_t)p1;
         }
+        const int d0 = C.src[(ty + i) * 64 + tx + x0] - p0, d1 = C.src[(ty + i) * 64 + tx + x0 + 1] - p1;
+        // row transform: columns (0, 1) on h = 0, (2, 3) on h = 1
+        const int s0 = d0 + d1, s1 = d0 - d1;
+        const int o0 = __shfl_xor_sync(FDVB_FULL, s0, 1), o1 = __shfl_xor_sync(FDVB_FULL, s1, 1);
+        int c0 = h ? o0 - s0 : s0 + o0, c1 = h ? o1 - s1 : s1 + o1;
+        // column transform over the rows: lanes q ^ 2 (rows i ^ 1), q ^ 4 (rows i ^ 2)
+        {
+            const int u0 = __shfl_xor_sync(FDVB_FULL, c0, 2), u1 = __shfl_xor_sync(FDVB_FULL, c1, 2);
+            c0 = (i & 1) ? u0 - c0 : c0 + u0;
+            c1 = (i & 1) ? u1 - c1 : c1 + u1;
+        }
+        {
+            const int u0 = __shfl_xor_sync(FDVB_FULL, c0, 4), u1 = __shfl_xor_sync(FDVB_FULL, c1, 4);
+            c0 = (i & 2) ? u0 - c0 : c0 + u0;
+            c1 = (i & 2) ? u1 - c1 : c1 + u1;
+        }
+        int sa = abs(c0) + abs(c1);
+        sa += __shfl_xor_sync(FDVB_FULL, sa, 1);
+        sa += __shfl_xor_sync(FDVB_FULL, sa, 2);
+        sa += __shfl_xor_sync(FDVB_FULL, sa, 4);
+        if (q == 0 && (w < 2 || lane < 8)) C.csat[m] = sa;
     }
     cbar();
     long long tp = prof_t0(c.prof, t);
@@ -665,6 +689,7 @@ iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ ta
         for (int k = 0; k < CS_NUM; ++k) c0[k] = isink_ccap(0, k);
         for (int i = 0; i < 4; ++i) cs_init(&S->H.sink[i], S->H.sinkmem[i], c0);
         for (int L = 0; L < 4; ++L) { C.done[L] = 0; C.issued[L] = 0; }
+        for (int k = 0; k < 9 * 16; ++k) C.p4[k] = g_p4tab.op[k];
         S->H.job.seq = 0;
     }
     int seen = 0;

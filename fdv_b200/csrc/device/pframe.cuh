@@ -85,6 +85,7 @@ struct PShared {
     float pjs[2];                // prejs of the macroblock
     int fast[2];                 // a pre-analysed zero-vector SKIP whose merge list is {0}
     int rok[2];                  // row_ok
+    int amz[2];                  // the above macroblock's mode is not SKIP
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -267,6 +268,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const typename LumaOf<WIN>::T L0 = luma_src<WIN>(U.ref[0], win, 0, wy0, wrows);
         const typename LumaOf<WIN>::T L1 = luma_src<WIN>(U.ref[1], win, nref - 1, wy0, wrows);
         int pmvx = 0, pmvy = 0, prev_mode = 0;
+        int pbits = 0;   // thread 0: the last published macroblock's progress bits
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
@@ -279,24 +281,52 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     // what the merge list offers iff the left vector is zero
                     // and the above / above-right macroblocks are not inter or
                     // carry the zero vector on reference 0 (fdv.h:5711-5729).
+                    // The row above's progress word describes its last two
+                    // macroblocks; when those are the two needed here, no
+                    // record has to be loaded.
                     const float pjs = __ldcg(&U.prejs[row * mbw + mbx]);
-                    const int ok = row > 0 ? wait_progress(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns) : 1;
+                    const int need = min(mbx + 2, mbw);
+                    const int v = row > 0 ? wait_count(&U.progress[row - 1], need, err, wait_ns) : 0;
+                    const int ok = v >= 0;
+                    const bool pz = pmvx == 0 && pmvy == 0;
+                    bool have = row == 0, zero = pz;
+                    int amz = 0;
+                    if (row > 0 && ok) {
+                        const int c = v >> 8;
+                        if (need == mbx + 2 && c == need) {          // macroblocks mbx, mbx + 1
+                            zero = pz && (v & 1) && (v & 4);
+                            amz = (v >> 3) & 1;
+                            have = true;
+                        } else if (need == mbw && c == mbw && mbx == mbw - 1) {   // mbx only (last column)
+                            zero = pz && (v & 1);
+                            amz = (v >> 1) & 1;
+                            have = true;
+                        }
+                    }
+                    bool fq = ok && pjs >= 0.f && have && zero;
                     uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
-                    for (int k = 0; k < 2; ++k)
-                        if (row > 0 && mbx + k < mbw)
-                            nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
-                    bool zero = pmvx == 0 && pmvy == 0;
-                    for (int k = 0; k < 2; ++k)
-                        if (((nb[k].y >> 8) & 0xffu) && (nb[k].x != 0 || (nb[k].y & 0xffu) != 0)) zero = false;
+                    if (ok && !fq && row > 0) {
+                        for (int k = 0; k < 2; ++k)
+                            if (mbx + k < mbw)
+                                nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
+                        if (!have) {
+                            zero = pz;
+                            for (int k = 0; k < 2; ++k)
+                                if (((nb[k].y >> 8) & 0xffu) && (nb[k].x != 0 || (nb[k].y & 0xffu) != 0)) zero = false;
+                            amz = ((nb[0].y >> 16) & 0xffu) != 0;
+                            fq = pjs >= 0.f && zero;
+                        }
+                    }
                     S.nbi[par][0] = nb[0]; S.nbi[par][1] = nb[1];
                     S.pjs[par] = pjs;
-                    S.fast[par] = pjs >= 0.f && zero;
+                    S.fast[par] = fq;
+                    S.amz[par] = amz;
                     S.rok[par] = ok;
                 }
                 __syncthreads();
             } else {
                 if (row > 0) {
-                    if (tid == 0) S.row_ok = wait_progress(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns);
+                    if (tid == 0) S.row_ok = wait_count(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns) >= 0;
                 } else if (tid == 0) S.row_ok = 1;
                 __syncthreads();
             }
@@ -312,14 +342,14 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 // the symbols and the record here (as the commit below)
                 __syncwarp();
                 if (tid == 0) {
-                    const int amode = row > 0 ? (int)((S.nbi[par][0].y >> 16) & 0xffu) : 0;
                     uint8_t m0 = 0;
-                    write_slot_structs(slot, (prev_mode != 0 ? 2 : 0) + (amode != 0 ? 1 : 0), &m0, 1, err);
+                    write_slot_structs(slot, (prev_mode != 0 ? 2 : 0) + S.amz[par], &m0, 1, err);
                     MBInfo mi = {0, 0, 0, 1, 0, 0};
                     U.mbi[row * mbw + mbx] = mi;
                     if (U.mbcost) U.mbcost[row * mbw + mbx] = S.pjs[par];
                     if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
-                    st_release_gpu(&U.progress[row], mbx + 1);
+                    st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | 1 | (pbits << 2));
+                    pbits = 1;
                     if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
                 }
                 pmvx = 0; pmvy = 0;
@@ -423,7 +453,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 prev_mode = 0;
                 __syncthreads();
                 if (tid == 0) {
-                    st_release_gpu(&U.progress[row], mbx + 1);
+                    st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | 1 | (pbits << 2));
+                    pbits = 1;
                 }
                 continue;
             }
@@ -787,7 +818,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             // barrier; the fence then orders them before the progress flag
             __syncthreads();
             if (tid == 0) {
-                st_release_gpu(&U.progress[row], mbx + 1);
+                // the count, and for the row below: this macroblock's and the
+                // previous one's (zero-vector-compatible, not SKIP) bits
+                const int zb = ((!info.inter || (info.x == 0 && info.y == 0 && info.ref == 0)) ? 1 : 0) |
+                               (chosen != 0 ? 2 : 0);
+                st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | zb | (pbits << 2));
+                pbits = zb;
                 if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
             }
             pc.mark(PP_OUT);
