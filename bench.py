@@ -668,6 +668,12 @@ def main() -> None:
             traffic = json.load(f).get("dram_bytes_per_launch")
     except OSError:
         pass
+    int_pipe = None   # the integer-pipe utilisation of the same kernel, from one ncu capture
+    try:
+        with open(os.path.join(ROOT, "profiles", "pframe_kernel_hd720_pipes.json")) as f:
+            int_pipe = json.load(f)
+    except OSError:
+        pass
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -703,7 +709,8 @@ def main() -> None:
                          "kernel": "pframe_kernel", "peak_source": peak_src,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": round(pk_avg_s * 1e3, 4),
-                         "note": "latency-bound wavefront; HBM is not the limiter"},
+                         "note": "latency-bound wavefront; HBM is not the limiter",
+                         "int_pipe": int_pipe},
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": round(e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": NF * FSIZE,
