@@ -490,8 +490,9 @@ def run_learned(local: int) -> dict:
         "bd_rate_pct": None if ev["bd_rate_pct"] is None else round(ev["bd_rate_pct"], 4),
         "rd_points": ev["points"],
         "setting": {"skip_conf": LEARN_CONF, "skip_gate_lambda": 400,
-                    "inter_conf": 0.9, "inter_path": "nearest-reference 16x16 and INTER8, seeded, 4 diamond steps",
-                    "intra": "full search", "other_mbs": "full search seeded with the proposals"},
+                    "inter_conf": LEARN_CONF, "inter_path": "nearest-reference 16x16 and INTER8, seeded, 4 diamond steps",
+                    "intra_conf": LEARN_CONF, "intra_path": "intra analysis only",
+                    "other_mbs": "full search seeded with the proposals"},
         "workload": f"learned: 1280x720, {LEARN_NF} frames (1 key), QP {LEARN_QP}, range 16, 6 moving rectangles "
                     f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, 20 frames",
         "weights": "fdv_b200/proposal_c4.f32",

@@ -753,7 +753,6 @@ extern "C" int fdvb_engine_commit_refs(fdvb_engine *E) {
 // candidate costs around 100-300 lambda, a wrongly predicted SKIP over moving
 // content far more.
 constexpr double kLearnSkipGate = 400.0;
-constexpr float kLearnInterConf = 0.9f;
 extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, float conf) {
     if (!E) return -1;
     CK(cudaSetDevice(E->device));
@@ -770,10 +769,10 @@ extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, floa
     }
     CK(cudaStreamSynchronize(E->st));
     if (fdvl_set_params(E->lnet, params) != 0) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
-    // the product setting: SKIP narrowing at `conf` behind the RD-cost gate;
-    // inter narrowing at kLearnInterConf, INTER8 kept; intra keeps the full
-    // search (every full search seeded with the proposals)
-    E->lconf = make_float3(conf, kLearnInterConf, 2.f);
+    // the product setting: every class narrowed at `conf` (SKIP behind the
+    // RD-cost gate, inter keeping INTER8); every full search seeded with the
+    // proposals
+    E->lconf = make_float3(conf, conf, conf);
     E->lgate = kLearnSkipGate;
     E->linter8 = 1;
     return 0;

@@ -38,7 +38,10 @@ constexpr int INT = 512;              // threads per block
 constexpr int ICL = 4;                // blocks per cluster
 constexpr int kTileW = 129;           // tile columns: x in [-1, 127] relative to the CTU
 constexpr int kChainNT = 128;         // chain threads (block 0, warps 0-3)
-constexpr int kH8NT = INT - kChainNT; // 8x8 leaf team (block 0, warps 4-15)
+// 8x8 leaf team (block 0, warps 4-11).  Warps 12-15 of block 0 stay idle:
+// the chain shares its SM with the team, and fewer team warps leave it more
+// issue slots (the team still finishes a job before the chain needs it).
+constexpr int kH8NT = 256;
 enum { BAR_CHAIN = 1, BAR_H8 = 2, BAR_TEAM = 3 };
 
 // Stream ids of the intra path (fdv.h:4273-4289).
@@ -705,7 +708,7 @@ iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ ta
         __syncthreads();
         if (rank == 0) {
             if (tid < kChainNT) chain_row(S, P, tasks[t].row, err, wait_ns, hlimit);
-            else team_loop<kH8NT, BAR_H8>(S, P, 3, err, hlimit, tid - kChainNT, seen);
+            else if (tid < kChainNT + kH8NT) team_loop<kH8NT, BAR_H8>(S, P, 3, err, hlimit, tid - kChainNT, seen);
         } else {
             team_loop<INT, BAR_TEAM>(S, P, 3 - rank, err, hlimit, tid, seen);
         }

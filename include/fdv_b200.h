@@ -348,8 +348,8 @@ int fdvl_gemm(int device, int M, int N, int K, const uint16_t *A, const uint16_t
  * params: fdvl_nparams() floats; NULL turns proposals off.  This call sets
  * the product configuration: the SKIP class at threshold `conf`, taken only
  * while the best merge candidate's RD cost is at most 400 lambda; the inter
- * class at 0.9, its narrowed analysis keeping INTER8 (four seeded, shortened
- * 8x8 searches); intra always on the full search.  Every full search starts
+ * class at `conf` too, its narrowed analysis keeping INTER8 (four seeded,
+ * shortened 8x8 searches); the intra class at `conf`.  Every full search starts
  * its motion searches from the proposed vectors too (doubled for the second
  * reference).  fdvg_set_learned_conf changes it. */
 int fdvg_set_learned(fdvg_ctx *g, const float *params, float conf);
