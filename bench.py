@@ -675,6 +675,22 @@ def main() -> None:
             int_pipe = json.load(f)
     except OSError:
         pass
+    # the integer-op roofline SURVEY-style: algorithmic ops of one P-frame (all
+    # bands), counted by the op-counting build of the CPU restatement
+    # (python -m oracle.opcount), over the live launch time, against a nominal
+    # peak of 148 SMs x 128 int32 lanes per clock at the maximum SM clock
+    int_ops = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "pframe_ops_hd720.json")) as f:
+            ops = json.load(f)["ops_per_pframe"]
+        mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
+        peak_t = 148 * 128 * mhz * 1e6 / 1e12
+        ach_t = ops / pk_avg_s / 1e12
+        int_ops = {"ops_per_launch": ops, "achieved": round(ach_t, 4), "peak": round(peak_t, 2), "unit": "Tops/s",
+                   "frac": round(ach_t / peak_t, 5), "peak_basis": "148 SMs x 128 int32 lanes/clock at sm_max_mhz",
+                   "source": "profiles/pframe_ops_hd720.json"}
+    except (OSError, KeyError, ValueError):
+        pass
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -711,7 +727,7 @@ def main() -> None:
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": round(pk_avg_s * 1e3, 4),
                          "note": "latency-bound wavefront; HBM is not the limiter",
-                         "int_pipe": int_pipe},
+                         "int_pipe": int_pipe, "int_ops": int_ops},
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": round(e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": NF * FSIZE,

@@ -31,6 +31,34 @@
 enum { PS_REF_ = 4, PS_MVX_ = 5, PS_MVY_ = 6, PS_SUB_ = 7, PS_MERGE_ = 8 };
 enum { IS_SPLIT0_ = 0, IS_MODEB_ = 4, IS_MODE0_ = 5, IS_MODE1_ = 6 };
 
+/* ----------------------------------------------------------- op count -- */
+/* With -DORACLE_OPCOUNT (a separate build, oracle/opcount.py) every primitive
+ * adds its integer-op cost to a category: the algorithmic op count of a frame
+ * for the integer-pipe roofline.  Costs per call (byte-lane ops count once
+ * per lane): SAD 2 per pixel (absolute difference, accumulate); luma MC per
+ * sample by phase (copy 1, a half-pel 6-tap sample 12, the centre j 66, a
+ * quarter-pel mean 2 plus its sources); chroma MC 10 per sample; 4x4
+ * transform 64 each way; 4x4 quantisation 64, dequantisation 32; an RDOQ
+ * truncation trial 48 (plus its dequantisation and inverse transform); 8x8
+ * transform 2048 each way (two 8x8x8 multiply-accumulate passes); 8x8
+ * quantisation 256, dequantisation 128; 4x4 SATD 112; intra prediction 3 per
+ * sample; residual, reconstruction and SSD 5 per pixel; a deblocking edge
+ * sample 20.  The normal build compiles all of it away. */
+#ifdef ORACLE_OPCOUNT
+enum { OPC_SAD, OPC_MC, OPC_SATD, OPC_TR4, OPC_Q4, OPC_RDOQ, OPC_TR8, OPC_Q8, OPC_PIX, OPC_INTRA, OPC_DBK, OPC_N };
+static unsigned long long g_opc[OPC_N];
+#define OPC(k, n) (g_opc[k] += (unsigned long long)(n))
+int oracle_opcount(unsigned long long *out, int reset) {
+    for (int k = 0; k < OPC_N; ++k) {
+        if (out) out[k] = g_opc[k];
+        if (reset) g_opc[k] = 0;
+    }
+    return OPC_N;
+}
+#else
+#define OPC(k, n) ((void)0)
+#endif
+
 /* ------------------------------------------------------------ helpers -- */
 static int clipb(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
 static int iabs(int v) { return v < 0 ? -v : v; }
@@ -74,11 +102,13 @@ static void inv_1d(const int *in, int *out) {
     out[0] = z0 + z3; out[1] = z1 + z2; out[2] = z1 - z2; out[3] = z0 - z3;
 }
 void oracle_fdct4x4(const int16_t r[16], int32_t c[16]) {
+    OPC(OPC_TR4, 64);
     int t[16], a[4], b[4];
     for (int i = 0; i < 4; ++i) { for (int j = 0; j < 4; ++j) a[j] = r[i * 4 + j]; fwd_1d(a, b); for (int j = 0; j < 4; ++j) t[i * 4 + j] = b[j]; }
     for (int j = 0; j < 4; ++j) { for (int i = 0; i < 4; ++i) a[i] = t[i * 4 + j]; fwd_1d(a, b); for (int i = 0; i < 4; ++i) c[i * 4 + j] = b[i]; }
 }
 void oracle_idct4x4(const int32_t d[16], int16_t r[16]) {
+    OPC(OPC_TR4, 64);
     int t[16], a[4], b[4];
     for (int i = 0; i < 4; ++i) { for (int j = 0; j < 4; ++j) a[j] = d[i * 4 + j]; inv_1d(a, b); for (int j = 0; j < 4; ++j) t[i * 4 + j] = b[j]; }
     for (int j = 0; j < 4; ++j) { for (int i = 0; i < 4; ++i) a[i] = t[i * 4 + j]; inv_1d(a, b); for (int i = 0; i < 4; ++i) r[i * 4 + j] = (int16_t)((b[i] + 32) >> 6); }
@@ -95,6 +125,7 @@ static int pos_class(int idx) {
     return 2;
 }
 void oracle_quant4x4(const int32_t c[16], int16_t l[16], int qp) {              /* fdv.h:2430 */
+    OPC(OPC_Q4, 64);
     int m = qp % 6, qbits = 15 + qp / 6, f = (1 << qbits) / 3;
     for (int i = 0; i < 16; ++i) {
         int w = c[i], sign = w < 0 ? -1 : 1;
@@ -103,6 +134,7 @@ void oracle_quant4x4(const int32_t c[16], int16_t l[16], int qp) {              
     }
 }
 void oracle_dequant4x4(const int16_t l[16], int32_t d[16], int qp) {            /* fdv.h:2546 */
+    OPC(OPC_Q4, 32);
     int m = qp % 6, sh = qp / 6;
     for (int i = 0; i < 16; ++i) d[i] = (int32_t)(l[i] * DQV[m][pos_class(i)]) * (int32_t)(1 << sh);
 }
@@ -122,6 +154,7 @@ void oracle_rdoq4x4(int16_t level[16], const int16_t res[16], int qp, double lam
             oracle_dequant4x4(trial, dc, qp);
             oracle_idct4x4(dc, rr);
             int64_t D = 0;
+            OPC(OPC_RDOQ, 48);
             for (int i = 0; i < 16; ++i) { int d = res[i] - rr[i]; D += (int64_t)d * d; }
             double J = (double)D + lambda * bits;
             if (bestJ < 0.0 || J < bestJ) { bestJ = J; bestL = L; }
@@ -150,28 +183,33 @@ void oracle_c8_tables(int32_t c8[64], int32_t q[52]) {
     for (int i = 0; i < 52; ++i) q[i] = QSTEP8[i];
 }
 void oracle_fdct8x8(const int16_t X[64], int32_t Y[64]) {
+    OPC(OPC_TR8, 2048);
     c8_init();
     int32_t A[64];
     for (int u = 0; u < 8; ++u) for (int x = 0; x < 8; ++x) { int32_t s = 0; for (int y = 0; y < 8; ++y) s += C8[u][y] * (int32_t)X[y * 8 + x]; A[u * 8 + x] = s; }
     for (int u = 0; u < 8; ++u) for (int v = 0; v < 8; ++v) { int32_t s = 0; for (int x = 0; x < 8; ++x) s += A[u * 8 + x] * C8[v][x]; Y[u * 8 + v] = s; }
 }
 void oracle_idct8x8(const int32_t Y[64], int16_t X[64]) {
+    OPC(OPC_TR8, 2048);
     c8_init();
     int64_t B[64];
     for (int y = 0; y < 8; ++y) for (int v = 0; v < 8; ++v) { int64_t s = 0; for (int u = 0; u < 8; ++u) s += (int64_t)C8[u][y] * Y[u * 8 + v]; B[y * 8 + v] = s; }
     for (int y = 0; y < 8; ++y) for (int x = 0; x < 8; ++x) { int64_t s = 0; for (int v = 0; v < 8; ++v) s += B[y * 8 + v] * C8[v][x]; X[y * 8 + x] = (int16_t)((s + ((int64_t)1 << 35)) >> 36); }
 }
 void oracle_quant8x8(const int32_t Y[64], int16_t l[64], int qp) {
+    OPC(OPC_Q8, 256);
     c8_init();
     int32_t q = QSTEP8[qp], f = q / 3;
     for (int i = 0; i < 64; ++i) { int32_t c = Y[i]; int sign = c < 0 ? -1 : 1; int32_t a = c < 0 ? -c : c; l[i] = (int16_t)(sign * ((a + f) / q)); }
 }
 void oracle_dequant8x8(const int16_t l[64], int32_t Y[64], int qp) {
+    OPC(OPC_Q8, 128);
     c8_init();
     int32_t q = QSTEP8[qp];
     for (int i = 0; i < 64; ++i) { int64_t v = (int64_t)l[i] * q; Y[i] = v < INT32_MIN ? INT32_MIN : (v > INT32_MAX ? INT32_MAX : (int32_t)v); }
 }
 int oracle_satd4x4(const uint8_t *src, int ss, const uint8_t *pred) {         /* fdv.h:3803 */
+    OPC(OPC_SATD, 112);
     int d[16];
     for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) d[i * 4 + j] = src[i * ss + j] - pred[i * 4 + j];
     for (int i = 0; i < 4; ++i) {
@@ -189,6 +227,7 @@ int oracle_satd4x4(const uint8_t *src, int ss, const uint8_t *pred) {         /*
 /* -------------------------------------------------------------- intra -- */
 void oracle_intra4x4(int mode, const uint8_t top[8], const uint8_t left[4], uint8_t tl,
                      int ht, int hl, uint8_t pred[16]) {                        /* fdv.h:2698 */
+    OPC(OPC_INTRA, 48);
     int Tn[9], Ln[5];
     Tn[0] = tl; for (int i = 0; i < 8; ++i) Tn[i + 1] = top[i];
     Ln[0] = tl; for (int i = 0; i < 4; ++i) Ln[i + 1] = left[i];
@@ -245,6 +284,7 @@ static int nn_mode_ok(int m, int n, int ht, int hl) {                           
 }
 void oracle_intra_nxn(int mode, const uint8_t *top, const uint8_t *left, uint8_t tl,
                       int n, int ht, int hl, uint8_t *pred) {                   /* fdv.h:2851-2910 */
+    OPC(OPC_INTRA, 3 * n * n);
     if (mode == 3 && nn_mode_ok(3, n, ht, hl)) {
         int half = n / 2, H = 0, V = 0;
         for (int k = 1; k <= half; ++k) {
@@ -313,10 +353,15 @@ static int interp(const cplane *r, int x, int y, int fx, int fy) {
 }
 static void mc_luma(const cplane *r, int bx, int by, int bw, int bh, int mvx, int mvy, uint8_t *dst, int ds) {
     int fx = mvx & 3, fy = mvy & 3, ix = bx + (mvx >> 2), iy = by + (mvy >> 2);
+#ifdef ORACLE_OPCOUNT
+    static const int kPhaseOps[16] = {1, 15, 12, 15, 15, 26, 80, 26, 12, 80, 66, 80, 15, 26, 80, 26};
+    OPC(OPC_MC, kPhaseOps[fy * 4 + fx] * bw * bh);
+#endif
     for (int i = 0; i < bh; ++i) for (int j = 0; j < bw; ++j) dst[i * ds + j] = (uint8_t)interp(r, ix + j, iy + i, fx, fy);
 }
 static void mc_chroma(const cplane *r, int bx, int by, int bw, int bh, int mvx, int mvy, uint8_t *dst, int ds) { /* :3260 */
     int fx = mvx & 3, fy = mvy & 3, ix = bx + (mvx >> 2), iy = by + (mvy >> 2);
+    OPC(OPC_MC, 10 * bw * bh);
     for (int i = 0; i < bh; ++i) for (int j = 0; j < bw; ++j) {
         int a = PX(r, ix + j, iy + i), b = PX(r, ix + j + 1, iy + i), c = PX(r, ix + j, iy + i + 1), d = PX(r, ix + j + 1, iy + i + 1);
         int top = a * (4 - fx) + b * fx, bot = c * (4 - fx) + d * fx;
@@ -336,6 +381,7 @@ void oracle_mc_chroma(const uint8_t *plane, int w, int h, int stride, int bx, in
 static int block_sad(const uint8_t *cur, int cs, const cplane *r, int bx, int by, int bw, int bh, int mvx, int mvy) { /* :3321 */
     uint8_t pred[256];
     mc_luma(r, bx, by, bw, bh, mvx, mvy, pred, bw);
+    OPC(OPC_SAD, 2 * bw * bh);
     int sad = 0;
     for (int i = 0; i < bh; ++i) for (int j = 0; j < bw; ++j) sad += iabs(cur[(size_t)(by + i) * cs + bx + j] - pred[i * bw + j]);
     return sad;
@@ -386,6 +432,7 @@ int oracle_me_search(const uint8_t *cur, int cs, const uint8_t *ref, int w, int 
 
 /* ------------------------------------------------------------ deblock -- */
 static void filter_edge(uint8_t *a, int step, int alpha, int beta, int tc) {    /* fdv.h:3491 */
+    OPC(OPC_DBK, 20);
     int p1 = a[-2 * step], p0 = a[-step], q0 = a[0], q1 = a[step];
     if (iabs(p0 - q0) < alpha && iabs(p1 - p0) < beta && iabs(q1 - q0) < beta) {
         int d = ((q0 - p0) * 4 + (p1 - q1) + 4) >> 3;
@@ -416,6 +463,7 @@ static void code_block4(const uint8_t *cur, int cs, int cx, int cy, const uint8_
                         uint8_t *rec, int rs, int rx, int ry, int qp, double lambda, cw_t *w, double *D, int *bits) {
     int16_t res[16], level[16], rr[16]; int32_t co[16], dc[16];
     const uint8_t *cb = &cur[(size_t)cy * cs + cx], *pb = &pred[(size_t)py * ps + px];
+    OPC(OPC_PIX, 5 * 16);
     for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) res[i * 4 + j] = (int16_t)(cb[i * cs + j] - pb[i * ps + j]);
     oracle_fdct4x4(res, co);
     oracle_quant4x4(co, level, qp);
@@ -457,6 +505,7 @@ static void code_residual(const uint8_t *cur, int cs, int ox, int oy, const uint
                     code_block4(cur, cs, ox + rx + sx, oy + ry + sy, pred, n, rx + sx, ry + sy, recA, 8, sx, sy, qp, lambda, &wA, &eA, &bA);
             int16_t res8[64], lev8[64], rr8[64]; int32_t co8[64], dc8[64];
             const uint8_t *cB = &cur[(size_t)(oy + ry) * cs + ox + rx], *pB = &pred[(size_t)ry * n + rx];
+            OPC(OPC_PIX, 5 * 64);
             for (int i = 0; i < 8; ++i) for (int j = 0; j < 8; ++j) res8[i * 8 + j] = (int16_t)(cB[i * cs + j] - pB[i * n + j]);
             oracle_fdct8x8(res8, co8);
             oracle_quant8x8(co8, lev8, qp);
@@ -511,6 +560,7 @@ static void chroma_block(const uint8_t *cur, uint8_t *rec, int cw, const cplane 
     for (int sy = 0; sy < 8; sy += 4)
         for (int sx = 0; sx < 8; sx += 4, ++bi) {
             int16_t res[16], rres[16]; int32_t co[16], dc[16];
+            OPC(OPC_PIX, 3 * 16);   /* residual and reconstruction */
             for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j)
                 res[i * 4 + j] = (int16_t)(cur[(cby + sy + i) * cw + cbx + sx + j] - pred[(sy + i) * 8 + sx + j]);
             oracle_fdct4x4(res, co);
@@ -657,6 +707,7 @@ static void pframe(ounit_t *u, const uint8_t *cy, const uint8_t *cu, const uint8
                 uint8_t tp[256];
                 mc_luma(&rY[cand[mi].ref], bx, by, 16, 16, cand[mi].x, cand[mi].y, tp, 16);
                 int32_t e = 0;
+                OPC(OPC_PIX, 3 * 256);   /* SSD */
                 for (int i = 0; i < 16; ++i) for (int j = 0; j < 16; ++j) { int d = cy[(by + i) * w + bx + j] - tp[i * 16 + j]; e += d * d; }
                 if (mi == 0 || e < Ds_i) { Ds_i = e; best_mi = mi; memcpy(pred_s, tp, 256); }
             }
@@ -901,6 +952,7 @@ static double intra_leaf4(ictx_t *x, int bx, int by, int *mode_out, cw_t *cw) { 
         if (c > 0 && qp >= 12 && (int64_t)cs[c] * 4 > (int64_t)cs[0] * 5) break;
         const uint8_t *pred = cp[c];
         int16_t res[16], level[16], rres[16]; int32_t co[16], dc[16];
+        OPC(OPC_PIX, 5 * 16);
         for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) res[i * 4 + j] = (int16_t)(sblk[i * stride + j] - pred[i * 4 + j]);
         oracle_fdct4x4(res, co);
         oracle_quant4x4(co, level, qp);
@@ -917,6 +969,7 @@ static double intra_leaf4(ictx_t *x, int bx, int by, int *mode_out, cw_t *cw) { 
     }
     int16_t res[16], level[16], rres[16]; int32_t co[16], dc[16];
     const uint8_t *pred = cp[best_c];
+    OPC(OPC_PIX, 5 * 16);
     for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) res[i * 4 + j] = (int16_t)(sblk[i * stride + j] - pred[i * 4 + j]);
     oracle_fdct4x4(res, co);
     oracle_quant4x4(co, level, qp);

@@ -241,3 +241,33 @@ def test_oracle_stream_equals_reference_live(built, golden):
                             f[w * sc["h"] * 5 // 4:].reshape(sc["h"] // 2, w // 2)[:bh // 2].ravel()]) for f in fr]
     ours = O.oracle_video_stream(band, w, bh, e["qp"], e["keyint"], e["search_range"])
     assert ours == O.ref_video_encode(band, w, bh, e["qp"], e["keyint"], e["search_range"])
+
+
+def test_opcount_build_counts_every_category():
+    """The op-counting build of the restatement (oracle.opcount) counts a P-frame's
+    searches, compensation, transforms and pixels; the normal build has no counter."""
+    import ctypes as C
+    import fdv_b200 as F
+    import oracle as O
+    import oracle.opcount as OC
+    path = OC.build_counting()
+    L = C.CDLL(path)
+    L.oracle_opcount.argtypes = [C.POINTER(C.c_ulonglong), C.c_int]
+    assert not hasattr(O.restatement(), "oracle_opcount")
+    saved, O._orc = O._orc, None
+    p0 = O._build.oracle_lib_path
+    O._build.oracle_lib_path = lambda: path
+    try:
+        u = O.OracleUnit(64, 48, 16)
+        fr = F.Scene(64, 48, 2, nrects=3, pan_qx=5, rect_max=24, seed=7).frames(2)
+        buf = (C.c_ulonglong * len(OC.CATS))()
+        u.frame(fr[0], 1, 24)
+        O._orc.oracle_opcount(buf, 1)
+        u.frame(fr[1], 0, 24)
+        O._orc.oracle_opcount(buf, 1)
+        got = dict(zip(OC.CATS, list(buf)))
+    finally:
+        O._build.oracle_lib_path = p0
+        O._orc = saved
+    for k in ("sad", "mc", "transform4", "quant4", "pixel", "deblock"):
+        assert got[k] > 0, k
