@@ -798,7 +798,24 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             }
             __syncthreads();
             pc.mark(PP_COMMIT);
-            // ---- coefficient streams of the chosen mode into the slot
+            prev_mode = chosen;
+            if (tid == 0) {
+                U.mbi[row * mbw + mbx] = info;
+                if (U.mbcost) U.mbcost[row * mbw + mbx] = (float)Jc;
+                // Publish now: the row below reads the reconstruction (ordered
+                // before this release by the barrier above) and the record,
+                // never the symbol slot.  The word also carries, for the row
+                // below, this macroblock's and the previous one's
+                // (zero-vector-compatible, not SKIP) bits.
+                const int zb = ((!info.inter || (info.x == 0 && info.y == 0 && info.ref == 0)) ? 1 : 0) |
+                               (chosen != 0 ? 2 : 0);
+                st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | zb | (pbits << 2));
+                pbits = zb;
+                if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
+            }
+            // ---- coefficient streams of the chosen mode into the slot (read
+            // after the kernel; the sinks are reset only after the next
+            // macroblock's first barrier)
             if (chosen != 0) {
                 for (int k = 0; k < CS_NUM; ++k) {
                     int n = M->len[k];
@@ -808,23 +825,6 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     for (int i = tid; i < n; i += PNT) d[i] = s[i];
                     if (tid == 0) slot_len(slot)[PS_CN + k] = (uint16_t)n;
                 }
-            }
-            if (tid == 0) {
-                U.mbi[row * mbw + mbx] = info;
-                if (U.mbcost) U.mbcost[row * mbw + mbx] = (float)Jc;
-            }
-            prev_mode = chosen;
-            // the block's writes are ordered before thread 0's fence by the
-            // barrier; the fence then orders them before the progress flag
-            __syncthreads();
-            if (tid == 0) {
-                // the count, and for the row below: this macroblock's and the
-                // previous one's (zero-vector-compatible, not SKIP) bits
-                const int zb = ((!info.inter || (info.x == 0 && info.y == 0 && info.ref == 0)) ? 1 : 0) |
-                               (chosen != 0 ? 2 : 0);
-                st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | zb | (pbits << 2));
-                pbits = zb;
-                if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
             }
             pc.mark(PP_OUT);
         }
