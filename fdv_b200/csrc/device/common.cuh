@@ -202,6 +202,33 @@ __device__ __forceinline__ bool wait_progress(const int *flag, int need, unsigne
     }
 }
 
+// 64-bit progress words (count in bits 0-11, a payload above).
+__device__ __forceinline__ unsigned long long ld_acquire_gpu64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// Waits until the count reaches need; returns the observed word, or ~0ull
+// after the limit or when another block has raised an error.
+__device__ __forceinline__ unsigned long long wait_count64(const unsigned long long *flag, int need, unsigned *err,
+                                                           unsigned long long limit_ns) {
+    unsigned long long v = ld_acquire_gpu64(flag);
+    if ((int)(v & 0xfffu) >= need) return v;
+    const unsigned long long t0 = globaltimer();
+    for (unsigned i = 1;; ++i) {
+        v = ld_acquire_gpu64(flag);
+        if ((int)(v & 0xfffu) >= need) return v;
+        if (!(i & 15)) {
+            if (*(volatile unsigned *)err) return ~0ull;
+            if (globaltimer() - t0 > limit_ns) { atomicOr(err, kErrWaitTimeout); return ~0ull; }
+        }
+        if (i > 256) __nanosleep(64);
+    }
+}
+
 // A progress word with the count in bits 8 and up (and a payload below):
 // waits until the count reaches need and returns the observed word, or -1
 // after the limit or when another block has raised an error.

@@ -207,7 +207,7 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     CK(cudaMalloc(&u.mbi, sizeof(MBInfo) * nmb));
     CK(cudaMalloc(&u.slots, (size_t)kSlotBytes * nmb));
     u.pw[0] = w; u.ph[0] = h; u.pw[1] = u.pw[2] = u.cw; u.ph[1] = u.ph[2] = u.ch;
-    int nprog = u.mbh;
+    int nprog = 2 * u.mbh;   // P-frame rows: one 64-bit progress word each
     for (int p = 0; p < 3; ++p) {
         u.icols[p] = (u.pw[p] + 63) / 64; u.irows[p] = (u.ph[p] + 63) / 64;
         nprog += u.irows[p];
@@ -456,7 +456,7 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
             CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[si], u.out_cap, u.hist_d[si]};
             cmp.push_back(c);
         } else {
-            int prog = u.mbh;
+            int prog = 2 * u.mbh;
             for (int p = 0; p < 3; ++p) {
                 IPlaneDevH P;
                 P.src = d.cur[p]; P.rec = d.rec[p]; P.mmap = u.mmap[p]; P.progress = u.progress + prog;
@@ -473,7 +473,7 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
             }
         }
         for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[i]});
-        int nprog = u.mbh + u.irows[0] + u.irows[1] + u.irows[2];
+        int nprog = 2 * u.mbh + u.irows[0] + u.irows[1] + u.irows[2];
         CK(cudaMemsetAsync(u.progress, 0, sizeof(int) * nprog, E->st));
     }
     // Interleave the rows of different units so the early rows of every unit

@@ -13,7 +13,7 @@ struct UnitDev {
     uint8_t *rec[3];            // reconstruction, tight
     RefPlanes ref[2];           // nearest, and second (== nearest when only one is valid)
     MBInfo *mbi;                // per macroblock, this frame
-    int *progress;              // per macroblock row: macroblocks finished
+    int *progress;              // per macroblock row: a 64-bit progress word (pframe.cuh), 8-byte aligned
     uint8_t *slots;             // per macroblock symbol slot (P-frames)
     double lambda;
     int qp, navail, force_skip, range;

@@ -242,7 +242,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     for (int r = 0; r < 2; ++r) o_ref[r] = take(4 * lsz + 2 * csz);
     o_mbi = take(sizeof(MBInfo) * nmb);
     o_slots = take((size_t)kSlotBytes * nmb);
-    o_prog = take(sizeof(int) * mbh);
+    o_prog = take(sizeof(unsigned long long) * mbh);
     o_misc = take(16);                       // ticket[2], error word
     o_unit = take(sizeof(UnitDev));
     o_rows = take(sizeof(RowTask) * mbh);
@@ -304,7 +304,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
               cudaMemcpyAsync(base + o_cmp, &cmp, sizeof cmp, cudaMemcpyHostToDevice, st) == cudaSuccess &&
               cudaMemcpyAsync(base + o_off, poff, sizeof poff, cudaMemcpyHostToDevice, st) == cudaSuccess &&
               // what must start at zero: progress flags, row ticket, error word
-              cudaMemsetAsync(base + o_prog, 0, sizeof(int) * mbh, st) == cudaSuccess &&
+              cudaMemsetAsync(base + o_prog, 0, sizeof(unsigned long long) * mbh, st) == cudaSuccess &&
               cudaMemsetAsync(base + o_misc, 0, 16, st) == cudaSuccess;
     if (!ok) return static_fail("descriptor upload failed");
     launch_refprep(base + o_prep, far_ref ? 2 : 1, w, h, B, st);

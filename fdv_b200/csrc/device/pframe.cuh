@@ -90,6 +90,21 @@ struct PShared {
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
 
+// A row's 64-bit progress word: bits 0-11 the macroblocks it has finished;
+// bits 16-63 the record of the last of them (reference bit 16, inter bit 17,
+// mode bits 18-19, vector x bits 32-47, y bits 48-63).
+__device__ __forceinline__ unsigned long long prog_word(int count, const MBInfo &m) {
+    return (unsigned long long)count | ((unsigned long long)(m.ref & 1u) << 16) |
+           ((unsigned long long)(m.inter & 1u) << 17) | ((unsigned long long)(m.mode & 3u) << 18) |
+           ((unsigned long long)(uint16_t)m.x << 32) | ((unsigned long long)(uint16_t)m.y << 48);
+}
+// The record in a progress word, packed as MBInfo is in memory ({x, y},
+// {ref, inter, mode, 0}).
+__device__ __forceinline__ uint2 prog_rec(unsigned long long v) {
+    return make_uint2((uint32_t)(v >> 32), (uint32_t)((v >> 16) & 1u) | ((uint32_t)((v >> 17) & 1u) << 8) |
+                                               ((uint32_t)((v >> 18) & 3u) << 16));
+}
+
 // Optional phase profile: thread 0 adds the cycles since the last mark.
 struct PhaseClock {
     unsigned long long *acc;
@@ -241,6 +256,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         }
         const UnitDev &U = units[rows[t].unit];
         const int row = rows[t].row, w = U.w, cw = w / 2, mbw = U.mbw;
+        unsigned long long *const prog64 = reinterpret_cast<unsigned long long *>(U.progress);
         if (row == U.stall_row) continue;   // injected stall: this row's progress flag is never set
         const double lambda = U.lambda;
         const int qp = U.qp, R = U.range, navail = U.navail;
@@ -268,69 +284,84 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const typename LumaOf<WIN>::T L0 = luma_src<WIN>(U.ref[0], win, 0, wy0, wrows);
         const typename LumaOf<WIN>::T L1 = luma_src<WIN>(U.ref[1], win, nref - 1, wy0, wrows);
         int pmvx = 0, pmvy = 0, prev_mode = 0;
-        int pbits = 0;   // thread 0: the last published macroblock's progress bits
+        unsigned long long pword = 0;   // thread 0: the row above's progress word seen last
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         for (int mbx = 0; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
             pc.start();
             cp_async_wait_all();   // this thread's strip and source copies; the barrier below publishes them
             const int par = mbx & 1;
-            if (LRN && U.prejs) {
-                if (tid == 0) {
+            // Past the row's first macroblock, this one's neighbour samples
+            // are final before its own wait: the row above's part was covered
+            // by the previous macroblock's wait (which needed one macroblock
+            // further), the left part is this block's own.  Threads 256-288
+            // load them now, overlapping the wait; the load phase below then
+            // skips them.
+            const bool early = mbx > 0;
+            if (early && tid >= 256 && tid < 256 + 33) {
+                const int k = tid - 256;
+                if (k < 16) {
+                    S.top[k] = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx + k]) : 0;
+                    S.left[k] = ldcg8(&U.rec[0][(size_t)(by + k) * w + bx - 1]);
+                } else if (k < 32) {
+                    const int pl = (k - 16) >> 3, q = k & 7;
+                    S.ctop[pl][q] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q]) : 0;
+                    S.cleft[pl][q] = ldcg8(&U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1]);
+                } else {
+                    S.tl = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
+                    for (int pl = 0; pl < 2; ++pl)
+                        S.ctl[pl] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
+                }
+            }
+            if (tid == 0) {
+                // The row above: wait until it has finished macroblock mbx + 1
+                // (the above-right neighbour), then the above and above-right
+                // records for the merge candidates (fdv.h:5711-5729).  Its
+                // progress word carries its last published macroblock's
+                // record, so when the word seen here (or at the previous
+                // macroblock) describes exactly the neighbour needed, no
+                // record has to be loaded.
+                const float pjs = (LRN && U.prejs) ? __ldcg(&U.prejs[row * mbw + mbx]) : -1.f;
+                const int need = min(mbx + 2, mbw);
+                int ok = 1;
+                uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
+                if (row > 0) {
+                    const unsigned long long v = wait_count64(prog64 + row - 1, need, err, wait_ns);
+                    ok = v != ~0ull;
+                    if (ok) {
+                        const int c = (int)(v & 0xfffu);
+                        bool h0 = false, h1 = mbx + 1 >= mbw;
+                        if (need == mbx + 2 && c == need) {
+                            nb[1] = prog_rec(v);
+                            h1 = true;
+                            if ((int)(pword & 0xfffu) == mbx + 1) { nb[0] = prog_rec(pword); h0 = true; }
+                        } else if (mbx == mbw - 1 && c == mbw) {
+                            nb[0] = prog_rec(v);
+                            h0 = true;
+                        }
+                        if (!h0) nb[0] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx]));
+                        if (!h1) nb[1] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + 1]));
+                        pword = v;
+                    }
+                }
+                S.nbi[par][0] = nb[0];
+                S.nbi[par][1] = nb[1];
+                S.rok[par] = ok;
+                if (LRN && U.prejs) {
                     // The learned form's pre-analysed SKIPs: the zero vector is
                     // what the merge list offers iff the left vector is zero
                     // and the above / above-right macroblocks are not inter or
-                    // carry the zero vector on reference 0 (fdv.h:5711-5729).
-                    // The row above's progress word describes its last two
-                    // macroblocks; when those are the two needed here, no
-                    // record has to be loaded.
-                    const float pjs = __ldcg(&U.prejs[row * mbw + mbx]);
-                    const int need = min(mbx + 2, mbw);
-                    const int v = row > 0 ? wait_count(&U.progress[row - 1], need, err, wait_ns) : 0;
-                    const int ok = v >= 0;
-                    const bool pz = pmvx == 0 && pmvy == 0;
-                    bool have = row == 0, zero = pz;
-                    int amz = 0;
-                    if (row > 0 && ok) {
-                        const int c = v >> 8;
-                        if (need == mbx + 2 && c == need) {          // macroblocks mbx, mbx + 1
-                            zero = pz && (v & 1) && (v & 4);
-                            amz = (v >> 3) & 1;
-                            have = true;
-                        } else if (need == mbw && c == mbw && mbx == mbw - 1) {   // mbx only (last column)
-                            zero = pz && (v & 1);
-                            amz = (v >> 1) & 1;
-                            have = true;
-                        }
-                    }
-                    bool fq = ok && pjs >= 0.f && have && zero;
-                    uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
-                    if (ok && !fq && row > 0) {
-                        for (int k = 0; k < 2; ++k)
-                            if (mbx + k < mbw)
-                                nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
-                        if (!have) {
-                            zero = pz;
-                            for (int k = 0; k < 2; ++k)
-                                if (((nb[k].y >> 8) & 0xffu) && (nb[k].x != 0 || (nb[k].y & 0xffu) != 0)) zero = false;
-                            amz = ((nb[0].y >> 16) & 0xffu) != 0;
-                            fq = pjs >= 0.f && zero;
-                        }
-                    }
-                    S.nbi[par][0] = nb[0]; S.nbi[par][1] = nb[1];
+                    // carry the zero vector on reference 0.
+                    bool zero = pmvx == 0 && pmvy == 0;
+                    for (int k = 0; k < 2; ++k)
+                        if (((nb[k].y >> 8) & 0xffu) && (nb[k].x != 0 || (nb[k].y & 0xffu) != 0)) zero = false;
                     S.pjs[par] = pjs;
-                    S.fast[par] = fq;
-                    S.amz[par] = amz;
-                    S.rok[par] = ok;
+                    S.fast[par] = ok && pjs >= 0.f && zero;
+                    S.amz[par] = ((nb[0].y >> 16) & 0xffu) != 0;
                 }
-                __syncthreads();
-            } else {
-                if (row > 0) {
-                    if (tid == 0) S.row_ok = wait_count(&U.progress[row - 1], min(mbx + 2, mbw), err, wait_ns) >= 0;
-                } else if (tid == 0) S.row_ok = 1;
-                __syncthreads();
             }
-            if (LRN && U.prejs ? !S.rok[par] : !S.row_ok) break;
+            __syncthreads();
+            if (!S.rok[par]) break;
             const bool fast = LRN && U.prejs && S.fast[par];
             if (WIN && mbx >= 1 && !fast) win_fill(win, U, nref, mbx + 4, mbx + 4, wy0, wrows, tid);
             pc.mark(PP_WAIT);
@@ -348,8 +379,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     U.mbi[row * mbw + mbx] = mi;
                     if (U.mbcost) U.mbcost[row * mbw + mbx] = S.pjs[par];
                     if (pc.acc) { atomicAdd(&pc.acc[PP_NMB], 1ull); atomicAdd(&pc.acc[PP_NSKIP], 1ull); }
-                    st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | 1 | (pbits << 2));
-                    pbits = 1;
+                    st_release_gpu64(prog64 + row, prog_word(mbx + 1, mi));
                     if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
                 }
                 pmvx = 0; pmvy = 0;
@@ -377,28 +407,27 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 *reinterpret_cast<uint32_t *>(&S.curc[pl][(k & 15) * 4]) =
                     *reinterpret_cast<const uint32_t *>(&U.cur[1 + pl][(size_t)(cby + r2) * cw + cbx + c2]);
             } else if (tid < 112) {
-                const int k = tid - 96;
-                S.top[k] = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx + k]) : 0;
-                S.left[k] = bx > 0 ? ldcg8(&U.rec[0][(size_t)(by + k) * w + bx - 1]) : 0;
+                if (!early) {
+                    const int k = tid - 96;
+                    S.top[k] = by > 0 ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx + k]) : 0;
+                    S.left[k] = bx > 0 ? ldcg8(&U.rec[0][(size_t)(by + k) * w + bx - 1]) : 0;
+                }
             } else if (tid < 128) {
-                const int k = tid - 112, pl = k >> 3, q = k & 7;
-                S.ctop[pl][q] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q]) : 0;
-                S.cleft[pl][q] = cbx > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1]) : 0;
+                if (!early) {
+                    const int k = tid - 112, pl = k >> 3, q = k & 7;
+                    S.ctop[pl][q] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx + q]) : 0;
+                    S.cleft[pl][q] = cbx > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby + q) * cw + cbx - 1]) : 0;
+                }
             } else if (tid == 128) {
                 // the above and above-right macroblock records (one 8-byte load
                 // each, issued together with the corner samples)
-                uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
-                if (LRN && U.prejs) {
-                    nb[0] = S.nbi[par][0]; nb[1] = S.nbi[par][1];
-                } else {
-                    for (int k = 0; k < 2; ++k)
-                        if (row > 0 && mbx + k < mbw)
-                            nb[k] = __ldcg(reinterpret_cast<const uint2 *>(&U.mbi[(row - 1) * mbw + mbx + k]));
-                }
+                const uint2 nb[2] = {S.nbi[par][0], S.nbi[par][1]};
                 S.ht = by > 0; S.hl = bx > 0;
-                S.tl = (by > 0 && bx > 0) ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
-                for (int pl = 0; pl < 2; ++pl)
-                    S.ctl[pl] = (cby > 0 && cbx > 0) ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
+                if (!early) {
+                    S.tl = (by > 0 && bx > 0) ? ldcg8(&U.rec[0][(size_t)(by - 1) * w + bx - 1]) : 128;
+                    for (int pl = 0; pl < 2; ++pl)
+                        S.ctl[pl] = (cby > 0 && cbx > 0) ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
+                }
                 // merge candidates (fdv.h:5711-5729)
                 int n = 1;
                 S.cand[0].x = (int16_t)pmvx; S.cand[0].y = (int16_t)pmvy; S.cand[0].ref = 0; S.cand[0].inter = 1;
@@ -453,8 +482,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 prev_mode = 0;
                 __syncthreads();
                 if (tid == 0) {
-                    st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | 1 | (pbits << 2));
-                    pbits = 1;
+                    const MBInfo mz = {0, 0, 0, 1, 0, 0};
+                    st_release_gpu64(prog64 + row, prog_word(mbx + 1, mz));
                 }
                 continue;
             }
@@ -803,14 +832,9 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 U.mbi[row * mbw + mbx] = info;
                 if (U.mbcost) U.mbcost[row * mbw + mbx] = (float)Jc;
                 // Publish now: the row below reads the reconstruction (ordered
-                // before this release by the barrier above) and the record,
-                // never the symbol slot.  The word also carries, for the row
-                // below, this macroblock's and the previous one's
-                // (zero-vector-compatible, not SKIP) bits.
-                const int zb = ((!info.inter || (info.x == 0 && info.y == 0 && info.ref == 0)) ? 1 : 0) |
-                               (chosen != 0 ? 2 : 0);
-                st_release_gpu(&U.progress[row], ((mbx + 1) << 8) | zb | (pbits << 2));
-                pbits = zb;
+                // before this release by the barrier above) and the record
+                // (also carried in the word), never the symbol slot.
+                st_release_gpu64(prog64 + row, prog_word(mbx + 1, info));
                 if (U.tl) U.tl[2 * (row * mbw + mbx) + 1] = globaltimer();
             }
             // ---- coefficient streams of the chosen mode into the slot (read
