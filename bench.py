@@ -62,6 +62,49 @@ WORKLOAD = ("hd720: 1280x720 I420, 120 frames, key interval 60, QP 24, 8 bands x
 METRIC = "720p encode Mpix/s on 1 B200 (plain, bit-exact)"
 
 
+class Ranks:
+    """The run's processes (torchrun's RANK / WORLD_SIZE / LOCAL_RANK): one
+    per GPU, each coding its own stream -- no collective on the data path, only
+    the barrier around the timed region and the MAX of the per-rank times."""
+
+    def __init__(self, backend: str, device: str):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        import torch
+        if self.device.startswith("cuda"):
+            torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def reduce_max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def weak_value(world: int, steps: int, frames: int, seconds: float) -> float:
+    """Whole-job Mpix/s: every rank codes `frames` frames per step."""
+    return world * steps * frames * W * H / 1e6 / seconds
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -540,16 +583,10 @@ def main() -> None:
         print(json.dumps(r))
         return
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                                timeout=datetime.timedelta(seconds=300))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ranks = Ranks("nccl" if torch.cuda.is_available() else "gloo", f"cuda:{local}")
+    rank, world = ranks.rank, ranks.world
     torch.cuda.set_device(local)
     import fdv_b200 as F
     L = F.lib()
@@ -596,17 +633,7 @@ def main() -> None:
         L.fdvg_stats(g._g, *[C.byref(x) for x in v])
         return [x.value for x in v]
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def reduce_max(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, reduce_max = ranks.barrier, ranks.reduce_max
 
     for _ in range(args.warmup):
         device_step()
@@ -622,7 +649,7 @@ def main() -> None:
     clocks = clk.stop()
     step_ms, pk_ms, pk_n, ik_ms, ik_n, launches, nsteps, d2h = stats()
     dev_s = reduce_max(step_ms / 1e3)
-    value = world * args.steps * NF * W * H / 1e6 / dev_s
+    value = weak_value(world, args.steps, NF, dev_s)
     ms_per_step = 1e3 * dev_s / args.steps
 
     # e2e through the C ABI, host buffers in and out
@@ -646,7 +673,7 @@ def main() -> None:
                 raise RuntimeError(F.last_error())
         barrier()
         e2e_s = reduce_max(time.perf_counter() - t1)
-        e2e = world * args.steps * NF * W * H / 1e6 / e2e_s
+        e2e = weak_value(world, args.steps, NF, e2e_s)
 
     # roofline of the dominant kernel (the P-frame analysis wavefront)
     peaks = {}
@@ -738,9 +765,7 @@ def main() -> None:
             "decode": decode,
         }))
     g.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
