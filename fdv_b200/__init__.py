@@ -70,6 +70,9 @@ def lib() -> C.CDLL:
         L.fdvg_pframe_hist.argtypes = [p, i, C.POINTER(C.c_uint32)]
         L.fdvg_submit.argtypes = [p, C.POINTER(u8p), C.POINTER(i), C.POINTER(i), C.c_void_p, C.c_void_p]
         L.fdvg_collect.argtypes = [p]
+        L.fdvg_submit_batch.argtypes = [p, i, C.POINTER(u8p), C.POINTER(i), C.POINTER(i), C.c_void_p, C.c_void_p]
+        L.fdvg_max_batch.argtypes = [p]
+        L.fdvg_frames_device.argtypes = [p, i, C.POINTER(u8p), C.POINTER(i), C.POINTER(i)]
         L.fdvg_iframe_hist.argtypes = [p, i, i, C.POINTER(C.c_uint32)]
         L.fdvg_recon.argtypes = [p, i, u8p]
         L.fdvg_set_learned.argtypes = [p, C.POINTER(C.c_float), C.c_float]
@@ -287,6 +290,29 @@ class Engine:
 
     def collect(self) -> None:
         if lib().fdvg_collect(self._g) != 0:
+            raise FdvError(last_error())
+
+    def max_batch(self) -> int:
+        return lib().fdvg_max_batch(self._g)
+
+    def submit_batch(self, frames, qp) -> None:
+        """Queue consecutive P-frames as one launch (fdvg_submit_batch):
+        frames[k][u] is frame k of unit u, qp[k][u] its quantiser; collect()
+        then returns them one by one."""
+        n, K = len(self.sizes), len(frames)
+        self._keep = []
+        planes = (u8p * (3 * n * K))()
+        for k in range(K):
+            for u, ((w, h), f) in enumerate(zip(self.sizes, frames[k])):
+                a = _as_frames([f], w, h)[0]
+                self._keep.append(a)
+                base = a.ctypes.data
+                planes[3 * (k * n + u)] = C.cast(base, u8p)
+                planes[3 * (k * n + u) + 1] = C.cast(base + w * h, u8p)
+                planes[3 * (k * n + u) + 2] = C.cast(base + w * h + (w // 2) * (h // 2), u8p)
+        intra = (C.c_int * (n * K))(*([0] * (n * K)))
+        q = (C.c_int * (n * K))(*[int(v) for row in qp for v in row])
+        if lib().fdvg_submit_batch(self._g, K, planes, intra, q, None, None) != 0:
             raise FdvError(last_error())
 
     def _call(self, fn, frames, is_intra, qp, lscale, force_skip) -> None:

@@ -117,6 +117,12 @@ struct RefPlanes {
     int ys, cs;          // luma / chroma strides
 };
 
+// The same planes as a reference being written (post.cuh).
+struct OutPlanes {
+    uint8_t *G, *B, *H, *J, *U, *V;
+    int ys, cs;
+};
+
 // Per-macroblock motion kept for merge candidates (fdv.h:5680) plus the mode.
 struct MBInfo {
     int16_t x, y;

@@ -7,22 +7,35 @@
 //   2. analysis: the P-frame wavefront kernel over every P unit's macroblock
 //      rows and the intra CTU-wavefront kernel over every key-frame unit's
 //      plane CTU rows;
-//   3. deblock, vertical edges then horizontal edges, every plane;
+//   3. key frames: deblock, vertical edges then horizontal edges, every plane
+//      (P-frames deblock inside the wavefront, post.cuh; the learned form's
+//      P-frames as key frames);
 //   4. compaction of the per-block symbol slots into the per-stream byte
 //      arrays the entropy tail reads, written straight into mapped host memory;
-//   5. reference preparation: the deblocked reconstruction becomes the
-//      unit's new nearest reference (integer + half-pel planes).
-// The reference pool rotates exactly as fdv_video_encode's (fdv.h:6842-6846).
+//   5. key frames: reference preparation, the deblocked reconstruction becomes
+//      the unit's new nearest reference (integer + half-pel planes); P-frames
+//      write theirs tile by tile inside the wavefront (learned form: as key
+//      frames).
+// The reference pool rotates as fdv_video_encode's (fdv.h:6842-6846): the
+// nearest and second-nearest references are the last two coded frames; they
+// live in a ring of kRefSlots planes sets, reference q in slot q % kRefSlots.
+//
+// Up to kMaxBatch consecutive P-frames go into one launch (a batch): frame
+// k + 1's rows start as soon as the reference tiles they read have been
+// written by frame k's rows, so the frames' wavefronts overlap and fill the
+// SMs that one frame's rows leave idle.  Each frame of a batch has its own
+// lane of per-frame buffers.
 //
 // A step is a submit (everything above enqueued, nothing waited on) and a
 // collect (wait for the oldest submitted frame, check its error word, point
-// the stream views at its output).  Two frames can be in flight: staging,
-// output buffers and events are double-buffered, so a host can entropy-code
-// frame f while the GPU analyses frame f + 1.
+// the stream views at its output).  Up to kSlots frames can be in flight (two
+// batches): staging, output buffers and events are per in-flight frame, so a
+// host can entropy-code one batch while the GPU analyses the next.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
+#include <deque>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -95,6 +108,10 @@ struct CompactTaskH {
     uint32_t *hist;
 };
 
+constexpr int kMaxBatch = 6;                // P-frames per launch at most
+constexpr int kRefSlots = kMaxBatch + 2;    // reference ring: a batch's outputs never alias its inputs
+constexpr int kSlots = 2 * kMaxBatch;       // frames in flight: two batches
+
 struct RefSlot {
     uint8_t *mem = nullptr;
     RefPlanes rp{};
@@ -103,27 +120,39 @@ struct RefSlot {
 
 struct Unit {
     int w, h, mbw, mbh, cw, ch;
-    uint8_t *cur = nullptr, *rec = nullptr;
-    RefSlot ref[2];
-    int near_i = 0, nref = 0;
-    MBInfo *mbi = nullptr;
-    int *progress = nullptr;      // P rows, then I rows for Y, U, V
-    uint8_t *slots = nullptr;     // P macroblock slots
+    // per lane (frame of a batch; key frames use lane 0): source,
+    // reconstruction (un-deblocked for P-frames), records, progress words
+    // (P rows: 64-bit words, then per row the count of reference tiles
+    // written; then I rows for Y, U, V), macroblock symbol slots
+    uint8_t *cur[kMaxBatch] = {}, *rec[kMaxBatch] = {};
+    MBInfo *mbi[kMaxBatch] = {};
+    int *progress[kMaxBatch] = {};
+    uint8_t *slots[kMaxBatch] = {};
+    RefSlot ref[kRefSlots];
+    long long seq = 0;            // references made so far (the next one goes to slot seq % kRefSlots)
+    int nref = 0;
+    int recon_slot = -1;          // ring slot holding the last coded frame's deblocked reconstruction
+                                  // (-1: it is in lane 0's reconstruction, deblocked in place)
     uint8_t *islots[3] = {nullptr, nullptr, nullptr};
     uint8_t *mmap[3] = {nullptr, nullptr, nullptr};
     int icols[3], irows[3], pw[3], ph[3];
-    uint8_t *out_h[2] = {nullptr, nullptr}, *out_d[2] = {nullptr, nullptr};   // per in-flight slot
+    uint8_t *out_h[kSlots] = {}, *out_d[kSlots] = {};   // per in-flight slot
     // per in-flight slot: the streams' symbol counts, [16][256] for a P-frame,
     // [3][12][256] for a key frame (host-mapped, written by the compaction)
-    uint32_t *hist_h[2] = {nullptr, nullptr}, *hist_d[2] = {nullptr, nullptr};
+    uint32_t *hist_h[kSlots] = {}, *hist_d[kSlots] = {};
     size_t out_cap = 0, out_off_i[3] = {0, 0, 0};
     int last_intra = 0, last_qp = 0;
     int mb_off = 0;               // first macroblock of this unit in engine-wide per-macroblock arrays
     fdvb_streams ps{}, is[3]{};
+    RefSlot &slot_of(long long q) { return ref[(int)(((q % kRefSlots) + kRefSlots) % kRefSlots)]; }
 };
 
-// One in-flight frame: pinned staging of its sources and descriptors, its
-// error word, its events, and what its units were.
+// Words of a lane's progress array before the I rows.
+static int p_progress_words(const Unit &u) { return 3 * u.mbh; }
+
+// One in-flight frame: pinned staging of its sources (and, for the first
+// frame of a batch, the batch's descriptors), its error word, its events, and
+// what its units were.
 struct Slot {
     uint8_t *stage = nullptr;
     size_t stage_cap = 0;
@@ -131,6 +160,7 @@ struct Slot {
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<int> intra;
     bool has_p = false, has_i = false;
+    int batch = 0;                // frames of the batch when this is its first frame, else 0
 };
 
 }  // namespace
@@ -151,8 +181,14 @@ struct fdvb_engine {
     int *d_poff = nullptr, *d_ioff = nullptr;
     int maxrows = 0, maxitasks = 0;
     unsigned long long wait_ns = 4000000000ull;
-    Slot slot[2];
-    int head = 0, inflight = 0;    // oldest in-flight slot, number in flight
+    Slot slot[kSlots];
+    // in-flight frames in submission order (slot indices); new frames take the
+    // lowest free slots, so callers with one or two frames in flight only
+    // ever use (and allocate output buffers for) the first slots
+    std::deque<int> order;
+    bool busy[kSlots] = {};
+    int inflight = 0;
+    size_t src_stage_bytes = 0;    // a slot's staging of one frame's sources (64-byte multiple)
     // timing (CUDA events on the engine's stream) and launch counts
     double step_ms = 0, pk_ms = 0, ik_ms = 0;
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
@@ -160,6 +196,7 @@ struct fdvb_engine {
     int stall_unit = -1, stall_row = -1;
     int defer_refs = 0;                     // leave the reference pool alone until commit
     std::vector<int> pending_intra;         // frame types of the uncommitted step
+    std::vector<int> pending_prep;          // its units whose reference is prepared at commit
     bool pending = false;
     unsigned long long *d_prof = nullptr;   // phase profile accumulators (when enabled)
     unsigned long long *d_tl = nullptr;     // per-macroblock timeline (with the phase profile)
@@ -183,13 +220,15 @@ extern "C" const char *fdvb_engine_error(void) { return g_err.c_str(); }
 static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     u.w = w; u.h = h; u.mbw = w / 16; u.mbh = h / 16; u.cw = w / 2; u.ch = h / 2;
     const size_t fs = (size_t)w * h * 3 / 2;
-    CK(cudaMalloc(&u.cur, fs));
-    CK(cudaMalloc(&u.rec, fs));
-    CK(cudaMemset(u.rec, 0, fs));
+    for (int k = 0; k < kMaxBatch; ++k) {
+        CK(cudaMalloc(&u.cur[k], fs));
+        CK(cudaMalloc(&u.rec[k], fs));
+        CK(cudaMemset(u.rec[k], 0, fs));
+    }
     const int B = E->border;
     const int ys = round_up(w + 2 * B, 64), cs = round_up(u.cw + 2 * B, 64);
     const size_t lsz = (size_t)ys * (h + 2 * B), csz = (size_t)cs * (u.ch + 2 * B);
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < kRefSlots; ++r) {
         RefSlot &s = u.ref[r];
         CK(cudaMalloc(&s.mem, 4 * lsz + 2 * csz));
         CK(cudaMemset(s.mem, 0, 4 * lsz + 2 * csz));
@@ -204,47 +243,56 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
         s.rp.ys = ys; s.rp.cs = cs;
     }
     const int nmb = u.mbw * u.mbh;
-    CK(cudaMalloc(&u.mbi, sizeof(MBInfo) * nmb));
-    CK(cudaMalloc(&u.slots, (size_t)kSlotBytes * nmb));
     u.pw[0] = w; u.ph[0] = h; u.pw[1] = u.pw[2] = u.cw; u.ph[1] = u.ph[2] = u.ch;
-    int nprog = 2 * u.mbh;   // P-frame rows: one 64-bit progress word each
+    // P-frame rows: one 64-bit progress word each, then the reference tile counts
+    int nprog = p_progress_words(u);
     for (int p = 0; p < 3; ++p) {
         u.icols[p] = (u.pw[p] + 63) / 64; u.irows[p] = (u.ph[p] + 63) / 64;
         nprog += u.irows[p];
         CK(cudaMalloc(&u.islots[p], (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p]));
         CK(cudaMalloc(&u.mmap[p], (size_t)(u.pw[p] / 4) * (u.ph[p] / 4)));
     }
-    CK(cudaMalloc(&u.progress, sizeof(int) * nprog));
+    for (int k = 0; k < kMaxBatch; ++k) {
+        CK(cudaMalloc(&u.mbi[k], sizeof(MBInfo) * nmb));
+        CK(cudaMalloc(&u.slots[k], (size_t)kSlotBytes * nmb));
+        CK(cudaMalloc(&u.progress[k], sizeof(int) * nprog));
+    }
     // host-mapped output: P-frame streams, or the three planes of a key frame
     size_t pcap = 64 + (size_t)nmb * kSlotData;
     size_t icap[3];
     for (int p = 0; p < 3; ++p) icap[p] = 64 + (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p];
     u.out_off_i[0] = 0; u.out_off_i[1] = icap[0]; u.out_off_i[2] = icap[0] + icap[1];
     u.out_cap = std::max(pcap, icap[0] + icap[1] + icap[2]);
-    for (int k = 0; k < 2; ++k) {
-        CK(cudaHostAlloc(&u.out_h[k], u.out_cap, cudaHostAllocMapped));
-        CK(cudaHostGetDevicePointer(&u.out_d[k], u.out_h[k], 0));
-        CK(cudaHostAlloc(&u.hist_h[k], sizeof(uint32_t) * 36 * 256, cudaHostAllocMapped));
-        CK(cudaHostGetDevicePointer(&u.hist_d[k], u.hist_h[k], 0));
-    }
+    return 0;
+}
+
+// A unit's host-mapped output of in-flight slot k, allocated at first use.
+static int unit_out(Unit &u, int k) {
+    if (u.out_h[k]) return 0;
+    CK(cudaHostAlloc(&u.out_h[k], u.out_cap, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(&u.out_d[k], u.out_h[k], 0));
+    CK(cudaHostAlloc(&u.hist_h[k], sizeof(uint32_t) * 36 * 256, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(&u.hist_d[k], u.hist_h[k], 0));
     return 0;
 }
 
 static void free_unit(Unit &u) {
-    cudaFree(u.cur); cudaFree(u.rec);
-    for (int r = 0; r < 2; ++r) cudaFree(u.ref[r].mem);
-    cudaFree(u.mbi); cudaFree(u.slots); cudaFree(u.progress);
+    for (int k = 0; k < kMaxBatch; ++k) {
+        cudaFree(u.cur[k]); cudaFree(u.rec[k]);
+        cudaFree(u.mbi[k]); cudaFree(u.slots[k]); cudaFree(u.progress[k]);
+    }
+    for (int r = 0; r < kRefSlots; ++r) cudaFree(u.ref[r].mem);
     for (int p = 0; p < 3; ++p) { cudaFree(u.islots[p]); cudaFree(u.mmap[p]); }
-    for (int k = 0; k < 2; ++k) if (u.out_h[k]) cudaFreeHost(u.out_h[k]);
-    for (int k = 0; k < 2; ++k) if (u.hist_h[k]) cudaFreeHost(u.hist_h[k]);
+    for (int k = 0; k < kSlots; ++k) if (u.out_h[k]) cudaFreeHost(u.out_h[k]);
+    for (int k = 0; k < kSlots; ++k) if (u.hist_h[k]) cudaFreeHost(u.hist_h[k]);
 }
 
 // Bytes of the descriptor area of a slot's staging buffer (each array 64-byte aligned).
 static size_t stage_desc_bytes(int nu, int maxrows, int maxitasks) {
     auto a = [](size_t n) { return (n + 63) / 64 * 64; };
-    return a(sizeof(UnitDev) * nu) + a(sizeof(RowTask) * maxrows) + a(sizeof(IPlaneDevH) * 3 * nu) +
-           a(sizeof(ITaskH) * maxitasks) + a(sizeof(PrepTaskH) * nu) + a(sizeof(DbTaskH) * 3 * nu) +
-           a(sizeof(CompactTaskH) * 3 * nu) + a(sizeof(int2) * nu);
+    return a(sizeof(UnitDev) * kMaxBatch * nu) + a(sizeof(RowTask) * kMaxBatch * maxrows) +
+           a(sizeof(IPlaneDevH) * 3 * nu) + a(sizeof(ITaskH) * maxitasks) + a(sizeof(PrepTaskH) * nu) +
+           a(sizeof(DbTaskH) * 3 * nu) + a(sizeof(CompactTaskH) * 3 * kMaxBatch * nu) + a(sizeof(int2) * nu);
 }
 
 extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
@@ -275,13 +323,13 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     }
     E->maxrows = maxrows; E->maxitasks = maxitasks;
     for (auto &u : E->units) { u.mb_off = E->total_mbs; E->total_mbs += u.mbw * u.mbh; }
-    bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * nunits) == cudaSuccess &&
-              cudaMalloc(&E->d_rows, sizeof(RowTask) * maxrows) == cudaSuccess &&
+    bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * kMaxBatch * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_rows, sizeof(RowTask) * kMaxBatch * maxrows) == cudaSuccess &&
               cudaMalloc(&E->d_planes, sizeof(IPlaneDevH) * 3 * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_itasks, sizeof(ITaskH) * maxitasks) == cudaSuccess &&
               cudaMalloc(&E->d_prep, sizeof(PrepTaskH) * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_db, sizeof(DbTaskH) * 3 * nunits) == cudaSuccess &&
-              cudaMalloc(&E->d_cmp, sizeof(CompactTaskH) * 3 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_cmp, sizeof(CompactTaskH) * 3 * kMaxBatch * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_ticket, sizeof(int) * 2) == cudaSuccess &&
               cudaMalloc(&E->d_err, sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc(&E->d_poff, sizeof(int) * 16) == cudaSuccess &&
@@ -289,8 +337,9 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
     size_t src_bytes = 0;
     for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
+    E->src_stage_bytes = (src_bytes + 63) / 64 * 64;
     for (auto &sl : E->slot) {
-        sl.stage_cap = (src_bytes + 63) / 64 * 64 + stage_desc_bytes(nunits, maxrows, maxitasks);
+        sl.stage_cap = E->src_stage_bytes + stage_desc_bytes(nunits, maxrows, maxitasks);
         if (cudaHostAlloc(&sl.stage, sl.stage_cap, cudaHostAllocDefault) != cudaSuccess ||
             cudaHostAlloc(&sl.err_h, 64, cudaHostAllocDefault) != cudaSuccess) {
             g_err = "pinned allocation failed";
@@ -341,17 +390,18 @@ static size_t parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
     return (size_t)(d - p);
 }
 
-// Enqueue the reference preparation of units `which`; the task array is
-// staged in `stage` (pinned, slot-owned) when given, else copied from the stack
-// (callers that synchronise before returning).
+// Enqueue the reference preparation of units `which` from lane 0's deblocked
+// reconstruction into ring slot seq % kRefSlots (the caller then advances
+// seq); the task array is staged in `stage` (pinned, slot-owned) when given,
+// else copied from the stack (callers that synchronise before returning).
 static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *stage = nullptr) {
     std::vector<PrepTaskH> pt;
     int maxw = 0, maxh = 0;
     for (int i : which) {
         Unit &u = E->units[i];
-        RefSlot &s = u.ref[1 - u.near_i];
+        RefSlot &s = u.slot_of(u.seq);
         PrepTaskH t;
-        t.rec[0] = u.rec; t.rec[1] = u.rec + (size_t)u.w * u.h; t.rec[2] = t.rec[1] + (size_t)u.cw * u.ch;
+        t.rec[0] = u.rec[0]; t.rec[1] = u.rec[0] + (size_t)u.w * u.h; t.rec[2] = t.rec[1] + (size_t)u.cw * u.ch;
         t.G = s.G; t.B = s.B; t.H = s.H; t.J = s.J; t.U = s.U; t.V = s.V;
         t.w = u.w; t.h = u.h; t.ys = s.rp.ys; t.cs = s.rp.cs; t.border = E->border;
         pt.push_back(t);
@@ -363,52 +413,70 @@ static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *sta
     CK(cudaMemcpyAsync(E->d_prep, src, sizeof(PrepTaskH) * pt.size(), cudaMemcpyHostToDevice, E->st));
     launch_refprep(E->d_prep, (int)pt.size(), maxw, maxh, E->border, E->st);
     CK(cudaGetLastError());
-    for (int i : which) {
-        Unit &u = E->units[i];
-        u.near_i = 1 - u.near_i;
-    }
     return 0;
 }
 
-extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
-                                  const double *lscale, const int *force_skip) {
+// Submit K frames (a batch, K <= kMaxBatch): arrays hold frame k's entries at
+// k * nunits (planes: 3 per unit).  K > 1 needs every unit of every frame to
+// be a P-frame, no learned proposals, no decision records and no deferred
+// references; the frames go into one P-frame launch.
+extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *const *planes, const int *is_intra,
+                                        const int *qp, const double *lscale, const int *force_skip) {
     if (!E) return -1;
-    if (E->inflight >= 2) { g_err = "two frames already in flight"; return -1; }
     const int nu = (int)E->units.size();
-    for (int i = 0; i < nu; ++i) {
-        if (qp[i] < 0 || qp[i] > 51) { g_err = "qp out of range"; return -1; }
-        bool fs = force_skip && force_skip[i];
-        if (!fs && (!planes || !planes[3 * i] || !planes[3 * i + 1] || !planes[3 * i + 2])) {
-            g_err = "missing source frame";
-            return -1;
-        }
-        if (fs && (is_intra[i] || E->units[i].nref == 0)) { g_err = "a held frame needs a reference"; return -1; }
-        if (!is_intra[i] && E->units[i].nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
+    if (K < 1 || K > kMaxBatch) { g_err = "batch size out of range"; return -1; }
+    if (E->inflight + K > kSlots) { g_err = "too many frames in flight"; return -1; }
+    if (K > 1 && (E->lnet || E->d_mbcost || E->defer_refs)) {
+        g_err = "batches of P-frames need the plain analysis without records or deferred references";
+        return -1;
     }
+    for (int k = 0; k < K; ++k)
+        for (int i = 0; i < nu; ++i) {
+            const int j = k * nu + i;
+            if (qp[j] < 0 || qp[j] > 51) { g_err = "qp out of range"; return -1; }
+            const bool fs = force_skip && force_skip[j];
+            if (!fs && (!planes || !planes[3 * j] || !planes[3 * j + 1] || !planes[3 * j + 2])) {
+                g_err = "missing source frame";
+                return -1;
+            }
+            if (K > 1 && is_intra[j]) { g_err = "a batch of several frames holds P-frames only"; return -1; }
+            const int nref = k == 0 ? E->units[i].nref : 1;
+            if (fs && (is_intra[j] || nref == 0)) { g_err = "a held frame needs a reference"; return -1; }
+            if (!is_intra[j] && nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
+        }
     CK(cudaSetDevice(E->device));
-    const int si = (E->head + E->inflight) & 1;
-    Slot &SL = E->slot[si];
+    int sis[kMaxBatch];
+    for (int k = 0, s = 0; k < K; ++k) {
+        while (E->busy[s]) ++s;
+        sis[k] = s++;
+        for (auto &u : E->units)
+            if (unit_out(u, sis[k]) != 0) return -3;
+    }
+    Slot &SL = E->slot[sis[0]];
     CK(cudaEventRecord(SL.ev[0], E->st));
-    // 1. sources (host sources through the slot's pinned staging buffer)
-    uint8_t *stage = SL.stage;
-    for (int i = 0; i < nu; ++i) {
-        Unit &u = E->units[i];
-        if (force_skip && force_skip[i]) continue;
-        const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
-        if (E->src_on_device) {
-            CK(cudaMemcpyAsync(u.cur, planes[3 * i], ys, cudaMemcpyDeviceToDevice, E->st));
-            CK(cudaMemcpyAsync(u.cur + ys, planes[3 * i + 1], cs, cudaMemcpyDeviceToDevice, E->st));
-            CK(cudaMemcpyAsync(u.cur + ys + cs, planes[3 * i + 2], cs, cudaMemcpyDeviceToDevice, E->st));
-        } else {
-            memcpy(stage, planes[3 * i], ys);
-            memcpy(stage + ys, planes[3 * i + 1], cs);
-            memcpy(stage + ys + cs, planes[3 * i + 2], cs);
-            CK(cudaMemcpyAsync(u.cur, stage, ys + 2 * cs, cudaMemcpyHostToDevice, E->st));
-            stage += ys + 2 * cs;
+    // 1. sources (host sources through each frame's pinned staging buffer)
+    for (int k = 0; k < K; ++k) {
+        uint8_t *stage = E->slot[sis[k]].stage;
+        for (int i = 0; i < nu; ++i) {
+            Unit &u = E->units[i];
+            const int j = k * nu + i;
+            if (force_skip && force_skip[j]) continue;
+            const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
+            if (E->src_on_device) {
+                CK(cudaMemcpyAsync(u.cur[k], planes[3 * j], ys, cudaMemcpyDeviceToDevice, E->st));
+                CK(cudaMemcpyAsync(u.cur[k] + ys, planes[3 * j + 1], cs, cudaMemcpyDeviceToDevice, E->st));
+                CK(cudaMemcpyAsync(u.cur[k] + ys + cs, planes[3 * j + 2], cs, cudaMemcpyDeviceToDevice, E->st));
+            } else {
+                memcpy(stage, planes[3 * j], ys);
+                memcpy(stage + ys, planes[3 * j + 1], cs);
+                memcpy(stage + ys + cs, planes[3 * j + 2], cs);
+                CK(cudaMemcpyAsync(u.cur[k], stage, ys + 2 * cs, cudaMemcpyHostToDevice, E->st));
+                stage += ys + 2 * cs;
+            }
         }
     }
-    stage = SL.stage + (stage - SL.stage + 63) / 64 * 64;
-    // descriptors are staged too: each array copied to the pinned buffer
+    // descriptors are staged after the first frame's sources
+    uint8_t *stage = SL.stage + E->src_stage_bytes;
     auto staged = [&](const void *src, size_t n) -> const void * {
         memcpy(stage, src, n);
         const void *r = stage;
@@ -416,76 +484,104 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         return r;
     };
     // 2. descriptors
-    std::vector<UnitDev> ud(nu);
+    std::vector<UnitDev> ud(K * nu);
     std::vector<RowTask> rows;
     std::vector<IPlaneDevH> iplanes;
     std::vector<ITaskH> itasks;
     std::vector<CompactTaskH> cmp;
     std::vector<DbTaskH> db;
-    std::vector<int2> pu;   // P units and their first macroblock in the hint array
+    // units deblocked and prepared after the frame by the whole-frame kernels:
+    // key frames, and P-frames of the learned form (its confident macroblocks
+    // take less time than a tile of the in-wavefront stage, which would then
+    // lengthen the wavefront; the form runs one frame per launch anyway)
+    std::vector<int> iunits;
+    std::vector<int2> pu;     // P units and their first macroblock in the hint array
     int nhint = 0;
-    for (int i = 0; i < nu; ++i) {
-        Unit &u = E->units[i];
-        UnitDev &d = ud[i];
-        d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh;
-        d.cur[0] = u.cur; d.cur[1] = u.cur + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
-        d.rec[0] = u.rec; d.rec[1] = u.rec + (size_t)u.w * u.h; d.rec[2] = d.rec[1] + (size_t)u.cw * u.ch;
-        const int navail = u.nref >= 2 ? 2 : 1;
-        d.ref[0] = u.ref[u.near_i].rp;
-        d.ref[1] = navail == 2 ? u.ref[1 - u.near_i].rp : u.ref[u.near_i].rp;
-        d.mbi = u.mbi; d.progress = u.progress; d.slots = u.slots;
-        d.lambda = fdvb_lambda(qp[i], lscale ? lscale[i] : 1.0);
-        d.qp = qp[i]; d.navail = navail; d.force_skip = force_skip ? force_skip[i] : 0; d.range = E->range;
-        d.stall_row = (i == E->stall_unit) ? E->stall_row : -1;
-        d.prof = E->d_prof;
-        d.hint = nullptr;
-        d.skip_gate = E->lgate;
-        d.inter8 = E->linter8;
-        d.mbcost = E->d_mbcost ? E->d_mbcost + u.mb_off : nullptr;
-        d.tl = E->d_tl ? E->d_tl + 2 * (size_t)u.mb_off : nullptr;
-        if (!is_intra[i] && E->lnet) {
-            pu.push_back(make_int2(i, nhint));
-            d.hint = E->d_hints + nhint;
-            d.prejs = E->d_prejs + nhint;
-            nhint += u.mbw * u.mbh;
-        }
-        SL.intra[i] = is_intra[i];
-        u.last_qp = qp[i];
-        if (!is_intra[i]) {
-            for (int r = 0; r < u.mbh; ++r) rows.push_back({i, r});
-            CompactTaskH c{u.slots, u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[si], u.out_cap, u.hist_d[si]};
-            cmp.push_back(c);
-        } else {
-            int prog = 2 * u.mbh;
-            for (int p = 0; p < 3; ++p) {
-                IPlaneDevH P;
-                P.src = d.cur[p]; P.rec = d.rec[p]; P.mmap = u.mmap[p]; P.progress = u.progress + prog;
-                P.slots = u.islots[p]; P.w = u.pw[p]; P.h = u.ph[p]; P.cols = u.icols[p]; P.rows = u.irows[p];
-                P.qp = qp[i]; P.lambda = fdvb_lambda(qp[i], 1.0); P.prof = E->d_prof ? E->d_prof + 16 : nullptr;
-                int pid = (int)iplanes.size();
-                iplanes.push_back(P);
-                for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
-                prog += u.irows[p];
-                CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
-                               u.out_d[si] + u.out_off_i[p], (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p],
-                               u.hist_d[si] + p * 12 * 256};
-                cmp.push_back(c);
+    for (int k = 0; k < K; ++k) {
+        std::vector<RowTask> frows;
+        E->slot[sis[k]].intra.assign(nu, 0);
+        for (int i = 0; i < nu; ++i) {
+            Unit &u = E->units[i];
+            const int j = k * nu + i;
+            UnitDev &d = ud[j];
+            d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh;
+            d.cur[0] = u.cur[k]; d.cur[1] = u.cur[k] + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
+            d.rec[0] = u.rec[k]; d.rec[1] = u.rec[k] + (size_t)u.w * u.h; d.rec[2] = d.rec[1] + (size_t)u.cw * u.ch;
+            // frame k's references: the outputs of the two frames before it
+            const int nref = k == 0 ? u.nref : std::min(2, u.nref + k);
+            const int navail = nref >= 2 ? 2 : 1;
+            d.ref[0] = u.slot_of(u.seq - 1 + k).rp;
+            d.ref[1] = navail == 2 ? u.slot_of(u.seq - 2 + k).rp : d.ref[0];
+            d.mbi = u.mbi[k]; d.progress = u.progress[k]; d.slots = u.slots[k];
+            d.lambda = fdvb_lambda(qp[j], lscale ? lscale[j] : 1.0);
+            d.qp = qp[j]; d.navail = navail; d.force_skip = force_skip ? force_skip[j] : 0; d.range = E->range;
+            d.stall_row = (i == E->stall_unit && k == 0) ? E->stall_row : -1;
+            d.prof = E->d_prof;
+            d.hint = nullptr;
+            d.prejs = nullptr;
+            d.skip_gate = E->lgate;
+            d.inter8 = E->linter8;
+            d.mbcost = E->d_mbcost ? E->d_mbcost + u.mb_off : nullptr;
+            d.tl = E->d_tl ? E->d_tl + 2 * (size_t)u.mb_off : nullptr;
+            d.out = OutPlanes{};
+            d.post_prog = nullptr;
+            d.ref_prog = nullptr;
+            if (!is_intra[j] && E->lnet) {
+                pu.push_back(make_int2(i, nhint));
+                d.hint = E->d_hints + nhint;
+                d.prejs = E->d_prejs + nhint;
+                nhint += u.mbw * u.mbh;
             }
+            u.last_qp = qp[j];
+            if (!is_intra[j]) {
+                if (E->lnet) {
+                    iunits.push_back(i);
+                    for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});
+                } else {
+                    // the frame's reference is written inside the wavefront,
+                    // into the ring slot after its own references
+                    const RefSlot &o = u.slot_of(u.seq + k);
+                    d.out = OutPlanes{o.G, o.B, o.H, o.J, o.U, o.V, o.rp.ys, o.rp.cs};
+                    d.post_prog = u.progress[k] + 2 * u.mbh;
+                    d.ref_prog = k > 0 ? u.progress[k - 1] + 2 * u.mbh : nullptr;
+                }
+                for (int r = 0; r < u.mbh; ++r) frows.push_back({j, r});
+                CompactTaskH c{u.slots[k], u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[sis[k]], u.out_cap,
+                               u.hist_d[sis[k]]};
+                cmp.push_back(c);
+            } else {
+                iunits.push_back(i);
+                int prog = p_progress_words(u);
+                for (int p = 0; p < 3; ++p) {
+                    IPlaneDevH P;
+                    P.src = d.cur[p]; P.rec = d.rec[p]; P.mmap = u.mmap[p]; P.progress = u.progress[0] + prog;
+                    P.slots = u.islots[p]; P.w = u.pw[p]; P.h = u.ph[p]; P.cols = u.icols[p]; P.rows = u.irows[p];
+                    P.qp = qp[j]; P.lambda = fdvb_lambda(qp[j], 1.0); P.prof = E->d_prof ? E->d_prof + 16 : nullptr;
+                    int pid = (int)iplanes.size();
+                    iplanes.push_back(P);
+                    for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
+                    prog += u.irows[p];
+                    CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
+                                   u.out_d[sis[k]] + u.out_off_i[p],
+                                   (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p],
+                                   u.hist_d[sis[k]] + p * 12 * 256};
+                    cmp.push_back(c);
+                }
+                for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});
+            }
+            const int nprog = p_progress_words(u) + u.irows[0] + u.irows[1] + u.irows[2];
+            CK(cudaMemsetAsync(u.progress[k], 0, sizeof(int) * nprog, E->st));
         }
-        for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[i]});
-        int nprog = 2 * u.mbh + u.irows[0] + u.irows[1] + u.irows[2];
-        CK(cudaMemsetAsync(u.progress, 0, sizeof(int) * nprog, E->st));
-    }
-    // Interleave the rows of different units so the early rows of every unit
-    // start first (each unit's rows stay in order, which is all the ticket
-    // scheme needs).
-    {
-        std::vector<RowTask> inter;
+        for (int i = 0; i < nu; ++i) E->slot[sis[k]].intra[i] = is_intra[k * nu + i];
+        // Interleave the rows of different units so the early rows of every
+        // unit start first; frames in order (a row only ever waits for rows
+        // of its own frame above it and of the frame before: earlier tickets).
         int maxh = 0;
         for (auto &u : E->units) maxh = std::max(maxh, u.mbh);
         for (int r = 0; r < maxh; ++r)
-            for (auto &t : rows) if (t.row == r) inter.push_back(t);
-        rows.swap(inter);
+            for (auto &t : frows) if (t.row == r) rows.push_back(t);
+    }
+    {
         std::vector<ITaskH> it2;
         int maxr = 0;
         for (auto &t : itasks) maxr = std::max(maxr, t.row + 1);
@@ -493,7 +589,8 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
             for (auto &t : itasks) if (t.row == r) it2.push_back(t);
         itasks.swap(it2);
     }
-    CK(cudaMemcpyAsync(E->d_units, staged(ud.data(), sizeof(UnitDev) * nu), sizeof(UnitDev) * nu, cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemcpyAsync(E->d_units, staged(ud.data(), sizeof(UnitDev) * K * nu), sizeof(UnitDev) * K * nu,
+                       cudaMemcpyHostToDevice, E->st));
     CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
     CK(cudaMemsetAsync(E->d_err, 0, sizeof(unsigned), E->st));
     if (!rows.empty()) {
@@ -530,38 +627,68 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
         CK(cudaEventRecord(SL.ev[4], E->st));
         E->launches += 1;
     }
-    // 3. deblock, 4. compact
-    CK(cudaMemcpyAsync(E->d_db, staged(db.data(), sizeof(DbTaskH) * db.size()), sizeof(DbTaskH) * db.size(),
-                       cudaMemcpyHostToDevice, E->st));
-    launch_deblock(E->d_db, (int)db.size(), E->st);
-    CK(cudaGetLastError());
-    E->launches += 2;
+    // 3. deblock (key frames), 4. compact
+    if (!db.empty()) {
+        CK(cudaMemcpyAsync(E->d_db, staged(db.data(), sizeof(DbTaskH) * db.size()), sizeof(DbTaskH) * db.size(),
+                           cudaMemcpyHostToDevice, E->st));
+        launch_deblock(E->d_db, (int)db.size(), E->st);
+        CK(cudaGetLastError());
+        E->launches += 2;
+    }
     CK(cudaMemcpyAsync(E->d_cmp, staged(cmp.data(), sizeof(CompactTaskH) * cmp.size()), sizeof(CompactTaskH) * cmp.size(),
                        cudaMemcpyHostToDevice, E->st));
     launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
     CK(cudaGetLastError());
     E->launches += 1;
-    // 5. the new reference (deferred: the caller may code this frame again)
+    // 5. the new references (deferred: the caller may code this frame again)
     if (E->defer_refs) {
         E->pending_intra.assign(is_intra, is_intra + nu);
+        E->pending_prep.assign(nu, 0);
+        for (int i : iunits) E->pending_prep[i] = 1;
         E->pending = true;
-    } else {
-        std::vector<int> all(nu);
-        for (int i = 0; i < nu; ++i) all[i] = i;
-        if (prep_refs(E, all, stage) != 0) return -3;
-        E->launches += 2;
         for (int i = 0; i < nu; ++i) {
             Unit &u = E->units[i];
-            u.nref = is_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+            u.recon_slot = E->pending_prep[i] ? -1 : (int)(u.seq % kRefSlots);
+        }
+    } else {
+        if (!iunits.empty()) {
+            if (prep_refs(E, iunits, stage) != 0) return -3;
+            E->launches += 2;
+        }
+        for (int i = 0; i < nu; ++i) {
+            Unit &u = E->units[i];
+            for (int k = 0; k < K; ++k) u.nref = is_intra[k * nu + i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+            u.recon_slot = (int)((u.seq + K - 1) % kRefSlots);
+            u.seq += K;
         }
     }
-    CK(cudaMemcpyAsync(SL.err_h, E->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
-    CK(cudaEventRecord(SL.ev[5], E->st));
-    SL.has_p = !rows.empty();
-    SL.has_i = !itasks.empty();
+    for (int k = 0; k < K; ++k) {
+        Slot &S = E->slot[sis[k]];
+        CK(cudaMemcpyAsync(S.err_h, E->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
+        CK(cudaEventRecord(S.ev[5], E->st));
+        S.has_p = !rows.empty();
+        S.has_i = !itasks.empty();
+        S.batch = k == 0 ? K : 0;
+    }
     E->stall_unit = E->stall_row = -1;     // an injected stall lasts one step
-    E->inflight += 1;
+    for (int k = 0; k < K; ++k) {
+        E->busy[sis[k]] = true;
+        E->order.push_back(sis[k]);
+    }
+    E->inflight += K;
     return 0;
+}
+
+extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                                  const double *lscale, const int *force_skip) {
+    return fdvb_engine_submit_batch(E, 1, planes, is_intra, qp, lscale, force_skip);
+}
+
+// The largest batch the engine takes in its present mode (1 with learned
+// proposals, decision records or deferred references).
+extern "C" int fdvb_engine_max_batch(const fdvb_engine *E) {
+    if (!E) return 0;
+    return (E->lnet || E->d_mbcost || E->defer_refs) ? 1 : kMaxBatch;
 }
 
 // Wait for the oldest submitted frame; on success the stream views
@@ -569,17 +696,20 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
 extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     if (!E) return -1;
     if (E->inflight == 0) { g_err = "no frame in flight"; return -1; }
-    Slot &SL = E->slot[E->head];
-    const int si = E->head;
-    E->head ^= 1;
+    const int si = E->order.front();
+    Slot &SL = E->slot[si];
+    E->order.pop_front();
+    E->busy[si] = false;
     E->inflight -= 1;
     CK(cudaEventSynchronize(SL.ev[5]));
-    {
+    E->steps += 1;
+    if (SL.batch) {
+        // the batch's first frame carries its timing: whole step, and the
+        // P-frame kernel time counted per P-frame
         float ms = 0;
         cudaEventElapsedTime(&ms, SL.ev[0], SL.ev[5]);
         E->step_ms += ms;
-        E->steps += 1;
-        if (SL.has_p) { cudaEventElapsedTime(&ms, SL.ev[1], SL.ev[2]); E->pk_ms += ms; E->pk_n += 1; }
+        if (SL.has_p) { cudaEventElapsedTime(&ms, SL.ev[1], SL.ev[2]); E->pk_ms += ms; E->pk_n += SL.batch; }
         if (SL.has_i) { cudaEventElapsedTime(&ms, SL.ev[3], SL.ev[4]); E->ik_ms += ms; E->ik_n += 1; }
     }
     const unsigned err = *SL.err_h;
@@ -626,7 +756,16 @@ extern "C" int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420) {
     if (!E || unit < 0 || unit >= (int)E->units.size() || !i420) return -1;
     Unit &u = E->units[unit];
     CK(cudaStreamSynchronize(E->st));
-    CK(cudaMemcpy(i420, u.rec, (size_t)u.w * u.h * 3 / 2, cudaMemcpyDeviceToHost));
+    if (u.recon_slot < 0) {
+        CK(cudaMemcpy(i420, u.rec[0], (size_t)u.w * u.h * 3 / 2, cudaMemcpyDeviceToHost));
+        return 0;
+    }
+    // the interior of the reference planes
+    const RefSlot &r = u.ref[u.recon_slot];
+    uint8_t *uo = i420 + (size_t)u.w * u.h, *vo = uo + (size_t)u.cw * u.ch;
+    CK(cudaMemcpy2D(i420, u.w, r.G, r.rp.ys, u.w, u.h, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy2D(uo, u.cw, r.U, r.rp.cs, u.cw, u.ch, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy2D(vo, u.cw, r.V, r.rp.cs, u.cw, u.ch, cudaMemcpyDeviceToHost));
     return 0;
 }
 // Seed a unit's reference pool from host frames (tight I420): nearest, and the
@@ -637,15 +776,18 @@ extern "C" int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *nea
     Unit &u = E->units[unit];
     const size_t fs = (size_t)u.w * u.h * 3 / 2;
     std::vector<int> one{unit};
-    u.near_i = 0;
     if (far_i420) {
-        // far first: prep writes slot 1 - near_i and then flips near_i
-        CK(cudaMemcpyAsync(u.rec, far_i420, fs, cudaMemcpyHostToDevice, E->st));
+        // far first: it becomes the second-nearest reference
+        CK(cudaMemcpyAsync(u.rec[0], far_i420, fs, cudaMemcpyHostToDevice, E->st));
         if (prep_refs(E, one) != 0) return -3;
+        CK(cudaStreamSynchronize(E->st));
+        u.seq += 1;
     }
-    CK(cudaMemcpyAsync(u.rec, near_i420, fs, cudaMemcpyHostToDevice, E->st));
+    CK(cudaMemcpyAsync(u.rec[0], near_i420, fs, cudaMemcpyHostToDevice, E->st));
     if (prep_refs(E, one) != 0) return -3;
     CK(cudaStreamSynchronize(E->st));
+    u.recon_slot = (int)(u.seq % kRefSlots);
+    u.seq += 1;
     u.nref = far_i420 ? 2 : 1;
     return 0;
 }
@@ -734,14 +876,20 @@ extern "C" int fdvb_engine_commit_refs(fdvb_engine *E) {
     if (E->inflight) { g_err = "a frame is still in flight"; return -1; }
     CK(cudaSetDevice(E->device));
     const int nu = (int)E->units.size();
-    std::vector<int> all(nu);
-    for (int i = 0; i < nu; ++i) all[i] = i;
-    if (prep_refs(E, all) != 0) return -3;
+    // key frames and learned-form P-frames: prepare the reference now; the
+    // other P-frames wrote theirs inside the wavefront
+    std::vector<int> iu;
+    for (int i = 0; i < nu; ++i) if (E->pending_prep[i]) iu.push_back(i);
+    if (!iu.empty()) {
+        if (prep_refs(E, iu) != 0) return -3;
+        E->launches += 2;
+    }
     CK(cudaStreamSynchronize(E->st));
-    E->launches += 2;
     for (int i = 0; i < nu; ++i) {
         Unit &u = E->units[i];
         u.nref = E->pending_intra[i] ? 1 : (u.nref < 2 ? u.nref + 1 : 2);
+        u.recon_slot = (int)(u.seq % kRefSlots);
+        u.seq += 1;
     }
     E->pending = false;
     return 0;
@@ -816,7 +964,7 @@ extern "C" int fdvb_engine_mb_records(fdvb_engine *E, int unit, uint8_t *mode, i
     Unit &u = E->units[unit];
     const int n = u.mbw * u.mbh;
     std::vector<MBInfo> mi(n);
-    CK(cudaMemcpy(mi.data(), u.mbi, sizeof(MBInfo) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mi.data(), u.mbi[0], sizeof(MBInfo) * n, cudaMemcpyDeviceToHost));
     for (int i = 0; i < n; ++i) {
         if (mode) mode[i] = mi[i].mode;
         if (mv) { mv[2 * i] = mi[i].x; mv[2 * i + 1] = mi[i].y; }

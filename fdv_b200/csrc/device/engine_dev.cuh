@@ -30,6 +30,17 @@ struct UnitDev {
     // per macroblock, with the phase profile on (NULL: off): %globaltimer when
     // its wait for the row above ended and when it published its progress
     unsigned long long *tl;
+    // The reference this frame becomes (post.cuh), written tile by tile as
+    // the wavefront passes, and per macroblock row the count of tiles written
+    // (NULL: no post stage; the deblock and reference-preparation kernels run
+    // after the frame instead).
+    OutPlanes out;
+    int *post_prog;
+    // The previous frame's tile counts when that frame is still being coded
+    // by the same launch (its output is this frame's nearest reference): each
+    // macroblock waits for the tiles its reference reads reach (NULL: the
+    // references are complete).
+    const int *ref_prog;
 };
 
 // Phases of a macroblock, for the optional cycle profile.

@@ -27,6 +27,21 @@ __device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
     return __funnelshift_r(q[0], q[1], (unsigned)(a & 3) * 8u);
 }
 
+// The same loads through L2 only (ld.global.cg), for reference planes that
+// other blocks of the same launch write (post.cuh): an L1 line filled by an
+// earlier read could hold bytes of a tile written after it.
+__device__ __forceinline__ int mc_cpx_cg(const uint8_t *P, int s, int x, int y, int fx, int fy) {
+    const uint8_t *p = P + (long)y * s + x;
+    int a = __ldcg(p), b = __ldcg(p + 1), c = __ldcg(p + s), d = __ldcg(p + s + 1);
+    int top = a * (4 - fx) + b * fx, bot = c * (4 - fx) + d * fx;
+    return (top * (4 - fy) + bot * fy + 8) >> 4;
+}
+__device__ __forceinline__ uint32_t ld4u_cg(const uint8_t *p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    return __funnelshift_r(__ldcg(q), __ldcg(q + 1), (unsigned)(a & 3) * 8u);
+}
+
 // Where a reference's four luma planes (0 = G, 1 = b, 2 = h, 3 = j) are read
 // from: the padded planes in global memory ...
 struct GlobalLuma {
@@ -36,6 +51,16 @@ struct GlobalLuma {
     __device__ __forceinline__ uint32_t ld(int p, int x, int y) const {
         const uint8_t *pl = p == 0 ? G : (p == 1 ? B : (p == 2 ? H : J));
         return ld4u(pl + (long)y * ys + x);
+    }
+};
+// ... the same through L2 only ...
+struct GlobalLumaCG {
+    const uint8_t *G, *B, *H, *J;
+    int ys;
+    __device__ explicit GlobalLumaCG(const RefPlanes &R) : G(R.G), B(R.B), H(R.H), J(R.J), ys(R.ys) {}
+    __device__ __forceinline__ uint32_t ld(int p, int x, int y) const {
+        const uint8_t *pl = p == 0 ? G : (p == 1 ? B : (p == 2 ? H : J));
+        return ld4u_cg(pl + (long)y * ys + x);
     }
 };
 // ... or a window of them staged in shared memory by the P-frame kernel: per

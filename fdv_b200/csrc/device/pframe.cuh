@@ -30,6 +30,7 @@
 #include "engine_dev.cuh"
 #include "inter.cuh"
 #include "intra.cuh"
+#include "post.cuh"
 #include "residual.cuh"
 
 namespace fdvb {
@@ -86,6 +87,8 @@ struct PShared {
     int fast[2];                 // a pre-analysed zero-vector SKIP whose merge list is {0}
     int rok[2];                  // row_ok
     int amz[2];                  // the above macroblock's mode is not SKIP
+    int pok;                     // the row's first reference wait succeeded
+    PostScratch post;            // the reference output stage (post.cuh)
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -174,12 +177,14 @@ __device__ void win_fill(uint8_t *win, const UnitDev &U, int nref, int s0, int s
     cp_async_commit();
 }
 
-template <bool WIN> struct LumaOf { using T = GlobalLuma; };
+template <bool WIN> struct LumaOf { using T = GlobalLumaCG; };
 template <> struct LumaOf<true> { using T = WindowLuma; };
 template <bool WIN>
 __device__ __forceinline__ typename LumaOf<WIN>::T luma_src(const RefPlanes &R, const uint8_t *win, int r, int wy0, int wrows);
 template <>
-__device__ __forceinline__ GlobalLuma luma_src<false>(const RefPlanes &R, const uint8_t *, int, int, int) { return GlobalLuma(R); }
+__device__ __forceinline__ GlobalLumaCG luma_src<false>(const RefPlanes &R, const uint8_t *, int, int, int) {
+    return GlobalLumaCG(R);
+}
 template <>
 __device__ __forceinline__ WindowLuma luma_src<true>(const RefPlanes &, const uint8_t *win, int r, int wy0, int wrows) {
     return WindowLuma{win + r * 4 * kWinPlane, wy0, wrows - 1};
@@ -263,8 +268,17 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         const double lam14 = __dmul_rn(lambda, 14.0), lam16 = __dmul_rn(lambda, 16.0), lam19 = __dmul_rn(lambda, 19.0);
         qp4_setup(&S.q, qp, tid);
         const int nref = navail > 1 ? 2 : 1, wy0 = row * 16 - R - 3, wrows = 2 * R + 23;
+        // With the previous frame in the same launch: the reference rows this
+        // row reads are its macroblock rows up to row + ref_dr, and macroblock
+        // mbx reads its columns up to mbx + ref_dc (the window strip mbx + 4
+        // filled at mbx, or +-(R + 3) samples read directly when R is 64).
+        const int ref_dr = WIN ? (R + 19) / 16 : R / 16 + 2, ref_dc = WIN ? 4 : R / 16 + 2;
+        const int ref_row = min(row + ref_dr, U.mbh - 1);
         cp_async_wait_all();   // this block's copies for an earlier row have landed
+        if (tid == 0)
+            S.pok = U.ref_prog ? wait_progress(U.ref_prog + ref_row, min(ref_dc, mbw - 1) + 1, err, wait_ns) : 1;
         __syncthreads();
+        if (!S.pok) continue;
         if (WIN) win_fill(win, U, nref, -3, 4, wy0, wrows, tid);   // macroblock 0's strips and macroblock 1's
         // source prefetch: each macroblock's luma and chroma are copied into
         // S.pre while the one before it is analysed (aligned planes only)
@@ -286,7 +300,20 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         int pmvx = 0, pmvy = 0, prev_mode = 0;
         unsigned long long pword = 0;   // thread 0: the row above's progress word seen last
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
-        for (int mbx = 0; mbx < mbw; ++mbx) {
+        // The post stage (post.cuh): this row posts the tiles of the row above
+        // (and the last row its own), one macroblock behind its progress, on
+        // threads 32..511 while thread 0 waits for the row above.
+        int posted = 0;
+        auto post_upto = [&](int ncols) {
+            for (; posted < ncols; ++posted)
+                for (int pr = row - 1; pr <= row; ++pr) {
+                    if (pr < 0 || (pr == row && row != U.mbh - 1)) continue;
+                    post_tile(S.post, U, pr, posted, tid - kPostT0);
+                    if (tid == kPostT0) st_release_gpu(U.post_prog + pr, posted + 1);
+                }
+        };
+        int mbx = 0;
+        for (; mbx < mbw; ++mbx) {
             const int bx = mbx * 16, by = row * 16, cbx = bx / 2, cby = by / 2;
             pc.start();
             cp_async_wait_all();   // this thread's strip and source copies; the barrier below publishes them
@@ -313,6 +340,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                         S.ctl[pl] = cby > 0 ? ldcg8(&U.rec[1 + pl][(size_t)(cby - 1) * cw + cbx - 1]) : 128;
                 }
             }
+            // tiles up to column mbx - 2: this row has finished macroblock mbx - 1
+            if (U.post_prog && tid >= kPostT0) post_upto(mbx - 1);
             if (tid == 0) {
                 // The row above: wait until it has finished macroblock mbx + 1
                 // (the above-right neighbour), then the above and above-right
@@ -324,8 +353,10 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const float pjs = (LRN && U.prejs) ? __ldcg(&U.prejs[row * mbw + mbx]) : -1.f;
                 const int need = min(mbx + 2, mbw);
                 int ok = 1;
+                if (U.ref_prog && mbx > 0)
+                    ok = wait_progress(U.ref_prog + ref_row, min(mbx + ref_dc, mbw - 1) + 1, err, wait_ns);
                 uint2 nb[2] = {make_uint2(0, 0), make_uint2(0, 0)};
-                if (row > 0) {
+                if (row > 0 && ok) {
                     const unsigned long long v = wait_count64(prog64 + row - 1, need, err, wait_ns);
                     ok = v != ~0ull;
                     if (ok) {
@@ -465,11 +496,11 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 if (tid < 64) {
                     const int r2 = tid >> 2, c2 = (tid & 3) * 4;
                     *reinterpret_cast<uint32_t *>(&U.rec[0][(size_t)(by + r2) * w + bx + c2]) =
-                        ld4u(R0.G + (long)(by + r2) * R0.ys + bx + c2);
+                        ld4u_cg(R0.G + (long)(by + r2) * R0.ys + bx + c2);
                 } else if (tid < 192) {
                     const int k = tid - 64, pl = k >> 6, p = k & 63;
                     const uint8_t *P = pl ? R0.V : R0.U;
-                    U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = P[(long)(cby + (p >> 3)) * R0.cs + cbx + (p & 7)];
+                    U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] = __ldcg(&P[(long)(cby + (p >> 3)) * R0.cs + cbx + (p & 7)]);
                 }
                 if (tid == 0) {
                     uint8_t m0 = 0;
@@ -682,7 +713,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     const RefPlanes &Rs = U.ref[sref];
                     const int cmx = smvx / 2, cmy = smvy / 2;
                     U.rec[1 + pl][(size_t)(cby + (p >> 3)) * cw + cbx + (p & 7)] =
-                        (uint8_t)mc_cpx(pl ? Rs.V : Rs.U, Rs.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
+                        (uint8_t)mc_cpx_cg(pl ? Rs.V : Rs.U, Rs.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
                 info.x = (int16_t)smvx; info.y = (int16_t)smvy; info.ref = (uint8_t)sref; info.inter = 1;
                 pmvx = smvx; pmvy = smvy;
@@ -715,7 +746,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const int cmx = mvx / 2, cmy = mvy / 2;
                 if (tid < 128) {
                     const int pl = tid >> 6, p = tid & 63;
-                    S.cpred[pl][p] = (uint8_t)mc_cpx(pl ? Rb.V : Rb.U, Rb.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
+                    S.cpred[pl][p] = (uint8_t)mc_cpx_cg(pl ? Rb.V : Rb.U, Rb.cs, cbx + (p & 7) + (cmx >> 2), cby + (p >> 3) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
                 __syncthreads();
                 if (warp < 8) {
@@ -802,7 +833,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 if (tid < 128) {
                     const int k = tid >> 4, p = tid & 15, pl = k >> 2, q = k & 3;
                     const int cmx = S.qmv[q][0] / 2, cmy = S.qmv[q][1] / 2, qcx = (q & 1) * 4, qcy = (q >> 1) * 4;
-                    S.cpred4[k][p] = (uint8_t)mc_cpx(pl ? R0.V : R0.U, R0.cs, cbx + qcx + (p & 3) + (cmx >> 2),
+                    S.cpred4[k][p] = (uint8_t)mc_cpx_cg(pl ? R0.V : R0.U, R0.cs, cbx + qcx + (p & 3) + (cmx >> 2),
                                                      cby + qcy + (p >> 2) + (cmy >> 2), cmx & 3, cmy & 3);
                 }
                 __syncthreads();
@@ -852,6 +883,8 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             }
             pc.mark(PP_OUT);
         }
+        // the row's last tiles (its last macroblock is finished)
+        if (U.post_prog && mbx == mbw && tid >= kPostT0) post_upto(mbw);
         __syncthreads();
     }
 }

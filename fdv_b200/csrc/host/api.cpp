@@ -12,6 +12,7 @@
 //   file head        "FDV1" [version u8][kind u8][fps u16][payload_len u32]
 //                                                                   fdv.h:7448-7464
 #include <algorithm>
+#include <deque>
 #include <cmath>
 #include <atomic>
 #include <condition_variable>
@@ -328,8 +329,10 @@ size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payl
 }
 
 // Encode nframes over a set of horizontal bands (nbands == 1: the plain
-// stream) and leave each band's video stream in us[b].bytes.  The GPU analyses
-// frame f while the host entropy-codes frame f - 1 (bands in parallel).
+// stream) and leave each band's video stream in us[b].bytes.  Runs of
+// consecutive P-frames go to the GPU as batches (one wavefront launch each,
+// the frames overlapping); the host entropy-codes one batch's frames, bands in
+// parallel, while the GPU analyses the next batch.
 static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
                         int bh_full, int nthreads, std::vector<UnitStream> &us) {
     const int nb = (h + bh_full - 1) / bh_full, cw = w / 2, ch = h / 2;
@@ -345,35 +348,55 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         us[b].tmp_cap = (size_t)w * H[b] * 3 + 8192;
         stream_header(us[b].bytes, nframes, w, H[b], qp, keyint);
     }
-    std::vector<const uint8_t *> planes(3 * nb);
-    std::vector<int> intra(nb), qps(nb, qp);
+    const int kmax = std::max(1, fdvb_engine_max_batch(E));
+    std::vector<const uint8_t *> planes(3 * nb * kmax);
+    std::vector<int> intra(nb * kmax), qps(nb * kmax, qp);
     Pool pool(std::max(1, std::min(nthreads, nb)));
     std::vector<int> urc(nb);
-    int rc = 0, inflight = 0, prev_intra = 0;
-    for (int f = 0; f <= nframes && rc == 0; ++f) {
-        int is_intra = 0;
+    auto key_at = [&](int f) { return f == 0 || (keyint > 0 && f % keyint == 0) ? 1 : 0; };
+    std::deque<int> types;    // frame types in flight, oldest first
+    int rc = 0;
+    size_t prev = 0;          // frames of the previous batch (in flight, not yet coded)
+    for (int f = 0; rc == 0;) {
+        int K = 0;
         if (f < nframes) {
-            const uint8_t *fy = frames[f], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
-            is_intra = (f == 0) || (keyint > 0 && f % keyint == 0);
-            for (int b = 0; b < nb; ++b) {
-                planes[3 * b] = fy + (size_t)Y0[b] * w;
-                planes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
-                planes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
-                intra[b] = is_intra;
+            K = 1;
+            if (!key_at(f))
+                while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
+            for (int k = 0; k < K; ++k) {
+                const uint8_t *fy = frames[f + k], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+                for (int b = 0; b < nb; ++b) {
+                    const int j = k * nb + b;
+                    planes[3 * j] = fy + (size_t)Y0[b] * w;
+                    planes[3 * j + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+                    planes[3 * j + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+                    intra[j] = key_at(f + k);
+                }
             }
-            if (fdvb_engine_submit(E, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) { set_engine_err(); rc = -1; break; }
-            ++inflight;
+            if (fdvb_engine_submit_batch(E, K, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) {
+                set_engine_err();
+                rc = -1;
+                break;
+            }
+            for (int k = 0; k < K; ++k) types.push_back(key_at(f + k));
         }
-        if (f > 0) {
-            --inflight;
+        // code the previous batch while the GPU runs this one
+        for (size_t c = 0; c < prev && rc == 0; ++c) {
+            const int ti = types.front();
+            types.pop_front();
             if (fdvb_engine_collect(E) != 0) { set_engine_err(); rc = -1; break; }
             std::fill(urc.begin(), urc.end(), 0);
-            pool.run(nb, [&](int u) { urc[u] = code_unit_frame(E, u, us[u], prev_intra, qp); });
+            pool.run(nb, [&](int u) { urc[u] = code_unit_frame(E, u, us[u], ti, qp); });
             for (int r : urc) if (r) { set_err("entropy coding failed"); rc = -1; }
         }
-        prev_intra = is_intra;
+        if (K == 0) break;
+        prev = (size_t)K;
+        f += K;
     }
-    while (inflight-- > 0) fdvb_engine_collect(E);
+    while (!types.empty()) {
+        types.pop_front();
+        fdvb_engine_collect(E);
+    }
     if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
     else fdvb_engine_destroy(E);
     return rc;
@@ -657,6 +680,51 @@ int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420) {
 }
 int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *far_i420) {
     int rc = fdvb_engine_set_refs(g, u, near_i420, far_i420);
+    if (rc) set_engine_err();
+    return rc;
+}
+
+int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                      const double *lscale, const int *force_skip) {
+    int rc = fdvb_engine_submit_batch(g, nframes, planes, is_intra, qp, lscale, force_skip);
+    if (rc) set_engine_err();
+    return rc;
+}
+int fdvg_max_batch(const fdvg_ctx *g) { return fdvb_engine_max_batch(g); }
+
+// nframes frame steps from device sources, runs of P-frames batched, each
+// batch collected while the next one runs; the stream views then describe the
+// last frame.
+int fdvg_frames_device(fdvg_ctx *g, int nframes, const uint8_t *const *dplanes, const int *is_intra, const int *qp) {
+    if (!g || nframes <= 0 || !dplanes || !is_intra || !qp) { set_err("bad arguments"); return -1; }
+    const int nu = fdvb_engine_units(g), kmax = std::max(1, fdvb_engine_max_batch(g));
+    auto key_at = [&](int f) {
+        for (int i = 0; i < nu; ++i) if (is_intra[(size_t)f * nu + i]) return true;
+        return false;
+    };
+    fdvb_engine_src_on_device(g, 1);
+    int rc = 0, prev = 0;
+    for (int f = 0; f < nframes;) {
+        int K = 1;
+        if (!key_at(f))
+            while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
+        rc = fdvb_engine_submit_batch(g, K, dplanes + (size_t)3 * nu * f, is_intra + (size_t)nu * f,
+                                      qp + (size_t)nu * f, nullptr, nullptr);
+        if (rc) break;
+        // the previous batch, all of it even after an error
+        for (int n = prev; n > 0; --n) {
+            const int r = fdvb_engine_collect(g);
+            if (!rc) rc = r;
+        }
+        prev = K;
+        if (rc) break;
+        f += K;
+    }
+    for (; prev > 0; --prev) {
+        const int r = fdvb_engine_collect(g);
+        if (!rc) rc = r;
+    }
+    fdvb_engine_src_on_device(g, 0);
     if (rc) set_engine_err();
     return rc;
 }

@@ -165,13 +165,29 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
 /* fdvg_frame in two halves, so a host can entropy-code one frame while the GPU
  * analyses the next: fdvg_submit copies the sources (through pinned staging;
  * the caller may reuse its buffers on return) and queues the frame; at most
- * two frames are in flight.  fdvg_collect waits for the oldest one, after which
- * the stream and count accessors describe it until the next fdvg_collect.  A
- * caller keeps the streams of collected frame f only until it submits frame
- * f + 2. */
+ * twelve frames are in flight.  fdvg_collect waits for the oldest one, after
+ * which the stream and count accessors describe it until the next
+ * fdvg_collect.  A collected frame's streams stay valid until the next
+ * submission. */
 int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
                 const double *lscale, const int *force_skip);
 int fdvg_collect(fdvg_ctx *g);
+/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (six; one
+ * while learned proposals, decision records or deferred references are on):
+ * the arrays hold frame k's entries at k * nunits (planes: 3 per unit).  The
+ * frames' wavefronts run in one launch, each frame's macroblock rows starting
+ * as soon as the reference tiles they read have been written by the frame
+ * before (deblocked and prepared inside the wavefront); the frames are then
+ * collected one by one as after fdvg_submit, with the same streams as
+ * frame-by-frame coding. */
+int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, const int *is_intra, const int *qp,
+                      const double *lscale, const int *force_skip);
+int fdvg_max_batch(const fdvg_ctx *g);
+/* nframes frame steps from device sources (planes: 3 * nunits device pointers
+ * per frame; is_intra and qp: nunits per frame): runs of P-frames go as
+ * batches, each collected while the next one runs.  The stream accessors then
+ * describe the last frame. */
+int fdvg_frames_device(fdvg_ctx *g, int nframes, const uint8_t *const *dplanes, const int *is_intra, const int *qp);
 /* The last frame's symbol streams of unit u.  P-frame: 16 streams in the
  * blob's order (9 structure streams by model, then 4x4 counts, 4x4 levels,
  * 8x8 counts, 8x8 levels, region flags, chroma counts, chroma levels).  Key

@@ -1,0 +1,79 @@
+"""GPU parity of batched P-frames (fdvg_submit_batch): several consecutive
+P-frames in one wavefront launch, each frame's rows starting while the frame
+before is still being coded, its reference deblocked and prepared tile by
+tile inside the wavefront.
+
+Every frame's 16 symbol streams must equal the CPU oracle's coding the same
+frames one after another (so every in-launch reference was right), and the
+last frame's reconstruction must equal the oracle's.  Cases cover one and two
+references, the three search ranges (the shared-memory window at 16 and 32,
+direct reads at 64), units one macroblock wide or high (tiles whose borders
+meet on both sides), several units of mixed sizes in one batch, and two
+batches in a row (the reference ring wrapping around).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(sizes, rng, nbatch, K, qp, seed):
+    import fdv_b200 as F
+    import oracle as O
+    nf = 1 + nbatch * K
+    frames = [F.Scene(w, h, nf, nrects=max(2, w * h // 3000), pan_qx=7, pan_qy=-5, static_pct=30,
+                      seed=seed + u).frames(nf) for u, (w, h) in enumerate(sizes)]
+    eng = F.Engine(sizes, rng)
+    assert eng.max_batch() >= K
+    units = [O.OracleUnit(w, h, rng) for (w, h) in sizes]
+    eng.step([frames[u][0] for u in range(len(sizes))], [1] * len(sizes), [qp] * len(sizes))
+    for u, o in enumerate(units):
+        o.frame(frames[u][0], 1, qp)
+    f = 1
+    for _ in range(nbatch):
+        eng.submit_batch([[frames[u][f + k] for u in range(len(sizes))] for k in range(K)],
+                         [[qp] * len(sizes) for _ in range(K)])
+        for k in range(K):
+            eng.collect()
+            for u, o in enumerate(units):
+                want, _ = o.frame(frames[u][f + k], 0, qp)
+                got = eng.pframe_streams(u)
+                for s in range(16):
+                    assert got[s] == want[s], f"frame {f + k} unit {u} stream {s}"
+        f += K
+    for u, o in enumerate(units):
+        assert np.array_equal(eng.recon(u), o.recon()), f"unit {u} reconstruction"
+    eng.close()
+
+
+@pytest.mark.parametrize("sizes,rng,nbatch,K,qp,seed", [
+    ([(160, 96)], 16, 1, 6, 26, 41),
+    ([(64, 48), (16, 32), (32, 16), (96, 64)], 32, 1, 5, 30, 42),
+    ([(128, 64)], 64, 1, 4, 22, 43),
+    ([(256, 144)], 32, 2, 6, 24, 44),
+    ([(16, 16), (48, 16)], 16, 2, 3, 36, 45),
+])
+def test_batched_pframes_match_oracle(built, sizes, rng, nbatch, K, qp, seed):
+    _run(sizes, rng, nbatch, K, qp, seed)
+
+
+def test_batch_size_limits(built):
+    """Batches hold P-frames only and at most fdvg_max_batch of them; learned
+    proposals bring the limit to one."""
+    import fdv_b200 as F
+    import fdv_b200.learned as LN
+    w, h = 64, 48
+    fr = F.Scene(w, h, 9, nrects=3, seed=5).frames(9)
+    eng = F.Engine([(w, h)], 16)
+    kmax = eng.max_batch()
+    assert kmax >= 2
+    with pytest.raises(F.FdvError):
+        eng.submit_batch([[fr[1]]], [[26]])      # no reference yet
+    eng.step([fr[0]], [1], [26])
+    with pytest.raises(F.FdvError):
+        eng.submit_batch([[fr[k]] for k in range(1, kmax + 2)], [[26]] * (kmax + 1))
+    eng.set_learned(LN.load_params(LN.DEFAULT_WEIGHTS), 0.8)
+    assert eng.max_batch() == 1
+    with pytest.raises(F.FdvError):
+        eng.submit_batch([[fr[1]], [fr[2]]], [[26], [26]])
+    eng.close()
