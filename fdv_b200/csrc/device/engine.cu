@@ -108,7 +108,7 @@ struct CompactTaskH {
     uint32_t *hist;
 };
 
-constexpr int kMaxBatch = 6;                // P-frames per launch at most
+constexpr int kMaxBatch = 12;               // P-frames per launch at most (12 beat 6 by 8% on hd720)
 constexpr int kRefSlots = kMaxBatch + 2;    // reference ring: a batch's outputs never alias its inputs
 constexpr int kSlots = 2 * kMaxBatch;       // frames in flight: two batches
 

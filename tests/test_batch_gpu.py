@@ -63,10 +63,10 @@ def test_batch_size_limits(built):
     import fdv_b200 as F
     import fdv_b200.learned as LN
     w, h = 64, 48
-    fr = F.Scene(w, h, 9, nrects=3, seed=5).frames(9)
     eng = F.Engine([(w, h)], 16)
     kmax = eng.max_batch()
     assert kmax >= 2
+    fr = F.Scene(w, h, kmax + 3, nrects=3, seed=5).frames(kmax + 3)
     with pytest.raises(F.FdvError):
         eng.submit_batch([[fr[1]]], [[26]])      # no reference yet
     eng.step([fr[0]], [1], [26])
