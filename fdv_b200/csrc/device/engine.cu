@@ -106,6 +106,7 @@ struct CompactTaskH {
     uint8_t *out;
     size_t cap;
     uint32_t *hist;
+    uint8_t *tmp;
 };
 
 constexpr int kMaxBatch = 12;               // P-frames per launch at most (12 beat 6 by 8% on hd720)
@@ -120,7 +121,8 @@ struct RefSlot {
 
 struct Unit {
     int w, h, mbw, mbh, cw, ch;
-    // per lane (frame of a batch; key frames use lane 0): source,
+    // per lane (frame of a batch; key frames use lane 0): source (inside the
+    // engine's lane buffer, units back to back in the staging order),
     // reconstruction (un-deblocked for P-frames), records, progress words
     // (P rows: 64-bit words, then per row the count of reference tiles
     // written; then I rows for Y, U, V), macroblock symbol slots
@@ -128,6 +130,7 @@ struct Unit {
     MBInfo *mbi[kMaxBatch] = {};
     int *progress[kMaxBatch] = {};
     uint8_t *slots[kMaxBatch] = {};
+    uint8_t *cout[kMaxBatch] = {};  // per lane: the compaction's device scratch (out_cap bytes)
     RefSlot ref[kRefSlots];
     long long seq = 0;            // references made so far (the next one goes to slot seq % kRefSlots)
     int nref = 0;
@@ -189,6 +192,8 @@ struct fdvb_engine {
     bool busy[kSlots] = {};
     int inflight = 0;
     size_t src_stage_bytes = 0;    // a slot's staging of one frame's sources (64-byte multiple)
+    size_t src_bytes = 0;          // one frame's sources, all units
+    uint8_t *lane_src[kMaxBatch] = {};   // per lane: every unit's source planes, one upload per frame
     // timing (CUDA events on the engine's stream) and launch counts
     double step_ms = 0, pk_ms = 0, ik_ms = 0;
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
@@ -221,7 +226,6 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     u.w = w; u.h = h; u.mbw = w / 16; u.mbh = h / 16; u.cw = w / 2; u.ch = h / 2;
     const size_t fs = (size_t)w * h * 3 / 2;
     for (int k = 0; k < kMaxBatch; ++k) {
-        CK(cudaMalloc(&u.cur[k], fs));
         CK(cudaMalloc(&u.rec[k], fs));
         CK(cudaMemset(u.rec[k], 0, fs));
     }
@@ -261,8 +265,10 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     size_t pcap = 64 + (size_t)nmb * kSlotData;
     size_t icap[3];
     for (int p = 0; p < 3; ++p) icap[p] = 64 + (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p];
+    for (int p = 0; p < 3; ++p) icap[p] = (icap[p] + 15) / 16 * 16;   // planes' outputs 16-byte aligned
     u.out_off_i[0] = 0; u.out_off_i[1] = icap[0]; u.out_off_i[2] = icap[0] + icap[1];
     u.out_cap = std::max(pcap, icap[0] + icap[1] + icap[2]);
+    for (int k = 0; k < kMaxBatch; ++k) CK(cudaMalloc(&u.cout[k], u.out_cap));
     return 0;
 }
 
@@ -278,7 +284,7 @@ static int unit_out(Unit &u, int k) {
 
 static void free_unit(Unit &u) {
     for (int k = 0; k < kMaxBatch; ++k) {
-        cudaFree(u.cur[k]); cudaFree(u.rec[k]);
+        cudaFree(u.rec[k]); cudaFree(u.cout[k]);
         cudaFree(u.mbi[k]); cudaFree(u.slots[k]); cudaFree(u.progress[k]);
     }
     for (int r = 0; r < kRefSlots; ++r) cudaFree(u.ref[r].mem);
@@ -337,7 +343,20 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
     size_t src_bytes = 0;
     for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
+    E->src_bytes = src_bytes;
     E->src_stage_bytes = (src_bytes + 63) / 64 * 64;
+    for (int k = 0; k < kMaxBatch; ++k) {
+        if (cudaMalloc(&E->lane_src[k], src_bytes) != cudaSuccess) {
+            g_err = "device allocation failed";
+            fdvb_engine_destroy(E);
+            return nullptr;
+        }
+        size_t off = 0;
+        for (auto &u : E->units) {
+            u.cur[k] = E->lane_src[k] + off;
+            off += (size_t)u.w * u.h * 3 / 2;
+        }
+    }
     for (auto &sl : E->slot) {
         sl.stage_cap = E->src_stage_bytes + stage_desc_bytes(nunits, maxrows, maxitasks);
         if (cudaHostAlloc(&sl.stage, sl.stage_cap, cudaHostAllocDefault) != cudaSuccess ||
@@ -365,6 +384,7 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
+    for (auto *p : E->lane_src) cudaFree(p);
     if (E->d_prof) cudaFree(E->d_prof);
     if (E->d_tl) cudaFree(E->d_tl);
     if (E->lnet) fdvl_destroy(E->lnet);
@@ -454,27 +474,25 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     }
     Slot &SL = E->slot[sis[0]];
     CK(cudaEventRecord(SL.ev[0], E->st));
-    // 1. sources (host sources through each frame's pinned staging buffer)
-    for (int k = 0; k < K; ++k) {
-        uint8_t *stage = E->slot[sis[k]].stage;
-        for (int i = 0; i < nu; ++i) {
-            Unit &u = E->units[i];
-            const int j = k * nu + i;
-            if (force_skip && force_skip[j]) continue;
-            const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
-            if (E->src_on_device) {
-                CK(cudaMemcpyAsync(u.cur[k], planes[3 * j], ys, cudaMemcpyDeviceToDevice, E->st));
-                CK(cudaMemcpyAsync(u.cur[k] + ys, planes[3 * j + 1], cs, cudaMemcpyDeviceToDevice, E->st));
-                CK(cudaMemcpyAsync(u.cur[k] + ys + cs, planes[3 * j + 2], cs, cudaMemcpyDeviceToDevice, E->st));
-            } else {
-                memcpy(stage, planes[3 * j], ys);
-                memcpy(stage + ys, planes[3 * j + 1], cs);
-                memcpy(stage + ys + cs, planes[3 * j + 2], cs);
-                CK(cudaMemcpyAsync(u.cur[k], stage, ys + 2 * cs, cudaMemcpyHostToDevice, E->st));
+    // 1. sources: device sources are read where they are; host sources go
+    // through each frame's pinned staging buffer, laid out as the lane buffer,
+    // in one upload per frame (a held unit's part is left as it is)
+    if (!E->src_on_device)
+        for (int k = 0; k < K; ++k) {
+            uint8_t *stage = E->slot[sis[k]].stage;
+            for (int i = 0; i < nu; ++i) {
+                Unit &u = E->units[i];
+                const int j = k * nu + i;
+                const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
+                if (!(force_skip && force_skip[j])) {
+                    memcpy(stage, planes[3 * j], ys);
+                    memcpy(stage + ys, planes[3 * j + 1], cs);
+                    memcpy(stage + ys + cs, planes[3 * j + 2], cs);
+                }
                 stage += ys + 2 * cs;
             }
+            CK(cudaMemcpyAsync(E->lane_src[k], E->slot[sis[k]].stage, E->src_bytes, cudaMemcpyHostToDevice, E->st));
         }
-    }
     // descriptors are staged after the first frame's sources
     uint8_t *stage = SL.stage + E->src_stage_bytes;
     auto staged = [&](const void *src, size_t n) -> const void * {
@@ -505,7 +523,11 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             const int j = k * nu + i;
             UnitDev &d = ud[j];
             d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh;
-            d.cur[0] = u.cur[k]; d.cur[1] = u.cur[k] + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
+            if (E->src_on_device && !(force_skip && force_skip[j])) {
+                d.cur[0] = planes[3 * j]; d.cur[1] = planes[3 * j + 1]; d.cur[2] = planes[3 * j + 2];
+            } else {
+                d.cur[0] = u.cur[k]; d.cur[1] = u.cur[k] + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
+            }
             d.rec[0] = u.rec[k]; d.rec[1] = u.rec[k] + (size_t)u.w * u.h; d.rec[2] = d.rec[1] + (size_t)u.cw * u.ch;
             // frame k's references: the outputs of the two frames before it
             const int nref = k == 0 ? u.nref : std::min(2, u.nref + k);
@@ -547,7 +569,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 }
                 for (int r = 0; r < u.mbh; ++r) frows.push_back({j, r});
                 CompactTaskH c{u.slots[k], u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[sis[k]], u.out_cap,
-                               u.hist_d[sis[k]]};
+                               u.hist_d[sis[k]], u.cout[k]};
                 cmp.push_back(c);
             } else {
                 iunits.push_back(i);
@@ -564,7 +586,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                     CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
                                    u.out_d[sis[k]] + u.out_off_i[p],
                                    (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p],
-                                   u.hist_d[sis[k]] + p * 12 * 256};
+                                   u.hist_d[sis[k]] + p * 12 * 256, u.cout[k] + u.out_off_i[p]};
                     cmp.push_back(c);
                 }
                 for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});

@@ -154,13 +154,17 @@ struct CompactTask {
     uint8_t *out;          // host-mapped: uint32 len[nstreams], then the streams back to back
     size_t cap;
     uint32_t *hist;        // host-mapped [nstreams][256] symbol counts, or NULL
+    uint8_t *tmp;          // device scratch of cap bytes, the output assembled before it is sent
+                           // (NULL: assembled in place, for an output in device memory)
 };
 
 // One block per task, 1024 threads: 64 threads per stream scan the slot
-// lengths, then each thread copies its chunk of slots and counts its bytes
-// into the stream's 256-bin histogram (the entropy tail's per-stream counts,
-// fdv.h:6228-6236 and :4899-4905), kept in shared memory and written out
-// beside the streams.
+// lengths, then each thread copies its chunk of slots into the device scratch
+// and counts its bytes into the stream's 256-bin histogram (the entropy
+// tail's per-stream counts, fdv.h:6228-6236 and :4899-4905), kept in shared
+// memory and written out beside the streams.  The assembled output then
+// crosses to host-mapped memory in 16-byte stores, consecutive threads on
+// consecutive words (scattered byte stores would each be a bus write).
 __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks, unsigned *err) {
     const CompactTask &T = tasks[blockIdx.x];
     const int tid = threadIdx.x, k = tid >> 6, t = tid & 63;
@@ -188,12 +192,13 @@ __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks,
     __syncthreads();
     const size_t hdr = 4 * (size_t)T.nstreams;
     if (hdr + s_base[16] > T.cap) { if (tid == 0) atomicOr(err, kErrSlotOverflow); return; }
+    uint8_t *const asmb = T.tmp ? T.tmp : T.out;
     if (tid < T.nstreams) {
         unsigned len = (tid + 1 < T.nstreams ? s_base[tid + 1] : s_base[16]) - s_base[tid];
-        reinterpret_cast<unsigned *>(T.out)[tid] = len;
+        reinterpret_cast<unsigned *>(asmb)[tid] = len;
     }
     if (k < T.nstreams) {
-        uint8_t *dst = T.out + hdr + s_base[k] + s_tot[k][t];
+        uint8_t *dst = asmb + hdr + s_base[k] + s_tot[k][t];
         for (int b = b0; b < b1; ++b) {
             const uint8_t *slot = T.slots + (size_t)b * T.slot_bytes;
             int n = reinterpret_cast<const uint16_t *>(slot)[k];
@@ -206,10 +211,20 @@ __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks,
             dst += n;
         }
     }
-    if (T.hist) {
-        __syncthreads();
-        for (int i = tid; i < T.nstreams * 256; i += 1024) T.hist[i] = s_hist[i >> 8][i & 255];
+    __syncthreads();
+    const size_t total = hdr + s_base[16];
+    if (!T.tmp) {
+        // assembled in place
+    } else if (((reinterpret_cast<uintptr_t>(T.out) | reinterpret_cast<uintptr_t>(T.tmp)) & 15) == 0) {
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(T.tmp);
+        uint4 *d4 = reinterpret_cast<uint4 *>(T.out);
+        for (size_t i = tid; i < total / 16; i += 1024) d4[i] = s4[i];
+        for (size_t i = total / 16 * 16 + tid; i < total; i += 1024) T.out[i] = T.tmp[i];
+    } else {
+        for (size_t i = tid; i < total; i += 1024) T.out[i] = T.tmp[i];
     }
+    if (T.hist)
+        for (int i = tid; i < T.nstreams * 256; i += 1024) T.hist[i] = s_hist[i >> 8][i & 255];
 }
 
 }  // namespace fdvb

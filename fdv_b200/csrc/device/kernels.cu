@@ -295,6 +295,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     CompactTask cmp;
     cmp.slots = base + o_slots; cmp.nslots = nmb; cmp.slot_bytes = kSlotBytes; cmp.nstreams = 16;
     cmp.off = reinterpret_cast<const int *>(base + o_off); cmp.out = out; cmp.cap = out_cap; cmp.hist = nullptr;
+    cmp.tmp = nullptr;   // the output is device memory: assembled in place
 
     int *ticket = reinterpret_cast<int *>(base + o_misc);
     unsigned *err = reinterpret_cast<unsigned *>(base + o_misc + 8);

@@ -207,7 +207,8 @@ int fdvg_iframe_hist(fdvg_ctx *g, int u, int plane, uint32_t *hist);
 int fdvg_recon(fdvg_ctx *g, int u, uint8_t *i420);
 /* Seed unit u's reference pool (nearest, and optionally the second). */
 int fdvg_set_refs(fdvg_ctx *g, int u, const uint8_t *near_i420, const uint8_t *far_i420);
-/* fdvg_frame with the planes already in device memory (device pointers). */
+/* fdvg_frame with the planes already in device memory (device pointers, read
+ * where they are; they stay unchanged until the call returns). */
 int fdvg_frame_device(fdvg_ctx *g, const uint8_t *const *dplanes, const int *is_intra, const int *qp,
                       const double *lscale, const int *force_skip);
 /* Device time accumulated since creation or the last reset, measured with
