@@ -301,16 +301,19 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         unsigned long long pword = 0;   // thread 0: the row above's progress word seen last
         PhaseClock pc{tid == 0 ? U.prof : nullptr, 0};
         // The post stage (post.cuh): this row posts the tiles of the row above
-        // (and the last row its own), one macroblock behind its progress, on
-        // threads 32..511 while thread 0 waits for the row above.
+        // (and the last row its own) in runs of kPostRun once that many are
+        // final, on threads 32..511 while thread 0 waits for the row above.
         int posted = 0;
-        auto post_upto = [&](int ncols) {
-            for (; posted < ncols; ++posted)
+        auto post_upto = [&](int ncols, bool all) {
+            while (ncols - posted >= kPostRun || (all && posted < ncols)) {
+                const int n = min(kPostRun, ncols - posted);
                 for (int pr = row - 1; pr <= row; ++pr) {
                     if (pr < 0 || (pr == row && row != U.mbh - 1)) continue;
-                    post_tile(S.post, U, pr, posted, tid - kPostT0);
-                    if (tid == kPostT0) st_release_gpu(U.post_prog + pr, posted + 1);
+                    post_run(S.post, U, pr, posted, posted + n, tid - kPostT0);
+                    if (tid == kPostT0) st_release_gpu(U.post_prog + pr, posted + n);
                 }
+                posted += n;
+            }
         };
         int mbx = 0;
         for (; mbx < mbw; ++mbx) {
@@ -341,7 +344,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 }
             }
             // tiles up to column mbx - 2: this row has finished macroblock mbx - 1
-            if (U.post_prog && tid >= kPostT0) post_upto(mbx - 1);
+            if (U.post_prog && tid >= kPostT0) post_upto(mbx - 1, false);
             if (tid == 0) {
                 // The row above: wait until it has finished macroblock mbx + 1
                 // (the above-right neighbour), then the above and above-right
@@ -884,7 +887,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             pc.mark(PP_OUT);
         }
         // the row's last tiles (its last macroblock is finished)
-        if (U.post_prog && mbx == mbw && tid >= kPostT0) post_upto(mbw);
+        if (U.post_prog && mbx == mbw && tid >= kPostT0) post_upto(mbw, true);
         __syncthreads();
     }
 }

@@ -22,9 +22,11 @@
 //
 // Tile (tr, tc) needs the reconstruction of macroblocks tr-1..tr+1 x
 // tc-1..tc+1 (rows 16tr-4 .. 16tr+20, the same columns).  The wavefront row
-// below posts it one macroblock behind its own progress; the last row posts
-// its own tiles.  Per macroblock row, a count of posted tiles is released at
-// GPU scope after the tile's stores (a block barrier between them).
+// below posts tiles in runs of up to kPostRun, behind its own progress; the
+// last row posts its own tiles.  Per macroblock row, a count of posted tiles
+// is released at GPU scope after the run's stores (a block barrier between).
+// A run shares the stage's fixed latencies (six barriers, a round trip to L2)
+// among its tiles.
 #pragma once
 #include "common.cuh"
 #include "engine_dev.cuh"
@@ -34,17 +36,20 @@ namespace fdvb {
 // Threads 32..511 of the P-frame block run the post stage (warp 0 is in the
 // wavefront wait meanwhile); named barrier 15 joins them.
 constexpr int kPostT0 = 32, kPostNT = 480;
+constexpr int kPostRun = 4;                 // tiles per run
+constexpr int kPW = 16 * kPostRun + 16;     // luma scratch pitch (a run's widest row plus slack)
+constexpr int kCW = 8 * kPostRun + 8;       // chroma scratch pitch
 __device__ __forceinline__ void post_bar() { asm volatile("bar.sync 15, 480;" ::: "memory"); }
 
 struct PostScratch {
-    uint8_t rec[25][28];       // reconstruction, rows vy0.., columns rx0..
-    uint8_t vp[25][24];        // after the vertical-edge pass, columns dx0..
-    uint8_t d[21][24];         // deblocked, rows dy0.., columns dx0..
-    int16_t hs[21][22];        // horizontal 6-tap sums, rows dy0.., core columns cx0..
-    uint8_t core[4][22][24];   // G, b, h, j at the core samples (rows cy0.., columns cx0..)
-    uint8_t crec[2][12][12];   // chroma reconstruction, rows cry0.., columns crx0..
-    uint8_t cv[2][12][8];      // chroma after the vertical-edge pass, columns 8tc..
-    uint8_t cd[2][8][8];       // deblocked chroma tile
+    uint8_t rec[25][kPW];       // reconstruction, rows vy0.., columns from rx4 (rx0 rounded down to 4)
+    uint8_t vp[25][kPW];        // after the vertical-edge pass, columns dx0..
+    uint8_t d[21][kPW];         // deblocked, rows dy0.., columns dx0..
+    int16_t hs[21][kPW];        // horizontal 6-tap sums, rows dy0.., core columns cx0..
+    uint8_t core[4][22][kPW];   // G, b, h, j at the core samples (rows cy0.., columns cx0..)
+    uint8_t crec[2][12][kCW];   // chroma reconstruction, rows cry0.., columns from crx4
+    uint8_t cv[2][12][kCW];     // chroma after the vertical-edge pass, columns 8tc0..
+    uint8_t cd[2][8][kCW];      // deblocked chroma, columns 8tc0..
 };
 
 // The deblocked value of the sample at a[0], position x on a line of n samples
@@ -73,64 +78,81 @@ __device__ __forceinline__ int tap6i(int a, int b, int c, int d, int e, int f) {
 }
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// Tile (tr, tc) of frame U into its reference output; t = thread index within
-// the post threads (0..479).  Ends with the post barrier after its stores.
-__device__ __noinline__ void post_tile(PostScratch &P, const UnitDev &U, int tr, int tc, int t) {
+// Tiles tc0..tc1-1 (at most kPostRun) of tile row tr of frame U into its
+// reference output; t = thread index within the post threads (0..479).  Ends
+// with the post barrier after its stores.
+__device__ __noinline__ void post_run(PostScratch &P, const UnitDev &U, int tr, int tc0, int tc1, int t) {
     const int w = U.w, h = U.h, cw = w >> 1, ch = h >> 1, mbw = U.mbw, mbh = U.mbh;
     const int B = U.range + 16;
     const int alpha = 6 + U.qp, beta = 2 + U.qp / 4, tcl = 1 + U.qp / 10;
-    const int cx0 = tc == 0 ? -3 : 16 * tc, cx1 = tc == mbw - 1 ? w + 3 : 16 * tc + 16;
+    const int cx0 = tc0 == 0 ? -3 : 16 * tc0, cx1 = tc1 == mbw ? w + 3 : 16 * tc1;
     const int cy0 = tr == 0 ? -3 : 16 * tr, cy1 = tr == mbh - 1 ? h + 3 : 16 * tr + 16;
     const int dx0 = max(0, cx0 - 2), dx1 = min(w, cx1 + 3), dy0 = max(0, cy0 - 2), dy1 = min(h, cy1 + 3);
-    const int vy0 = max(0, dy0 - 2), vy1 = min(h, dy1 + 2), rx0 = max(0, dx0 - 2), rx1 = min(w, dx1 + 2);
+    const int vy0 = max(0, dy0 - 2), vy1 = min(h, dy1 + 2);
+    const int rx4 = max(0, dx0 - 2) & ~3, rx1 = min(w, dx1 + 2);
     const int cry0 = max(0, 8 * tr - 2), cry1 = min(ch, 8 * tr + 10);
-    const int crx0 = max(0, 8 * tc - 2), crx1 = min(cw, 8 * tc + 10);
-    // a. the reconstruction (through L2: other blocks wrote most of it)
+    const int ccx0 = 8 * tc0, ccx1 = 8 * tc1;
+    const int crx4 = max(0, ccx0 - 2) & ~3, crx1 = min(cw, ccx1 + 2);
+    // a. the reconstruction (through L2: other blocks wrote most of it), in
+    // aligned 32-bit words (rows start 16-byte aligned, widths multiples of 8)
     {
-        const int nrw = rx1 - rx0, nl = (vy1 - vy0) * nrw, ncw = crx1 - crx0, ncl = (cry1 - cry0) * ncw;
-        for (int i = t; i < nl + 2 * ncl; i += kPostNT) {
+        const int nlw = (rx1 - rx4 + 3) >> 2, ncw = (crx1 - crx4 + 3) >> 2;
+        const int nl = (vy1 - vy0) * (kPW / 4), nc = (cry1 - cry0) * (kCW / 4);
+        for (int i = t; i < nl + 2 * nc; i += kPostNT) {
             if (i < nl) {
-                const int y = i / nrw, x = i - y * nrw;
-                P.rec[y][x] = __ldcg(&U.rec[0][(size_t)(vy0 + y) * w + rx0 + x]);
+                const int y = i / (kPW / 4), q = i - y * (kPW / 4);
+                if (q < nlw)
+                    *reinterpret_cast<uint32_t *>(&P.rec[y][4 * q]) =
+                        __ldcg(reinterpret_cast<const uint32_t *>(&U.rec[0][(size_t)(vy0 + y) * w + rx4 + 4 * q]));
             } else {
-                const int k = i - nl, pl = k >= ncl ? 1 : 0, kk = k - pl * ncl, y = kk / ncw, x = kk - y * ncw;
-                P.crec[pl][y][x] = __ldcg(&U.rec[1 + pl][(size_t)(cry0 + y) * cw + crx0 + x]);
+                const int k = i - nl, pl = k >= nc ? 1 : 0, kk = k - pl * nc, y = kk / (kCW / 4), q = kk - y * (kCW / 4);
+                if (q < ncw)
+                    *reinterpret_cast<uint32_t *>(&P.crec[pl][y][4 * q]) = __ldcg(
+                        reinterpret_cast<const uint32_t *>(&U.rec[1 + pl][(size_t)(cry0 + y) * cw + crx4 + 4 * q]));
             }
         }
     }
     post_bar();
     // b. vertical edges
     {
-        const int ndw = dx1 - dx0, nv = (vy1 - vy0) * ndw, ncv = (cry1 - cry0) * 8;
+        const int ndw = dx1 - dx0, nv = (vy1 - vy0) * kPW, ncv = (cry1 - cry0) * kCW, ncc = ccx1 - ccx0;
         for (int i = t; i < nv + 2 * ncv; i += kPostNT) {
             if (i < nv) {
-                const int y = i / ndw, x = dx0 + (i - y * ndw);
-                P.vp[y][x - dx0] = (uint8_t)dbk_sample(&P.rec[y][x - rx0], 1, x, w, alpha, beta, tcl);
+                const int y = i / kPW, xx = i - y * kPW;
+                if (xx < ndw) {
+                    const int x = dx0 + xx;
+                    P.vp[y][xx] = (uint8_t)dbk_sample(&P.rec[y][x - rx4], 1, x, w, alpha, beta, tcl);
+                }
             } else {
-                const int k = i - nv, pl = k >= ncv ? 1 : 0, kk = k - pl * ncv, y = kk >> 3, x = 8 * tc + (kk & 7);
-                P.cv[pl][y][kk & 7] = (uint8_t)dbk_sample(&P.crec[pl][y][x - crx0], 1, x, cw, alpha, beta, tcl);
+                const int k = i - nv, pl = k >= ncv ? 1 : 0, kk = k - pl * ncv, y = kk / kCW, xx = kk - y * kCW;
+                if (xx < ncc) {
+                    const int x = ccx0 + xx;
+                    P.cv[pl][y][xx] = (uint8_t)dbk_sample(&P.crec[pl][y][x - crx4], 1, x, cw, alpha, beta, tcl);
+                }
             }
         }
     }
     post_bar();
     // c. horizontal edges
     {
-        const int ndw = dx1 - dx0, nd = (dy1 - dy0) * ndw;
-        for (int i = t; i < nd + 2 * 64; i += kPostNT) {
+        const int ndw = dx1 - dx0, nd = (dy1 - dy0) * kPW, ncc = ccx1 - ccx0;
+        for (int i = t; i < nd + 2 * 8 * kCW; i += kPostNT) {
             if (i < nd) {
-                const int yy = i / ndw, xx = i - yy * ndw, y = dy0 + yy;
-                P.d[yy][xx] = (uint8_t)dbk_sample(&P.vp[y - vy0][xx], 24, y, h, alpha, beta, tcl);
+                const int yy = i / kPW, xx = i - yy * kPW, y = dy0 + yy;
+                if (xx < ndw) P.d[yy][xx] = (uint8_t)dbk_sample(&P.vp[y - vy0][xx], kPW, y, h, alpha, beta, tcl);
             } else {
-                const int k = i - nd, pl = k >> 6, y = 8 * tr + ((k >> 3) & 7), x = k & 7;
-                P.cd[pl][(k >> 3) & 7][x] = (uint8_t)dbk_sample(&P.cv[pl][y - cry0][x], 8, y, ch, alpha, beta, tcl);
+                const int k = i - nd, pl = k >= 8 * kCW ? 1 : 0, kk = k - pl * 8 * kCW, r = kk / kCW, xx = kk - r * kCW;
+                const int y = 8 * tr + r;
+                if (xx < ncc) P.cd[pl][r][xx] = (uint8_t)dbk_sample(&P.cv[pl][y - cry0][xx], kCW, y, ch, alpha, beta, tcl);
             }
         }
     }
     post_bar();
     // d. horizontal 6-tap sums at the core columns, every deblocked row
     const int ncx = cx1 - cx0, ncy = cy1 - cy0;
-    for (int i = t; i < (dy1 - dy0) * ncx; i += kPostNT) {
-        const int yy = i / ncx, xx = i - yy * ncx, x = cx0 + xx;
+    for (int i = t; i < (dy1 - dy0) * kPW; i += kPostNT) {
+        const int yy = i / kPW, xx = i - yy * kPW, x = cx0 + xx;
+        if (xx >= ncx) continue;
         const uint8_t *r = P.d[yy];
         int v[6];
 #pragma unroll
@@ -139,8 +161,9 @@ __device__ __noinline__ void post_tile(PostScratch &P, const UnitDev &U, int tr,
     }
     post_bar();
     // e. the four luma planes at the core samples
-    for (int i = t; i < ncy * ncx; i += kPostNT) {
-        const int yy = i / ncx, xx = i - yy * ncx, y = cy0 + yy, x = cx0 + xx;
+    for (int i = t; i < ncy * kPW; i += kPostNT) {
+        const int yy = i / kPW, xx = i - yy * kPW, y = cy0 + yy, x = cx0 + xx;
+        if (xx >= ncx) continue;
         const int yc = clampi(y, 0, h - 1) - dy0, xc = clampi(x, 0, w - 1) - dx0;
         int rv[6], rh[6];
 #pragma unroll
@@ -157,18 +180,18 @@ __device__ __noinline__ void post_tile(PostScratch &P, const UnitDev &U, int tr,
         P.core[3][yy][xx] = (uint8_t)clipb((jj + 512) >> 10);
     }
     post_bar();
-    // f. the tile's part of the padded planes, border included, as 32-bit words
+    // f. the run's part of the padded planes, border included, as 32-bit words
     {
-        const int xa = tc == 0 ? -B : 16 * tc, xb = tc == mbw - 1 ? w + B : 16 * tc + 16;
+        const int xa = tc0 == 0 ? -B : 16 * tc0, xb = tc1 == mbw ? w + B : 16 * tc1;
         const int ya = tr == 0 ? -B : 16 * tr, yb = tr == mbh - 1 ? h + B : 16 * tr + 16;
-        const int nwx = (xb - xa) >> 2, nl = 4 * (yb - ya) * nwx;
-        const int xca = tc == 0 ? -B : 8 * tc, xcb = tc == mbw - 1 ? cw + B : 8 * tc + 8;
+        const int nwx = (xb - xa) >> 2, npl = (yb - ya) * nwx, nl = 4 * npl;
+        const int xca = tc0 == 0 ? -B : 8 * tc0, xcb = tc1 == mbw ? cw + B : 8 * tc1;
         const int yca = tr == 0 ? -B : 8 * tr, ycb = tr == mbh - 1 ? ch + B : 8 * tr + 8;
         const int ncwx = (xcb - xca) >> 2, ncl = (ycb - yca) * ncwx;
         uint8_t *const lp[4] = {U.out.G, U.out.B, U.out.H, U.out.J};
         for (int i = t; i < nl + 2 * ncl; i += kPostNT) {
             if (i < nl) {
-                const int p = i / ((yb - ya) * nwx), k = i - p * (yb - ya) * nwx, yy = k / nwx, q = k - yy * nwx;
+                const int p = i / npl, k = i - p * npl, yy = k / nwx, q = k - yy * nwx;
                 const int y = ya + yy, x = xa + 4 * q;
                 const uint8_t *cr = P.core[p][clampi(y, -3, h + 2) - cy0];
                 uint32_t word = 0;
@@ -181,7 +204,7 @@ __device__ __noinline__ void post_tile(PostScratch &P, const UnitDev &U, int tr,
                 const uint8_t *cr = P.cd[pl][clampi(y, 0, ch - 1) - 8 * tr];
                 uint32_t word = 0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b) word |= (uint32_t)cr[clampi(x + b, 0, cw - 1) - 8 * tc] << (8 * b);
+                for (int b = 0; b < 4; ++b) word |= (uint32_t)cr[clampi(x + b, 0, cw - 1) - ccx0] << (8 * b);
                 *reinterpret_cast<uint32_t *>((pl ? U.out.V : U.out.U) + (long)y * U.out.cs + x) = word;
             }
         }
