@@ -693,7 +693,7 @@ def main() -> None:
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "pframe_kernel_hd720_traffic.json")) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            traffic = json.load(f).get("dram_bytes_per_pframe")
     except OSError:
         pass
     int_pipe = None   # the integer-pipe utilisation of the same kernel, from one ncu capture
