@@ -446,8 +446,8 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     const int nu = (int)E->units.size();
     if (K < 1 || K > kMaxBatch) { g_err = "batch size out of range"; return -1; }
     if (E->inflight + K > kSlots) { g_err = "too many frames in flight"; return -1; }
-    if (K > 1 && (E->lnet || E->d_mbcost || E->defer_refs)) {
-        g_err = "batches of P-frames need the plain analysis without records or deferred references";
+    if (K > 1 && (E->d_mbcost || E->defer_refs)) {
+        g_err = "batches of P-frames need decision records and deferred references off";
         return -1;
     }
     for (int k = 0; k < K; ++k)
@@ -514,7 +514,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     // lengthen the wavefront; the form runs one frame per launch anyway)
     std::vector<int> iunits;
     std::vector<int2> pu;     // P units and their first macroblock in the hint array
-    int nhint = 0;
+    int nhint = 0, npu0 = 0, nhint0 = 0;   // frame 0's share (its SKIP pre-analysis)
     for (int k = 0; k < K; ++k) {
         std::vector<RowTask> frows;
         E->slot[sis[k]].intra.assign(nu, 0);
@@ -548,15 +548,22 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             d.out = OutPlanes{};
             d.post_prog = nullptr;
             d.ref_prog = nullptr;
+            d.lref = nullptr;
+            d.lrs = 0;
             if (!is_intra[j] && E->lnet) {
-                pu.push_back(make_int2(i, nhint));
+                pu.push_back(make_int2(j, nhint));
                 d.hint = E->d_hints + nhint;
-                d.prejs = E->d_prejs + nhint;
+                // the SKIP pre-analysis needs the reference before the
+                // launch: frame 0 of a batch only; later frames infer
+                // against the previous frame's source
+                d.prejs = k == 0 ? E->d_prejs + nhint : nullptr;
+                if (k > 0) { d.lref = ud[j - nu].cur[0]; d.lrs = u.w; }
                 nhint += u.mbw * u.mbh;
+                if (k == 0) { npu0 = (int)pu.size(); nhint0 = nhint; }
             }
             u.last_qp = qp[j];
             if (!is_intra[j]) {
-                if (E->lnet) {
+                if (E->lnet && K == 1) {
                     iunits.push_back(i);
                     for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});
                 } else {
@@ -629,7 +636,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 g_err = std::string("learned inference: ") + fdvl_last_error();
                 return -3;
             }
-            launch_lrn_preskip(E->d_units, E->d_pu, (int)pu.size(), nhint, E->st);
+            if (npu0 > 0) launch_lrn_preskip(E->d_units, E->d_pu, npu0, nhint0, E->st);
             E->launches += 2;
         }
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range,
@@ -710,7 +717,7 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
 // proposals, decision records or deferred references).
 extern "C" int fdvb_engine_max_batch(const fdvb_engine *E) {
     if (!E) return 0;
-    return (E->lnet || E->d_mbcost || E->defer_refs) ? 1 : kMaxBatch;
+    return (E->d_mbcost || E->defer_refs) ? 1 : kMaxBatch;
 }
 
 // Wait for the oldest submitted frame; on success the stream views
@@ -931,11 +938,12 @@ extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, floa
         return 0;
     }
     if (!E->lnet) {
-        E->lnet = lrn_create(E->device, E->total_mbs, 0, 16, 16);
+        // sized for a batch: every P-frame of a launch is inferred in one pass
+        E->lnet = lrn_create(E->device, kMaxBatch * E->total_mbs, 0, 16, 16);
         if (!E->lnet) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
-        if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * E->total_mbs));
-        if (!E->d_prejs) CK(cudaMalloc(&E->d_prejs, sizeof(float) * E->total_mbs));
-        if (!E->d_pu) CK(cudaMalloc(&E->d_pu, sizeof(int2) * E->units.size()));
+        if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * kMaxBatch * E->total_mbs));
+        if (!E->d_prejs) CK(cudaMalloc(&E->d_prejs, sizeof(float) * kMaxBatch * E->total_mbs));
+        if (!E->d_pu) CK(cudaMalloc(&E->d_pu, sizeof(int2) * kMaxBatch * E->units.size()));
     }
     CK(cudaStreamSynchronize(E->st));
     if (fdvl_set_params(E->lnet, params) != 0) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }

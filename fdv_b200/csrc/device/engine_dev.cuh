@@ -41,6 +41,12 @@ struct UnitDev {
     // macroblock waits for the tiles its reference reads reach (NULL: the
     // references are complete).
     const int *ref_prog;
+    // The learned inference's reference luma (stride lrs) when it is not the
+    // nearest reference: frames after the first of a batched launch use the
+    // previous frame's source (their reference does not exist before the
+    // launch).  NULL: ref[0].G.
+    const uint8_t *lref;
+    int lrs;
 };
 
 // Phases of a macroblock, for the optional cycle profile.

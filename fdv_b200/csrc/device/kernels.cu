@@ -286,7 +286,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     u.lambda = fdvb_lambda(qp, lscale);
     u.qp = qp; u.navail = far_ref ? 2 : 1; u.force_skip = 0; u.range = range; u.stall_row = -1; u.prof = nullptr;
     u.hint = nullptr; u.mbcost = nullptr; u.skip_gate = 0.0; u.inter8 = 0; u.prejs = nullptr; u.tl = nullptr;
-    u.out = OutPlanes{}; u.post_prog = nullptr; u.ref_prog = nullptr;
+    u.out = OutPlanes{}; u.post_prog = nullptr; u.ref_prog = nullptr; u.lref = nullptr; u.lrs = 0;
     RowTask rows[8192 / 16];
     for (int r = 0; r < mbh; ++r) rows[r] = {0, r};
     DbTask db[3] = {{rec, w, h, qp}, {rec + (size_t)w * h, cw, ch, qp}, {rec + (size_t)w * h + (size_t)cw * ch, cw, ch, qp}};

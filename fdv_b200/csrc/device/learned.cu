@@ -773,8 +773,8 @@ __global__ void unit_samples_kernel(const UnitDev *__restrict__ U, const int2 *_
     Sample q{};
     q.cur = u.cur[0];
     q.cs = u.w;
-    q.ref = u.ref[0].G;
-    q.rs = u.ref[0].ys;
+    q.ref = u.lref ? u.lref : u.ref[0].G;
+    q.rs = u.lref ? u.lrs : u.ref[0].ys;
     q.w = u.w;
     q.h = u.h;
     q.bx = (mb % u.mbw) * 16;

@@ -267,11 +267,16 @@ def container(w: int, h: int, qp: int, keyint: int, blobs: list[bytes]) -> bytes
 
 
 def encode_engine(frames, w: int, h: int, qp: int, keyint: int = 0, params=None, conf=0.8,
-                  search_range: int = RANGE, device: int = 0):
+                  search_range: int = RANGE, device: int = 0, batch: int = 1):
     """One stream through the engine and the host entropy tail, plain or with
-    learned proposals; returns (stream, reconstructions, P-frame analysis ms)."""
+    learned proposals; returns (stream, reconstructions, P-frame analysis ms).
+    batch > 1: runs of up to `batch` P-frames per launch (fdvg_submit_batch),
+    the reconstructions then taken from decoding the stream (the decoder's
+    frames equal the encoder's reconstruction)."""
     import struct
-    from . import Engine, TabCache, entropy_image, entropy_pframe
+    from . import Engine, TabCache, entropy_image, entropy_pframe, video_decode
+    if batch > 1:
+        return _encode_engine_batched(frames, w, h, qp, keyint, params, conf, search_range, device, batch)
     eng = Engine([(w, h)], search_range, device)
     if params is not None:
         if np.ndim(conf):
@@ -298,6 +303,47 @@ def encode_engine(frames, w: int, h: int, qp: int, keyint: int = 0, params=None,
     st = eng.stats()
     eng.close()
     return container(w, h, qp, keyint, blobs), recs, st
+
+
+def _encode_engine_batched(frames, w, h, qp, keyint, params, conf, search_range, device, batch):
+    import struct
+    from . import Engine, TabCache, entropy_image, entropy_pframe, video_decode
+    eng = Engine([(w, h)], search_range, device)
+    if params is not None:
+        if np.ndim(conf):
+            eng.set_learned(params, 0.8)
+            eng.set_learned_conf(conf[:3], conf[3] if len(conf) > 3 else 0.0, bool(conf[4]) if len(conf) > 4 else False)
+        else:
+            eng.set_learned(params, conf)
+    batch = min(batch, eng.max_batch())
+    tc = TabCache()
+    blobs = []
+    pw, ph = [w, w // 2, w // 2], [h, h // 2, h // 2]
+    key = lambda f: f == 0 or (keyint > 0 and f % keyint == 0)
+    f = 0
+    while f < len(frames):
+        if key(f):
+            eng.step([frames[f]], [1], [qp])
+            tc.reset()
+            b = bytearray()
+            for p in range(3):
+                pb = entropy_image(eng.iframe_streams(0, p), pw[p], ph[p], qp)
+                b += struct.pack("<I", len(pb)) + pb
+            blobs.append(bytes(b))
+            f += 1
+            continue
+        n = 1
+        while n < batch and f + n < len(frames) and not key(f + n):
+            n += 1
+        eng.submit_batch([[frames[f + k]] for k in range(n)], [[qp]] * n)
+        for _ in range(n):
+            eng.collect()
+            blobs.append(entropy_pframe(eng.pframe_streams(0), qp, tc))
+        f += n
+    st = eng.stats()
+    eng.close()
+    stream = container(w, h, qp, keyint, blobs)
+    return stream, list(video_decode(stream)), st
 
 
 def psnr_y(src, rec, w: int, h: int) -> float:
@@ -346,7 +392,7 @@ def bd_rate(ref_pts, new_pts):
 
 
 def evaluate(params, conf=0.8, qps=QPS, nframes: int = 30, seeds=(1, 2), w: int = W, h: int = H,
-             search_range: int = RANGE, device: int = 0) -> dict:
+             search_range: int = RANGE, device: int = 0, batch: int = 1) -> dict:
     """The learned form against the plain form on held-out seeds: per QP the
     bytes, luma PSNR and P-frame analysis time of both, and the BD-rate."""
     from . import Scene
@@ -358,8 +404,8 @@ def evaluate(params, conf=0.8, qps=QPS, nframes: int = 30, seeds=(1, 2), w: int 
         pp = pl = 0.0
         for sd in seeds:
             frames = Scene(w, h, nframes, seed=sd, **CONTENT).frames(nframes)
-            s0, r0, st0 = encode_engine(frames, w, h, qp, 0, None, conf, search_range, device)
-            s1, r1, st1 = encode_engine(frames, w, h, qp, 0, params, conf, search_range, device)
+            s0, r0, st0 = encode_engine(frames, w, h, qp, 0, None, conf, search_range, device, batch)
+            s1, r1, st1 = encode_engine(frames, w, h, qp, 0, params, conf, search_range, device, batch)
             bp += len(s0)
             bl += len(s1)
             pp += psnr_y(frames, r0, w, h) / len(seeds)

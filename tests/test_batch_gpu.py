@@ -58,10 +58,9 @@ def test_batched_pframes_match_oracle(built, sizes, rng, nbatch, K, qp, seed):
 
 
 def test_batch_size_limits(built):
-    """Batches hold P-frames only and at most fdvg_max_batch of them; learned
-    proposals bring the limit to one."""
+    """Batches hold P-frames only and at most fdvg_max_batch of them; decision
+    records bring the limit to one."""
     import fdv_b200 as F
-    import fdv_b200.learned as LN
     w, h = 64, 48
     eng = F.Engine([(w, h)], 16)
     kmax = eng.max_batch()
@@ -72,8 +71,25 @@ def test_batch_size_limits(built):
     eng.step([fr[0]], [1], [26])
     with pytest.raises(F.FdvError):
         eng.submit_batch([[fr[k]] for k in range(1, kmax + 2)], [[26]] * (kmax + 1))
-    eng.set_learned(LN.load_params(LN.DEFAULT_WEIGHTS), 0.8)
+    eng.set_records(True)
     assert eng.max_batch() == 1
     with pytest.raises(F.FdvError):
         eng.submit_batch([[fr[1]], [fr[2]]], [[26], [26]])
     eng.close()
+
+
+def test_learned_batch_stream(built):
+    """The learned form in batches: the stream decodes; the batch's first
+    P-frame (reference-based inference and SKIP pre-analysis, as one frame per
+    launch) reconstructs exactly as frame-by-frame coding; the later frames
+    (inference against the previous source) keep the quality within 0.3 dB."""
+    import fdv_b200 as F
+    import fdv_b200.learned as LN
+    w, h, n = 160, 96, 9
+    frames = F.Scene(w, h, n, seed=7, **LN.CONTENT).frames(n)
+    p = LN.load_params(LN.DEFAULT_WEIGHTS)
+    sb, rb, _ = LN.encode_engine(frames, w, h, 23, 0, p, 0.8, LN.RANGE, 0, batch=8)
+    s1, r1, _ = LN.encode_engine(frames, w, h, 23, 0, p, 0.8, LN.RANGE, 0, batch=1)
+    assert len(rb) == n
+    assert np.array_equal(rb[0], r1[0]) and np.array_equal(rb[1], r1[1])
+    assert abs(LN.psnr_y(frames, rb, w, h) - LN.psnr_y(frames, r1, w, h)) < 0.3
