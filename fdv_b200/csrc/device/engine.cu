@@ -109,7 +109,7 @@ struct CompactTaskH {
     uint8_t *tmp;
 };
 
-constexpr int kMaxBatch = 12;               // P-frames per launch at most (12 beat 6 by 8% on hd720)
+constexpr int kMaxBatch = 30;               // P-frames per launch at most (hd720 Mpix/s: 6 -> 505, 12 -> 667, 24 -> 696, 30 -> 711)
 constexpr int kRefSlots = kMaxBatch + 2;    // reference ring: a batch's outputs never alias its inputs
 constexpr int kSlots = 2 * kMaxBatch;       // frames in flight: two batches
 

@@ -165,15 +165,15 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
 /* fdvg_frame in two halves, so a host can entropy-code one frame while the GPU
  * analyses the next: fdvg_submit copies the sources (through pinned staging;
  * the caller may reuse its buffers on return) and queues the frame; at most
- * 24 frames are in flight.  fdvg_collect waits for the oldest one, after
+ * 60 frames are in flight.  fdvg_collect waits for the oldest one, after
  * which the stream and count accessors describe it until the next
  * fdvg_collect.  A collected frame's streams stay valid until the next
  * submission. */
 int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
                 const double *lscale, const int *force_skip);
 int fdvg_collect(fdvg_ctx *g);
-/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (twelve; one
- * while learned proposals, decision records or deferred references are on):
+/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (thirty; one
+ * while decision records or deferred references are on):
  * the arrays hold frame k's entries at k * nunits (planes: 3 per unit).  The
  * frames' wavefronts run in one launch, each frame's macroblock rows starting
  * as soon as the reference tiles they read have been written by the frame
