@@ -408,11 +408,14 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     prof_add(c.prof, t, IP_L4TRIAL, tp);
     tp = prof_t0(c.prof, t);
     // commit: every warp writes the winner into the tile (the next leaf's
-    // neighbours come from this warp's own writes), thread 0 the symbols
+    // neighbours come from this warp's own writes); warp 3, which does not
+    // screen, the symbols, while warps 0-2 go on to the next leaf's screen
+    // (it reaches the barrier after that screen before the next trials
+    // rewrite C.fin)
     const Blk4 &F = C.fin[fsel];
     if (lane < 16) TL(C, ty + (lane >> 2), tx + (lane & 3)) = C.frec[fsel][lane];
     __syncwarp();
-    if (t == 0) {
+    if (t == 96) {
         cs_put1(&tgt->c, CS_N, (uint8_t)F.count, c.err);
         cs_put(&tgt->c, CS_L, F.bytes, F.nbytes, c.err);
         const int lcx = tx >> 2, lcy = ty >> 2;
