@@ -61,6 +61,31 @@ void stream_header(std::vector<uint8_t> &b, int nframes, int w, int h, int qp, i
 
 // Entropy-code unit u's analysis output of the engine's last step into
 // us.tmp; returns the blob length (0 on failure).
+// The blob of one unit-frame from its streams (P-frame: s[0]; key frame:
+// s[0..2], the planes).
+size_t code_blob_streams(const fdvb_streams *s, UnitStream &us, int is_intra, int qp) {
+    size_t blob = 0;
+    if (us.tmp.size() < us.tmp_cap) us.tmp.resize(us.tmp_cap);
+    if (is_intra) {
+        memset(us.tc.get(), 0, sizeof(fdvb_tabcache));
+        const int pw[3] = {us.w, us.w / 2, us.w / 2}, ph[3] = {us.h, us.h / 2, us.h / 2};
+        size_t o = 0;
+        for (int p = 0; p < 3; ++p) {
+            size_t bcap = (size_t)pw[p] * ph[p] * 2 + 4096;
+            std::vector<uint8_t> pb(bcap);
+            size_t bl = fdvb_image_blob(&s[p], pw[p], ph[p], qp, pb.data(), bcap, nullptr);
+            if (!bl || o + 4 + bl > us.tmp_cap) return 0;
+            o = fdvb_put32(us.tmp.data(), o, (uint32_t)bl);
+            memcpy(us.tmp.data() + o, pb.data(), bl);
+            o += bl;
+        }
+        blob = o;
+    } else {
+        blob = fdvb_pframe_blob(&s[0], qp, us.tc.get(), us.tmp.data(), us.tmp_cap, nullptr);
+    }
+    return blob;
+}
+
 size_t code_unit_blob(fdvb_engine *E, int u, UnitStream &us, int is_intra, int qp) {
     size_t blob = 0;
     if (us.tmp.size() < us.tmp_cap) us.tmp.resize(us.tmp_cap);
@@ -363,6 +388,10 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             K = 1;
             if (!key_at(f))
                 while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
+            // the sequence's last batch is coded after the GPU has finished:
+            // keep it short
+            constexpr int kTail = 6;
+            if (f + K == nframes && K > 2 * kTail) K -= kTail;
             for (int k = 0; k < K; ++k) {
                 const uint8_t *fy = frames[f + k], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
                 for (int b = 0; b < nb; ++b) {
@@ -380,13 +409,34 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             }
             for (int k = 0; k < K; ++k) types.push_back(key_at(f + k));
         }
-        // code the previous batch while the GPU runs this one
+        // code the previous batch while the GPU runs this one: collect its
+        // frames (their streams stay in their slots until the next
+        // submission), then every band codes them in order as one task
+        std::vector<int> btype;
+        std::vector<std::vector<fdvb_streams>> bst(nb);
         for (size_t c = 0; c < prev && rc == 0; ++c) {
             const int ti = types.front();
             types.pop_front();
             if (fdvb_engine_collect(E) != 0) { set_engine_err(); rc = -1; break; }
+            btype.push_back(ti);
+            for (int b = 0; b < nb; ++b)
+                for (int p = 0; p < (ti ? 3 : 1); ++p) {
+                    const fdvb_streams *s = ti ? fdvb_engine_istreams(E, b, p) : fdvb_engine_pstreams(E, b);
+                    if (!s) { set_err("no streams for a collected frame"); rc = -1; break; }
+                    bst[b].push_back(*s);
+                }
+        }
+        if (rc == 0 && !btype.empty()) {
             std::fill(urc.begin(), urc.end(), 0);
-            pool.run(nb, [&](int u) { urc[u] = code_unit_frame(E, u, us[u], ti, qp); });
+            pool.run(nb, [&](int u) {
+                size_t o = 0;
+                for (int ti : btype) {
+                    const size_t blob = code_blob_streams(&bst[u][o], us[u], ti, qp);
+                    if (!blob) { urc[u] = -1; return; }
+                    append_blob(us[u], blob);
+                    o += ti ? 3 : 1;
+                }
+            });
             for (int r : urc) if (r) { set_err("entropy coding failed"); rc = -1; }
         }
         if (K == 0) break;
