@@ -211,9 +211,21 @@ struct fdvb_engine {
     float3 lconf = {0.8f, 0.8f, 0.8f};       // per class: SKIP, inter, intra (> 1: never)
     double lgate = 0.0;                      // confident SKIP needs J <= lgate * lambda (0: always)
     int linter8 = 0;                         // confident inter also tries INTER8
-    lrn::Hint *d_hints = nullptr;
+    lrn::Hint *d_hints = nullptr;            // two buffers (by batch parity) of kMaxBatch x total_mbs
     float *d_prejs = nullptr;                // per hinted macroblock: the SKIP pre-analysis (lrn_preskip_kernel)
     int2 *d_pu = nullptr;
+    // The inference runs on its own stream.  With device-resident sources a
+    // batch's inference needs nothing of the batch before it (every frame
+    // infers against the previous frame's source), so it runs while that
+    // batch is analysed, on SMs the analysis leaves free; otherwise the
+    // inference stream waits for the main one.
+    cudaStream_t st_inf = nullptr;
+    cudaEvent_t ev_inf = nullptr, ev_main = nullptr, ev_hfree[2] = {nullptr, nullptr};
+    UnitDev *d_units_inf[2] = {nullptr, nullptr};
+    int2 *d_pu_inf[2] = {nullptr, nullptr};
+    unsigned *d_err_inf = nullptr;           // two words, by batch parity
+    int hpar = 0;                            // hint buffer of the next batch
+    std::vector<const uint8_t *> prev_luma;  // per unit: the last submitted frame's luma (device sources)
     int total_mbs = 0;
     float *d_mbcost = nullptr;              // per-macroblock RD cost records (when enabled)
 };
@@ -315,7 +327,16 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     E->border = range + 16;
     if (cudaSetDevice(device) != cudaSuccess) { g_err = "cudaSetDevice failed (no GPU?)"; delete E; return nullptr; }
     cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, device);
-    if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess) { g_err = "stream create failed"; delete E; return nullptr; }
+    if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&E->st_inf, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_inf, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_main, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_hfree[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_hfree[1], cudaEventDisableTiming) != cudaSuccess) {
+        g_err = "stream create failed";
+        fdvb_engine_destroy(E);
+        return nullptr;
+    }
     for (auto &sl : E->slot) for (auto &e : sl.ev) cudaEventCreate(&e);
     int32_t c8[64], q8[52];
     fdvb_c8_tables(c8, q8);
@@ -328,6 +349,7 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
         for (int p = 0; p < 3; ++p) maxitasks += E->units[i].irows[p];
     }
     E->maxrows = maxrows; E->maxitasks = maxitasks;
+    E->prev_luma.assign(nunits, nullptr);
     for (auto &u : E->units) { u.mb_off = E->total_mbs; E->total_mbs += u.mbw * u.mbh; }
     bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * kMaxBatch * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_rows, sizeof(RowTask) * kMaxBatch * maxrows) == cudaSuccess &&
@@ -338,6 +360,7 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
               cudaMalloc(&E->d_cmp, sizeof(CompactTaskH) * 3 * kMaxBatch * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_ticket, sizeof(int) * 2) == cudaSuccess &&
               cudaMalloc(&E->d_err, sizeof(unsigned)) == cudaSuccess &&
+              cudaMalloc(&E->d_err_inf, 2 * sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc(&E->d_poff, sizeof(int) * 16) == cudaSuccess &&
               cudaMalloc(&E->d_ioff, sizeof(int) * 12) == cudaSuccess;
     if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
@@ -389,6 +412,10 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     if (E->d_tl) cudaFree(E->d_tl);
     if (E->lnet) fdvl_destroy(E->lnet);
     cudaFree(E->d_hints); cudaFree(E->d_prejs); cudaFree(E->d_pu); cudaFree(E->d_mbcost);
+    for (int k = 0; k < 2; ++k) { cudaFree(E->d_units_inf[k]); cudaFree(E->d_pu_inf[k]); }
+    cudaFree(E->d_err_inf);
+    if (E->st_inf) { cudaStreamSynchronize(E->st_inf); cudaStreamDestroy(E->st_inf); }
+    for (cudaEvent_t e : {E->ev_inf, E->ev_main, E->ev_hfree[0], E->ev_hfree[1]}) if (e) cudaEventDestroy(e);
     for (auto &sl : E->slot) {
         for (auto &e : sl.ev) if (e) cudaEventDestroy(e);
         if (sl.stage) cudaFreeHost(sl.stage);
@@ -515,6 +542,14 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     std::vector<int> iunits;
     std::vector<int2> pu;     // P units and their first macroblock in the hint array
     int nhint = 0, npu0 = 0, nhint0 = 0;   // frame 0's share (its SKIP pre-analysis)
+    // Inference ahead of the analysis (device sources, several frames, every
+    // unit's previous frame known): frame 0 too infers against the previous
+    // frame's source, so nothing of the batch before is needed.
+    bool ahead = E->lnet && E->src_on_device && K > 1;
+    for (int i = 0; i < nu && ahead; ++i) if (!E->prev_luma[i]) ahead = false;
+    const int hpar = E->hpar;
+    lrn::Hint *const hbase = E->d_hints ? E->d_hints + (size_t)hpar * kMaxBatch * E->total_mbs : nullptr;
+    float *const pbase = E->d_prejs ? E->d_prejs + (size_t)hpar * kMaxBatch * E->total_mbs : nullptr;
     for (int k = 0; k < K; ++k) {
         std::vector<RowTask> frows;
         E->slot[sis[k]].intra.assign(nu, 0);
@@ -552,12 +587,13 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             d.lrs = 0;
             if (!is_intra[j] && E->lnet) {
                 pu.push_back(make_int2(j, nhint));
-                d.hint = E->d_hints + nhint;
+                d.hint = hbase + nhint;
                 // the SKIP pre-analysis needs the reference before the
                 // launch: frame 0 of a batch only; later frames infer
                 // against the previous frame's source
-                d.prejs = k == 0 ? E->d_prejs + nhint : nullptr;
+                d.prejs = k == 0 ? pbase + nhint : nullptr;
                 if (k > 0) { d.lref = ud[j - nu].cur[0]; d.lrs = u.w; }
+                else if (ahead) { d.lref = E->prev_luma[i]; d.lrs = u.w; }
                 nhint += u.mbw * u.mbh;
                 if (k == 0) { npu0 = (int)pu.size(); nhint0 = nhint; }
             }
@@ -618,24 +654,50 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             for (auto &t : itasks) if (t.row == r) it2.push_back(t);
         itasks.swap(it2);
     }
-    CK(cudaMemcpyAsync(E->d_units, staged(ud.data(), sizeof(UnitDev) * K * nu), sizeof(UnitDev) * K * nu,
-                       cudaMemcpyHostToDevice, E->st));
+    const void *ud_st = staged(ud.data(), sizeof(UnitDev) * K * nu);
+    CK(cudaMemcpyAsync(E->d_units, ud_st, sizeof(UnitDev) * K * nu, cudaMemcpyHostToDevice, E->st));
     CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
     CK(cudaMemsetAsync(E->d_err, 0, sizeof(unsigned), E->st));
     if (!rows.empty()) {
         CK(cudaMemcpyAsync(E->d_rows, staged(rows.data(), sizeof(RowTask) * rows.size()), sizeof(RowTask) * rows.size(),
                            cudaMemcpyHostToDevice, E->st));
         int grid = std::min((int)rows.size(), E->nsm);
-        if (!pu.empty())
-            CK(cudaMemcpyAsync(E->d_pu, staged(pu.data(), sizeof(int2) * pu.size()), sizeof(int2) * pu.size(),
-                               cudaMemcpyHostToDevice, E->st));
+        // with the next batch's inference running beside this launch, leave
+        // it some SMs
+        constexpr int kInferSMs = 40;
+        if (E->lnet && E->src_on_device && K > 1) grid = std::min(grid, std::max(1, E->nsm - kInferSMs));
+        const void *pu_st = nullptr;
+        if (!pu.empty()) {
+            pu_st = staged(pu.data(), sizeof(int2) * pu.size());
+            CK(cudaMemcpyAsync(E->d_pu, pu_st, sizeof(int2) * pu.size(), cudaMemcpyHostToDevice, E->st));
+        }
         CK(cudaEventRecord(SL.ev[1], E->st));
         if (!pu.empty()) {
-            if (lrn_infer_units(E->lnet, E->d_units, E->d_pu, (int)pu.size(), nhint, E->lconf, 4 * E->range,
-                                E->d_hints, E->d_err, E->st) != 0) {
+            // the inference stream: not before the analysis that last read
+            // this hint buffer; ahead of this batch's analysis when it can
+            // be, else after this batch's uploads
+            const UnitDev *iu = E->d_units;
+            const int2 *ip = E->d_pu;
+            CK(cudaStreamWaitEvent(E->st_inf, E->ev_hfree[hpar], 0));
+            if (ahead) {
+                CK(cudaMemcpyAsync(E->d_units_inf[hpar], ud_st, sizeof(UnitDev) * K * nu, cudaMemcpyHostToDevice,
+                                   E->st_inf));
+                CK(cudaMemcpyAsync(E->d_pu_inf[hpar], pu_st, sizeof(int2) * pu.size(), cudaMemcpyHostToDevice,
+                                   E->st_inf));
+                iu = E->d_units_inf[hpar];
+                ip = E->d_pu_inf[hpar];
+            } else {
+                CK(cudaEventRecord(E->ev_main, E->st));
+                CK(cudaStreamWaitEvent(E->st_inf, E->ev_main, 0));
+            }
+            CK(cudaMemsetAsync(E->d_err_inf + hpar, 0, sizeof(unsigned), E->st_inf));
+            if (lrn_infer_units(E->lnet, iu, ip, (int)pu.size(), nhint, E->lconf, 4 * E->range, hbase,
+                                E->d_err_inf + hpar, E->st_inf) != 0) {
                 g_err = std::string("learned inference: ") + fdvl_last_error();
                 return -3;
             }
+            CK(cudaEventRecord(E->ev_inf, E->st_inf));
+            CK(cudaStreamWaitEvent(E->st, E->ev_inf, 0));
             if (npu0 > 0) launch_lrn_preskip(E->d_units, E->d_pu, npu0, nhint0, E->st);
             E->launches += 2;
         }
@@ -643,6 +705,10 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                       !pu.empty(), E->st);
         CK(cudaGetLastError());
         CK(cudaEventRecord(SL.ev[2], E->st));
+        if (!pu.empty()) {
+            CK(cudaEventRecord(E->ev_hfree[hpar], E->st));   // this hint buffer is free again
+            E->hpar ^= 1;
+        }
         E->launches += 1;
     }
     if (!itasks.empty()) {
@@ -691,9 +757,17 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             u.seq += K;
         }
     }
+    for (int i = 0; i < nu; ++i) {
+        const int j = (K - 1) * nu + i;
+        E->prev_luma[i] = (E->src_on_device && !(force_skip && force_skip[j])) ? ud[j].cur[0] : nullptr;
+    }
     for (int k = 0; k < K; ++k) {
         Slot &S = E->slot[sis[k]];
         CK(cudaMemcpyAsync(S.err_h, E->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
+        if (!pu.empty())   // the inference's error word (the main stream has waited for it)
+            CK(cudaMemcpyAsync(S.err_h + 1, E->d_err_inf + hpar, sizeof(unsigned), cudaMemcpyDeviceToHost, E->st));
+        else
+            S.err_h[1] = 0;
         CK(cudaEventRecord(S.ev[5], E->st));
         S.has_p = !rows.empty();
         S.has_i = !itasks.empty();
@@ -741,7 +815,7 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
         if (SL.has_p) { cudaEventElapsedTime(&ms, SL.ev[1], SL.ev[2]); E->pk_ms += ms; E->pk_n += SL.batch; }
         if (SL.has_i) { cudaEventElapsedTime(&ms, SL.ev[3], SL.ev[4]); E->ik_ms += ms; E->ik_n += 1; }
     }
-    const unsigned err = *SL.err_h;
+    const unsigned err = SL.err_h[0] | SL.err_h[1];
     if (err) {
         g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out"
                 : (err & kErrMmaTimeout) ? "tensor-core completion wait timed out" : "symbol slot overflow";
@@ -941,9 +1015,13 @@ extern "C" int fdvb_engine_set_learned(fdvb_engine *E, const float *params, floa
         // sized for a batch: every P-frame of a launch is inferred in one pass
         E->lnet = lrn_create(E->device, kMaxBatch * E->total_mbs, 0, 16, 16);
         if (!E->lnet) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
-        if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * kMaxBatch * E->total_mbs));
-        if (!E->d_prejs) CK(cudaMalloc(&E->d_prejs, sizeof(float) * kMaxBatch * E->total_mbs));
+        if (!E->d_hints) CK(cudaMalloc(&E->d_hints, sizeof(lrn::Hint) * 2 * kMaxBatch * E->total_mbs));
+        if (!E->d_prejs) CK(cudaMalloc(&E->d_prejs, sizeof(float) * 2 * kMaxBatch * E->total_mbs));
         if (!E->d_pu) CK(cudaMalloc(&E->d_pu, sizeof(int2) * kMaxBatch * E->units.size()));
+        for (int k = 0; k < 2; ++k) {
+            if (!E->d_units_inf[k]) CK(cudaMalloc(&E->d_units_inf[k], sizeof(UnitDev) * kMaxBatch * E->units.size()));
+            if (!E->d_pu_inf[k]) CK(cudaMalloc(&E->d_pu_inf[k], sizeof(int2) * kMaxBatch * E->units.size()));
+        }
     }
     CK(cudaStreamSynchronize(E->st));
     if (fdvl_set_params(E->lnet, params) != 0) { g_err = std::string("learned network: ") + fdvl_last_error(); return -3; }
