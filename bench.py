@@ -539,8 +539,9 @@ def run_learned(local: int) -> dict:
                     "other_mbs": "full search seeded with the proposals"},
         "workload": f"learned: 1280x720, {LEARN_NF} frames (1 key), QP {LEARN_QP}, range 16, 6 moving rectangles "
                     f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, 20 frames; "
-                    "P-frames in launches of up to 12 (after a batch's first frame the inference reads the "
-                    "previous frame's source; the SKIP pre-analysis runs for a batch's first frame)",
+                    "P-frames in launches of up to 30 (the inference reads the previous frame's source: for "
+                    "every frame with device-resident sources, after a batch's first frame with host sources; "
+                    "the SKIP pre-analysis runs for a batch's first frame)",
         "weights": "fdv_b200/proposal_c4.f32",
     }
 
