@@ -8,14 +8,15 @@
 //      rows and the intra CTU-wavefront kernel over every key-frame unit's
 //      plane CTU rows;
 //   3. key frames: deblock, vertical edges then horizontal edges, every plane
-//      (P-frames deblock inside the wavefront, post.cuh; the learned form's
-//      P-frames as key frames);
+//      (P-frames deblock inside the wavefront, post.cuh, except single-frame
+//      launches whose rows fill the SMs and the learned form's single frames,
+//      which are deblocked as key frames);
 //   4. compaction of the per-block symbol slots into the per-stream byte
 //      arrays the entropy tail reads, written straight into mapped host memory;
 //   5. key frames: reference preparation, the deblocked reconstruction becomes
 //      the unit's new nearest reference (integer + half-pel planes); P-frames
-//      write theirs tile by tile inside the wavefront (learned form: as key
-//      frames).
+//      write theirs tile by tile inside the wavefront (with the same
+//      exceptions as in 3).
 // The reference pool rotates as fdv_video_encode's (fdv.h:6842-6846): the
 // nearest and second-nearest references are the last two coded frames; they
 // live in a ring of kRefSlots planes sets, reference q in slot q % kRefSlots.
@@ -550,6 +551,17 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     const int hpar = E->hpar;
     lrn::Hint *const hbase = E->d_hints ? E->d_hints + (size_t)hpar * kMaxBatch * E->total_mbs : nullptr;
     float *const pbase = E->d_prejs ? E->d_prejs + (size_t)hpar * kMaxBatch * E->total_mbs : nullptr;
+    // One frame per launch whose P rows fill the SMs by themselves (many
+    // streams in one engine): deblocking and reference preparation run as
+    // whole-frame kernels after the analysis, at full width in a fraction of
+    // a millisecond, instead of taking SM time from the rows.  Batches (the
+    // next frame reads the reference while it is written) and frames whose
+    // rows leave SMs idle use the in-wavefront stage.  The learned form's
+    // single frames also use the whole-frame kernels (its confident
+    // macroblocks are shorter than the stage's tiles).
+    int p_rows = 0;
+    for (int i = 0; i < nu; ++i) if (!is_intra[i]) p_rows += E->units[i].mbh;
+    const bool whole_frame_refs = K == 1 && (E->lnet || p_rows >= E->nsm);
     for (int k = 0; k < K; ++k) {
         std::vector<RowTask> frows;
         E->slot[sis[k]].intra.assign(nu, 0);
@@ -599,7 +611,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             }
             u.last_qp = qp[j];
             if (!is_intra[j]) {
-                if (E->lnet && K == 1) {
+                if (whole_frame_refs) {
                     iunits.push_back(i);
                     for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});
                 } else {
