@@ -504,10 +504,14 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     CK(cudaEventRecord(SL.ev[0], E->st));
     // 1. sources: device sources are read where they are; host sources go
     // through each frame's pinned staging buffer, laid out as the lane buffer,
-    // in one upload per frame (a held unit's part is left as it is)
+    // uploaded in chunks of at least 4 MB as units are staged, so the copies
+    // overlap the staging while staying few (a held unit's part is left as
+    // it is)
     if (!E->src_on_device)
         for (int k = 0; k < K; ++k) {
-            uint8_t *stage = E->slot[sis[k]].stage;
+            uint8_t *const stage0 = E->slot[sis[k]].stage;
+            uint8_t *stage = stage0;
+            size_t sent = 0;
             for (int i = 0; i < nu; ++i) {
                 Unit &u = E->units[i];
                 const int j = k * nu + i;
@@ -518,8 +522,12 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                     memcpy(stage + ys + cs, planes[3 * j + 2], cs);
                 }
                 stage += ys + 2 * cs;
+                const size_t done = (size_t)(stage - stage0);
+                if (done - sent >= ((size_t)4 << 20) || i == nu - 1) {
+                    CK(cudaMemcpyAsync(E->lane_src[k] + sent, stage0 + sent, done - sent, cudaMemcpyHostToDevice, E->st));
+                    sent = done;
+                }
             }
-            CK(cudaMemcpyAsync(E->lane_src[k], E->slot[sis[k]].stage, E->src_bytes, cudaMemcpyHostToDevice, E->st));
         }
     // descriptors are staged after the first frame's sources
     uint8_t *stage = SL.stage + E->src_stage_bytes;
