@@ -520,7 +520,7 @@ def run_learned(local: int) -> dict:
     plain = run(None)
     learned = run(p)
     seeded = run(p, (2.0, 2.0, 2.0, 0.0))   # inference and seeded searches, no narrowing
-    ev = LN.evaluate(p, LEARN_CONF, nframes=20, seeds=(1,), batch=12)
+    ev = LN.evaluate(p, LEARN_CONF, nframes=20, seeds=(1,), batch=30)
     mpix = LEARN_NF * W * H / 1e6
     pf = lambda st: st["p_ms"] / max(1, st["p_launches"])
     return {
@@ -541,7 +541,8 @@ def run_learned(local: int) -> dict:
                     f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, 20 frames; "
                     "P-frames in launches of up to 30 (the inference reads the previous frame's source: for "
                     "every frame with device-resident sources, after a batch's first frame with host sources; "
-                    "the SKIP pre-analysis runs for a batch's first frame)",
+                    "the SKIP pre-analysis runs for a batch's first frame); the BD-rate codes from host sources "
+                    "in the same launches",
         "weights": "fdv_b200/proposal_c4.f32",
     }
 
