@@ -33,7 +33,10 @@ One step = encoding all 120 frames.
   Its roofline is the P-frame reconstruction kernel's, timed by the decoder's
   own CUDA events.  ``--workload decode`` runs this leg alone.
 
-``--impl reference`` times that reference encoder alone (rank 0).
+``--impl reference`` times that reference encoder alone (rank 0) on the same
+120 frames, with the same ``config``.  Both arms read the workload's frames
+from one ``.yuv`` cache that a separate process renders (``--render-cache``),
+so the reference arm's process loads none of this library.
 Under torchrun each rank encodes its own stream (weak scaling, no collective on
 the data path); timings are reduced with MAX over ranks.
 """
@@ -94,10 +97,48 @@ class Ranks:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
+    def shard(self, work: list[int]) -> list[int]:
+        """Indices of the independent streams this rank codes.  Streams are
+        whole units (a stream's frames depend on each other, streams do not):
+        largest first, each to the rank with the least work so far (ties to
+        the lower rank), so every rank computes the same assignment."""
+        load = [0] * self.world
+        owner = [0] * len(work)
+        for i in sorted(range(len(work)), key=lambda i: (-work[i], i)):
+            r = min(range(self.world), key=lambda k: (load[k], k))
+            owner[i] = r
+            load[r] += work[i]
+        return [i for i in range(len(work)) if owner[i] == self.rank]
+
+    def gather_in_order(self, n: int, mine: dict) -> list | None:
+        """Every stream's output on rank 0, in stream order (as the reference
+        concatenates its independent bands, fdv.h:7228-7236); None elsewhere.
+        A single process returns its own outputs in order."""
+        if self.dist is None:
+            return [mine[i] for i in range(n)]
+        parts = [None] * self.world if self.rank == 0 else None
+        self.dist.gather_object(mine, parts, dst=0)
+        if self.rank != 0:
+            return None
+        merged = {}
+        for d in parts:
+            merged.update(d)
+        if sorted(merged) != list(range(n)):
+            raise RuntimeError("gathered streams do not cover every index exactly once")
+        return [merged[i] for i in range(n)]
+
     def close(self) -> None:
         if self.dist is not None:
             self.dist.barrier()
             self.dist.destroy_process_group()
+
+
+def encode_sharded(ranks: "Ranks", specs: list[dict], encode_one) -> list | None:
+    """Independent streams split across the ranks (Ranks.shard, by luma
+    pixels x frames), each rank coding its own with `encode_one(spec)`, and
+    the outputs gathered on rank 0 in stream order."""
+    mine = ranks.shard([sp["w"] * sp["h"] * sp.get("nframes", 1) for sp in specs])
+    return ranks.gather_in_order(len(specs), {i: encode_one(specs[i]) for i in mine})
 
 
 def weak_value(world: int, steps: int, frames: int, seconds: float) -> float:
@@ -156,11 +197,47 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def render(seed: int):
+def render(seed: int, nframes: int | None = None):
     import fdv_b200 as F
-    sc = F.Scene(W, H, NF, nrects=40, rect_min=8, rect_max=64, vmax_qpel=24, pan_qx=9, pan_qy=0,
+    n = nframes or NF
+    sc = F.Scene(W, H, n, nrects=40, rect_min=8, rect_max=64, vmax_qpel=24, pan_qx=9, pan_qy=0,
                  static_pct=40, seed=seed)
-    return [sc.frame(f) for f in range(NF)]
+    return [sc.frame(f) for f in range(n)]
+
+
+def cache_path(seed: int, nframes: int) -> str:
+    return os.path.join(tempfile.gettempdir(), f"fdvb_hd720_seed{seed}_{nframes}f.yuv")
+
+
+def write_cache(path: str, seed: int, nframes: int) -> None:
+    """Render the workload's frames and write them as one raw I420 file
+    (written aside, then renamed, so a reader never sees a partial file)."""
+    fr = render(seed, nframes)
+    tmp = f"{path}.{os.getpid()}.part"
+    with open(tmp, "wb") as f:
+        for x in fr:
+            f.write(x.tobytes())
+    os.replace(tmp, path)
+
+
+def cached_frames(seed: int, nframes: int) -> np.ndarray:
+    """The workload's frames (nframes x I420) from the .yuv cache, rendered
+    first by a separate process when the cache is missing: the process that
+    reads them loads no rendering code."""
+    path = cache_path(seed, nframes)
+    if not os.path.exists(path) or os.path.getsize(path) != nframes * FSIZE:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--render-cache", path, "--seed", str(seed),
+                            "--frames", str(nframes)], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("rendering the frame cache failed: " + r.stderr[-2000:])
+    return np.fromfile(path, dtype=np.uint8).reshape(nframes, FSIZE)
+
+
+def config_of(world: int) -> dict:
+    """The workload's config, printed identically by both arms."""
+    return {"workload": WORKLOAD if NF == 120 else WORKLOAD + f" (first {NF} frames only)",
+            "frames_per_step": NF, "global_batch": world * NF,
+            "l2": "inputs larger than L2 (166 MB of source frames per step)"}
 
 
 def band_layout():
@@ -169,8 +246,9 @@ def band_layout():
     return [(b * bh_full, min(bh_full, H - b * bh_full)) for b in range(nb)]
 
 
-def reference_encode_seconds(frames, nthreads: int, band_mbrows: int = BAND_MBROWS) -> float:
-    """One fdv_vtile_encode of `frames` by the reference compiled from its sources."""
+def reference_encode(frames, nthreads: int, band_mbrows: int = BAND_MBROWS) -> tuple[float, bytes]:
+    """One fdv_vtile_encode of `frames` by the reference compiled from its
+    sources: (seconds, stream)."""
     import oracle as O
     L = O.ref(RANGE)
     u8p = C.POINTER(C.c_uint8)
@@ -182,28 +260,53 @@ def reference_encode_seconds(frames, nthreads: int, band_mbrows: int = BAND_MBRO
     dt = time.perf_counter() - t0
     if n == 0:
         raise RuntimeError("reference encode failed")
-    return dt
+    return dt, out[:n].tobytes()
+
+
+def reference_encode_seconds(frames, nthreads: int, band_mbrows: int = BAND_MBROWS) -> float:
+    return reference_encode(frames, nthreads, band_mbrows)[0]
 
 
 def best_cpu(frames, repeats: int = 1) -> dict:
-    """The reference on the host cores, two ways: the workload's own 8-band
-    layout (its parallelism capped at 8 threads) and one macroblock row per band
-    (45 bands) on every core; the faster one is the baseline."""
+    """The reference on the host cores, in the workload's own 8-band layout
+    (its parallelism capped at 8 threads) and in narrower bands that use every
+    core (3, 2 and 1 macroblock rows); the fastest that codes the frames is
+    the baseline.  The reference's tiled encoder gives each band a fixed
+    capacity (twice its raw frame plus 64 KiB for the whole stream), which
+    one-row bands outgrow on long sequences: such a layout is skipped and
+    noted.  Also returns the 8-band stream (the workload's own layout, for the
+    identity check)."""
     ncpu = os.cpu_count() or 1
     mpix = len(frames) * W * H / 1e6
-    nb8 = len(band_layout())
-    t8 = min(reference_encode_seconds(frames, ncpu) for _ in range(repeats))
-    t1 = min(reference_encode_seconds(frames, ncpu, 1) for _ in range(repeats))
-    v8, v1 = mpix / t8, mpix / t1
-    if v1 > v8:
-        return {"value": round(v1, 3), "cores": ncpu, "seconds": t1, "band_mbrows": 1,
-                "sample": f"frames 0-{len(frames) - 1} (1 key + {len(frames) - 1} P) of the workload, the reference's "
-                          f"fdv_vtile_encode with one macroblock row per band (45 bands) on {ncpu} threads "
-                          f"(faster than the workload's 8-band layout on {min(ncpu, nb8)} threads: {v8:.1f} Mpix/s)"}
-    return {"value": round(v8, 3), "cores": min(ncpu, nb8), "seconds": t8, "band_mbrows": BAND_MBROWS,
-            "sample": f"frames 0-{len(frames) - 1} (1 key + {len(frames) - 1} P) of the workload, the reference's "
-                      f"fdv_vtile_encode, 8 bands on {min(ncpu, nb8)} threads (faster than one macroblock row per "
-                      f"band on {ncpu} threads: {v1:.1f} Mpix/s)"}
+    rates, failed, stream8 = {}, [], None
+    for bm in (BAND_MBROWS, 3, 2, 1):
+        try:
+            runs = [reference_encode(frames, ncpu, bm) for _ in range(repeats)]
+        except RuntimeError:
+            failed.append(bm)
+            continue
+        rates[bm] = mpix / min(r[0] for r in runs)
+        if bm == BAND_MBROWS:
+            stream8 = runs[0][1]
+    if not rates:
+        raise RuntimeError("the reference coded the frames in no band layout")
+    bm = max(rates, key=lambda k: rates[k])
+    gop1 = None
+    if 1 in failed and len(frames) > KEYINT:
+        # one-row bands over the first GOP alone, which they can code: stated
+        # beside the baseline, not used for it (a different frame range)
+        gop1 = round(KEYINT * W * H / 1e6 / reference_encode_seconds(frames[:KEYINT], ncpu, 1), 3)
+    nb = (H + 16 * bm - 1) // (16 * bm)
+    threads = min(ncpu, nb)
+    others = ", ".join(f"{(H + 16 * k - 1) // (16 * k)} bands {rates[k]:.1f}" for k in rates if k != bm)
+    note = f"; {' and '.join(str(k) for k in failed)}-row bands outgrow the reference's band capacity" if failed else ""
+    if gop1 is not None:
+        note += f" over {len(frames)} frames; over the first {KEYINT} frames alone, 45 bands of 1 row: {gop1} Mpix/s"
+    return {"value": round(rates[bm], 3), "cores": threads, "seconds": mpix / rates[bm], "band_mbrows": bm,
+            "stream8": stream8, "first_gop_1row": gop1,
+            "sample": f"frames 0-{len(frames) - 1} of the workload ({len(frames)} frames, key frames every {KEYINT}), "
+                      f"the reference's fdv_vtile_encode with {nb} bands of {bm} macroblock rows on {threads} threads "
+                      f"(the fastest layout; other layouts, Mpix/s: {others}{note})"}
 
 
 # ---------------------------------------------------------------- batch48 --
@@ -375,7 +478,8 @@ def run_reference(args) -> None:
     if not O.have_ref(RANGE):
         print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built (needs the reference sources at build time)"}))
         return
-    frames = render(1)[:KEYINT]              # one GOP: 1 key frame + 59 P-frames
+    fa = cached_frames(1, NF)                # the workload's frames, rendered by another process
+    frames = [fa[f] for f in range(NF)]
     nthreads = os.cpu_count() or 1
     # the faster of the two band layouts on the host cores, then timed alone
     choice = best_cpu(frames)
@@ -392,9 +496,11 @@ def run_reference(args) -> None:
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * statistics.mean(ts), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "step": "one GOP (60 frames) on the host CPU"},
+        "config": config_of(1),
+        "reference_layout": {"band_mbrows": bm, "threads": used,
+                             "note": "the faster of the workload's 8-band layout and one macroblock row per band"},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": used, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample + f"; each step encodes all {NF} frames"},
         "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -547,6 +653,60 @@ def run_learned(local: int) -> dict:
     }
 
 
+def pframe_roofline(pk_ms: float, pk_n: int, clocks: dict, local: int) -> dict:
+    """Roofline of the dominant kernel, the P-frame analysis wavefront.
+
+    Bound: the integer pipes.  Algorithmic integer ops of one hd720 P-frame
+    (all 8 bands), counted by the op-counting build of the CPU restatement
+    (``python -m oracle.opcount``: a fixed cost per primitive -- SAD, MC taps,
+    transforms, quantisers, RDOQ trials, SATD, intra prediction, residual and
+    reconstruction pixels, deblocking edges), divided by this run's
+    event-timed kernel time per P-frame, against the device's integer rate
+    measured in this run (fdvb_measure_int_rate).  HBM is reported beside it:
+    source + two references read + reconstruction written per P-frame.
+    ``traffic`` (DRAM bytes per P-frame) and ``int_pipe`` come from the ncu
+    capture of the same kernel named in ``capture``, not from this run."""
+    import fdv_b200 as F
+    pk_avg_s = (pk_ms / pk_n) / 1e3 if pk_n else float("nan")
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    alg_bytes = 1.5 * W * H * 4
+    hbm_ach = alg_bytes / pk_avg_s / 1e9
+    with open(os.path.join(ROOT, "profiles", "pframe_ops_hd720.json")) as f:
+        ops = json.load(f)["ops_per_pframe"]
+    measured = F.measure_int_rate(local) / 1e12
+    mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
+    nominal = 148 * 128 * mhz * 1e6 / 1e12
+    peak = measured if measured > 0 else nominal
+    ach = ops / pk_avg_s / 1e12
+    capture = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "pframe_kernel_hd720_capture.json")) as f:
+            capture = json.load(f)
+    except OSError:
+        pass
+    return {"bound": "int", "kernel": "pframe_kernel", "achieved": round(ach, 4), "peak": round(peak, 3),
+            "unit": "Tops/s", "frac": round(ach / peak, 5),
+            "traffic": capture.get("dram_bytes_per_pframe"),
+            "ops_per_pframe": ops, "ops_source": "profiles/pframe_ops_hd720.json (python -m oracle.opcount)",
+            "peak_source": ("measured in this run: int32 multiply-add / add chains on every SM "
+                            "(fdvb_measure_int_rate)") if measured > 0 else "nominal",
+            "nominal_peak": round(nominal, 2),
+            "nominal_basis": "148 SMs x 128 int32 lanes/clock at sm_max_mhz",
+            "avg_ms_per_pframe": round(pk_avg_s * 1e3, 4),
+            "hbm": {"achieved": round(hbm_ach, 3), "peak": hbm_peak, "unit": "GB/s",
+                    "frac": round(hbm_ach / hbm_peak, 6), "algorithmic_bytes_per_pframe": alg_bytes,
+                    "peak_source": "measured (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else "fallback"},
+            "int_pipe": capture.get("int_pipe"),
+            "capture": capture.get("capture"),
+            "note": "latency-bound wavefront (kernel time per P-frame, up to 30 P-frames overlapping per launch)"}
+
+
 def main() -> None:
     global NF
     ap = argparse.ArgumentParser()
@@ -562,7 +722,12 @@ def main() -> None:
     ap.add_argument("--workload", default="hd720", choices=["hd720", "batch48", "decode"],
                     help="batch48: the 48-stream batched workload (timed steps = P-frame steps); "
                          "decode: the decoder leg alone")
+    ap.add_argument("--render-cache", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--seed", type=int, default=1, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.render_cache:
+        write_cache(args.render_cache, args.seed, args.frames)
+        return
     if args.workload == "batch48":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the batched workload's reference timing is its "
@@ -598,10 +763,9 @@ def main() -> None:
     L.fdvb_set_device(local)
     F.set_search_range(RANGE)
 
-    frames = render(1 + rank)
     # host frames in pinned memory (e2e), and the same frames resident in HBM (value)
     host = torch.empty((NF, FSIZE), dtype=torch.uint8).pin_memory()
-    host.numpy()[:] = np.stack(frames)
+    host.numpy()[:] = cached_frames(1 + rank, NF)
     dev = host.to(f"cuda:{local}")
     torch.cuda.synchronize()
     bands = band_layout()
@@ -680,57 +844,20 @@ def main() -> None:
         e2e_s = reduce_max(time.perf_counter() - t1)
         e2e = weak_value(world, args.steps, NF, e2e_s)
 
-    # roofline of the dominant kernel (the P-frame analysis wavefront)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs")
-    peak_src = "measured" if peak else "fallback"
-    peak = peak or 6650.0
-    # algorithmic bytes of one P-frame launch (all 8 bands): the source frame,
-    # two reference frames read, the reconstruction written (1.5*W*H*(2+2)).
-    alg_bytes = 1.5 * W * H * 4
-    pk_avg_s = (pk_ms / pk_n) / 1e3 if pk_n else float("nan")
-    achieved = alg_bytes / pk_avg_s / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "pframe_kernel_hd720_traffic.json")) as f:
-            traffic = json.load(f).get("dram_bytes_per_pframe")
-    except OSError:
-        pass
-    int_pipe = None   # the integer-pipe utilisation of the same kernel, from one ncu capture
-    try:
-        with open(os.path.join(ROOT, "profiles", "pframe_kernel_hd720_pipes.json")) as f:
-            int_pipe = json.load(f)
-    except OSError:
-        pass
-    # the integer-op roofline SURVEY-style: algorithmic ops of one P-frame (all
-    # bands), counted by the op-counting build of the CPU restatement
-    # (python -m oracle.opcount), over the live launch time, against a nominal
-    # peak of 148 SMs x 128 int32 lanes per clock at the maximum SM clock
-    int_ops = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "pframe_ops_hd720.json")) as f:
-            ops = json.load(f)["ops_per_pframe"]
-        mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
-        peak_t = 148 * 128 * mhz * 1e6 / 1e12
-        ach_t = ops / pk_avg_s / 1e12
-        int_ops = {"ops_per_launch": ops, "achieved": round(ach_t, 4), "peak": round(peak_t, 2), "unit": "Tops/s",
-                   "frac": round(ach_t / peak_t, 5), "peak_basis": "148 SMs x 128 int32 lanes/clock at sm_max_mhz",
-                   "source": "profiles/pframe_ops_hd720.json"}
-    except (OSError, KeyError, ValueError):
-        pass
+    roofline = pframe_roofline(pk_ms, pk_n, clocks, local)
 
-    cpu = None
+    cpu, identical = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle as O
         if O.have_ref(RANGE):
-            b = best_cpu(hframes[:KEYINT])
+            # the reference on this host's cores over the same frames; its
+            # stream in the workload's own 8-band layout must equal the one the
+            # e2e leg produced through fdv_vtile_encode
+            b = best_cpu(hframes)
             cpu = {"value": b["value"], "unit": "Mpix/s", "cores": b["cores"], "kind": "reference",
-                   "sample": b["sample"]}
+                   "sample": b["sample"], "first_gop_1row": b["first_gop_1row"]}
+            if e2e is not None:
+                identical = out[:n].tobytes() == b["stream8"]
 
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
@@ -748,19 +875,11 @@ def main() -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD if NF == 120 else WORKLOAD + f" (first {NF} frames only)",
-                       "global_batch": world * NF, "frames_per_step": NF,
-                       "parallelism": f"bands{nb} per GPU, {world} GPU(s) each with its own stream",
-                       "l2": "inputs larger than L2 (166 MB of source frames per step)",
-                       "wall_s_timed": round(wall, 3)},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 6), "traffic": traffic,
-                         "kernel": "pframe_kernel", "peak_source": peak_src,
-                         "algorithmic_bytes_per_pframe": alg_bytes,
-                         "avg_ms_per_pframe": round(pk_avg_s * 1e3, 4),
-                         "note": f"latency-bound wavefront, up to {batch} P-frames overlapping per launch "
-                                 "(kernel time per P-frame); HBM is not the limiter",
-                         "int_pipe": int_pipe, "int_ops": int_ops},
+            "config": config_of(world),
+            "run": {"parallelism": f"bands{nb} per GPU, {world} GPU(s) each with its own stream",
+                    "p_frames_per_launch": batch, "wall_s_timed": round(wall, 3)},
+            "identical_to_reference": identical,
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": None if e2e is None else {
                 "value": round(e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": NF * FSIZE,

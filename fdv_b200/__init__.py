@@ -100,6 +100,13 @@ def lib() -> C.CDLL:
         L.fdvb_scene_frame.argtypes = [p, i, u8p]
         L.fdvb_scene_close.argtypes = [p]
         L.fdvb_scene_close.restype = None
+        L.fdvb_measure_int_rate.argtypes = [i, i]
+        L.fdvb_measure_int_rate.restype = C.c_double
+        L.fdvb_camscene_open.argtypes = [p]
+        L.fdvb_camscene_open.restype = p
+        L.fdvb_camscene_frame.argtypes = [p, i, u8p]
+        L.fdvb_camscene_close.argtypes = [p]
+        L.fdvb_camscene_close.restype = None
         ip = C.POINTER(i)
         L.fdv_video_decode.argtypes = [u8p, sz, u8p, ip, ip, ip]
         L.fdv_vtile_decode.argtypes = [u8p, sz, u8p, ip, ip, ip, i]
@@ -135,6 +142,12 @@ def _as_frames(frames, w: int, h: int) -> list[np.ndarray]:
             raise ValueError(f"frame has {a.size} bytes, expected {fs}")
         out.append(a)
     return out
+
+
+def measure_int_rate(device: int = 0, reps: int = 5) -> float:
+    """32-bit integer lane-operations per second the device retires
+    (fdvb_measure_int_rate); 0.0 on error."""
+    return float(lib().fdvb_measure_int_rate(device, reps))
 
 
 def set_search_range(r: int) -> int:
@@ -508,6 +521,46 @@ class Scene:
     def __del__(self):
         try:
             lib().fdvb_scene_close(self._s)
+        except Exception:
+            pass
+
+
+class CamSceneParams(C.Structure):
+    _fields_ = [("w", C.c_int), ("h", C.c_int), ("nframes", C.c_int), ("nobjects", C.c_int),
+                ("obj_min", C.c_int), ("obj_max", C.c_int), ("vmax_qpel", C.c_int), ("zoom_ppm", C.c_int),
+                ("pan_qx", C.c_int), ("pan_qy", C.c_int), ("noise_y_x16", C.c_int), ("noise_c_x16", C.c_int),
+                ("cut_every", C.c_int), ("seed", C.c_ulonglong)]
+
+
+class CamScene:
+    """Camera-like stress content (fdvb_camscene_*): a 1/f^2 fractal canvas
+    under a per-frame affine pan/zoom, fast textured objects, sensor noise and
+    a hard cut every ``cut_every`` frames.  ``frames`` renders on several host
+    threads (the library call releases the interpreter lock)."""
+
+    def __init__(self, w, h, nframes, nobjects=200, obj_min=8, obj_max=96, vmax_qpel=96, zoom_ppm=5000,
+                 pan_qx=9, pan_qy=-4, noise_y_x16=32, noise_c_x16=16, cut_every=100, seed=1):
+        self.w, self.h, self.nframes = w, h, nframes
+        self._prm = CamSceneParams(w, h, nframes, nobjects, obj_min, obj_max, vmax_qpel, zoom_ppm, pan_qx, pan_qy,
+                                   noise_y_x16, noise_c_x16, cut_every, seed)
+        self._s = lib().fdvb_camscene_open(C.byref(self._prm))
+        if not self._s:
+            raise FdvError("bad camera scene parameters")
+
+    def frame(self, f: int) -> np.ndarray:
+        out = np.empty(self.w * self.h * 3 // 2, np.uint8)
+        if lib().fdvb_camscene_frame(self._s, f, _ptr(out)) != 0:
+            raise FdvError("frame out of range")
+        return out
+
+    def frames(self, n: int, start: int = 0, threads: int | None = None) -> list[np.ndarray]:
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(max_workers=threads or min(16, os.cpu_count() or 1)) as ex:
+            return list(ex.map(self.frame, range(start, start + n)))
+
+    def __del__(self):
+        try:
+            lib().fdvb_camscene_close(self._s)
         except Exception:
             pass
 

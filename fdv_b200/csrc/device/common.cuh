@@ -157,7 +157,16 @@ enum : unsigned {
     kErrWaitTimeout = 1u,    // a wavefront wait gave up
     kErrSlotOverflow = 2u,   // a symbol stream exceeded its per-block slot
     kErrMmaTimeout = 4u,     // a tensor-core completion wait gave up
+    kErrOutCap = 8u,         // the compacted streams do not fit the output buffer
 };
+
+// The host-side text of a status word (the first error bit that is set).
+inline const char *status_text(unsigned e) {
+    return (e & kErrWaitTimeout)  ? "wavefront wait timed out"
+           : (e & kErrMmaTimeout) ? "tensor-core completion wait timed out"
+           : (e & kErrOutCap)     ? "output buffer too small for the symbol streams"
+                                  : "symbol slot overflow";
+}
 
 // Bounded spin until *flag >= need.  Gives up after `limit_ns` of wall time
 // (device global timer) or when another block has already raised an error.

@@ -837,8 +837,7 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     }
     const unsigned err = SL.err_h[0] | SL.err_h[1];
     if (err) {
-        g_err = (err & kErrWaitTimeout) ? "wavefront wait timed out"
-                : (err & kErrMmaTimeout) ? "tensor-core completion wait timed out" : "symbol slot overflow";
+        g_err = status_text(err);
         return -4;
     }
     for (int i = 0; i < (int)E->units.size(); ++i) {

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks,
     }
     __syncthreads();
     const size_t hdr = 4 * (size_t)T.nstreams;
-    if (hdr + s_base[16] > T.cap) { if (tid == 0) atomicOr(err, kErrSlotOverflow); return; }
+    if (hdr + s_base[16] > T.cap) { if (tid == 0) atomicOr(err, kErrOutCap); return; }
     uint8_t *const asmb = T.tmp ? T.tmp : T.out;
     if (tid < T.nstreams) {
         unsigned len = (tid + 1 < T.nstreams ? s_base[tid + 1] : s_base[16]) - s_base[tid];

@@ -27,11 +27,18 @@ int upload_tables(const int32_t c8[64], const int32_t q8[52]) {
 
 void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticket, unsigned *err,
                    unsigned long long wait_ns, int grid, cudaStream_t st) {
-    static bool attr = false;
+    // the shared-memory opt-in is a per-device attribute: set once per device
+    static std::mutex mu;
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
     const size_t smem = sizeof(IShared);
-    if (!attr) {
-        cudaFuncSetAttribute(iframe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64 && !attr[dev]) {
+            cudaFuncSetAttribute(iframe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr[dev] = true;
+        }
     }
     // clusters of ICL blocks, one CTU row each at a time; `grid` is the SM count
     const int ncl = std::max(1, std::min(ntasks, grid / ICL));
@@ -204,6 +211,10 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     using namespace fdvb;
     g_static_err[0] = 0;
     if (!cur || !near_ref || !rec || !out) return static_fail("null buffer");
+    // the kernels read and write these buffers in 4- to 16-byte words
+    if ((reinterpret_cast<uintptr_t>(cur) | reinterpret_cast<uintptr_t>(near_ref) |
+         reinterpret_cast<uintptr_t>(far_ref) | reinterpret_cast<uintptr_t>(rec) | reinterpret_cast<uintptr_t>(out)) & 15)
+        return static_fail("cur, near_ref, far_ref, rec and out must be 16-byte aligned");
     if (w <= 0 || h <= 0 || (w & 15) || (h & 15) || w > 8192 || h > 8192)
         return static_fail("dimensions must be positive multiples of 16");
     if (qp < 0 || qp > 51) return static_fail("qp out of range");
@@ -319,6 +330,6 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     if (cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return static_fail("device error");
-    if (herr) return static_fail((herr & kErrWaitTimeout) ? "wavefront wait timed out" : "symbol slot overflow");
+    if (herr) return static_fail(status_text(herr));
     return 0;
 }

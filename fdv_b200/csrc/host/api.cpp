@@ -358,8 +358,13 @@ size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payl
 // consecutive P-frames go to the GPU as batches (one wavefront launch each,
 // the frames overlapping); the host entropy-codes one batch's frames, bands in
 // parallel, while the GPU analyses the next batch.
+//
+// band_capped: each band's stream is held to the capacity the reference's
+// tiled encoder gives it, twice the band's I420 frame size plus 64 KiB for all
+// frames (encode_band, fdv.h:7111-7113, checked per frame as fdv_video_encode
+// does, :6800-6804): a band that outgrows it fails the call, as there.
 static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
-                        int bh_full, int nthreads, std::vector<UnitStream> &us) {
+                        int bh_full, int nthreads, std::vector<UnitStream> &us, bool band_capped = false) {
     const int nb = (h + bh_full - 1) / bh_full, cw = w / 2, ch = h / 2;
     std::vector<int> W(nb, w), H(nb), Y0(nb);
     for (int b = 0; b < nb; ++b) { Y0[b] = b * bh_full; H[b] = std::min(bh_full, h - Y0[b]); }
@@ -430,14 +435,17 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             std::fill(urc.begin(), urc.end(), 0);
             pool.run(nb, [&](int u) {
                 size_t o = 0;
+                const size_t band_cap = (size_t)w * H[u] * 3 + 65536;   // 2 x (w*bh + 2 * (w/2)*(bh/2)) + 65536
                 for (int ti : btype) {
                     const size_t blob = code_blob_streams(&bst[u][o], us[u], ti, qp);
                     if (!blob) { urc[u] = -1; return; }
+                    if (band_capped && us[u].bytes.size() + 4 + blob > band_cap) { urc[u] = -2; return; }
                     append_blob(us[u], blob);
                     o += ti ? 3 : 1;
                 }
             });
-            for (int r : urc) if (r) { set_err("entropy coding failed"); rc = -1; }
+            for (int r : urc)
+                if (r) { set_err(r == -2 ? "a band's stream outgrew the tiled encoder's capacity" : "entropy coding failed"); rc = -1; }
         }
         if (K == 0) break;
         prev = (size_t)K;
@@ -478,7 +486,7 @@ size_t fdv_vtile_encode(const uint8_t *const *frames, int nframes, int w, int h,
     if (keyint > 255) keyint = 255;
     if (nthreads < 1) nthreads = 1;
     std::vector<UnitStream> us;
-    if (encode_bands(frames, nframes, w, h, qp, keyint, bh_full, nthreads, us) != 0) return 0;
+    if (encode_bands(frames, nframes, w, h, qp, keyint, bh_full, nthreads, us, true) != 0) return 0;
     size_t o = 0;
     o = fdvb_put16(out, o, (unsigned)w);
     o = fdvb_put16(out, o, (unsigned)h);

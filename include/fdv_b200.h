@@ -254,11 +254,14 @@ int fdvg_mb_timeline(fdvg_ctx *g, int u, unsigned long long *out);
  *
  * cur, near_ref, far_ref (NULL: one reference) and rec are device pointers to
  * tight I420 frames of the unit; rec receives the deblocked reconstruction.
- * out (device or host-mapped, out_cap bytes) receives uint32 len[16] followed
- * by the 16 P-frame symbol streams back to back, in fdvg_pframe_streams'
- * order.  stream is a cudaStream_t (NULL: the default stream); the call
- * synchronises it before returning 0, or a negative value with
- * fdvg_pframe_static_error() set.
+ * out (device memory, out_cap bytes) receives uint32 len[16] followed by the
+ * 16 P-frame symbol streams back to back, in fdvg_pframe_streams' order; the
+ * streams are assembled in place, so out must be device memory, not
+ * host-mapped.  Every pointer must be 16-byte aligned (a misaligned one is
+ * rejected before anything is queued).  An out_cap too small for the streams
+ * is reported as "output buffer too small ...".  stream is a cudaStream_t
+ * (NULL: the default stream); the call synchronises it before returning 0, or
+ * a negative value with fdvg_pframe_static_error() set.
  *
  * The first call on a device looks up the array's device address and uploads
  * the transform tables with that device current; make it before any stream
@@ -284,6 +287,14 @@ size_t fdvb_entropy_pframe(const uint8_t *const *s16, const size_t *n16, int qp,
 size_t fdvb_entropy_image(const uint8_t *const *s12, const size_t *n12, int w, int h, int qp,
                           uint8_t *out, size_t cap);
 
+/* ------------------------------------------------------ measurement -- */
+
+/* 32-bit integer lane-operations per second the device retires (best of reps
+ * timed launches of independent multiply-add / add chains over every SM):
+ * the measured denominator of the analysis kernels' integer-op roofline.  No
+ * counterpart in the reference.  Returns 0 on error. */
+double fdvb_measure_int_rate(int device, int reps);
+
 /* -------------------------------------------- synthetic test content -- */
 
 /* Seeded moving-rectangle content: band-limited noise background (sigma 3 px,
@@ -303,6 +314,31 @@ typedef struct fdvb_scene_params {
 fdvb_scene_state *fdvb_scene_open(const fdvb_scene_params *params);
 int fdvb_scene_frame(const fdvb_scene_state *s, int f, uint8_t *i420);
 void fdvb_scene_close(fdvb_scene_state *s);
+
+/* Camera-like stress content: a fractal canvas (value-noise octaves with
+ * amplitude proportional to wavelength: a 1/f^2 power spectrum; luma mean 128
+ * / sd 40, chroma sd 14) seen through a window that pans by (pan_qx, pan_qy)
+ * quarter-pels per frame and zooms by zoom_ppm parts per million per frame
+ * (in on even segments, out on odd ones); nobjects textured objects with sides
+ * in [obj_min, obj_max] moving at up to vmax_qpel quarter-pels per frame per
+ * axis; additive noise of sd noise_y_x16 / 16 on luma and noise_c_x16 / 16 on
+ * chroma; a hard cut to a new canvas and new objects every cut_every frames
+ * (0: never).  Integer arithmetic: the same bytes on every machine.  Frames
+ * may be rendered from several threads at once. */
+typedef struct fdvb_camscene_state fdvb_camscene_state;
+typedef struct fdvb_camscene_params {
+    int w, h, nframes;
+    int nobjects, obj_min, obj_max;
+    int vmax_qpel;
+    int zoom_ppm;
+    int pan_qx, pan_qy;
+    int noise_y_x16, noise_c_x16;
+    int cut_every;
+    unsigned long long seed;
+} fdvb_camscene_params;
+fdvb_camscene_state *fdvb_camscene_open(const fdvb_camscene_params *params);
+int fdvb_camscene_frame(const fdvb_camscene_state *s, int f, uint8_t *i420);
+void fdvb_camscene_close(fdvb_camscene_state *s);
 
 
 /* ---- Learned proposal network (no counterpart in the reference) ----------

@@ -30,8 +30,12 @@ def built():
 
 
 def scene_frames(kw):
+    """Frames of a golden case's scene: the moving-rectangle generator, or
+    the camera-like stress generator when kind is "camera"."""
     import fdv_b200 as F
     kw = dict(kw)
     n = kw.pop("nframes")
     w, h = kw.pop("w"), kw.pop("h")
+    if kw.pop("kind", "rects") == "camera":
+        return F.CamScene(w, h, n, **kw).frames(n)
     return F.Scene(w, h, n, **kw).frames(n)

@@ -51,7 +51,26 @@ CASES = [
     ("c3_1088_r64", dict(w=1920, h=1088, nframes=4, nrects=200, rect_min=8, rect_max=96, vmax_qpel=96, pan_qx=6,
                          pan_qy=-3, static_pct=0, seed=3),
      dict(qp=20, keyint=60, band_mbrows=4, search_range=64)),
+    # the whole 720p workload the benchmark times: 120 frames, two key frames
+    # (0 and 60), P-frames in launches of up to thirty, the reference ring
+    # wrapping several times
+    ("hd720_full", dict(w=1280, h=720, nframes=120, nrects=40, pan_qx=9, static_pct=40, seed=1),
+     dict(qp=24, keyint=60, band_mbrows=6, search_range=32)),
 ]
+
+# The camera-like stress content at the 1080p stress shape: a 1/f^2 fractal
+# canvas under a 0.5 %/frame zoom and a pan, 200 objects at up to 24 px/frame,
+# sensor noise sd 2 / 1, a hard cut every 100 frames; 17 bands of 4 macroblock
+# rows, range +-64, QP 20, key interval 60.
+C3_SCENE = dict(kind="camera", w=1920, h=1088, nframes=300, nobjects=200, obj_min=8, obj_max=96, vmax_qpel=96,
+                zoom_ppm=5000, pan_qx=9, pan_qy=-4, noise_y_x16=32, noise_c_x16=16, cut_every=100, seed=3)
+C3_ENCODE = dict(qp=20, keyint=60, band_mbrows=4, search_range=64)
+# The reference's whole-array tiled encoder gives each band twice its raw
+# frame size plus 64 KiB for the whole stream (fdv.h:7111-7113), which this
+# noisy content outgrows within the first GOP: it returns 0 there, and so must
+# the library.  The streaming tiled encoder grows its buffer (fdv.h:8341-8347)
+# and codes all 300 frames; the full-length parity case goes through it.
+C3_VTILE_FRAMES = 60
 
 # Independent streams of mixed sizes and QPs coded together (one engine, one
 # launch per frame step): each must equal the reference's fdv_video_encode.
@@ -88,6 +107,8 @@ def scene(kw) -> list[np.ndarray]:
     kw = dict(kw)
     n = kw.pop("nframes")
     w, h = kw.pop("w"), kw.pop("h")
+    if kw.pop("kind", "rects") == "camera":
+        return F.CamScene(w, h, n, **kw).frames(n)
     return F.Scene(w, h, n, **kw).frames(n)
 
 
@@ -100,14 +121,35 @@ def main() -> None:
             s = O.ref_video_encode(fr, w, h, ekw["qp"], ekw["keyint"], ekw["search_range"])
             dec = O.ref_video_decode(s, ekw["search_range"])
         else:
-            s = O.ref_vtile_encode(fr, w, h, ekw["qp"], ekw["keyint"], ekw["band_mbrows"], 1, ekw["search_range"])
+            s = O.ref_vtile_encode(fr, w, h, ekw["qp"], ekw["keyint"], ekw["band_mbrows"], os.cpu_count() or 1,
+                                   ekw["search_range"])
             dec = O.ref_vtile_decode(s, ekw["search_range"])
         out["cases"][name] = {
             "scene": skw, "encode": ekw, "stream_sha256": sha(s), "stream_len": len(s),
             "frames_sha256": sha(b"".join(f.tobytes() for f in fr)),
-            "decoded_sha256": sha(dec.tobytes()),
+            "decoded_sha256": sha(dec.tobytes()), "last_decoded_sha256": sha(dec[-1].tobytes()),
         }
         print(name, len(s), flush=True)
+    # the camera-like stress case: the whole-array tiled encoder's capacity
+    # failure, and the full 300 frames through the streaming tiled encoder
+    fr = scene(C3_SCENE)
+    e = C3_ENCODE
+    w, h = C3_SCENE["w"], C3_SCENE["h"]
+    try:
+        O.ref_vtile_encode(fr[:C3_VTILE_FRAMES], w, h, e["qp"], e["keyint"], e["band_mbrows"], os.cpu_count() or 1,
+                           e["search_range"])
+        vtile_fails = False
+    except RuntimeError:
+        vtile_fails = True
+    s = O.ref_enc_stream(fr, w, h, e["qp"], e["keyint"], e["search_range"], 0, 30, 1.0, e["band_mbrows"],
+                         os.cpu_count() or 1)
+    dec = O.ref_vtile_decode(s[12:], e["search_range"], os.cpu_count() or 1)
+    out["c3"] = {"scene": C3_SCENE, "encode": e, "vtile_frames": C3_VTILE_FRAMES, "vtile_fails": vtile_fails,
+                 "file_sha256": sha(s), "file_len": len(s), "fps": 30,
+                 "frames_sha256": sha(b"".join(f.tobytes() for f in fr)),
+                 "decoded_sha256": sha(dec.tobytes()), "last_decoded_sha256": sha(dec[-1].tobytes())}
+    print("c3", vtile_fails, len(s), flush=True)
+    del fr, dec
     out["batch"] = {"keyint": BATCH_KEYINT, "search_range": 16, "streams": []}
     for bk in BATCH:
         skw = {k: v for k, v in bk.items() if k != "qp"}

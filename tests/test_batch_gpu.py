@@ -93,3 +93,49 @@ def test_learned_batch_stream(built):
     assert len(rb) == n
     assert np.array_equal(rb[0], r1[0]) and np.array_equal(rb[1], r1[1])
     assert abs(LN.psnr_y(frames, rb, w, h) - LN.psnr_y(frames, r1, w, h)) < 0.3
+
+
+def test_long_batched_sequence_matches_oracle(built):
+    """A long sequence in launches of the largest batch: 76 frames with key
+    frames at 0 and 38, so each GOP holds a full thirty-frame launch and a
+    shorter one, and the reference ring (thirty-two slots) wraps within the
+    first GOP.  Two units of different sizes; every frame's streams (key
+    frames: all three planes) and the final reconstruction equal the CPU
+    oracle's."""
+    import fdv_b200 as F
+    import oracle as O
+    sizes, rng, qp, nf, keyat = [(160, 96), (64, 48)], 32, 27, 76, (0, 38)
+    frames = [F.Scene(w, h, nf, nrects=max(2, w * h // 3000), pan_qx=9, pan_qy=-3, static_pct=25,
+                      seed=61 + u).frames(nf) for u, (w, h) in enumerate(sizes)]
+    eng = F.Engine(sizes, rng)
+    kmax = eng.max_batch()
+    assert kmax == 30
+    units = [O.OracleUnit(w, h, rng) for (w, h) in sizes]
+    nu = len(sizes)
+    f, launches = 0, 0
+    while f < nf:
+        if f in keyat:
+            eng.step([frames[u][f] for u in range(nu)], [1] * nu, [qp] * nu)
+            for u, o in enumerate(units):
+                want, _ = o.frame(frames[u][f], 1, qp)
+                for p in range(3):
+                    assert eng.iframe_streams(u, p) == list(want[p]), f"key frame {f} unit {u} plane {p}"
+            f += 1
+            continue
+        K = 1
+        while K < kmax and f + K < nf and (f + K) not in keyat:
+            K += 1
+        eng.submit_batch([[frames[u][f + k] for u in range(nu)] for k in range(K)], [[qp] * nu for _ in range(K)])
+        launches += 1
+        for k in range(K):
+            eng.collect()
+            for u, o in enumerate(units):
+                want, _ = o.frame(frames[u][f + k], 0, qp)
+                got = eng.pframe_streams(u)
+                for s in range(16):
+                    assert got[s] == want[s], f"frame {f + k} unit {u} stream {s}"
+        f += K
+    assert launches == 4
+    for u, o in enumerate(units):
+        assert np.array_equal(eng.recon(u), o.recon()), f"unit {u} reconstruction"
+    eng.close()

@@ -1,7 +1,8 @@
 """The multi-GPU run's host plumbing on CPU: two gloo ranks (127.0.0.1) as
 torchrun starts them -- the barrier, the MAX of the per-rank step times and
-the whole-job (weak-scaling) rate -- and the reference arm under torchrun, where
-only rank 0 works."""
+the whole-job (weak-scaling) rate, a real partition of independent streams
+across the ranks with the outputs gathered in stream order -- and the
+reference arm under torchrun, where only rank 0 works."""
 import json
 import os
 import socket
@@ -71,3 +72,51 @@ def test_single_process_needs_no_group():
             if v is not None:
                 os.environ[k] = v
     assert json.dumps({"v": bench.weak_value(1, 1, 1, 1.0)})
+
+
+# Six independent streams of mixed sizes and QPs, as the batched workload
+# mixes them (small enough for the CPU oracle).
+SPECS = [dict(w=64, h=48, nframes=3, qp=22, seed=71), dict(w=96, h=64, nframes=3, qp=30, seed=72),
+         dict(w=48, h=32, nframes=4, qp=18, seed=73), dict(w=128, h=64, nframes=2, qp=36, seed=74),
+         dict(w=32, h=32, nframes=3, qp=26, seed=75), dict(w=64, h=64, nframes=3, qp=33, seed=76)]
+
+
+def _oracle_stream(sp) -> bytes:
+    import fdv_b200 as F
+    import oracle as O
+    fr = F.Scene(sp["w"], sp["h"], sp["nframes"], nrects=3, pan_qx=5, seed=sp["seed"]).frames(sp["nframes"])
+    return O.oracle_video_stream(fr, sp["w"], sp["h"], sp["qp"], 2, 16)
+
+
+def _partition_rank(rank: int, world: int, port: int, q) -> None:
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    import bench
+    r = bench.Ranks("gloo", "cpu")
+    mine = r.shard([sp["w"] * sp["h"] * sp["nframes"] for sp in SPECS])
+    out = bench.encode_sharded(r, SPECS, _oracle_stream)
+    q.put((r.rank, mine, out))
+    r.close()
+
+
+def test_streams_partitioned_across_two_ranks_gather_in_order():
+    """Each rank codes only its share of the streams (no stream on both, none
+    left out, the work balanced), and rank 0 gathers them in stream order,
+    equal to one process coding all of them."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_partition_rank, args=(k, 2, port, q)) for k in range(2)]
+    for p in ps:
+        p.start()
+    got = dict((r, (m, o)) for r, m, o in (q.get(timeout=300) for _ in range(2)))
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    m0, m1 = got[0][0], got[1][0]
+    assert sorted(m0 + m1) == list(range(len(SPECS))) and m0 and m1
+    work = [sp["w"] * sp["h"] * sp["nframes"] for sp in SPECS]
+    assert abs(sum(work[i] for i in m0) - sum(work[i] for i in m1)) <= max(work)
+    assert got[1][1] is None
+    assert got[0][1] == [_oracle_stream(sp) for sp in SPECS]

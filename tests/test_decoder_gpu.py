@@ -34,7 +34,7 @@ def _encode(F, fr, w, h, e):
 
 
 @pytest.mark.parametrize("name", ["cif30", "pan256_k5", "tiny_q0", "tiny_q51_r64", "bands_q12", "hd720_g12",
-                                  "c3_1088_r64"])
+                                  "c3_1088_r64", "hd720_full"])
 def test_golden_streams_decode_like_reference(built, golden, name):
     import fdv_b200 as F
     case = golden["cases"][name]

@@ -78,7 +78,7 @@ def test_keyframe_matches_oracle(built, w, h, qp, seed):
 
 
 @pytest.mark.parametrize("name", ["cif30", "pan256_k5", "tiny_q0", "tiny_q51_r64", "bands_q12", "hd720_g12",
-                                  "c3_1088_r64"])
+                                  "c3_1088_r64", "hd720_full"])
 def test_stream_matches_reference(built, golden, name):
     import fdv_b200 as F
     case = golden["cases"][name]
@@ -301,3 +301,52 @@ def test_submit_collect_pipeline_equals_step(built):
             got.append([eng.iframe_streams(0, p) for p in range(3)] if f == 1 else eng.pframe_streams(0))
     eng.close()
     assert got == want
+
+
+def test_camera_stress_tiled_capacity_matches_reference(built, golden):
+    """The camera-like stress content (noise at QP 20) outgrows the capacity the
+    reference's whole-array tiled encoder gives each band (twice its raw frame
+    plus 64 KiB, fdv.h:7111-7113) within the first GOP: the reference returns
+    0 there, and so does fdv_vtile_encode."""
+    import fdv_b200 as F
+    c3 = golden["c3"]
+    sc, e = dict(c3["scene"]), c3["encode"]
+    sc["nframes"] = c3["vtile_frames"]
+    fr = scene_frames(sc)
+    F.set_search_range(e["search_range"])
+    try:
+        if c3["vtile_fails"]:
+            with pytest.raises(F.FdvError, match="capacity"):
+                F.vtile_encode(fr, sc["w"], sc["h"], e["qp"], e["keyint"], e["band_mbrows"], 8)
+        else:
+            F.vtile_encode(fr, sc["w"], sc["h"], e["qp"], e["keyint"], e["band_mbrows"], 8)
+    finally:
+        F.set_search_range(16)
+
+
+def test_camera_stress_stream_matches_reference(built, golden):
+    """The camera-like stress configuration at full length: 1920x1088, 300
+    frames (a 1/f^2 canvas under a 0.5 %/frame zoom and a pan, 200 objects at
+    up to 24 px/frame, sensor noise, hard cuts at frames 100 and 200), 17
+    bands of 4 macroblock rows, range +-64, QP 20, key interval 60, through
+    the streaming tiled encoder (fdv_enc_open_tiled): the .fdv file equals the
+    reference's byte for byte, and the GPU decoder's frames equal the
+    reference decoder's."""
+    import fdv_b200 as F
+    c3 = golden["c3"]
+    sc, e = c3["scene"], c3["encode"]
+    fr = scene_frames(sc)
+    assert sha(b"".join(f.tobytes() for f in fr)) == c3["frames_sha256"]
+    F.set_search_range(e["search_range"])
+    try:
+        enc = F.Encoder(sc["w"], sc["h"], e["qp"], e["keyint"], e["band_mbrows"], 8)
+        for x in fr:
+            enc.frame(x)
+        data = enc.finish(c3["fps"])
+        del fr
+        assert len(data) == c3["file_len"]
+        assert sha(data) == c3["file_sha256"]
+        dec = F.vtile_decode(data[12:])
+    finally:
+        F.set_search_range(16)
+    assert sha(dec.tobytes()) == c3["decoded_sha256"]
