@@ -498,7 +498,8 @@ def run_reference(args) -> None:
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": config_of(1),
         "reference_layout": {"band_mbrows": bm, "threads": used,
-                             "note": "the faster of the workload's 8-band layout and one macroblock row per band"},
+                             "note": "the fastest of the workload's 8-band layout and narrower bands (3, 2 and 1 "
+                                     "macroblock rows) that code all the frames"},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": used, "kind": "reference",
                          "sample": sample + f"; each step encodes all {NF} frames"},
         "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

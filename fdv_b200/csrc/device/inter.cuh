@@ -141,19 +141,27 @@ __device__ __forceinline__ int sp_dy(int k) { return k == 0 ? -1 : (k == 1 ? 1 :
 // (lane -> row lane/2, 8 bytes); BS = 8: each half-warp covers one block
 // (lane -> row (lane&15)/2, 4 bytes), the two halves may score different
 // candidates (different phases), and the result is per half.
-template <int BS, class Src>
+//
+// INT: the vector is whole-pel (every step of the diamond walks and their
+// starting points), so the samples are the integer plane's alone; the sub-pel
+// crosses take any phase through the branch-free form.  Both keep the code of
+// a step small: the walks' many inlined steps otherwise overflow the SM's
+// instruction cache.
+template <int BS, bool INT = false, class Src>
 __device__ __forceinline__ int sad_packed(uint32_t c0, uint32_t c1, const Src &R, int bx, int by,
                                           int mvx, int mvy, int lane) {
     const int ph = (mvy & 3) * 4 + (mvx & 3);
     if (BS == 16) {
         const int row = lane >> 1, half = lane & 1;
         const int x = bx + (mvx >> 2) + half * 8, y = by + (mvy >> 2) + row;
-        int v = __vsadu4(c0, mc_word(R, x, y, ph)) + __vsadu4(c1, mc_word(R, x + 4, y, ph));
+        int v;
+        if (INT) v = __vsadu4(c0, R.ld(0, x, y)) + __vsadu4(c1, R.ld(0, x + 4, y));
+        else v = __vsadu4(c0, mc_word_nb(R, x, y, ph)) + __vsadu4(c1, mc_word_nb(R, x + 4, y, ph));
         return __reduce_add_sync(FDVB_FULL, v);
     } else {
         const int l = lane & 15, row = l >> 1, half = l & 1;
         const int x = bx + (mvx >> 2) + half * 4, y = by + (mvy >> 2) + row;
-        const int v = __vsadu4(c0, mc_word_nb(R, x, y, ph));
+        const int v = __vsadu4(c0, INT ? R.ld(0, x, y) : mc_word_nb(R, x, y, ph));
         const int lo = __reduce_add_sync(FDVB_FULL, lane < 16 ? v : 0);
         const int hi = __reduce_add_sync(FDVB_FULL, lane < 16 ? 0 : v);
         return lane < 16 ? lo : hi;
@@ -204,24 +212,24 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
     {   // the zero vector (k = 0), the seed (k = 1) and any proposals (k = 2..)
         int *s = scores();
         if (BS == 16) {
-            if (gw == 0) { int v = sad_packed<16>(c0, c1, R, bx, by, 0, 0, lane); if (lane == 0) s[0] = v; }
-            if (gw == 1 && seed) { int v = sad_packed<16>(c0, c1, R, bx, by, px, py, lane); if (lane == 0) s[1] = v; }
+            if (gw == 0) { int v = sad_packed<16, true>(c0, c1, R, bx, by, 0, 0, lane); if (lane == 0) s[0] = v; }
+            if (gw == 1 && seed) { int v = sad_packed<16, true>(c0, c1, R, bx, by, px, py, lane); if (lane == 0) s[1] = v; }
             for (int k = 2 + gw; k < 2 + ncands; k += 4) {
                 int x, y;
                 cand_at(k - 2, x, y);
-                int v = sad_packed<16>(c0, c1, R, bx, by, x, y, lane);
+                int v = sad_packed<16, true>(c0, c1, R, bx, by, x, y, lane);
                 if (lane == 0) s[k] = v;
             }
         } else if (gw == 0) {
             const int hk = lane >> 4;
-            int v = sad_packed<8>(c0, c1, R, bx, by, hk ? px : 0, hk ? py : 0, lane);
+            int v = sad_packed<8, true>(c0, c1, R, bx, by, hk ? px : 0, hk ? py : 0, lane);
             if ((lane & 15) == 0 && (hk == 0 || seed)) s[hk] = v;
         } else if (gw <= 2 && ncands > 0) {
             // up to four proposals on the half-warps of warps 1 and 2
             const int ci = 2 * (gw - 1) + (lane >> 4);
             int x, y;
             cand_at(ci < ncands ? ci : 0, x, y);
-            int v = sad_packed<8>(c0, c1, R, bx, by, x, y, lane);
+            int v = sad_packed<8, true>(c0, c1, R, bx, by, x, y, lane);
             if ((lane & 15) == 0 && ci < ncands) s[2 + ci] = v;
         }
         gbar(bar, 128);
@@ -241,14 +249,14 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
             for (int k = gw; k < 8; k += 4) {
                 const int nx = cx + ld_dx(k), ny = cy + ld_dy(k);
                 if (!inb(nx, ny)) continue;
-                int v = sad_packed<16>(c0, c1, R, bx, by, nx, ny, lane);
+                int v = sad_packed<16, true>(c0, c1, R, bx, by, nx, ny, lane);
                 if (lane == 0) s[k] = v;
             }
         } else {
             const int k = 2 * gw + (lane >> 4);
             const int nx = cx + ld_dx(k), ny = cy + ld_dy(k);
             const bool in = inb(nx, ny);
-            int v = sad_packed<8>(c0, c1, R, bx, by, in ? nx : cx, in ? ny : cy, lane);
+            int v = sad_packed<8, true>(c0, c1, R, bx, by, in ? nx : cx, in ? ny : cy, lane);
             if ((lane & 15) == 0 && in) s[k] = v;
         }
         gbar(bar, 128);
@@ -269,13 +277,13 @@ __device__ int me_search_group(const uint8_t *cur, const Src &R, int bx, int by,
         if (BS == 16) {
             const int k = gw, nx = cx + sd_dx(k), ny = cy + sd_dy(k);
             if (inb(nx, ny)) {
-                int v = sad_packed<16>(c0, c1, R, bx, by, nx, ny, lane);
+                int v = sad_packed<16, true>(c0, c1, R, bx, by, nx, ny, lane);
                 if (lane == 0) s[k] = v;
             }
         } else if (gw < 2) {
             const int k = 2 * gw + (lane >> 4), nx = cx + sd_dx(k), ny = cy + sd_dy(k);
             const bool in = inb(nx, ny);
-            int v = sad_packed<8>(c0, c1, R, bx, by, in ? nx : cx, in ? ny : cy, lane);
+            int v = sad_packed<8, true>(c0, c1, R, bx, by, in ? nx : cx, in ? ny : cy, lane);
             if ((lane & 15) == 0 && in) s[k] = v;
         }
         gbar(bar, 128);

@@ -131,7 +131,7 @@ template <class Src>
 __device__ __forceinline__ void mc16_group(const Src &R, int bx, int by, int mvx, int mvy, uint8_t *dst, int gt) {
     if (gt < 64) {
         const int row = gt >> 2, col = (gt & 3) * 4, ph = (mvy & 3) * 4 + (mvx & 3);
-        reinterpret_cast<uint32_t *>(dst)[gt] = mc_word(R, bx + col + (mvx >> 2), by + row + (mvy >> 2), ph);
+        reinterpret_cast<uint32_t *>(dst)[gt] = mc_word_nb(R, bx + col + (mvx >> 2), by + row + (mvy >> 2), ph);
     }
 }
 
@@ -529,7 +529,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 const MBInfo &c = S.cand[mi];
                 const int r2 = k >> 2, c2 = (k & 3) * 4, ph = (c.y & 3) * 4 + (c.x & 3);
                 reinterpret_cast<uint32_t *>(S.predS[mi])[k] =
-                    mc_word(c.ref ? L1 : L0, bx + c2 + (c.x >> 2), by + r2 + (c.y >> 2), ph);
+                    mc_word_nb(c.ref ? L1 : L0, bx + c2 + (c.x >> 2), by + r2 + (c.y >> 2), ph);
             }
             __syncthreads();
             if (warp < ncand) {
@@ -601,7 +601,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                             if (gt < 16) {
                                 const int r2 = gt >> 1, c2 = (gt & 1) * 4, ph = (my & 3) * 4 + (mx & 3);
                                 reinterpret_cast<uint32_t *>(S.pred8[q])[gt] =
-                                    mc_word(L0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
+                                    mc_word_nb(L0, bx + qx + c2 + (mx >> 2), by + qy + r2 + (my >> 2), ph);
                             }
                         }
                         if (gt == 0) S.ssad = ssad;
