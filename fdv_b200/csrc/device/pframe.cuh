@@ -193,7 +193,10 @@ __device__ __forceinline__ WindowLuma luma_src<true>(const RefPlanes &, const ui
 // One residual warp task of region g (regions 4c..4c+3 belong to candidate c:
 // 0, 1 INTER16 on the two references, 2 INTRA16, 3 INTER8): j = 0, 1 the 4x4
 // block pairs 0-1 and 2-3 (one per half-warp), j = 2 the 8x8 option.
-__device__ __forceinline__ void resid_task(PShared &S, int g, int j, int qp, double lambda, int warp, int lane) {
+// Not inlined (nor group_decide below): one copy of their code serves every
+// call site, which keeps the kernel's instruction footprint within the SM's
+// instruction cache.
+__device__ __noinline__ void resid_task(PShared &S, int g, int j, int qp, double lambda, int warp, int lane) {
     const uint8_t *cp, *pp;
     int pstr;
     if (g < 12) {
@@ -216,7 +219,7 @@ __device__ __forceinline__ void resid_task(PShared &S, int g, int j, int qp, dou
 // Candidate c's region decisions (fdv.h:5379-5411) on the four warps of a
 // group (barrier `bar`): transform choices, stream offsets in region order,
 // one warp per region copying its symbols; distortion and rate to cD/cB.
-__device__ __forceinline__ void group_decide(PShared &S, int c, double lambda, int gw, int gt, int lane, int bar,
+__device__ __noinline__ void group_decide(PShared &S, int c, double lambda, int gw, int gt, int lane, int bar,
                                              unsigned *err) {
     if (gt < 4) region_choice(&S.blk[4 * (4 * c + gt)], S.reg[4 * c + gt], lambda, S.dec[4 * c + gt]);
     gbar(bar, 128);
@@ -566,25 +569,22 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 // ---- phase 1: searches on four warp groups
                 const long long tg0 = (U.prof && gt == 0) ? clock64() : 0;
                 if (tid < 4) cs_reset(&S.sink[tid]);
-                if (grp == 0) {
-                    if (!l_intra) {
+                if (grp < 2) {
+                    // the 16x16 search on reference grp (one call site for both
+                    // references keeps one copy of its code); with proposals
+                    // it also starts from them (doubled for the second
+                    // reference); a full search (not confident) still runs the
+                    // diamond to the end
+                    if (grp == 0 ? !l_intra : (navail > 1 && !lfast)) {
                         int mx, my;
-                        // with proposals the search also starts from them; a full
-                        // search (not confident) still runs the diamond to the end
-                        int sd = me_search_group<16>(S.cur, L0, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[0], gw, lane, 9,
-                                                     U.prof ? &U.prof[PP_IT16] : nullptr, (LRN && U.hint) ? S.lmv : nullptr,
-                                                     (LRN && U.hint) ? lrn::kMvHyp : 0, lfast ? kLearnLd : 64);
-                        if (gt == 0) { S.mv[0][0] = mx; S.mv[0][1] = my; S.sad[0] = sd; }
-                        mc16_group(L0, bx, by, mx, my, S.pr[0], gt);
-                    }
-                } else if (grp == 1) {
-                    if (navail > 1 && !lfast) {
-                        int mx, my;
-                        int sd = me_search_group<16>(S.cur, L1, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[1], gw, lane, 10,
-                                                     nullptr, (LRN && U.hint) ? S.lmv2 : nullptr,
-                                                     (LRN && U.hint) ? lrn::kMvHyp : 0);
-                        if (gt == 0) { S.mv[1][0] = mx; S.mv[1][1] = my; S.sad[1] = sd; }
-                        mc16_group(L1, bx, by, mx, my, S.pr[1], gt);
+                        const bool hinted = LRN && U.hint;
+                        const typename LumaOf<WIN>::T &Lg = grp ? L1 : L0;
+                        int sd = me_search_group<16>(S.cur, Lg, bx, by, R, pmvx, pmvy, &mx, &my, S.gsad[grp], gw, lane,
+                                                     9 + grp, (grp == 0 && U.prof) ? &U.prof[PP_IT16] : nullptr,
+                                                     hinted ? (grp ? S.lmv2 : S.lmv) : nullptr, hinted ? lrn::kMvHyp : 0,
+                                                     lfast ? kLearnLd : 64);
+                        if (gt == 0) { S.mv[grp][0] = mx; S.mv[grp][1] = my; S.sad[grp] = sd; }
+                        mc16_group(Lg, bx, by, mx, my, S.pr[grp], gt);
                     }
                 } else if (grp == 2) {
                     if (l8) {
