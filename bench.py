@@ -720,6 +720,7 @@ def main() -> None:
     ap.add_argument("--frames", type=int, default=NF, help="frames per step (profiling runs use a few)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-decode", action="store_true", help="skip the decoder leg")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape (no autotuner)")
     ap.add_argument("--workload", default="hd720", choices=["hd720", "batch48", "decode"],
                     help="batch48: the 48-stream batched workload (timed steps = P-frame steps); "
                          "decode: the decoder leg alone")
@@ -771,7 +772,21 @@ def main() -> None:
     torch.cuda.synchronize()
     bands = band_layout()
     nb = len(bands)
+    # the launch shape: the autotuner's choice for this geometry (it also
+    # applies to the e2e leg's fdv_vtile_encode), timed on its own seeded
+    # sequence before the timed region
+    tuning = None
+    if not args.no_tune:
+        import fdv_b200.tune as T
+        tr = T.autotune([(W, bh) for _, bh in bands], RANGE, local)
+        tuning = {k: tr[k] for k in ("max_batch", "p_grid", "p_ms_per_frame", "default_p_ms_per_frame", "cached")}
+        tuning["gain_vs_default"] = round(tr["default_p_ms_per_frame"] / tr["p_ms_per_frame"], 4)
+        tuning["default"] = {"max_batch": 30, "p_grid": tr["nsm"]}
+        tuning["candidates"] = tr["candidates"]
+        tuning["sequence"] = tr["sequence"]
     g = F.Engine([(W, bh) for _, bh in bands], RANGE, local)
+    if tuning:
+        g.set_tuning(tuning["max_batch"], tuning["p_grid"])
     dd, ll = C.c_double, C.c_longlong
     L.fdvg_stats.argtypes = [C.c_void_p] + [C.POINTER(dd), C.POINTER(dd), C.POINTER(ll), C.POINTER(dd),
                                             C.POINTER(ll), C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
@@ -879,6 +894,7 @@ def main() -> None:
             "config": config_of(world),
             "run": {"parallelism": f"bands{nb} per GPU, {world} GPU(s) each with its own stream",
                     "p_frames_per_launch": batch, "wall_s_timed": round(wall, 3)},
+            "tuning": tuning,
             "identical_to_reference": identical,
             "roofline": roofline,
             "cpu_baseline": cpu,

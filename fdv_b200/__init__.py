@@ -72,6 +72,10 @@ def lib() -> C.CDLL:
         L.fdvg_collect.argtypes = [p]
         L.fdvg_submit_batch.argtypes = [p, i, C.POINTER(u8p), C.POINTER(i), C.POINTER(i), C.c_void_p, C.c_void_p]
         L.fdvg_max_batch.argtypes = [p]
+        L.fdvg_set_tuning.argtypes = [p, i, i]
+        L.fdvg_get_tuning.argtypes = [p, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+        L.fdvg_get_tuning.restype = None
+        L.fdvb_set_tuning.argtypes = [i, C.POINTER(i), C.POINTER(i), i, i, i]
         L.fdvg_frames_device.argtypes = [p, i, C.POINTER(u8p), C.POINTER(i), C.POINTER(i)]
         L.fdvg_iframe_hist.argtypes = [p, i, i, C.POINTER(C.c_uint32)]
         L.fdvg_recon.argtypes = [p, i, u8p]
@@ -142,6 +146,16 @@ def _as_frames(frames, w: int, h: int) -> list[np.ndarray]:
             raise ValueError(f"frame has {a.size} bytes, expected {fs}")
         out.append(a)
     return out
+
+
+def set_tuning(sizes, search_range: int, max_batch: int, p_grid: int = 0) -> None:
+    """Record a launch shape for the fdv_* encoders' engines of this geometry
+    (fdvb_set_tuning); max_batch 0 removes it."""
+    n = len(sizes)
+    w = (C.c_int * n)(*[s[0] for s in sizes])
+    h = (C.c_int * n)(*[s[1] for s in sizes])
+    if lib().fdvb_set_tuning(n, w, h, search_range, max_batch, p_grid) != 0:
+        raise FdvError(last_error())
 
 
 def measure_int_rate(device: int = 0, reps: int = 5) -> float:
@@ -307,6 +321,17 @@ class Engine:
 
     def max_batch(self) -> int:
         return lib().fdvg_max_batch(self._g)
+
+    def set_tuning(self, max_batch: int, p_grid: int = 0) -> None:
+        """Launch shape (fdvg_set_tuning): P-frames per launch at most and
+        P-kernel blocks (0: one per SM)."""
+        if lib().fdvg_set_tuning(self._g, max_batch, p_grid) != 0:
+            raise FdvError(last_error())
+
+    def tuning(self) -> dict:
+        k, g, n = C.c_int(), C.c_int(), C.c_int()
+        lib().fdvg_get_tuning(self._g, C.byref(k), C.byref(g), C.byref(n))
+        return {"max_batch": k.value, "p_grid": g.value, "nsm": n.value}
 
     def submit_batch(self, frames, qp) -> None:
         """Queue consecutive P-frames as one launch (fdvg_submit_batch):

@@ -229,6 +229,10 @@ struct fdvb_engine {
     std::vector<const uint8_t *> prev_luma;  // per unit: the last submitted frame's luma (device sources)
     int total_mbs = 0;
     float *d_mbcost = nullptr;              // per-macroblock RD cost records (when enabled)
+    // run-time launch shape (fdvb_engine_set_tuning): P-frames per launch at
+    // most, and blocks of the P-frame wavefront kernel (macroblock rows in
+    // flight; 0: one per SM)
+    int tune_k = kMaxBatch, tune_pgrid = 0;
 };
 
 static int round_up(int v, int a) { return (v + a - 1) / a * a; }
@@ -685,7 +689,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         // this launch leaves while it ramps up and drains; reserving 16 or 40
         // SMs for it made the learned P-frame slower (0.46 / 0.52 against
         // 0.39 ms on the learned 720p workload)
-        const int grid = std::min((int)rows.size(), E->nsm);
+        const int grid = std::min((int)rows.size(), E->tune_pgrid > 0 ? std::min(E->tune_pgrid, E->nsm) : E->nsm);
         const void *pu_st = nullptr;
         if (!pu.empty()) {
             pu_st = staged(pu.data(), sizeof(int2) * pu.size());
@@ -811,7 +815,23 @@ extern "C" int fdvb_engine_submit(fdvb_engine *E, const uint8_t *const *planes, 
 // proposals, decision records or deferred references).
 extern "C" int fdvb_engine_max_batch(const fdvb_engine *E) {
     if (!E) return 0;
-    return (E->d_mbcost || E->defer_refs) ? 1 : kMaxBatch;
+    return (E->d_mbcost || E->defer_refs) ? 1 : E->tune_k;
+}
+
+// The launch shape: P-frames per launch at most (1..kMaxBatch) and blocks of
+// the P-frame wavefront kernel (0: one per SM; at most the SM count).
+extern "C" int fdvb_engine_set_tuning(fdvb_engine *E, int max_batch, int p_grid) {
+    if (!E) return -1;
+    if (max_batch < 1 || max_batch > kMaxBatch || p_grid < 0) { g_err = "tuning out of range"; return -1; }
+    E->tune_k = max_batch;
+    E->tune_pgrid = p_grid > E->nsm ? E->nsm : p_grid;
+    return 0;
+}
+extern "C" void fdvb_engine_get_tuning(const fdvb_engine *E, int *max_batch, int *p_grid, int *nsm) {
+    if (!E) return;
+    if (max_batch) *max_batch = E->tune_k;
+    if (p_grid) *p_grid = E->tune_pgrid > 0 ? E->tune_pgrid : E->nsm;
+    if (nsm) *nsm = E->nsm;
 }
 
 // Wait for the oldest submitted frame; on success the stream views

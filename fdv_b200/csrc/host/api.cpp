@@ -241,6 +241,29 @@ int g_learn_ver = 0;       // bumped on every change; 0 never reused
 int g_learn_on = 0;
 std::map<fdvb_engine *, int> *g_engine_lver = new std::map<fdvb_engine *, int>();
 
+// Launch shapes chosen for engine geometries (fdvb_set_tuning, written by the
+// autotuner): key = search range and unit sizes; value = P-frames per launch
+// and P-kernel blocks.  Applied whenever the fdv_* encoders take an engine.
+std::mutex g_tune_mu;
+std::map<std::vector<int>, std::pair<int, int>> *g_tune = new std::map<std::vector<int>, std::pair<int, int>>();
+std::vector<int> tune_key(int n, const int *w, const int *h, int range) {
+    std::vector<int> k{range, n};
+    for (int i = 0; i < n; ++i) { k.push_back(w[i]); k.push_back(h[i]); }
+    return k;
+}
+// The engine's launch shape: the tuned one for its geometry, else the default
+// (thirty P-frames per launch, one block per SM).
+void apply_tuning(fdvb_engine *E, int n, const int *w, const int *h, int range) {
+    std::pair<int, int> t{0, 0};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune->find(tune_key(n, w, h, range));
+        if (it != g_tune->end()) t = it->second;
+    }
+    if (t.first > 0) fdvb_engine_set_tuning(E, t.first, t.second);
+    else fdvb_engine_set_tuning(E, 30, 0);
+}
+
 fdvb_engine *engine_acquire(int n, const int *w, const int *h, int range, int device) {
     fdvb_engine *E = nullptr;
     int ver = 0;
@@ -259,6 +282,7 @@ fdvb_engine *engine_acquire(int n, const int *w, const int *h, int range, int de
     }
     if (!E) E = fdvb_engine_create(n, w, h, range, device);
     if (!E) return nullptr;
+    apply_tuning(E, n, w, h, range);
     std::vector<float> params;
     float conf;
     int want, on;
@@ -524,6 +548,7 @@ static fdv_encoder *enc_new(int w, int h, int qp, int keyint, int band_mbrows, i
     for (int b = 0; b < nb; ++b) { e->by0.push_back(b * bh_full); H[b] = std::min(bh_full, h - b * bh_full); e->bh.push_back(H[b]); }
     e->E = fdvb_engine_create(nb, W.data(), H.data(), g_range, g_device);
     if (!e->E) { set_engine_err(); delete e; return nullptr; }
+    apply_tuning(e->E, nb, W.data(), H.data(), g_range);
     e->us.resize(nb);
     for (int b = 0; b < nb; ++b) {
         e->us[b].w = w; e->us[b].h = H[b];
@@ -749,6 +774,21 @@ int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, co
     return rc;
 }
 int fdvg_max_batch(const fdvg_ctx *g) { return fdvb_engine_max_batch(g); }
+int fdvg_set_tuning(fdvg_ctx *g, int max_batch, int p_grid) {
+    const int rc = fdvb_engine_set_tuning(g, max_batch, p_grid);
+    if (rc) set_engine_err();
+    return rc;
+}
+void fdvg_get_tuning(const fdvg_ctx *g, int *max_batch, int *p_grid, int *nsm) {
+    fdvb_engine_get_tuning(g, max_batch, p_grid, nsm);
+}
+int fdvb_set_tuning(int nunits, const int *w, const int *h, int range, int max_batch, int p_grid) {
+    if (nunits <= 0 || !w || !h || max_batch < 0 || max_batch > 30 || p_grid < 0) { set_err("bad tuning"); return -1; }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (max_batch == 0) g_tune->erase(tune_key(nunits, w, h, range));
+    else (*g_tune)[tune_key(nunits, w, h, range)] = {max_batch, p_grid};
+    return 0;
+}
 
 // nframes frame steps from device sources, runs of P-frames batched, each
 // batch collected while the next one runs; the stream views then describe the

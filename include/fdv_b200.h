@@ -172,8 +172,9 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
 int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
                 const double *lscale, const int *force_skip);
 int fdvg_collect(fdvg_ctx *g);
-/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (thirty; one
- * while decision records or deferred references are on):
+/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (thirty by
+ * default, fdvg_set_tuning; one while decision records or deferred references
+ * are on):
  * the arrays hold frame k's entries at k * nunits (planes: 3 per unit).  The
  * frames' wavefronts run in one launch, each frame's macroblock rows starting
  * as soon as the reference tiles they read have been written by the frame
@@ -183,6 +184,16 @@ int fdvg_collect(fdvg_ctx *g);
 int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, const int *is_intra, const int *qp,
                       const double *lscale, const int *force_skip);
 int fdvg_max_batch(const fdvg_ctx *g);
+/* The engine's launch shape, the autotuner's knobs (no counterpart in the
+ * reference): max_batch P-frames per launch at most (1..30) and p_grid blocks
+ * of the P-frame wavefront kernel, i.e. macroblock rows in flight (0: one per
+ * SM; capped at the SM count).  fdvg_get_tuning reports the shape in force and
+ * the SM count.  fdvb_set_tuning records a shape for every engine the fdv_*
+ * encoders create or reuse for that geometry (units of w[i] x h[i] at search
+ * range `range`); max_batch 0 removes the record.  Returns 0 or -1. */
+int fdvg_set_tuning(fdvg_ctx *g, int max_batch, int p_grid);
+void fdvg_get_tuning(const fdvg_ctx *g, int *max_batch, int *p_grid, int *nsm);
+int fdvb_set_tuning(int nunits, const int *w, const int *h, int range, int max_batch, int p_grid);
 /* nframes frame steps from device sources (planes: 3 * nunits device pointers
  * per frame; is_intra and qp: nunits per frame): runs of P-frames go as
  * batches, each collected while the next one runs.  The stream accessors then
