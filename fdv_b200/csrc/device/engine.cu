@@ -148,6 +148,11 @@ struct Unit {
     int last_intra = 0, last_qp = 0;
     int mb_off = 0;               // first macroblock of this unit in engine-wide per-macroblock arrays
     fdvb_streams ps{}, is[3]{};
+    // the key-frame lookahead lane (allocated at first use): a later key
+    // frame analysed in the launch of an earlier one -- its reconstruction
+    // (deblocked there), per-CTU symbol slots, mode maps and CTU-row progress
+    uint8_t *krec = nullptr, *kislots[3] = {nullptr, nullptr, nullptr}, *kmmap[3] = {nullptr, nullptr, nullptr};
+    int *kprog = nullptr;
     RefSlot &slot_of(long long q) { return ref[(int)(((q % kRefSlots) + kRefSlots) % kRefSlots)]; }
 };
 
@@ -233,6 +238,18 @@ struct fdvb_engine {
     // most, and blocks of the P-frame wavefront kernel (macroblock rows in
     // flight; 0: one per SM)
     int tune_k = kMaxBatch, tune_pgrid = 0;
+    // Key-frame lookahead (fdvb_engine_key_lookahead).  A key frame's
+    // analysis is a latency-bound chain per CTU row that keeps few SMs busy,
+    // and it reads nothing but its own source: the next key frame of a
+    // sequence is analysed in the same launch as the current one (its rows
+    // after the current frame's luma rows) into the units' lookahead lanes, and
+    // its own submission then only compacts its symbols and prepares its
+    // reference.  `ka_*`: the frame armed for the next key submission;
+    // `kr_*`: the frame analysed and waiting.
+    bool ka_armed = false, kr_ready = false;
+    std::vector<const uint8_t *> ka_planes, kr_planes;
+    std::vector<int> ka_qp, kr_qp;
+    uint8_t *key_src = nullptr, *key_stage = nullptr;   // host sources: device copy and pinned staging
 };
 
 static int round_up(int v, int a) { return (v + a - 1) / a * a; }
@@ -306,6 +323,8 @@ static void free_unit(Unit &u) {
     }
     for (int r = 0; r < kRefSlots; ++r) cudaFree(u.ref[r].mem);
     for (int p = 0; p < 3; ++p) { cudaFree(u.islots[p]); cudaFree(u.mmap[p]); }
+    cudaFree(u.krec); cudaFree(u.kprog);
+    for (int p = 0; p < 3; ++p) { cudaFree(u.kislots[p]); cudaFree(u.kmmap[p]); }
     for (int k = 0; k < kSlots; ++k) if (u.out_h[k]) cudaFreeHost(u.out_h[k]);
     for (int k = 0; k < kSlots; ++k) if (u.hist_h[k]) cudaFreeHost(u.hist_h[k]);
 }
@@ -313,9 +332,10 @@ static void free_unit(Unit &u) {
 // Bytes of the descriptor area of a slot's staging buffer (each array 64-byte aligned).
 static size_t stage_desc_bytes(int nu, int maxrows, int maxitasks) {
     auto a = [](size_t n) { return (n + 63) / 64 * 64; };
+    // key-frame descriptors twice over: a key frame and the lookahead beside it
     return a(sizeof(UnitDev) * kMaxBatch * nu) + a(sizeof(RowTask) * kMaxBatch * maxrows) +
-           a(sizeof(IPlaneDevH) * 3 * nu) + a(sizeof(ITaskH) * maxitasks) + a(sizeof(PrepTaskH) * nu) +
-           a(sizeof(DbTaskH) * 3 * nu) + a(sizeof(CompactTaskH) * 3 * kMaxBatch * nu) + a(sizeof(int2) * nu);
+           a(sizeof(IPlaneDevH) * 6 * nu) + a(sizeof(ITaskH) * 2 * maxitasks) + 2 * a(sizeof(PrepTaskH) * nu) +
+           a(sizeof(DbTaskH) * 6 * nu) + a(sizeof(CompactTaskH) * 3 * kMaxBatch * nu) + a(sizeof(int2) * nu);
 }
 
 extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
@@ -358,10 +378,10 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     for (auto &u : E->units) { u.mb_off = E->total_mbs; E->total_mbs += u.mbw * u.mbh; }
     bool ok = cudaMalloc(&E->d_units, sizeof(UnitDev) * kMaxBatch * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_rows, sizeof(RowTask) * kMaxBatch * maxrows) == cudaSuccess &&
-              cudaMalloc(&E->d_planes, sizeof(IPlaneDevH) * 3 * nunits) == cudaSuccess &&
-              cudaMalloc(&E->d_itasks, sizeof(ITaskH) * maxitasks) == cudaSuccess &&
+              cudaMalloc(&E->d_planes, sizeof(IPlaneDevH) * 6 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_itasks, sizeof(ITaskH) * 2 * maxitasks) == cudaSuccess &&
               cudaMalloc(&E->d_prep, sizeof(PrepTaskH) * nunits) == cudaSuccess &&
-              cudaMalloc(&E->d_db, sizeof(DbTaskH) * 3 * nunits) == cudaSuccess &&
+              cudaMalloc(&E->d_db, sizeof(DbTaskH) * 6 * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_cmp, sizeof(CompactTaskH) * 3 * kMaxBatch * nunits) == cudaSuccess &&
               cudaMalloc(&E->d_ticket, sizeof(int) * 2) == cudaSuccess &&
               cudaMalloc(&E->d_err, sizeof(unsigned)) == cudaSuccess &&
@@ -426,6 +446,8 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
         if (sl.stage) cudaFreeHost(sl.stage);
         if (sl.err_h) cudaFreeHost(sl.err_h);
     }
+    cudaFree(E->key_src);
+    if (E->key_stage) cudaFreeHost(E->key_stage);
     if (E->st) cudaStreamDestroy(E->st);
     delete E;
 }
@@ -443,17 +465,19 @@ static size_t parse_streams(const uint8_t *p, int n, fdvb_streams *s) {
 }
 
 // Enqueue the reference preparation of units `which` from lane 0's deblocked
-// reconstruction into ring slot seq % kRefSlots (the caller then advances
-// seq); the task array is staged in `stage` (pinned, slot-owned) when given,
-// else copied from the stack (callers that synchronise before returning).
-static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *stage = nullptr) {
+// reconstruction (or the lookahead lane's, key_lane) into ring slot
+// seq % kRefSlots (the caller then advances seq); the task array is staged
+// in `stage` (pinned, slot-owned) when given, else copied from the stack
+// (callers that synchronise before returning).
+static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *stage = nullptr, bool key_lane = false) {
     std::vector<PrepTaskH> pt;
     int maxw = 0, maxh = 0;
     for (int i : which) {
         Unit &u = E->units[i];
         RefSlot &s = u.slot_of(u.seq);
         PrepTaskH t;
-        t.rec[0] = u.rec[0]; t.rec[1] = u.rec[0] + (size_t)u.w * u.h; t.rec[2] = t.rec[1] + (size_t)u.cw * u.ch;
+        const uint8_t *src = key_lane ? u.krec : u.rec[0];
+        t.rec[0] = src; t.rec[1] = src + (size_t)u.w * u.h; t.rec[2] = t.rec[1] + (size_t)u.cw * u.ch;
         t.G = s.G; t.B = s.B; t.H = s.H; t.J = s.J; t.U = s.U; t.V = s.V;
         t.w = u.w; t.h = u.h; t.ys = s.rp.ys; t.cs = s.rp.cs; t.border = E->border;
         pt.push_back(t);
@@ -465,6 +489,47 @@ static int prep_refs(fdvb_engine *E, const std::vector<int> &which, uint8_t *sta
     CK(cudaMemcpyAsync(E->d_prep, src, sizeof(PrepTaskH) * pt.size(), cudaMemcpyHostToDevice, E->st));
     launch_refprep(E->d_prep, (int)pt.size(), maxw, maxh, E->border, E->st);
     CK(cudaGetLastError());
+    return 0;
+}
+
+// The units' lookahead lanes and the lookahead's source buffers, at first use.
+static int alloc_key_lanes(fdvb_engine *E) {
+    for (auto &u : E->units) {
+        if (u.krec) continue;
+        CK(cudaMalloc(&u.krec, (size_t)u.w * u.h * 3 / 2));
+        int nrows = 0;
+        for (int p = 0; p < 3; ++p) {
+            CK(cudaMalloc(&u.kislots[p], (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p]));
+            CK(cudaMalloc(&u.kmmap[p], (size_t)(u.pw[p] / 4) * (u.ph[p] / 4)));
+            nrows += u.irows[p];
+        }
+        CK(cudaMalloc(&u.kprog, sizeof(int) * nrows));
+    }
+    if (!E->key_src) CK(cudaMalloc(&E->key_src, E->src_bytes));
+    if (!E->key_stage) CK(cudaHostAlloc(&E->key_stage, E->src_bytes, cudaHostAllocDefault));
+    return 0;
+}
+
+// Arm the key-frame lookahead: the next key-frame submission also analyses
+// this frame (planes: 3 per unit, host or device as the engine's sources;
+// qp: one per unit), and when this frame is itself submitted as a key frame,
+// with the same plane pointers and quantisers, its analysis is reused.  The
+// planes must stay valid and unchanged until then.  NULL planes disarm it and
+// drop an analysed frame that was never submitted.
+extern "C" int fdvb_engine_key_lookahead(fdvb_engine *E, const uint8_t *const *planes, const int *qp) {
+    if (!E) return -1;
+    if (!planes) { E->ka_armed = false; E->kr_ready = false; return 0; }
+    const int nu = (int)E->units.size();
+    if (!qp) { g_err = "bad arguments"; return -1; }
+    for (int i = 0; i < nu; ++i) {
+        if (qp[i] < 0 || qp[i] > 51) { g_err = "qp out of range"; return -1; }
+        if (!planes[3 * i] || !planes[3 * i + 1] || !planes[3 * i + 2]) { g_err = "missing source frame"; return -1; }
+    }
+    CK(cudaSetDevice(E->device));
+    if (alloc_key_lanes(E) != 0) return -3;
+    E->ka_planes.assign(planes, planes + 3 * nu);
+    E->ka_qp.assign(qp, qp + nu);
+    E->ka_armed = true;
     return 0;
 }
 
@@ -496,6 +561,20 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             if (fs && (is_intra[j] || nref == 0)) { g_err = "a held frame needs a reference"; return -1; }
             if (!is_intra[j] && nref == 0) { g_err = "a P-frame needs a reference"; return -1; }
         }
+    // A key frame for every unit: either the lookahead analysed it already
+    // (same planes and quantisers), or it is analysed now, with the armed
+    // lookahead frame beside it in the same launch.
+    bool all_key = K == 1;
+    for (int i = 0; i < nu && all_key; ++i) if (!is_intra[i] || (force_skip && force_skip[i])) all_key = false;
+    bool prefetched = false;
+    if (all_key && E->kr_ready && !E->defer_refs) {
+        prefetched = std::equal(E->kr_planes.begin(), E->kr_planes.end(), planes) &&
+                     std::equal(E->kr_qp.begin(), E->kr_qp.end(), qp);
+        E->kr_ready = false;
+    }
+    // (an armed frame that is this very frame is simply coded now)
+    const bool joint = all_key && !prefetched && E->ka_armed && !E->defer_refs &&
+                       !std::equal(E->ka_planes.begin(), E->ka_planes.end(), planes);
     CK(cudaSetDevice(E->device));
     int sis[kMaxBatch];
     for (int k = 0, s = 0; k < K; ++k) {
@@ -533,6 +612,26 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 }
             }
         }
+    // the lookahead frame's sources: read in place, or staged and uploaded
+    std::vector<const uint8_t *> kplanes;
+    if (joint) {
+        kplanes = E->ka_planes;
+        if (!E->src_on_device) {
+            size_t off = 0;
+            for (int i = 0; i < nu; ++i) {
+                Unit &u = E->units[i];
+                const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
+                memcpy(E->key_stage + off, kplanes[3 * i], ys);
+                memcpy(E->key_stage + off + ys, kplanes[3 * i + 1], cs);
+                memcpy(E->key_stage + off + ys + cs, kplanes[3 * i + 2], cs);
+                kplanes[3 * i] = E->key_src + off;
+                kplanes[3 * i + 1] = E->key_src + off + ys;
+                kplanes[3 * i + 2] = E->key_src + off + ys + cs;
+                off += ys + 2 * cs;
+            }
+            CK(cudaMemcpyAsync(E->key_src, E->key_stage, off, cudaMemcpyHostToDevice, E->st));
+        }
+    }
     // descriptors are staged after the first frame's sources
     uint8_t *stage = SL.stage + E->src_stage_bytes;
     auto staged = [&](const void *src, size_t n) -> const void * {
@@ -553,6 +652,8 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     // take less time than a tile of the in-wavefront stage, which would then
     // lengthen the wavefront; the form runs one frame per launch anyway)
     std::vector<int> iunits;
+    std::vector<int> kunits;  // key frames analysed by the lookahead: reference from its lane
+    std::vector<char> iluma;  // per key-frame plane descriptor: a luma plane
     std::vector<int2> pu;     // P units and their first macroblock in the hint array
     int nhint = 0, npu0 = 0, nhint0 = 0;   // frame 0's share (its SKIP pre-analysis)
     // Inference ahead of the analysis (device sources, several frames, every
@@ -638,6 +739,17 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 CompactTaskH c{u.slots[k], u.mbw * u.mbh, kSlotBytes, 16, E->d_poff, u.out_d[sis[k]], u.out_cap,
                                u.hist_d[sis[k]], u.cout[k]};
                 cmp.push_back(c);
+            } else if (prefetched) {
+                // analysed (and deblocked) in an earlier key frame's launch:
+                // compact its symbols; its reference comes from the lookahead lane
+                kunits.push_back(i);
+                for (int p = 0; p < 3; ++p) {
+                    CompactTaskH c{u.kislots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
+                                   u.out_d[sis[k]] + u.out_off_i[p],
+                                   (p < 2 ? u.out_off_i[p + 1] : u.out_cap) - u.out_off_i[p],
+                                   u.hist_d[sis[k]] + p * 12 * 256, u.cout[k] + u.out_off_i[p]};
+                    cmp.push_back(c);
+                }
             } else {
                 iunits.push_back(i);
                 int prog = p_progress_words(u);
@@ -648,6 +760,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                     P.qp = qp[j]; P.lambda = fdvb_lambda(qp[j], 1.0); P.prof = E->d_prof ? E->d_prof + 16 : nullptr;
                     int pid = (int)iplanes.size();
                     iplanes.push_back(P);
+                    iluma.push_back(p == 0);
                     for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
                     prog += u.irows[p];
                     CompactTaskH c{u.islots[p], u.icols[p] * u.irows[p], iframe_slot_bytes(), 12, E->d_ioff,
@@ -657,6 +770,27 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                     cmp.push_back(c);
                 }
                 for (int p = 0; p < 3; ++p) db.push_back({d.rec[p], u.pw[p], u.ph[p], qp[j]});
+                if (joint) {
+                    // the lookahead frame: the same unit's planes into its lane
+                    // (deblocked here too; compacted at its own submission)
+                    const size_t ys = (size_t)u.w * u.h, cs = (size_t)u.cw * u.ch;
+                    uint8_t *krec[3] = {u.krec, u.krec + ys, u.krec + ys + cs};
+                    int kp = 0;
+                    for (int p = 0; p < 3; ++p) {
+                        IPlaneDevH P;
+                        P.src = kplanes[3 * i + p]; P.rec = krec[p]; P.mmap = u.kmmap[p]; P.progress = u.kprog + kp;
+                        P.slots = u.kislots[p]; P.w = u.pw[p]; P.h = u.ph[p]; P.cols = u.icols[p]; P.rows = u.irows[p];
+                        P.qp = E->ka_qp[i]; P.lambda = fdvb_lambda(E->ka_qp[i], 1.0);
+                        P.prof = E->d_prof ? E->d_prof + 16 : nullptr;
+                        const int pid = (int)iplanes.size();
+                        iplanes.push_back(P);
+                        iluma.push_back(p == 0);
+                        for (int r = 0; r < u.irows[p]; ++r) itasks.push_back({pid, r});
+                        kp += u.irows[p];
+                        db.push_back({krec[p], u.pw[p], u.ph[p], E->ka_qp[i]});
+                    }
+                    CK(cudaMemsetAsync(u.kprog, 0, sizeof(int) * kp, E->st));
+                }
             }
             const int nprog = p_progress_words(u) + u.irows[0] + u.irows[1] + u.irows[2];
             CK(cudaMemsetAsync(u.progress[k], 0, sizeof(int) * nprog, E->st));
@@ -670,14 +804,12 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         for (int r = 0; r < maxh; ++r)
             for (auto &t : frows) if (t.row == r) rows.push_back(t);
     }
-    {
-        std::vector<ITaskH> it2;
-        int maxr = 0;
-        for (auto &t : itasks) maxr = std::max(maxr, t.row + 1);
-        for (int r = 0; r < maxr; ++r)
-            for (auto &t : itasks) if (t.row == r) it2.push_back(t);
-        itasks.swap(it2);
-    }
+    // Key-frame CTU rows in ticket order: by row, a row's luma planes (the
+    // longest chains) before its chroma planes.  A row waits only for the row
+    // above in its own plane, which comes earlier in this order.
+    std::stable_sort(itasks.begin(), itasks.end(), [&](const ITaskH &a, const ITaskH &b) {
+        return 2 * a.row + (iluma[a.plane] ? 0 : 1) < 2 * b.row + (iluma[b.plane] ? 0 : 1);
+    });
     const void *ud_st = staged(ud.data(), sizeof(UnitDev) * K * nu);
     CK(cudaMemcpyAsync(E->d_units, ud_st, sizeof(UnitDev) * K * nu, cudaMemcpyHostToDevice, E->st));
     CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
@@ -772,6 +904,11 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     } else {
         if (!iunits.empty()) {
             if (prep_refs(E, iunits, stage) != 0) return -3;
+            stage += (sizeof(PrepTaskH) * iunits.size() + 63) / 64 * 64;
+            E->launches += 2;
+        }
+        if (!kunits.empty()) {
+            if (prep_refs(E, kunits, stage, true) != 0) return -3;
             E->launches += 2;
         }
         for (int i = 0; i < nu; ++i) {
@@ -796,6 +933,12 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         S.has_p = !rows.empty();
         S.has_i = !itasks.empty();
         S.batch = k == 0 ? K : 0;
+    }
+    if (joint) {   // the lookahead frame waits in its lane for its own submission
+        E->kr_ready = true;
+        E->kr_planes = E->ka_planes;
+        E->kr_qp = E->ka_qp;
+        E->ka_armed = false;
     }
     E->stall_unit = E->stall_row = -1;     // an injected stall lasts one step
     for (int k = 0; k < K; ++k) {

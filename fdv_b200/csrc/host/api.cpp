@@ -403,7 +403,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         stream_header(us[b].bytes, nframes, w, H[b], qp, keyint);
     }
     const int kmax = std::max(1, fdvb_engine_max_batch(E));
-    std::vector<const uint8_t *> planes(3 * nb * kmax);
+    std::vector<const uint8_t *> planes(3 * nb * kmax), kplanes(3 * nb);
     std::vector<int> intra(nb * kmax), qps(nb * kmax, qp);
     Pool pool(std::max(1, std::min(nthreads, nb)));
     std::vector<int> urc(nb);
@@ -429,6 +429,21 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
                     planes[3 * j + 1] = fu + (size_t)(Y0[b] / 2) * cw;
                     planes[3 * j + 2] = fv + (size_t)(Y0[b] / 2) * cw;
                     intra[j] = key_at(f + k);
+                }
+            }
+            if (key_at(f)) {
+                // the sequence's next key frame is analysed in this key
+                // frame's launch (fdvb_engine_key_lookahead)
+                int f2 = f + 1;
+                while (f2 < nframes && !key_at(f2)) ++f2;
+                if (f2 < nframes) {
+                    const uint8_t *fy = frames[f2], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+                    for (int b = 0; b < nb; ++b) {
+                        kplanes[3 * b] = fy + (size_t)Y0[b] * w;
+                        kplanes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+                        kplanes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+                    }
+                    if (fdvb_engine_key_lookahead(E, kplanes.data(), qps.data()) != 0) { set_engine_err(); rc = -1; break; }
                 }
             }
             if (fdvb_engine_submit_batch(E, K, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) {
@@ -479,6 +494,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         types.pop_front();
         fdvb_engine_collect(E);
     }
+    fdvb_engine_key_lookahead(E, nullptr, nullptr);   // the next call's frames are other buffers
     if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
     else fdvb_engine_destroy(E);
     return rc;
@@ -774,6 +790,11 @@ int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, co
     return rc;
 }
 int fdvg_max_batch(const fdvg_ctx *g) { return fdvb_engine_max_batch(g); }
+int fdvg_key_lookahead(fdvg_ctx *g, const uint8_t *const *planes, const int *qp) {
+    const int rc = fdvb_engine_key_lookahead(g, planes, qp);
+    if (rc) set_engine_err();
+    return rc;
+}
 int fdvg_set_tuning(fdvg_ctx *g, int max_batch, int p_grid) {
     const int rc = fdvb_engine_set_tuning(g, max_batch, p_grid);
     if (rc) set_engine_err();
@@ -802,10 +823,23 @@ int fdvg_frames_device(fdvg_ctx *g, int nframes, const uint8_t *const *dplanes, 
     };
     fdvb_engine_src_on_device(g, 1);
     int rc = 0, prev = 0;
+    auto all_key = [&](int f) {
+        for (int i = 0; i < nu; ++i) if (!is_intra[(size_t)f * nu + i]) return false;
+        return true;
+    };
     for (int f = 0; f < nframes;) {
         int K = 1;
         if (!key_at(f))
             while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
+        if (all_key(f)) {
+            // the next all-key frame is analysed in this one's launch
+            int f2 = f + 1;
+            while (f2 < nframes && !all_key(f2)) ++f2;
+            if (f2 < nframes && fdvb_engine_key_lookahead(g, dplanes + (size_t)3 * nu * f2, qp + (size_t)nu * f2) != 0) {
+                rc = -1;
+                break;
+            }
+        }
         rc = fdvb_engine_submit_batch(g, K, dplanes + (size_t)3 * nu * f, is_intra + (size_t)nu * f,
                                       qp + (size_t)nu * f, nullptr, nullptr);
         if (rc) break;
@@ -822,6 +856,7 @@ int fdvg_frames_device(fdvg_ctx *g, int nframes, const uint8_t *const *dplanes, 
         const int r = fdvb_engine_collect(g);
         if (!rc) rc = r;
     }
+    fdvb_engine_key_lookahead(g, nullptr, nullptr);
     fdvb_engine_src_on_device(g, 0);
     if (rc) set_engine_err();
     return rc;

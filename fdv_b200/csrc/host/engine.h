@@ -19,6 +19,7 @@ int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *const *planes
                              const double *lscale, const int *force_skip);
 int fdvb_engine_max_batch(const fdvb_engine *E);
 int fdvb_engine_set_tuning(fdvb_engine *E, int max_batch, int p_grid);
+int fdvb_engine_key_lookahead(fdvb_engine *E, const uint8_t *const *planes, const int *qp);
 void fdvb_engine_get_tuning(const fdvb_engine *E, int *max_batch, int *p_grid, int *nsm);
 void fdvb_engine_defer_refs(fdvb_engine *E, int on);
 int fdvb_engine_commit_refs(fdvb_engine *E);

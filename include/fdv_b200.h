@@ -192,6 +192,20 @@ int fdvg_max_batch(const fdvg_ctx *g);
  * encoders create or reuse for that geometry (units of w[i] x h[i] at search
  * range `range`); max_batch 0 removes the record.  Returns 0 or -1. */
 int fdvg_set_tuning(fdvg_ctx *g, int max_batch, int p_grid);
+/* Key-frame lookahead (no counterpart in the reference: the reference codes
+ * its frames in order).  A key frame's analysis reads nothing but its own
+ * source, and one key frame's CTU-row chains keep few SMs busy, so the next
+ * key frame of a sequence can be analysed in the same launch.  Arms `planes`
+ * (3 per unit, host or device pointers as the engine's sources) and `qp` (one
+ * per unit) for the next key-frame submission of every unit: that launch also
+ * analyses and deblocks this frame into a lookahead lane, and when this frame
+ * is later submitted as a key frame with the same plane pointers and
+ * quantisers, only its symbols are compacted and its reference prepared.  The
+ * planes must stay valid and unchanged until that submission; any other key
+ * frame drops the analysed one.  NULL planes disarm.  The streams are the
+ * same as without it.  fdvg_frames_device, fdv_video_encode and
+ * fdv_vtile_encode arm it themselves. */
+int fdvg_key_lookahead(fdvg_ctx *g, const uint8_t *const *planes, const int *qp);
 void fdvg_get_tuning(const fdvg_ctx *g, int *max_batch, int *p_grid, int *nsm);
 int fdvb_set_tuning(int nunits, const int *w, const int *h, int range, int max_batch, int p_grid);
 /* nframes frame steps from device sources (planes: 3 * nunits device pointers

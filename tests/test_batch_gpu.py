@@ -139,3 +139,49 @@ def test_long_batched_sequence_matches_oracle(built):
     for u, o in enumerate(units):
         assert np.array_equal(eng.recon(u), o.recon()), f"unit {u} reconstruction"
     eng.close()
+
+
+@pytest.mark.parametrize("nf", [14, 11])
+def test_frames_device_key_lookahead_matches_oracle(built, nf):
+    """fdvg_frames_device from device-resident sources, key frames at 0, 5
+    and 10: frame 5 is analysed in frame 0's launch (the key-frame lookahead)
+    and reused at its own turn, frame 10 is coded at its own; the last frame's
+    streams (a P-frame, or key frame 10 when the sequence ends there) and
+    every unit's reconstruction equal the CPU oracle coding the frames in
+    order."""
+    import ctypes as C
+    import torch
+    import fdv_b200 as F
+    import oracle as O
+    sizes, rng, qp = [(160, 96), (64, 48)], 32, 26
+    nu = len(sizes)
+    frames = [F.Scene(w, h, nf, nrects=max(2, w * h // 3000), pan_qx=7, pan_qy=-3, static_pct=20,
+                      seed=81 + u).frames(nf) for u, (w, h) in enumerate(sizes)]
+    dev = [torch.from_numpy(np.stack(fr)).to("cuda:0") for fr in frames]
+    torch.cuda.synchronize()
+    keys = [1 if f % 5 == 0 else 0 for f in range(nf)]
+    planes = (F.u8p * (3 * nu * nf))()
+    for f in range(nf):
+        for u, (w, h) in enumerate(sizes):
+            b = dev[u].data_ptr() + f * w * h * 3 // 2
+            j = 3 * (f * nu + u)
+            planes[j], planes[j + 1], planes[j + 2] = (C.cast(b, F.u8p), C.cast(b + w * h, F.u8p),
+                                                       C.cast(b + w * h * 5 // 4, F.u8p))
+    intra = (C.c_int * (nu * nf))(*[keys[f] for f in range(nf) for _ in range(nu)])
+    qps = (C.c_int * (nu * nf))(*([qp] * (nu * nf)))
+    eng = F.Engine(sizes, rng)
+    assert F.lib().fdvg_frames_device(eng._g, nf, planes, intra, qps) == 0, F.last_error()
+    units = [O.OracleUnit(w, h, rng) for (w, h) in sizes]
+    last = None
+    for f in range(nf):
+        last = [o.frame(frames[u][f], keys[f], qp)[0] for u, o in enumerate(units)]
+    for u, o in enumerate(units):
+        if keys[nf - 1]:
+            for p in range(3):
+                assert eng.iframe_streams(u, p) == list(last[u][p]), f"unit {u} plane {p}"
+        else:
+            got = eng.pframe_streams(u)
+            for s in range(16):
+                assert got[s] == last[u][s], f"unit {u} stream {s}"
+        assert np.array_equal(eng.recon(u), o.recon()), f"unit {u} reconstruction"
+    eng.close()
