@@ -342,10 +342,13 @@ def render_batch(specs, nframes: int):
 
 
 def run_batch(args) -> None:
-    """Aggregate Mpix/s and per-frame-step latency of the batched workload."""
+    """Aggregate Mpix/s and per-frame-step latency of the batched workload,
+    plain and learned forms.  One key frame (step 0), then P-frame steps, each
+    one launch over all 48 streams' macroblock rows."""
     import concurrent.futures as cf
     import torch
     import fdv_b200 as F
+    import fdv_b200.learned as LN
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -361,73 +364,94 @@ def run_batch(args) -> None:
     L.fdvg_frame_device.argtypes = [C.c_void_p, C.POINTER(F.u8p), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.c_void_p, C.c_void_p]
     n = len(specs)
+    sizes = [(sp["w"], sp["h"]) for sp in specs]
     qps = (C.c_int * n)(*[sp["qp"] for sp in specs])
     lumapix = sum(sp["w"] * sp["h"] for sp in specs)
+    params = LN.load_params(LN.DEFAULT_WEIGHTS)
 
     def step_ms_of(g):
         v = [dd(), dd(), ll(), dd(), ll(), ll(), ll(), ll()]
         L.fdvg_stats(g, *[C.byref(x) for x in v])
         return v[0].value
 
-    # device leg: every stream's frames resident in HBM
+    def pct(lat, q):
+        s = sorted(lat)
+        return round(s[min(len(s) - 1, int(q * len(s)))], 3)
+
+    # device legs: every stream's frames resident in HBM
     dev = [torch.from_numpy(np.stack(fr)).to("cuda:0") for fr in frames]
     torch.cuda.synchronize()
-    g = F.Engine([(sp["w"], sp["h"]) for sp in specs], 16)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")   # larger than L2, written between steps
-    lat = []
-    for f in range(nf):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ps = (F.u8p * (3 * n))()
-        for u, sp in enumerate(specs):
-            w, h = sp["w"], sp["h"]
-            b = dev[u].data_ptr() + f * w * h * 3 // 2
-            ps[3 * u], ps[3 * u + 1], ps[3 * u + 2] = (C.cast(b, F.u8p), C.cast(b + w * h, F.u8p),
-                                                       C.cast(b + w * h * 5 // 4, F.u8p))
-        intra = (C.c_int * n)(*([1 if f == 0 else 0] * n))
-        before = step_ms_of(g._g)
-        if L.fdvg_frame_device(g._g, ps, intra, qps, None, None) != 0:
-            raise RuntimeError(F.last_error())
-        if f >= warm:
-            lat.append(step_ms_of(g._g) - before)
-    g.close()
-    dev_s = sum(lat) / 1e3
-    value = len(lat) * lumapix / 1e6 / dev_s
 
-    # e2e leg: host frames through the engine ABI (fdvg_submit / fdvg_collect),
+    def device_leg(learned: bool) -> list:
+        g = F.Engine(sizes, 16)
+        if learned:
+            g.set_learned(params, LEARN_CONF)
+        lat = []
+        for f in range(nf):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ps = (F.u8p * (3 * n))()
+            for u, sp in enumerate(specs):
+                w, h = sp["w"], sp["h"]
+                b = dev[u].data_ptr() + f * w * h * 3 // 2
+                ps[3 * u], ps[3 * u + 1], ps[3 * u + 2] = (C.cast(b, F.u8p), C.cast(b + w * h, F.u8p),
+                                                           C.cast(b + w * h * 5 // 4, F.u8p))
+            intra = (C.c_int * n)(*([1 if f == 0 else 0] * n))
+            before = step_ms_of(g._g)
+            if L.fdvg_frame_device(g._g, ps, intra, qps, None, None) != 0:
+                raise RuntimeError(F.last_error())
+            if f >= warm:
+                lat.append(step_ms_of(g._g) - before)
+        g.close()
+        return lat
+
+    # e2e legs: host frames through the engine ABI (fdvg_submit / fdvg_collect),
     # every stream entropy-coded on the host threads while the GPU analyses
     # the next frame step
-    g = F.Engine([(sp["w"], sp["h"]) for sp in specs], 16)
-    tcs = [F.TabCache() for _ in specs]
-    pool = cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4)
     qpl = [sp["qp"] for sp in specs]
 
-    def code(f):
-        if f == 0:
-            for tc in tcs:
-                tc.reset()
-            return list(pool.map(lambda u: sum(len(F.entropy_image(g.iframe_streams(u, p), specs[u]["w"] >> (p > 0),
-                                                                   specs[u]["h"] >> (p > 0), qpl[u]))
-                                               for p in range(3)), range(n)))
-        return list(pool.map(lambda u: len(F.entropy_pframe(g.pframe_streams(u), qpl[u], tcs[u])), range(n)))
+    def e2e_leg(learned: bool):
+        g = F.Engine(sizes, 16)
+        if learned:
+            g.set_learned(params, LEARN_CONF)
+        tcs = [F.TabCache() for _ in specs]
+        pool = cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4)
 
-    d2h = 0
-    t_start = None
-    for f in range(nf + 1):
-        if f == warm:
-            t_start = time.perf_counter()
-        if f < nf:
-            g.submit([frames[u][f] for u in range(n)], [1 if f == 0 else 0] * n, qpl)
-        if f > 0:
-            g.collect()
-            sizes = code(f - 1)
-            if f - 1 >= warm:
-                d2h += sum(sizes)
-    t_e2e = time.perf_counter() - t_start
-    g.close()
-    pool.shutdown()
-    e2e = len(lat) * lumapix / 1e6 / t_e2e
-    h2d = len(lat) * sum(sp["w"] * sp["h"] * 3 // 2 for sp in specs)
+        def code(f):
+            if f == 0:
+                for tc in tcs:
+                    tc.reset()
+                return list(pool.map(lambda u: sum(len(F.entropy_image(g.iframe_streams(u, p),
+                                                                       specs[u]["w"] >> (p > 0),
+                                                                       specs[u]["h"] >> (p > 0), qpl[u]))
+                                                   for p in range(3)), range(n)))
+            return list(pool.map(lambda u: len(F.entropy_pframe(g.pframe_streams(u), qpl[u], tcs[u])), range(n)))
+
+        d2h = 0
+        t_start = None
+        for f in range(nf + 1):
+            if f == warm:
+                t_start = time.perf_counter()
+            if f < nf:
+                g.submit([frames[u][f] for u in range(n)], [1 if f == 0 else 0] * n, qpl)
+            if f > 0:
+                g.collect()
+                sizes_f = code(f - 1)
+                if f - 1 >= warm:
+                    d2h += sum(sizes_f)
+        t = time.perf_counter() - t_start
+        g.close()
+        pool.shutdown()
+        return (nf - warm) * lumapix / 1e6 / t, d2h // max(1, nf - warm)
+
+    lat = device_leg(False)
+    lat_l = device_leg(True)
+    dev_s, dev_sl = sum(lat) / 1e3, sum(lat_l) / 1e3
+    value, value_l = len(lat) * lumapix / 1e6 / dev_s, len(lat_l) * lumapix / 1e6 / dev_sl
+    e2e, d2h = e2e_leg(False)
+    e2e_l, d2h_l = e2e_leg(True)
+    h2d = sum(sp["w"] * sp["h"] * 3 // 2 for sp in specs)
 
     # reference: the reference's fdv_video_encode, one stream per host thread;
     # P-frame rate from a key-frame-only pass and a key + 4 P pass
@@ -439,7 +463,7 @@ def run_batch(args) -> None:
         def ref_pass(k):
             def one(u):
                 sp = specs[u]
-                O.ref_video_encode(frames[u][:k], sp["w"], sp["h"], sp["qp"], 60, 16)
+                O.ref_video_encode(frames[u][:k], sp["w"], sp["h"], sp["qp"], 0, 16)
             t0 = time.perf_counter()
             with cf.ThreadPoolExecutor(max_workers=ncpu) as ex:
                 list(ex.map(one, range(n)))
@@ -450,23 +474,29 @@ def run_batch(args) -> None:
                "kind": "reference",
                "sample": f"P-frames 1-{kp - 1} of all 48 streams (the key-frame-only pass subtracted), the "
                          f"reference's fdv_video_encode, one stream per thread on {ncpu} threads"}
-    lat_sorted = sorted(lat)
     print(json.dumps({
         "metric": "batched multi-stream encode Mpix/s on 1 B200 (48 streams, plain, bit-exact)",
         "value": round(value, 3), "unit": "Mpix/s", "n_gpus": 1, "steps": len(lat), "warmup": warm,
         "ms_per_step": round(1e3 * dev_s / len(lat), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "batch48: 48 streams, 12 each of 320x240, 640x368, 1280x720, 1920x1088, QP U{18..36} "
-                               "per stream, key interval 60, range 16, seeded moving rectangles; one step = one "
-                               "P-frame of every stream (one launch)",
+        "config": {"workload": f"batch48: 48 streams, 12 each of 320x240, 640x368, 1280x720, 1920x1088, QP U{{18..36}} "
+                               f"per stream, range 16, seeded moving rectangles, {nf} frames per stream: one key "
+                               "frame (step 0), then P-frames (the configuration gives no key interval); one step = "
+                               "one frame of every stream (one launch)",
                    "luma_pixels_per_step": lumapix,
                    "l2": "a 256 MB buffer is written between timed steps (inputs per step are 58 MB)"},
-        "latency_ms": {"p50": round(lat_sorted[len(lat) // 2], 3),
-                       "p99": round(lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
+        "latency_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99)},
         "cpu_baseline": cpu,
-        "e2e": {"value": round(e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": h2d // max(1, len(lat)),
-                "d2h_bytes_per_step": d2h // max(1, len(lat)),
+        "e2e": {"value": round(e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "note": "fdvg_submit / fdvg_collect with host entropy of step f-1 during the GPU's step f"},
+        "learned": {"metric": "batched multi-stream encode Mpix/s on 1 B200 (48 streams, learned-proposal form)",
+                    "value": round(value_l, 3), "unit": "Mpix/s", "ms_per_step": round(1e3 * dev_sl / len(lat_l), 3),
+                    "speedup": round(value_l / value, 4),
+                    "latency_ms": {"p50": pct(lat_l, 0.5), "p99": pct(lat_l, 0.99)},
+                    "e2e": {"value": round(e2e_l, 3), "unit": "Mpix/s", "h2d_bytes_per_step": h2d,
+                            "d2h_bytes_per_step": d2h_l},
+                    "setting": f"confidence {LEARN_CONF}, weights fdv_b200/proposal_c4.f32, one inference launch "
+                               "over all 48 streams' macroblocks per step"},
     }))
 
 
@@ -590,44 +620,18 @@ def run_learned(local: int) -> dict:
     import torch
     import fdv_b200 as F
     import fdv_b200.learned as LN
-    L = F.lib()
     p = LN.load_params(LN.DEFAULT_WEIGHTS)
     sc = F.Scene(W, H, LEARN_NF, seed=1, **LN.CONTENT)
-    frames = np.stack([sc.frame(f) for f in range(LEARN_NF)])
-    dev = torch.from_numpy(frames).to(f"cuda:{local}")
-    torch.cuda.synchronize()
-    cw = W // 2
-    # every frame's planes (device pointers); runs of P-frames go as batched
-    # launches (fdvg_frames_device), as in the plain workload
-    planes = (F.u8p * (3 * LEARN_NF))()
-    for f in range(LEARN_NF):
-        fb = dev.data_ptr() + f * FSIZE
-        planes[3 * f], planes[3 * f + 1], planes[3 * f + 2] = (C.cast(fb, F.u8p), C.cast(fb + W * H, F.u8p),
-                                                               C.cast(fb + W * H + (H // 2) * cw, F.u8p))
-    qp = (C.c_int * LEARN_NF)(*([LEARN_QP] * LEARN_NF))
-    intra = (C.c_int * LEARN_NF)(*[1 if f == 0 else 0 for f in range(LEARN_NF)])
+    frames = [sc.frame(f) for f in range(LEARN_NF)]
 
     def run(params, conf4=None):
-        g = F.Engine([(W, H)], LN.RANGE, local)
-        if params is not None:
-            g.set_learned(params, LEARN_CONF)
-            if conf4 is not None:
-                g.set_learned_conf(conf4[:3], conf4[3], bool(conf4[4]) if len(conf4) > 4 else False)
-
-        def step():
-            if L.fdvg_frames_device(g._g, LEARN_NF, planes, intra, qp) != 0:
-                raise RuntimeError(F.last_error())
-        step()
-        g.stats_reset()
-        step()
-        st = g.stats()
-        g.close()
-        return st
+        conf = LEARN_CONF if conf4 is None else conf4
+        return LN.device_stats(frames, W, H, LEARN_QP, params, conf, LN.RANGE, local)
 
     plain = run(None)
     learned = run(p)
     seeded = run(p, (2.0, 2.0, 2.0, 0.0))   # inference and seeded searches, no narrowing
-    ev = LN.evaluate(p, LEARN_CONF, nframes=20, seeds=(1,), batch=30)
+    ev = LN.evaluate(p, LEARN_CONF, nframes=30, seeds=(1, 2), batch=30)
     mpix = LEARN_NF * W * H / 1e6
     pf = lambda st: st["p_ms"] / max(1, st["p_launches"])
     return {
@@ -645,7 +649,8 @@ def run_learned(local: int) -> dict:
                     "intra_conf": LEARN_CONF, "intra_path": "intra analysis only",
                     "other_mbs": "full search seeded with the proposals"},
         "workload": f"learned: 1280x720, {LEARN_NF} frames (1 key), QP {LEARN_QP}, range 16, 6 moving rectangles "
-                    f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, 20 frames; "
+                    f"on band-limited noise, seed 1 (held out from training); BD-rate over QP 18/23/28/32, seeds 1 and 2 "
+                    "(held out) x 30 frames; "
                     "P-frames in launches of up to 30 (the inference reads the previous frame's source: for "
                     "every frame with device-resident sources, after a batch's first frame with host sources; "
                     "the SKIP pre-analysis runs for a batch's first frame); the BD-rate codes from host sources "
@@ -712,7 +717,8 @@ def main() -> None:
     global NF
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 3; batch48: 237, so 240 frames with the warm-up)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -727,6 +733,8 @@ def main() -> None:
     ap.add_argument("--render-cache", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--seed", type=int, default=1, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 237 if args.workload == "batch48" else 3
     if args.render_cache:
         write_cache(args.render_cache, args.seed, args.frames)
         return

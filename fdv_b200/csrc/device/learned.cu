@@ -691,29 +691,36 @@ fdvl_net *lrn_create(int device, int max_batch, int bank_frames, int w, int h) {
     bool ok = cudaStreamCreateWithFlags(&n->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem) == cudaSuccess;
     if (ok) {
+        // An encoder engine's network (no training bank) only runs the fused
+        // inference: sample descriptors, weights and the error word.  The
+        // per-macroblock layer activations of the layered forward and of
+        // training (tens of kilobytes per macroblock) exist only with a bank.
         n->w = dalloc<float>(kNParams, o);
         n->wimg = dalloc<uint8_t>(kWImage, o);
-        n->outf = dalloc<float>(B * kOutPad, o);
-        n->hints = dalloc<Hint>(B, o);
-        ok = ok && n->wimg && n->outf && n->hints &&
+        ok = ok && n->wimg &&
              cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem) ==
                  cudaSuccess &&
              cudaDeviceGetAttribute(&n->nsm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
         n->S = dalloc<Sample>(B, o);
-        n->X0 = dalloc<bf16>(B * 1024 * kChan, o);
-        n->O = dalloc<float>(B * kOutPad, o);
         n->err = dalloc<unsigned>(1, o);
-        ok = ok && n->w && n->S && n->X0 && n->O && n->err;
+        ok = ok && n->w && n->S && n->err;
         for (int l = 0; l < 4; ++l) {
             const LayerGeo &G = kGeo[l];
             n->Wb[l] = dalloc<bf16>((size_t)G.gn * G.kp, o);
             ok = ok && n->Wb[l];
         }
-        for (int l = 0; l < 3; ++l) {
-            const size_t rows = B * pos_per_mb(l);
-            n->col[l] = dalloc<bf16>(rows * kGeo[l].kp, o);
-            n->Y[l] = dalloc<bf16>(rows * kGeo[l].gn, o);
-            ok = ok && n->col[l] && n->Y[l];
+        if (train) {
+            n->outf = dalloc<float>(B * kOutPad, o);
+            n->hints = dalloc<Hint>(B, o);
+            n->X0 = dalloc<bf16>(B * 1024 * kChan, o);
+            n->O = dalloc<float>(B * kOutPad, o);
+            ok = ok && n->outf && n->hints && n->X0 && n->O;
+            for (int l = 0; l < 3; ++l) {
+                const size_t rows = B * pos_per_mb(l);
+                n->col[l] = dalloc<bf16>(rows * kGeo[l].kp, o);
+                n->Y[l] = dalloc<bf16>(rows * kGeo[l].gn, o);
+                ok = ok && n->col[l] && n->Y[l];
+            }
         }
         if (train) {
             n->bank = dalloc<uint8_t>((size_t)w * h * bank_frames, o);

@@ -410,48 +410,72 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     auto key_at = [&](int f) { return f == 0 || (keyint > 0 && f % keyint == 0) ? 1 : 0; };
     std::deque<int> types;    // frame types in flight, oldest first
     int rc = 0;
-    size_t prev = 0;          // frames of the previous batch (in flight, not yet coded)
-    for (int f = 0; rc == 0;) {
-        int K = 0;
-        if (f < nframes) {
-            K = 1;
-            if (!key_at(f))
-                while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
-            // the sequence's last batch is coded after the GPU has finished:
-            // keep it short
-            constexpr int kTail = 6;
-            if (f + K == nframes && K > 2 * kTail) K -= kTail;
-            for (int k = 0; k < K; ++k) {
-                const uint8_t *fy = frames[f + k], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+    size_t prev = 0;          // frames of the previous submissions (in flight, not yet coded)
+    int ahead = -1;           // the key frame the lookahead was armed with
+    // frames in one submission from f: a key frame alone, else a run of
+    // P-frames; the sequence's last run is coded after the GPU has finished,
+    // so it is kept short
+    auto run_len = [&](int f) {
+        int K = 1;
+        if (!key_at(f))
+            while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
+        constexpr int kTail = 6;
+        if (f + K == nframes && K > 2 * kTail) K -= kTail;
+        return K;
+    };
+    auto submit_at = [&](int f, int K) -> int {
+        for (int k = 0; k < K; ++k) {
+            const uint8_t *fy = frames[f + k], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
+            for (int b = 0; b < nb; ++b) {
+                const int j = k * nb + b;
+                planes[3 * j] = fy + (size_t)Y0[b] * w;
+                planes[3 * j + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+                planes[3 * j + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+                intra[j] = key_at(f + k);
+            }
+        }
+        if (key_at(f)) {
+            // the sequence's next key frame is analysed in this key frame's
+            // launch (fdvb_engine_key_lookahead)
+            int f2 = f + 1;
+            while (f2 < nframes && !key_at(f2)) ++f2;
+            if (f2 < nframes) {
+                const uint8_t *fy = frames[f2], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
                 for (int b = 0; b < nb; ++b) {
-                    const int j = k * nb + b;
-                    planes[3 * j] = fy + (size_t)Y0[b] * w;
-                    planes[3 * j + 1] = fu + (size_t)(Y0[b] / 2) * cw;
-                    planes[3 * j + 2] = fv + (size_t)(Y0[b] / 2) * cw;
-                    intra[j] = key_at(f + k);
+                    kplanes[3 * b] = fy + (size_t)Y0[b] * w;
+                    kplanes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
+                    kplanes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
+                }
+                if (fdvb_engine_key_lookahead(E, kplanes.data(), qps.data()) != 0) { set_engine_err(); return -1; }
+                ahead = f2;
+            }
+        }
+        if (fdvb_engine_submit_batch(E, K, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) {
+            set_engine_err();
+            return -1;
+        }
+        for (int k = 0; k < K; ++k) types.push_back(key_at(f + k));
+        return 0;
+    };
+    for (int f = 0; rc == 0;) {
+        size_t now = 0;
+        if (f < nframes) {
+            const bool analysed = f == ahead;   // a key frame whose analysis ran in an earlier launch
+            const int K = run_len(f);
+            if (submit_at(f, K) != 0) { rc = -1; break; }
+            now += (size_t)K;
+            f += K;
+            // such a key frame keeps the GPU busy for a moment only: the run
+            // after it goes in now too, so the GPU has work while the host
+            // codes the previous run (within the frames the engine holds)
+            if (analysed && f < nframes && !key_at(f)) {
+                const int K2 = std::min(run_len(f), 2 * kmax - (int)(prev + now));
+                if (K2 >= 1) {
+                    if (submit_at(f, K2) != 0) { rc = -1; break; }
+                    now += (size_t)K2;
+                    f += K2;
                 }
             }
-            if (key_at(f)) {
-                // the sequence's next key frame is analysed in this key
-                // frame's launch (fdvb_engine_key_lookahead)
-                int f2 = f + 1;
-                while (f2 < nframes && !key_at(f2)) ++f2;
-                if (f2 < nframes) {
-                    const uint8_t *fy = frames[f2], *fu = fy + (size_t)w * h, *fv = fu + (size_t)cw * ch;
-                    for (int b = 0; b < nb; ++b) {
-                        kplanes[3 * b] = fy + (size_t)Y0[b] * w;
-                        kplanes[3 * b + 1] = fu + (size_t)(Y0[b] / 2) * cw;
-                        kplanes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
-                    }
-                    if (fdvb_engine_key_lookahead(E, kplanes.data(), qps.data()) != 0) { set_engine_err(); rc = -1; break; }
-                }
-            }
-            if (fdvb_engine_submit_batch(E, K, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) {
-                set_engine_err();
-                rc = -1;
-                break;
-            }
-            for (int k = 0; k < K; ++k) types.push_back(key_at(f + k));
         }
         // code the previous batch while the GPU runs this one: collect its
         // frames (their streams stay in their slots until the next
@@ -486,9 +510,8 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             for (int r : urc)
                 if (r) { set_err(r == -2 ? "a band's stream outgrew the tiled encoder's capacity" : "entropy coding failed"); rc = -1; }
         }
-        if (K == 0) break;
-        prev = (size_t)K;
-        f += K;
+        if (now == 0) break;
+        prev = now;
     }
     while (!types.empty()) {
         types.pop_front();

@@ -346,6 +346,46 @@ def _encode_engine_batched(frames, w, h, qp, keyint, params, conf, search_range,
     return stream, list(video_decode(stream)), st
 
 
+def device_stats(frames, w: int, h: int, qp: int, params=None, conf=0.8, search_range: int = RANGE,
+                 device: int = 0) -> dict:
+    """Device-timed engine statistics (fdvg_stats) of one stream coded from
+    device-resident sources through fdvg_frames_device, as the product path
+    runs it: one key frame, then P-frames in launches of up to thirty, the
+    learned form's inference on its own stream ahead of each launch.  A
+    warm-up pass runs first; the figures are the second pass's."""
+    import ctypes as C
+    import torch
+    from . import Engine, last_error, lib as flib, u8p
+    L = flib()
+    nf = len(frames)
+    dev = torch.from_numpy(np.stack(frames)).to(f"cuda:{device}")
+    torch.cuda.synchronize(device)
+    fs, cw = w * h * 3 // 2, w // 2
+    planes = (u8p * (3 * nf))()
+    for f in range(nf):
+        fb = dev.data_ptr() + f * fs
+        planes[3 * f], planes[3 * f + 1], planes[3 * f + 2] = (C.cast(fb, u8p), C.cast(fb + w * h, u8p),
+                                                               C.cast(fb + w * h + (h // 2) * cw, u8p))
+    qps = (C.c_int * nf)(*([qp] * nf))
+    intra = (C.c_int * nf)(*[1 if f == 0 else 0 for f in range(nf)])
+    g = Engine([(w, h)], search_range, device)
+    try:
+        if params is not None:
+            if np.ndim(conf):
+                g.set_learned(params, 0.8)
+                g.set_learned_conf(conf[:3], conf[3], bool(conf[4]) if len(conf) > 4 else False)
+            else:
+                g.set_learned(params, conf)
+        for k in range(2):
+            if k:
+                g.stats_reset()
+            if L.fdvg_frames_device(g._g, nf, planes, intra, qps) != 0:
+                raise RuntimeError(last_error())
+        return g.stats()
+    finally:
+        g.close()
+
+
 def psnr_y(src, rec, w: int, h: int) -> float:
     """Mean over frames of the luma PSNR (dB)."""
     vals = []
