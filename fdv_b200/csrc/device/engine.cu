@@ -110,7 +110,7 @@ struct CompactTaskH {
     uint8_t *tmp;
 };
 
-constexpr int kMaxBatch = 30;               // P-frames per launch at most (hd720 Mpix/s: 6 -> 505, 12 -> 667, 24 -> 696, 30 -> 711)
+constexpr int kMaxBatch = 60;               // P-frames per launch at most (a 60-frame GOP's P-frames in one launch)
 constexpr int kRefSlots = kMaxBatch + 2;    // reference ring: a batch's outputs never alias its inputs
 constexpr int kSlots = 2 * kMaxBatch;       // frames in flight: two batches
 
@@ -132,6 +132,7 @@ struct Unit {
     int *progress[kMaxBatch] = {};
     uint8_t *slots[kMaxBatch] = {};
     uint8_t *cout[kMaxBatch] = {};  // per lane: the compaction's device scratch (out_cap bytes)
+    int nprog = 0;                  // a lane's progress words (P rows, tile counts, I rows)
     RefSlot ref[kRefSlots];
     long long seq = 0;            // references made so far (the next one goes to slot seq % kRefSlots)
     int nref = 0;
@@ -200,10 +201,13 @@ struct fdvb_engine {
     size_t src_stage_bytes = 0;    // a slot's staging of one frame's sources (64-byte multiple)
     size_t src_bytes = 0;          // one frame's sources, all units
     uint8_t *lane_src[kMaxBatch] = {};   // per lane: every unit's source planes, one upload per frame
+    int lanes = 0;                       // lanes allocated so far (at first use)
+    size_t stage_cap = 0;                // a slot's pinned staging (allocated at first use)
     // timing (CUDA events on the engine's stream) and launch counts
     double step_ms = 0, pk_ms = 0, ik_ms = 0;
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
     int src_on_device = 0;
+    int direct_upload = 0;       // host sources that stay valid until collected: pinned ones are copied without staging
     int stall_unit = -1, stall_row = -1;
     int defer_refs = 0;                     // leave the reference pool alone until commit
     std::vector<int> pending_intra;         // frame types of the uncommitted step
@@ -258,11 +262,6 @@ extern "C" const char *fdvb_engine_error(void) { return g_err.c_str(); }
 
 static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     u.w = w; u.h = h; u.mbw = w / 16; u.mbh = h / 16; u.cw = w / 2; u.ch = h / 2;
-    const size_t fs = (size_t)w * h * 3 / 2;
-    for (int k = 0; k < kMaxBatch; ++k) {
-        CK(cudaMalloc(&u.rec[k], fs));
-        CK(cudaMemset(u.rec[k], 0, fs));
-    }
     const int B = E->border;
     const int ys = round_up(w + 2 * B, 64), cs = round_up(u.cw + 2 * B, 64);
     const size_t lsz = (size_t)ys * (h + 2 * B), csz = (size_t)cs * (u.ch + 2 * B);
@@ -290,11 +289,7 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
         CK(cudaMalloc(&u.islots[p], (size_t)iframe_slot_bytes() * u.icols[p] * u.irows[p]));
         CK(cudaMalloc(&u.mmap[p], (size_t)(u.pw[p] / 4) * (u.ph[p] / 4)));
     }
-    for (int k = 0; k < kMaxBatch; ++k) {
-        CK(cudaMalloc(&u.mbi[k], sizeof(MBInfo) * nmb));
-        CK(cudaMalloc(&u.slots[k], (size_t)kSlotBytes * nmb));
-        CK(cudaMalloc(&u.progress[k], sizeof(int) * nprog));
-    }
+    u.nprog = nprog;
     // host-mapped output: P-frame streams, or the three planes of a key frame
     size_t pcap = 64 + (size_t)nmb * kSlotData;
     size_t icap[3];
@@ -302,7 +297,33 @@ static int alloc_unit(fdvb_engine *E, Unit &u, int w, int h) {
     for (int p = 0; p < 3; ++p) icap[p] = (icap[p] + 15) / 16 * 16;   // planes' outputs 16-byte aligned
     u.out_off_i[0] = 0; u.out_off_i[1] = icap[0]; u.out_off_i[2] = icap[0] + icap[1];
     u.out_cap = std::max(pcap, icap[0] + icap[1] + icap[2]);
-    for (int k = 0; k < kMaxBatch; ++k) CK(cudaMalloc(&u.cout[k], u.out_cap));
+    return 0;
+}
+
+// Lanes 0..n-1 of every unit (per frame of a batch: reconstruction, records,
+// symbol slots, progress words, compaction scratch, source planes), allocated
+// at first use: a batch of K frames needs K lanes, and engines that only ever
+// step one frame at a time (many streams in one engine) hold one.
+static int ensure_lanes(fdvb_engine *E, int n) {
+    for (int k = E->lanes; k < n; ++k) {
+        for (auto &u : E->units) {
+            const size_t fs = (size_t)u.w * u.h * 3 / 2;
+            const int nmb = u.mbw * u.mbh;
+            CK(cudaMalloc(&u.rec[k], fs));
+            CK(cudaMemset(u.rec[k], 0, fs));
+            CK(cudaMalloc(&u.mbi[k], sizeof(MBInfo) * nmb));
+            CK(cudaMalloc(&u.slots[k], (size_t)kSlotBytes * nmb));
+            CK(cudaMalloc(&u.progress[k], sizeof(int) * u.nprog));
+            CK(cudaMalloc(&u.cout[k], u.out_cap));
+        }
+        CK(cudaMalloc(&E->lane_src[k], E->src_bytes));
+        size_t off = 0;
+        for (auto &u : E->units) {
+            u.cur[k] = E->lane_src[k] + off;
+            off += (size_t)u.w * u.h * 3 / 2;
+        }
+        E->lanes = k + 1;
+    }
     return 0;
 }
 
@@ -393,22 +414,11 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
     E->src_bytes = src_bytes;
     E->src_stage_bytes = (src_bytes + 63) / 64 * 64;
-    for (int k = 0; k < kMaxBatch; ++k) {
-        if (cudaMalloc(&E->lane_src[k], src_bytes) != cudaSuccess) {
-            g_err = "device allocation failed";
-            fdvb_engine_destroy(E);
-            return nullptr;
-        }
-        size_t off = 0;
-        for (auto &u : E->units) {
-            u.cur[k] = E->lane_src[k] + off;
-            off += (size_t)u.w * u.h * 3 / 2;
-        }
-    }
+    if (ensure_lanes(E, 1) != 0) { fdvb_engine_destroy(E); return nullptr; }
+    E->stage_cap = E->src_stage_bytes + stage_desc_bytes(nunits, maxrows, maxitasks);
     for (auto &sl : E->slot) {
-        sl.stage_cap = E->src_stage_bytes + stage_desc_bytes(nunits, maxrows, maxitasks);
-        if (cudaHostAlloc(&sl.stage, sl.stage_cap, cudaHostAllocDefault) != cudaSuccess ||
-            cudaHostAlloc(&sl.err_h, 64, cudaHostAllocDefault) != cudaSuccess) {
+        sl.stage_cap = E->stage_cap;
+        if (cudaHostAlloc(&sl.err_h, 64, cudaHostAllocDefault) != cudaSuccess) {
             g_err = "pinned allocation failed";
             fdvb_engine_destroy(E);
             return nullptr;
@@ -576,12 +586,14 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     const bool joint = all_key && !prefetched && E->ka_armed && !E->defer_refs &&
                        !std::equal(E->ka_planes.begin(), E->ka_planes.end(), planes);
     CK(cudaSetDevice(E->device));
+    if (ensure_lanes(E, K) != 0) return -3;
     int sis[kMaxBatch];
     for (int k = 0, s = 0; k < K; ++k) {
         while (E->busy[s]) ++s;
         sis[k] = s++;
         for (auto &u : E->units)
             if (unit_out(u, sis[k]) != 0) return -3;
+        if (!E->slot[sis[k]].stage) CK(cudaHostAlloc(&E->slot[sis[k]].stage, E->stage_cap, cudaHostAllocDefault));
     }
     Slot &SL = E->slot[sis[0]];
     CK(cudaEventRecord(SL.ev[0], E->st));
@@ -590,8 +602,41 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     // uploaded in chunks of at least 4 MB as units are staged, so the copies
     // overlap the staging while staying few (a held unit's part is left as
     // it is)
+    // Pinned host sources whose caller keeps them unchanged until the frame
+    // is collected (direct_upload), when a frame's planes tile one contiguous
+    // span (the bands of one frame do), are copied in one piece straight from
+    // the caller's memory, with no staging copy on the host; the units then
+    // read their planes at their offsets in the span.
+    auto pinned = [](const void *p) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+        return a.type == cudaMemoryTypeHost;
+    };
+    std::vector<const uint8_t *> span_lo(K, nullptr);   // frame k copied as one span from here (else null)
+    if (!E->src_on_device && E->direct_upload && !force_skip)
+        for (int k = 0; k < K; ++k) {
+            const uint8_t *lo = nullptr, *hi = nullptr;
+            size_t sum = 0;
+            for (int i = 0; i < nu; ++i) {
+                const Unit &u = E->units[i];
+                const size_t sz[3] = {(size_t)u.w * u.h, (size_t)u.cw * u.ch, (size_t)u.cw * u.ch};
+                for (int p = 0; p < 3; ++p) {
+                    const uint8_t *q = planes[3 * (k * nu + i) + p];
+                    if (!lo || q < lo) lo = q;
+                    if (!hi || q + sz[p] > hi) hi = q + sz[p];
+                    sum += sz[p];
+                }
+            }
+            if ((size_t)(hi - lo) != sum || sum > E->src_bytes || !pinned(lo) || !pinned(hi - 1)) continue;
+            if (cudaMemcpyAsync(E->lane_src[k], lo, sum, cudaMemcpyHostToDevice, E->st) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            span_lo[k] = lo;
+        }
     if (!E->src_on_device)
         for (int k = 0; k < K; ++k) {
+            if (span_lo[k]) continue;
             uint8_t *const stage0 = E->slot[sis[k]].stage;
             uint8_t *stage = stage0;
             size_t sent = 0;
@@ -685,6 +730,8 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             d.w = u.w; d.h = u.h; d.mbw = u.mbw; d.mbh = u.mbh;
             if (E->src_on_device && !(force_skip && force_skip[j])) {
                 d.cur[0] = planes[3 * j]; d.cur[1] = planes[3 * j + 1]; d.cur[2] = planes[3 * j + 2];
+            } else if (span_lo[k]) {
+                for (int p = 0; p < 3; ++p) d.cur[p] = E->lane_src[k] + (planes[3 * j + p] - span_lo[k]);
             } else {
                 d.cur[0] = u.cur[k]; d.cur[1] = u.cur[k] + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
             }
@@ -1079,6 +1126,9 @@ extern "C" int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *nea
 
 // Sources of the next steps are device pointers (already resident in HBM).
 extern "C" void fdvb_engine_src_on_device(fdvb_engine *E, int on) { if (E) E->src_on_device = on; }
+// Host sources of the next steps stay valid and unchanged until their frames
+// are collected: pinned ones are then copied without host staging.
+extern "C" void fdvb_engine_direct_upload(fdvb_engine *E, int on) { if (E) E->direct_upload = on; }
 
 // Accumulated device time (CUDA events on the engine stream) of the steps, of
 // the P-frame analysis kernel and of the key-frame kernel, with their counts,

@@ -651,22 +651,12 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                 if (U.prof && gt == 0) atomicAdd(&U.prof[PP_G0 + grp], (unsigned long long)(clock64() - tg0));
                 __syncthreads();
                 pc.mark(PP_SEARCH);
-                // ---- phase 2: the INTER8 residual, on every warp
+                // ---- phase 3, first part: the reference's decision on the
+                // INTER16 and INTRA16 results, which decides whether INTER8
+                // is evaluated at all
                 const int isel = S.isel, ssad = S.ssad;
-                const bool have1 = navail > 1 && !lfast, haveI = isel >= 0;
-                // needed unless the SAD gate rejects the split whichever INTER16
-                // reference ends up chosen
+                const bool haveI = isel >= 0;
                 auto gate_skip = [&](int s16) { return s16 > 0 && ssad * 10 >= s16 * 9; };
-                const bool need8 = l8 && !(gate_skip(S.sad[0]) && (!have1 || gate_skip(S.sad[1])));
-                if (need8) {
-                    if (warp < 12) resid_task(S, 12 + warp / 3, warp % 3, qp, lambda, warp, lane);
-                    __syncthreads();
-                    pc.mark(PP_RESID);
-                    if (grp == 2) group_decide(S, 3, lambda, gw, gt, lane, 11, err);
-                    __syncthreads();
-                }
-                pc.mark(PP_DECIDE);
-                // ---- phase 3: the reference's decision on these results
                 double Jbest = Js, Ji = 1e30, Jintra = 1e30, J8 = 1e30;
                 int sad16 = 0;
                 const int nsearch = l_intra ? 0 : (lfast ? 1 : navail);
@@ -683,7 +673,20 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     best_sub = isel;
                     if (Jintra < Jbest) Jbest = Jintra;
                 }
-                if (l8 && Jbest > lam19 && !gate_skip(sad16)) {
+                // ---- phase 2: the INTER8 residual, on every warp, only where
+                // the reference evaluates INTER8 (the same condition as below;
+                // every thread holds the same values)
+                const bool need8 = l8 && Jbest > lam19 && !gate_skip(sad16);
+                if (need8) {
+                    if (warp < 12) resid_task(S, 12 + warp / 3, warp % 3, qp, lambda, warp, lane);
+                    __syncthreads();
+                    pc.mark(PP_RESID);
+                    if (grp == 2) group_decide(S, 3, lambda, gw, gt, lane, 11, err);
+                    __syncthreads();
+                }
+                pc.mark(PP_DECIDE);
+                // ---- phase 3, second part: INTER8 and the final choice
+                if (need8) {
                     int b8 = kBitsMode, px = pmvx, py = pmvy;
                     for (int q = 0; q < 4; ++q) {
                         b8 += bits_val(zz_enc(S.qmv[q][0] - px)) + bits_val(zz_enc(S.qmv[q][1] - py));

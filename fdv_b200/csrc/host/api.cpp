@@ -252,7 +252,7 @@ std::vector<int> tune_key(int n, const int *w, const int *h, int range) {
     return k;
 }
 // The engine's launch shape: the tuned one for its geometry, else the default
-// (thirty P-frames per launch, one block per SM).
+// (up to sixty P-frames per launch, one block per SM).
 void apply_tuning(fdvb_engine *E, int n, const int *w, const int *h, int range) {
     std::pair<int, int> t{0, 0};
     {
@@ -261,7 +261,7 @@ void apply_tuning(fdvb_engine *E, int n, const int *w, const int *h, int range) 
         if (it != g_tune->end()) t = it->second;
     }
     if (t.first > 0) fdvb_engine_set_tuning(E, t.first, t.second);
-    else fdvb_engine_set_tuning(E, 30, 0);
+    else fdvb_engine_set_tuning(E, 60, 0);
 }
 
 fdvb_engine *engine_acquire(int n, const int *w, const int *h, int range, int device) {
@@ -413,14 +413,19 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     size_t prev = 0;          // frames of the previous submissions (in flight, not yet coded)
     int ahead = -1;           // the key frame the lookahead was armed with
     // frames in one submission from f: a key frame alone, else a run of
-    // P-frames; the sequence's last run is coded after the GPU has finished,
-    // so it is kept short
+    // P-frames.  The host codes a run while the GPU analyses the next one, so
+    // the sequence's last run is coded after the GPU has finished: the final
+    // stretch goes in halving runs (each coded while the GPU runs the next,
+    // smaller one), down to a short last run.
     auto run_len = [&](int f) {
         int K = 1;
         if (!key_at(f))
             while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
         constexpr int kTail = 6;
-        if (f + K == nframes && K > 2 * kTail) K -= kTail;
+        if (f + K == nframes) {
+            const int rem = nframes - f;
+            K = std::max(std::min(rem, kTail), (rem + 1) / 2);
+        }
         return K;
     };
     auto submit_at = [&](int f, int K) -> int {
@@ -457,6 +462,9 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         for (int k = 0; k < K; ++k) types.push_back(key_at(f + k));
         return 0;
     };
+    // the caller's frames stay valid for the whole call: pinned ones are
+    // copied to the GPU without staging
+    fdvb_engine_direct_upload(E, 1);
     for (int f = 0; rc == 0;) {
         size_t now = 0;
         if (f < nframes) {
@@ -518,6 +526,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         fdvb_engine_collect(E);
     }
     fdvb_engine_key_lookahead(E, nullptr, nullptr);   // the next call's frames are other buffers
+    fdvb_engine_direct_upload(E, 0);
     if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
     else fdvb_engine_destroy(E);
     return rc;
@@ -827,7 +836,7 @@ void fdvg_get_tuning(const fdvg_ctx *g, int *max_batch, int *p_grid, int *nsm) {
     fdvb_engine_get_tuning(g, max_batch, p_grid, nsm);
 }
 int fdvb_set_tuning(int nunits, const int *w, const int *h, int range, int max_batch, int p_grid) {
-    if (nunits <= 0 || !w || !h || max_batch < 0 || max_batch > 30 || p_grid < 0) { set_err("bad tuning"); return -1; }
+    if (nunits <= 0 || !w || !h || max_batch < 0 || max_batch > 60 || p_grid < 0) { set_err("bad tuning"); return -1; }
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (max_batch == 0) g_tune->erase(tune_key(nunits, w, h, range));
     else (*g_tune)[tune_key(nunits, w, h, range)] = {max_batch, p_grid};

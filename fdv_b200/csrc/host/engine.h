@@ -29,6 +29,7 @@ int fdvb_engine_recon(fdvb_engine *E, int unit, uint8_t *i420);
 int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *near_i420, const uint8_t *far_i420);
 const char *fdvb_engine_error(void);
 void fdvb_engine_src_on_device(fdvb_engine *E, int on);
+void fdvb_engine_direct_upload(fdvb_engine *E, int on);
 void fdvb_engine_stats(const fdvb_engine *E, double *step_ms, double *pk_ms, long long *pk_n, double *ik_ms,
                        long long *ik_n, long long *launches, long long *steps, long long *d2h_bytes);
 void fdvb_engine_stats_reset(fdvb_engine *E);

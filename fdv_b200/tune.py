@@ -4,7 +4,7 @@ The P-frame analysis runs as one persistent wavefront kernel per batch of
 consecutive P-frames.  Two choices set how well that kernel fills the SMs,
 and both depend on the unit geometry and the search range:
 
-* P-frames per launch (1..30).  The frames of a batch overlap: frame k + 1's
+* P-frames per launch (1..60).  The frames of a batch overlap: frame k + 1's
   macroblock rows start as soon as frame k has written the reference tiles
   they read.  More frames keep more rows in flight and spread the launch's
   ramp-up and drain over more frames; fewer frames start the host's entropy
@@ -33,7 +33,7 @@ import numpy as np
 
 from . import Engine, Scene, lib, set_search_range, get_search_range, set_tuning, u8p
 
-BATCHES = (6, 12, 20, 30)
+BATCHES = (6, 12, 20, 30, 60)
 GRID_CUTS = (0, 8, 20, 40)          # SMs left free by the wavefront kernel
 
 
@@ -106,7 +106,8 @@ def measure(eng: Engine, planes, intra, qps, nframes: int, reps: int = 2) -> flo
 
 def autotune(sizes, search_range: int, device: int = 0, nframes: int = 61, qp: int = 24, use_cache: bool = True,
              record: bool = True, seed: int = 7) -> dict:
-    """Choose the launch shape for units of `sizes` at `search_range`.
+    """Choose the launch shape for units of `sizes` at `search_range`
+    (the default shape: the largest batch size at one block per SM).
 
     Sweeps the P-frames per launch at one block per SM, then the block count
     at the best batch size; returns {"max_batch", "p_grid", "p_ms_per_frame",

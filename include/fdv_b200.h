@@ -172,7 +172,7 @@ int fdvg_frame(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, c
 int fdvg_submit(fdvg_ctx *g, const uint8_t *const *planes, const int *is_intra, const int *qp,
                 const double *lscale, const int *force_skip);
 int fdvg_collect(fdvg_ctx *g);
-/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (thirty by
+/* Up to fdvg_max_batch(g) consecutive P-frames in one submission (sixty by
  * default, fdvg_set_tuning; one while decision records or deferred references
  * are on):
  * the arrays hold frame k's entries at k * nunits (planes: 3 per unit).  The
@@ -185,7 +185,7 @@ int fdvg_submit_batch(fdvg_ctx *g, int nframes, const uint8_t *const *planes, co
                       const double *lscale, const int *force_skip);
 int fdvg_max_batch(const fdvg_ctx *g);
 /* The engine's launch shape, the autotuner's knobs (no counterpart in the
- * reference): max_batch P-frames per launch at most (1..30) and p_grid blocks
+ * reference): max_batch P-frames per launch at most (1..60) and p_grid blocks
  * of the P-frame wavefront kernel, i.e. macroblock rows in flight (0: one per
  * SM; capped at the SM count).  fdvg_get_tuning reports the shape in force and
  * the SM count.  fdvb_set_tuning records a shape for every engine the fdv_*

@@ -95,21 +95,21 @@ def test_learned_batch_stream(built):
     assert abs(LN.psnr_y(frames, rb, w, h) - LN.psnr_y(frames, r1, w, h)) < 0.3
 
 
-def test_long_batched_sequence_matches_oracle(built):
-    """A long sequence in launches of the largest batch: 76 frames with key
-    frames at 0 and 38, so each GOP holds a full thirty-frame launch and a
-    shorter one, and the reference ring (thirty-two slots) wraps within the
-    first GOP.  Two units of different sizes; every frame's streams (key
-    frames: all three planes) and the final reconstruction equal the CPU
-    oracle's."""
+@pytest.mark.parametrize("kmax,nf,keyat", [(30, 76, (0, 38)), (60, 130, (0, 65))])
+def test_long_batched_sequence_matches_oracle(built, kmax, nf, keyat):
+    """A long sequence in launches of a given largest batch: each GOP holds a
+    full launch of kmax frames and a shorter one, and the ring of reference
+    slots (kmax + 2 are read or written by a launch; the ring holds 62) wraps.
+    Two units of different sizes; every frame's streams (key frames: all three
+    planes) and the final reconstruction equal the CPU oracle's."""
     import fdv_b200 as F
     import oracle as O
-    sizes, rng, qp, nf, keyat = [(160, 96), (64, 48)], 32, 27, 76, (0, 38)
+    sizes, rng, qp = [(160, 96), (64, 48)], 32, 27
     frames = [F.Scene(w, h, nf, nrects=max(2, w * h // 3000), pan_qx=9, pan_qy=-3, static_pct=25,
                       seed=61 + u).frames(nf) for u, (w, h) in enumerate(sizes)]
     eng = F.Engine(sizes, rng)
-    kmax = eng.max_batch()
-    assert kmax == 30
+    eng.set_tuning(kmax, 0)
+    assert eng.max_batch() == kmax
     units = [O.OracleUnit(w, h, rng) for (w, h) in sizes]
     nu = len(sizes)
     f, launches = 0, 0

@@ -32,7 +32,7 @@ def test_launch_shape_never_changes_the_stream(built, golden):
     sizes = [(w, min(bh, h - y0)) for y0 in range(0, h, bh)]
     F.set_search_range(e["search_range"])
     try:
-        for k, grid in ((1, 0), (2, 3), (5, 0), (30, 1), (30, 0)):
+        for k, grid in ((1, 0), (2, 3), (5, 0), (60, 1), (60, 0)):
             F.set_tuning(sizes, e["search_range"], k, grid)
             s = F.vtile_encode(fr, w, h, e["qp"], e["keyint"], bm, 4)
             assert sha(s) == case["stream_sha256"], (k, grid)
@@ -45,12 +45,12 @@ def test_engine_tuning_bounds(built):
     import fdv_b200 as F
     eng = F.Engine([(64, 48)], 16)
     t = eng.tuning()
-    assert t["max_batch"] == 30 and t["p_grid"] == t["nsm"] > 0
+    assert t["max_batch"] == 60 and t["p_grid"] == t["nsm"] > 0
     eng.set_tuning(7, 5)
     assert eng.max_batch() == 7 and eng.tuning()["p_grid"] == 5
     eng.set_tuning(30, 100000)
     assert eng.tuning()["p_grid"] == t["nsm"]
-    for bad in ((0, 0), (31, 0), (5, -1)):
+    for bad in ((0, 0), (61, 0), (5, -1)):
         with pytest.raises(F.FdvError):
             eng.set_tuning(*bad)
     eng.close()
