@@ -1,5 +1,5 @@
 // Key-frame analysis: the intra quadtree of the image codec as a persistent
-// wavefront kernel over coding tree units, run by clusters of four blocks.
+// wavefront kernel over coding tree units, run by clusters of three blocks.
 //
 // Work unit: one 64x64 CTU row of one plane of one encoder unit; clusters take
 // rows from an atomic ticket in plane order.  CTU (c, r) starts once row r-1
@@ -15,9 +15,14 @@
 //   * block 0, warps 0-3 ("the chain"): the walk in the reference's order, the
 //     4x4 leaves (intra_leaf4, fdv.h:3907-4111), the split/leaf decisions and
 //     the CTU's symbols; it holds the CTU's reconstruction and mode map;
-//   * block 0, warps 4-15: the 8x8 leaf trials; blocks 1, 2, 3 (all 16 warps):
-//     the 16x16, 32x32 and 64x64 leaf trials (intra_leafn, fdv.h:4442-4484),
-//     every allowed mode at once.
+//   * block 0, warps 4-11: the 8x8 leaf trials; block 1 (all 16 warps): the
+//     16x16 leaf trials; block 2: the 32x32 and the 64x64 leaf trials
+//     (intra_leafn, fdv.h:4442-4484), every allowed mode at once.  A CTU
+//     has one 64x64 node and four 32x32 ones, whose trials keep a block busy
+//     a fifth of the time or less, so they share one: each size has its own
+//     job slot and result area, and the block codes whichever job is posted
+//     (a 32x32 one first).  Three blocks per cluster let more CTU rows run at
+//     once (the two key frames of a lookahead launch: 49 rows instead of 37).
 // When the chain enters a node it posts the node's neighbours to the team of
 // that size through distributed shared memory; the team codes the leaf and
 // posts back its cost; the chain reads the winner's reconstruction and symbols
@@ -35,7 +40,7 @@ namespace cg = cooperative_groups;
 __device__ const P4Tab g_p4tab = make_p4tab();
 
 constexpr int INT = 512;              // threads per block
-constexpr int ICL = 4;                // blocks per cluster
+constexpr int ICL = 3;                // blocks per cluster
 constexpr int kTileW = 129;           // tile columns: x in [-1, 127] relative to the CTU
 constexpr int kChainNT = 128;         // chain threads (block 0, warps 0-3)
 // 8x8 leaf team (block 0, warps 4-11).  Warps 12-15 of block 0 stay idle:
@@ -99,6 +104,9 @@ __host__ __device__ constexpr int isink_bytes(int d) {
 // k at a fixed offset so that the chain can address it in another block.
 __host__ __device__ constexpr int leaf_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += isink_ccap(0, i); return o; }
 constexpr int kLeafSinkBytes = leaf_off(CS_NUM);
+// The same for a 32x32 leaf (the merged block's second result area).
+__host__ __device__ constexpr int leaf32_off(int k) { int o = 0; for (int i = 0; i < k; ++i) o += isink_ccap(1, i); return o; }
+constexpr int kLeaf32SinkBytes = leaf32_off(CS_NUM);
 
 // A leaf-trial job (written by the chain) and its result (read by the chain).
 struct HJob {
@@ -109,7 +117,8 @@ struct HJob {
 };
 struct HelperArea {
     HJob job;
-    int ok, nm, ml[4];
+    HJob job64;              // block 2: the 64x64 node's job (job: the 32x32 ones)
+    int ok, sel, nm, ml[4];
     NNPred nn[4];
     long long e[4];
     int b[4];
@@ -119,6 +128,11 @@ struct HelperArea {
     __align__(16) uint8_t rec[4][64 * 64];
     __align__(16) uint8_t sinkmem[4][kLeafSinkBytes];
     TeamResidScratch<INT / 32> ts;
+    // block 2: the 32x32 trials' results (the 64x64 trial's go to rec / sink
+    // above), so that neither job overwrites a result the chain has not read
+    CoefSink sink32[4];
+    __align__(16) uint8_t rec32[4][32 * 32];
+    __align__(16) uint8_t sinkmem32[4][kLeaf32SinkBytes];
 };
 struct ChainArea {
     uint8_t tile[65 * kTileW];            // reconstruction: rows -1..63, cols -1..127
@@ -182,8 +196,11 @@ __device__ bool wait_cluster_flag(const int *p, int need, unsigned *err, unsigne
         __nanosleep(32);
     }
 }
-// The leaf trials of nodes of side 64 >> L run in cluster block 3 - L.
-__device__ __forceinline__ int level_rank(int L) { return 3 - L; }
+// The leaf trials of nodes of side 64 >> L run in cluster block 3 - L, the
+// 64x64 ones (L = 0) in block 2 beside the 32x32 ones.
+__device__ __forceinline__ int level_rank(int L) { return L == 0 ? 2 : 3 - L; }
+// The job slot of level L in its block's helper area (a local address).
+__device__ __forceinline__ HJob *job_slot(HelperArea *H, int L) { return L == 0 ? &H->job64 : &H->job; }
 
 __device__ __forceinline__ void cbar() { team_bar(BAR_CHAIN, kChainNT); }
 __device__ __forceinline__ uint8_t &TL(ChainArea &C, int ty, int tx) { return C.tile[(ty + 1) * kTileW + tx + 1]; }
@@ -222,19 +239,22 @@ __device__ void chain_isink_append(ISink *dst, const ISink *src, unsigned *err) 
     }
     cbar();
 }
-// dst += the team's sink `idx` (in cluster block `rank`), by the chain.
-__device__ void chain_append_leaf(CoefSink *dst, IShared *S, int rank, int idx, unsigned *err) {
+// dst += the level-L team's sink `idx` (in cluster block `rank`), by the chain.
+__device__ void chain_append_leaf(CoefSink *dst, IShared *S, int L, int rank, int idx, unsigned *err) {
     const int t = threadIdx.x;
     cg::cluster_group cl = cg::this_cluster();
-    const CoefSink *rs = rank ? cl.map_shared_rank(&S->H.sink[idx], rank) : &S->H.sink[idx];
-    const uint8_t *rm = rank ? cl.map_shared_rank(&S->H.sinkmem[idx][0], rank) : &S->H.sinkmem[idx][0];
+    const bool s32 = L == 1;
+    const CoefSink *ls = s32 ? &S->H.sink32[idx] : &S->H.sink[idx];
+    const uint8_t *lm = s32 ? &S->H.sinkmem32[idx][0] : &S->H.sinkmem[idx][0];
+    const CoefSink *rs = rank ? cl.map_shared_rank(ls, rank) : ls;
+    const uint8_t *rm = rank ? cl.map_shared_rank(lm, rank) : lm;
     int len[CS_NUM];
     for (int k = 0; k < CS_NUM; ++k) len[k] = rs->len[k];
     for (int k = 0; k < CS_NUM; ++k) {
         const int n = len[k], b = dst->len[k];
         if (n == 0) continue;
         if (b + n > dst->cap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        const uint8_t *src = rm + leaf_off(k);
+        const uint8_t *src = rm + (s32 ? leaf32_off(k) : leaf_off(k));
         for (int i = t; i < n; i += kChainNT) dst->buf[k][b + i] = src[i];
     }
     cbar();
@@ -437,7 +457,7 @@ __device__ void post_leaf_job(CCtx &c, int L, int bx, int by, int n, ISink *ss) 
     ChainArea &C = c.S->C;
     const int t = threadIdx.x, tx = bx - c.bx0, ty = by - c.by0;
     const int ht = by > 0, hl = bx > 0;
-    HJob *J = cg::this_cluster().map_shared_rank(&c.S->H.job, level_rank(L));
+    HJob *J = cg::this_cluster().map_shared_rank(job_slot(&c.S->H, L), level_rank(L));
     if (t < n) J->top[t] = ht ? TL(C, ty - 1, tx + t) : 0;
     if (t >= 64 && t - 64 < n) J->left[t - 64] = hl ? TL(C, ty + t - 64, tx - 1) : 0;
     if (t == 1) {
@@ -455,7 +475,7 @@ __device__ void post_row_end(IShared *S) {
     ChainArea &C = S->C;
     if (threadIdx.x == 0) {
         for (int L = 0; L < 4; ++L) {
-            HJob *J = cg::this_cluster().map_shared_rank(&S->H.job, level_rank(L));
+            HJob *J = cg::this_cluster().map_shared_rank(job_slot(&S->H, L), level_rank(L));
             J->kind = 1;
             st_release_cluster(&J->seq, ++C.issued[L]);
         }
@@ -514,7 +534,7 @@ __device__ double CNode<D>::run(CCtx &c, int bx, int by, ISink *tgt) {
         RH = cg::this_cluster().map_shared_rank(&S->H, rank);
     }
     const int tx = bx - c.bx0, ty = by - c.by0;
-    const uint32_t *rw = reinterpret_cast<const uint32_t *>(RH->rec[bi]);
+    const uint32_t *rw = reinterpret_cast<const uint32_t *>(D == 1 ? RH->rec32[bi] : RH->rec[bi]);
     for (int p = t; p < n * n / 4; p += kChainNT) {
         const uint32_t v = rw[p];
         const int y = (p * 4) / n, x = (p * 4) % n;
@@ -524,7 +544,7 @@ __device__ double CNode<D>::run(CCtx &c, int bx, int by, ISink *tgt) {
     constexpr int cells = n / 4;
     const int m4 = mode == 1 ? 1 : (mode == 2 ? 2 : 0);   // nn_to_4x4_mode
     for (int p = t; p < cells * cells; p += kChainNT) MM(C, (ty >> 2) + p / cells, (tx >> 2) + p % cells) = (uint8_t)m4;
-    chain_append_leaf(&tgt->c, S, rank, bi, c.err);
+    chain_append_leaf(&tgt->c, S, D, rank, bi, c.err);
     return Jl;
 }
 
@@ -608,18 +628,67 @@ __device__ void chain_row(IShared *S, const IPlaneDev &P, int r, unsigned *err, 
 }
 
 // ------------------------------------------------------- leaf teams --
-// A team codes the leaf trials of one node size until the chain ends the row:
-// every allowed mode (fdv_intra_nn_mode_ok) of the n x n leaf at once through
-// team_residuals, then the reference's choice among them (the first strictly
-// cheaper, fdv.h:4467-4471).  `seen` counts the jobs this team has taken.
+// A team codes the leaf trial of one node: every allowed mode
+// (fdv_intra_nn_mode_ok) of the n x n leaf at once through team_residuals,
+// then the reference's choice among them (the first strictly cheaper,
+// fdv.h:4467-4471), into the result area (rec, sink), then posts the cost,
+// the choice and job number `seq` of level L to the chain.
+template <int NT, int BAR>
+__device__ void team_code(IShared *S, const IPlaneDev &P, int L, const HJob &job, uint8_t *const *rec,
+                          CoefSink *const *sink, int seq, unsigned *err, int tt) {
+    HelperArea &H = S->H;
+    const int n = 64 >> L;
+    ChainArea *RC = cg::this_cluster().map_shared_rank(&S->C, 0);
+    unsigned long long *prof = P.prof;
+    const long long t0 = prof_t0(prof, tt);
+    const int bx = job.bx, by = job.by, ht = job.ht, hl = job.hl, tl = job.tl;
+    for (int p = tt; p < n * n; p += NT) {
+        const int y = p / n, x = p % n;
+        H.src[y * 64 + x] = P.src[(size_t)(by + y) * P.w + bx + x];
+    }
+    if (tt < 4) {
+        H.nn[tt] = nn_setup(tt, job.top, job.left, tl, n, ht, hl);
+        cs_reset(sink[tt]);
+    }
+    if (tt == 0) {
+        int nm = 0;
+        for (int m = 0; m < 4; ++m) if (nn_mode_ok(m, n, ht, hl)) H.ml[nm++] = m;
+        H.nm = nm;
+    }
+    team_bar(BAR, NT);
+    const int M = H.nm, nn2 = n * n;
+    for (int p = tt; p < M * nn2; p += NT) {
+        const int i = p / nn2, q = p - i * nn2;
+        H.pred[i][q] = (uint8_t)nn_px(H.nn[H.ml[i]], job.top, job.left, q % n, q / n);
+    }
+    team_bar(BAR, NT);
+    uint8_t *pr[4] = {H.pred[0], H.pred[1], H.pred[2], H.pred[3]};
+    team_residuals<NT>(H.src, 64, pr, rec, sink, M, n, S->q, P.qp, P.lambda, H.e, H.b, &H.ts, err, tt, BAR);
+    if (tt == 0) {
+        double best = -1.0;
+        int bi = 0;
+        for (int i = 0; i < M; ++i) {
+            const double J = rd_cost((double)H.e[i], P.lambda, kBitsMode + H.b[i]);
+            if (best < 0.0 || J < best) { best = J; bi = i; }
+        }
+        RC->res_J[L] = best;
+        RC->res_idx[L] = bi;
+        RC->res_mode[L] = H.ml[bi];
+    }
+    if (L < 3) fence_cluster();
+    team_bar(BAR, NT);
+    if (tt == 0) st_release_cluster(&RC->done[L], seq);
+    prof_add(prof, tt, IP_LEAF64 - L, t0);
+}
+
+// The team of one node size (block 0's 8x8 team, block 1's 16x16 team) until
+// the chain ends the CTU row.  `seen` counts the jobs this team has taken.
 template <int NT, int BAR>
 __device__ void team_loop(IShared *S, const IPlaneDev &P, int L, unsigned *err, unsigned long long hlimit, int tt,
                           int &seen) {
     HelperArea &H = S->H;
-    const int n = 64 >> L;
-    cg::cluster_group cl = cg::this_cluster();
-    ChainArea *RC = cl.map_shared_rank(&S->C, 0);
-    unsigned long long *prof = P.prof;
+    uint8_t *rec[4] = {H.rec[0], H.rec[1], H.rec[2], H.rec[3]};
+    CoefSink *sink[4] = {&H.sink[0], &H.sink[1], &H.sink[2], &H.sink[3]};
     for (;;) {
         if (tt == 0) H.ok = wait_cluster_flag(&H.job.seq, seen + 1, err, hlimit);
         team_bar(BAR, NT);
@@ -627,47 +696,50 @@ __device__ void team_loop(IShared *S, const IPlaneDev &P, int L, unsigned *err, 
         if (!H.ok) break;
         ++seen;
         if (H.job.kind != 0) break;
-        const long long t0 = prof_t0(prof, tt);
-        const int bx = H.job.bx, by = H.job.by, ht = H.job.ht, hl = H.job.hl, tl = H.job.tl;
-        for (int p = tt; p < n * n; p += NT) {
-            const int y = p / n, x = p % n;
-            H.src[y * 64 + x] = P.src[(size_t)(by + y) * P.w + bx + x];
-        }
-        if (tt < 4) {
-            H.nn[tt] = nn_setup(tt, H.job.top, H.job.left, tl, n, ht, hl);
-            cs_reset(&H.sink[tt]);
-        }
+        team_code<NT, BAR>(S, P, L, H.job, rec, sink, seen, err, tt);
+    }
+}
+
+// Block 2: the 32x32 jobs (slot job, results in rec32 / sink32) and the
+// 64x64 job (slot job64, results in rec / sink) until the chain has ended the
+// CTU row on both.  seen32 / seen64 count the jobs taken from each slot.
+template <int NT, int BAR>
+__device__ void team_loop_3264(IShared *S, const IPlaneDev &P, unsigned *err, unsigned long long hlimit, int tt,
+                               int &seen32, int &seen64) {
+    HelperArea &H = S->H;
+    uint8_t *rec64[4] = {H.rec[0], H.rec[1], H.rec[2], H.rec[3]};
+    CoefSink *sink64[4] = {&H.sink[0], &H.sink[1], &H.sink[2], &H.sink[3]};
+    uint8_t *rec32[4] = {H.rec32[0], H.rec32[1], H.rec32[2], H.rec32[3]};
+    CoefSink *sink32[4] = {&H.sink32[0], &H.sink32[1], &H.sink32[2], &H.sink32[3]};
+    bool end32 = false, end64 = false;
+    while (!(end32 && end64)) {
         if (tt == 0) {
-            int nm = 0;
-            for (int m = 0; m < 4; ++m) if (nn_mode_ok(m, n, ht, hl)) H.ml[nm++] = m;
-            H.nm = nm;
-        }
-        team_bar(BAR, NT);
-        const int M = H.nm, nn2 = n * n;
-        for (int p = tt; p < M * nn2; p += NT) {
-            const int i = p / nn2, q = p - i * nn2;
-            H.pred[i][q] = (uint8_t)nn_px(H.nn[H.ml[i]], H.job.top, H.job.left, q % n, q / n);
-        }
-        team_bar(BAR, NT);
-        uint8_t *pr[4] = {H.pred[0], H.pred[1], H.pred[2], H.pred[3]};
-        uint8_t *rc[4] = {H.rec[0], H.rec[1], H.rec[2], H.rec[3]};
-        CoefSink *sk[4] = {&H.sink[0], &H.sink[1], &H.sink[2], &H.sink[3]};
-        team_residuals<NT>(H.src, 64, pr, rc, sk, M, n, S->q, P.qp, P.lambda, H.e, H.b, &H.ts, err, tt, BAR);
-        if (tt == 0) {
-            double best = -1.0;
-            int bi = 0;
-            for (int i = 0; i < M; ++i) {
-                const double J = rd_cost((double)H.e[i], P.lambda, kBitsMode + H.b[i]);
-                if (best < 0.0 || J < best) { best = J; bi = i; }
+            // bounded wait for a job in either slot, a 32x32 one first
+            int ok = 0, sel = 0;
+            const unsigned long long t0 = globaltimer();
+            for (;;) {
+                if (!end32 && ld_acquire_cluster(&H.job.seq) >= seen32 + 1) { ok = 1; sel = 1; break; }
+                if (!end64 && ld_acquire_cluster(&H.job64.seq) >= seen64 + 1) { ok = 1; sel = 0; break; }
+                if (*(volatile unsigned *)err) break;
+                if (globaltimer() - t0 > hlimit) { atomicOr(err, kErrWaitTimeout); break; }
+                __nanosleep(32);
             }
-            RC->res_J[L] = best;
-            RC->res_idx[L] = bi;
-            RC->res_mode[L] = H.ml[bi];
+            H.ok = ok;
+            H.sel = sel;
         }
-        if (L < 3) fence_cluster();
         team_bar(BAR, NT);
-        if (tt == 0) st_release_cluster(&RC->done[L], seen);
-        prof_add(prof, tt, IP_LEAF64 - L, t0);
+        fence_cluster();
+        if (!H.ok) break;
+        const int L = H.sel ? 1 : 0;
+        const HJob &job = L ? H.job : H.job64;
+        const int seq = L ? ++seen32 : ++seen64;
+        if (job.kind != 0) {
+            if (L) end32 = true;
+            else end64 = true;
+            team_bar(BAR, NT);   // every thread has read the slot before the next wait
+            continue;
+        }
+        team_code<NT, BAR>(S, P, L, job, L ? rec32 : rec64, L ? sink32 : sink64, seq, err, tt);
     }
 }
 
@@ -694,11 +766,15 @@ iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ ta
         int c0[CS_NUM];
         for (int k = 0; k < CS_NUM; ++k) c0[k] = isink_ccap(0, k);
         for (int i = 0; i < 4; ++i) cs_init(&S->H.sink[i], S->H.sinkmem[i], c0);
+        int c1[CS_NUM];
+        for (int k = 0; k < CS_NUM; ++k) c1[k] = isink_ccap(1, k);
+        for (int i = 0; i < 4; ++i) cs_init(&S->H.sink32[i], S->H.sinkmem32[i], c1);
         for (int L = 0; L < 4; ++L) { C.done[L] = 0; C.issued[L] = 0; }
         for (int k = 0; k < 9 * 16; ++k) C.p4[k] = g_p4tab.op[k];
         S->H.job.seq = 0;
+        S->H.job64.seq = 0;
     }
-    int seen = 0;
+    int seen = 0, seen64 = 0;
     cl.sync();
     for (;;) {
         if (rank == 0 && tid == 0) S->C.task = atomicAdd(ticket, 1);
@@ -712,8 +788,10 @@ iframe_kernel(const IPlaneDev *__restrict__ planes, const ITask *__restrict__ ta
         if (rank == 0) {
             if (tid < kChainNT) chain_row(S, P, tasks[t].row, err, wait_ns, hlimit);
             else if (tid < kChainNT + kH8NT) team_loop<kH8NT, BAR_H8>(S, P, 3, err, hlimit, tid - kChainNT, seen);
+        } else if (rank == 1) {
+            team_loop<INT, BAR_TEAM>(S, P, 2, err, hlimit, tid, seen);
         } else {
-            team_loop<INT, BAR_TEAM>(S, P, 3 - rank, err, hlimit, tid, seen);
+            team_loop_3264<INT, BAR_TEAM>(S, P, err, hlimit, tid, seen, seen64);
         }
     }
 }
