@@ -127,7 +127,8 @@ struct Unit {
     // reconstruction (un-deblocked for P-frames), records, progress words
     // (P rows: 64-bit words, then per row the count of reference tiles
     // written; then I rows for Y, U, V), macroblock symbol slots
-    uint8_t *cur[kMaxBatch] = {}, *rec[kMaxBatch] = {};
+    uint8_t *rec[kMaxBatch] = {};
+    size_t src_off = 0;           // this unit's planes in a lane's source buffer
     MBInfo *mbi[kMaxBatch] = {};
     int *progress[kMaxBatch] = {};
     uint8_t *slots[kMaxBatch] = {};
@@ -200,7 +201,13 @@ struct fdvb_engine {
     int inflight = 0;
     size_t src_stage_bytes = 0;    // a slot's staging of one frame's sources (64-byte multiple)
     size_t src_bytes = 0;          // one frame's sources, all units
-    uint8_t *lane_src[kMaxBatch] = {};   // per lane: every unit's source planes, one upload per frame
+    // per lane, in two sets alternating by submission: every unit's source
+    // planes, uploaded on their own stream (st_up) so that a submission's
+    // copies overlap the previous submission's kernels
+    uint8_t *lane_src[2][kMaxBatch] = {};
+    int upar = 0;                        // the set the next submission uploads into
+    cudaStream_t st_up = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_srcfree[2] = {nullptr, nullptr};
     int lanes = 0;                       // lanes allocated so far (at first use)
     size_t stage_cap = 0;                // a slot's pinned staging (allocated at first use)
     // timing (CUDA events on the engine's stream) and launch counts
@@ -316,12 +323,8 @@ static int ensure_lanes(fdvb_engine *E, int n) {
             CK(cudaMalloc(&u.progress[k], sizeof(int) * u.nprog));
             CK(cudaMalloc(&u.cout[k], u.out_cap));
         }
-        CK(cudaMalloc(&E->lane_src[k], E->src_bytes));
-        size_t off = 0;
-        for (auto &u : E->units) {
-            u.cur[k] = E->lane_src[k] + off;
-            off += (size_t)u.w * u.h * 3 / 2;
-        }
+        CK(cudaMalloc(&E->lane_src[0][k], E->src_bytes));
+        CK(cudaMalloc(&E->lane_src[1][k], E->src_bytes));
         E->lanes = k + 1;
     }
     return 0;
@@ -414,6 +417,18 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
     for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
     E->src_bytes = src_bytes;
     E->src_stage_bytes = (src_bytes + 63) / 64 * 64;
+    {
+        size_t off = 0;
+        for (auto &u : E->units) { u.src_off = off; off += (size_t)u.w * u.h * 3 / 2; }
+    }
+    if (cudaStreamCreateWithFlags(&E->st_up, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_up, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_srcfree[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&E->ev_srcfree[1], cudaEventDisableTiming) != cudaSuccess) {
+        g_err = "stream create failed";
+        fdvb_engine_destroy(E);
+        return nullptr;
+    }
     if (ensure_lanes(E, 1) != 0) { fdvb_engine_destroy(E); return nullptr; }
     E->stage_cap = E->src_stage_bytes + stage_desc_bytes(nunits, maxrows, maxitasks);
     for (auto &sl : E->slot) {
@@ -442,7 +457,9 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
     cudaFree(E->d_poff); cudaFree(E->d_ioff);
-    for (auto *p : E->lane_src) cudaFree(p);
+    for (int s = 0; s < 2; ++s) for (auto *p : E->lane_src[s]) cudaFree(p);
+    if (E->st_up) { cudaStreamSynchronize(E->st_up); cudaStreamDestroy(E->st_up); }
+    for (cudaEvent_t e : {E->ev_up, E->ev_srcfree[0], E->ev_srcfree[1]}) if (e) cudaEventDestroy(e);
     if (E->d_prof) cudaFree(E->d_prof);
     if (E->d_tl) cudaFree(E->d_tl);
     if (E->lnet) fdvl_destroy(E->lnet);
@@ -613,6 +630,10 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         return a.type == cudaMemoryTypeHost;
     };
     std::vector<const uint8_t *> span_lo(K, nullptr);   // frame k copied as one span from here (else null)
+    // this submission's source set: free once the kernels of the submission
+    // before the last one (which read it) have run
+    const int par = E->upar;
+    if (!E->src_on_device) CK(cudaStreamWaitEvent(E->st_up, E->ev_srcfree[par], 0));
     if (!E->src_on_device && E->direct_upload && !force_skip)
         for (int k = 0; k < K; ++k) {
             const uint8_t *lo = nullptr, *hi = nullptr;
@@ -628,7 +649,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 }
             }
             if ((size_t)(hi - lo) != sum || sum > E->src_bytes || !pinned(lo) || !pinned(hi - 1)) continue;
-            if (cudaMemcpyAsync(E->lane_src[k], lo, sum, cudaMemcpyHostToDevice, E->st) != cudaSuccess) {
+            if (cudaMemcpyAsync(E->lane_src[par][k], lo, sum, cudaMemcpyHostToDevice, E->st_up) != cudaSuccess) {
                 cudaGetLastError();
                 continue;
             }
@@ -652,11 +673,17 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
                 stage += ys + 2 * cs;
                 const size_t done = (size_t)(stage - stage0);
                 if (done - sent >= ((size_t)4 << 20) || i == nu - 1) {
-                    CK(cudaMemcpyAsync(E->lane_src[k] + sent, stage0 + sent, done - sent, cudaMemcpyHostToDevice, E->st));
+                    CK(cudaMemcpyAsync(E->lane_src[par][k] + sent, stage0 + sent, done - sent, cudaMemcpyHostToDevice,
+                                       E->st_up));
                     sent = done;
                 }
             }
         }
+    if (!E->src_on_device) {
+        // the kernels below read the sources once they are copied
+        CK(cudaEventRecord(E->ev_up, E->st_up));
+        CK(cudaStreamWaitEvent(E->st, E->ev_up, 0));
+    }
     // the lookahead frame's sources: read in place, or staged and uploaded
     std::vector<const uint8_t *> kplanes;
     if (joint) {
@@ -731,9 +758,11 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             if (E->src_on_device && !(force_skip && force_skip[j])) {
                 d.cur[0] = planes[3 * j]; d.cur[1] = planes[3 * j + 1]; d.cur[2] = planes[3 * j + 2];
             } else if (span_lo[k]) {
-                for (int p = 0; p < 3; ++p) d.cur[p] = E->lane_src[k] + (planes[3 * j + p] - span_lo[k]);
+                for (int p = 0; p < 3; ++p) d.cur[p] = E->lane_src[par][k] + (planes[3 * j + p] - span_lo[k]);
             } else {
-                d.cur[0] = u.cur[k]; d.cur[1] = u.cur[k] + (size_t)u.w * u.h; d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
+                d.cur[0] = E->lane_src[par][k] + u.src_off;
+                d.cur[1] = d.cur[0] + (size_t)u.w * u.h;
+                d.cur[2] = d.cur[1] + (size_t)u.cw * u.ch;
             }
             d.rec[0] = u.rec[k]; d.rec[1] = u.rec[k] + (size_t)u.w * u.h; d.rec[2] = d.rec[1] + (size_t)u.cw * u.ch;
             // frame k's references: the outputs of the two frames before it
@@ -980,6 +1009,11 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         S.has_p = !rows.empty();
         S.has_i = !itasks.empty();
         S.batch = k == 0 ? K : 0;
+    }
+    if (!E->src_on_device) {
+        // this source set is free again once the kernels enqueued above have run
+        CK(cudaEventRecord(E->ev_srcfree[par], E->st));
+        E->upar ^= 1;
     }
     if (joint) {   // the lookahead frame waits in its lane for its own submission
         E->kr_ready = true;
