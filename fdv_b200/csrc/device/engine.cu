@@ -35,7 +35,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
+#include <thread>
 #include <deque>
 #include <cstring>
 #include <string>
@@ -50,7 +52,9 @@ namespace fdvb {
 // kernels (pframe.cu, iframe.cu, frame_ops.cu)
 void launch_lrn_preskip(const UnitDev *units, const int2 *pu, int np, int total, cudaStream_t st);
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st);
+                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st,
+                   const FrameSync *fsync = nullptr, const void *ctasks = nullptr, int *fdone = nullptr, int nu = 1,
+                   int nunits = 0);
 struct IPlaneDev;
 struct ITask;
 size_t iframe_smem_bytes();
@@ -171,7 +175,9 @@ struct Slot {
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<int> intra;
     bool has_p = false, has_i = false;
-    int batch = 0;                // frames of the batch when this is its first frame, else 0
+    int batch = 0;                // frames of the batch when this is its last frame, else 0
+    bool streamed = false;        // compacted inside the P launch: ready once its ready word says so
+    unsigned ready_val = 0;
 };
 
 }  // namespace
@@ -215,6 +221,15 @@ struct fdvb_engine {
     long long steps = 0, pk_n = 0, ik_n = 0, launches = 0, d2h = 0;
     int src_on_device = 0;
     int direct_upload = 0;       // host sources that stay valid until collected: pinned ones are copied without staging
+    // Frames streamed out of P launches (fdvb_engine_stream_frames): each
+    // frame is compacted inside the launch as soon as its rows are done and
+    // its host-mapped ready word set, so a host can collect and entropy-code
+    // it while the launch goes on.
+    int stream_frames = 0;
+    unsigned *ready_h = nullptr, *ready_d = nullptr;   // per in-flight slot (host-mapped)
+    unsigned ready_seq = 0;
+    FrameSync *d_fsync = nullptr;                      // per lane of a launch
+    int *d_fdone = nullptr;                            // per unit-frame: rows finished; per frame: units compacted
     int stall_unit = -1, stall_row = -1;
     int defer_refs = 0;                     // leave the reference pool alone until commit
     std::vector<int> pending_intra;         // frame types of the uncommitted step
@@ -359,7 +374,8 @@ static size_t stage_desc_bytes(int nu, int maxrows, int maxitasks) {
     // key-frame descriptors twice over: a key frame and the lookahead beside it
     return a(sizeof(UnitDev) * kMaxBatch * nu) + a(sizeof(RowTask) * kMaxBatch * maxrows) +
            a(sizeof(IPlaneDevH) * 6 * nu) + a(sizeof(ITaskH) * 2 * maxitasks) + 2 * a(sizeof(PrepTaskH) * nu) +
-           a(sizeof(DbTaskH) * 6 * nu) + a(sizeof(CompactTaskH) * 3 * kMaxBatch * nu) + a(sizeof(int2) * nu);
+           a(sizeof(DbTaskH) * 6 * nu) + a(sizeof(CompactTaskH) * 3 * kMaxBatch * nu) + a(sizeof(int2) * nu) +
+           a(sizeof(FrameSync) * kMaxBatch);
 }
 
 extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *h, int range, int device) {
@@ -411,7 +427,11 @@ extern "C" fdvb_engine *fdvb_engine_create(int nunits, const int *w, const int *
               cudaMalloc(&E->d_err, sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc(&E->d_err_inf, 2 * sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc(&E->d_poff, sizeof(int) * 16) == cudaSuccess &&
-              cudaMalloc(&E->d_ioff, sizeof(int) * 12) == cudaSuccess;
+              cudaMalloc(&E->d_ioff, sizeof(int) * 12) == cudaSuccess &&
+              cudaMalloc(&E->d_fsync, sizeof(FrameSync) * kMaxBatch) == cudaSuccess &&
+              cudaMalloc(&E->d_fdone, sizeof(int) * kMaxBatch * (nunits + 1)) == cudaSuccess &&
+              cudaHostAlloc(&E->ready_h, sizeof(unsigned) * kSlots, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer(&E->ready_d, E->ready_h, 0) == cudaSuccess;
     if (!ok) { g_err = "device allocation failed"; fdvb_engine_destroy(E); return nullptr; }
     size_t src_bytes = 0;
     for (auto &u : E->units) src_bytes += (size_t)u.w * u.h * 3 / 2;
@@ -456,7 +476,8 @@ extern "C" void fdvb_engine_destroy(fdvb_engine *E) {
     for (auto &u : E->units) free_unit(u);
     cudaFree(E->d_units); cudaFree(E->d_rows); cudaFree(E->d_planes); cudaFree(E->d_itasks);
     cudaFree(E->d_prep); cudaFree(E->d_db); cudaFree(E->d_cmp); cudaFree(E->d_ticket); cudaFree(E->d_err);
-    cudaFree(E->d_poff); cudaFree(E->d_ioff);
+    cudaFree(E->d_poff); cudaFree(E->d_ioff); cudaFree(E->d_fsync); cudaFree(E->d_fdone);
+    if (E->ready_h) cudaFreeHost(E->ready_h);
     for (int s = 0; s < 2; ++s) for (auto *p : E->lane_src[s]) cudaFree(p);
     if (E->st_up) { cudaStreamSynchronize(E->st_up); cudaStreamDestroy(E->st_up); }
     for (cudaEvent_t e : {E->ev_up, E->ev_srcfree[0], E->ev_srcfree[1]}) if (e) cudaEventDestroy(e);
@@ -612,7 +633,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             if (unit_out(u, sis[k]) != 0) return -3;
         if (!E->slot[sis[k]].stage) CK(cudaHostAlloc(&E->slot[sis[k]].stage, E->stage_cap, cudaHostAllocDefault));
     }
-    Slot &SL = E->slot[sis[0]];
+    Slot &SL = E->slot[sis[K - 1]];   // the batch's last frame carries its timing
     CK(cudaEventRecord(SL.ev[0], E->st));
     // 1. sources: device sources are read where they are; host sources go
     // through each frame's pinned staging buffer, laid out as the lane buffer,
@@ -890,6 +911,28 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
     CK(cudaMemcpyAsync(E->d_units, ud_st, sizeof(UnitDev) * K * nu, cudaMemcpyHostToDevice, E->st));
     CK(cudaMemsetAsync(E->d_ticket, 0, sizeof(int) * 2, E->st));
     CK(cudaMemsetAsync(E->d_err, 0, sizeof(unsigned), E->st));
+    // Frames streamed out of the P launch: every unit of every frame a
+    // P-frame with its reference written inside the wavefront; the frame's
+    // compaction tasks (one per unit, cmp[k * nu + i]) run inside the launch.
+    bool all_p = true;
+    for (int j = 0; j < K * nu; ++j) if (is_intra[j]) all_p = false;
+    const bool streamable = E->stream_frames && !rows.empty() && itasks.empty() && all_p && !whole_frame_refs &&
+                            (int)cmp.size() == K * nu;
+    std::vector<unsigned> fs_val(K, 0u);
+    if (streamable) {
+        CK(cudaMemcpyAsync(E->d_cmp, staged(cmp.data(), sizeof(CompactTaskH) * cmp.size()),
+                           sizeof(CompactTaskH) * cmp.size(), cudaMemcpyHostToDevice, E->st));
+        std::vector<FrameSync> fsv(K);
+        for (int k = 0; k < K; ++k) {
+            if (++E->ready_seq == 0) ++E->ready_seq;
+            fs_val[k] = E->ready_seq;
+            E->ready_h[sis[k]] = 0u;
+            fsv[k] = FrameSync{E->ready_d + sis[k], fs_val[k]};
+        }
+        CK(cudaMemcpyAsync(E->d_fsync, staged(fsv.data(), sizeof(FrameSync) * K), sizeof(FrameSync) * K,
+                           cudaMemcpyHostToDevice, E->st));
+        CK(cudaMemsetAsync(E->d_fdone, 0, sizeof(int) * K * (nu + 1), E->st));
+    }
     if (!rows.empty()) {
         CK(cudaMemcpyAsync(E->d_rows, staged(rows.data(), sizeof(RowTask) * rows.size()), sizeof(RowTask) * rows.size(),
                            cudaMemcpyHostToDevice, E->st));
@@ -934,7 +977,7 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
             E->launches += 2;
         }
         launch_pframe(E->d_units, E->d_rows, (int)rows.size(), E->d_ticket, E->d_err, E->wait_ns, grid, E->range,
-                      !pu.empty(), E->st);
+                      !pu.empty(), E->st, streamable ? E->d_fsync : nullptr, E->d_cmp, E->d_fdone, nu, K * nu);
         CK(cudaGetLastError());
         CK(cudaEventRecord(SL.ev[2], E->st));
         if (!pu.empty()) {
@@ -962,11 +1005,13 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         CK(cudaGetLastError());
         E->launches += 2;
     }
-    CK(cudaMemcpyAsync(E->d_cmp, staged(cmp.data(), sizeof(CompactTaskH) * cmp.size()), sizeof(CompactTaskH) * cmp.size(),
-                       cudaMemcpyHostToDevice, E->st));
-    launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
-    CK(cudaGetLastError());
-    E->launches += 1;
+    if (!streamable) {
+        CK(cudaMemcpyAsync(E->d_cmp, staged(cmp.data(), sizeof(CompactTaskH) * cmp.size()),
+                           sizeof(CompactTaskH) * cmp.size(), cudaMemcpyHostToDevice, E->st));
+        launch_compact(E->d_cmp, (int)cmp.size(), E->d_err, E->st);
+        CK(cudaGetLastError());
+        E->launches += 1;
+    }
     // 5. the new references (deferred: the caller may code this frame again)
     if (E->defer_refs) {
         E->pending_intra.assign(is_intra, is_intra + nu);
@@ -1008,7 +1053,9 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         CK(cudaEventRecord(S.ev[5], E->st));
         S.has_p = !rows.empty();
         S.has_i = !itasks.empty();
-        S.batch = k == 0 ? K : 0;
+        S.batch = k == K - 1 ? K : 0;
+        S.streamed = streamable;
+        S.ready_val = streamable ? fs_val[k] : 0u;
     }
     if (!E->src_on_device) {
         // this source set is free again once the kernels enqueued above have run
@@ -1068,7 +1115,21 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     E->order.pop_front();
     E->busy[si] = false;
     E->inflight -= 1;
-    CK(cudaEventSynchronize(SL.ev[5]));
+    // A streamed frame that is not its batch's last is ready once its word is
+    // set (the batch's errors are reported at its last frame); otherwise, or
+    // when the batch ended without setting it, wait for the batch.
+    bool early = false;
+    if (SL.streamed && !SL.batch) {
+        for (unsigned i = 0;; ++i) {
+            if (*(volatile unsigned *)&E->ready_h[si] == SL.ready_val) { early = true; break; }
+            const cudaError_t q = cudaEventQuery(SL.ev[5]);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) CK(q);
+            if (i > 64) std::this_thread::yield();
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+    }
+    if (!early) CK(cudaEventSynchronize(SL.ev[5]));
     E->steps += 1;
     if (SL.batch) {
         // the batch's first frame carries its timing: whole step, and the
@@ -1079,7 +1140,7 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
         if (SL.has_p) { cudaEventElapsedTime(&ms, SL.ev[1], SL.ev[2]); E->pk_ms += ms; E->pk_n += SL.batch; }
         if (SL.has_i) { cudaEventElapsedTime(&ms, SL.ev[3], SL.ev[4]); E->ik_ms += ms; E->ik_n += 1; }
     }
-    const unsigned err = SL.err_h[0] | SL.err_h[1];
+    const unsigned err = early ? 0u : (SL.err_h[0] | SL.err_h[1]);
     if (err) {
         g_err = status_text(err);
         return -4;
@@ -1163,6 +1224,19 @@ extern "C" void fdvb_engine_src_on_device(fdvb_engine *E, int on) { if (E) E->sr
 // Host sources of the next steps stay valid and unchanged until their frames
 // are collected: pinned ones are then copied without host staging.
 extern "C" void fdvb_engine_direct_upload(fdvb_engine *E, int on) { if (E) E->direct_upload = on; }
+// P-frames of the next submissions are streamed out of their launch: a frame
+// can be collected as soon as its own rows are done (the errors of a batch are
+// reported when its last frame is collected).
+extern "C" void fdvb_engine_stream_frames(fdvb_engine *E, int on) { if (E) E->stream_frames = on; }
+// Whether the oldest frame in flight can be collected without waiting:
+// 1 yes, 0 not yet, -1 no frame in flight.
+extern "C" int fdvb_engine_ready(fdvb_engine *E) {
+    if (!E || E->inflight == 0) return -1;
+    const int si = E->order.front();
+    const Slot &SL = E->slot[si];
+    if (SL.streamed && !SL.batch && *(volatile unsigned *)&E->ready_h[si] == SL.ready_val) return 1;
+    return cudaEventQuery(SL.ev[5]) == cudaSuccess ? 1 : 0;
+}
 
 // Accumulated device time (CUDA events on the engine stream) of the steps, of
 // the P-frame analysis kernel and of the key-frame kernel, with their counts,

@@ -58,4 +58,14 @@ struct RowTask { int unit, row; };
 // Stream ids of the P-frame slot (fdv.h:4170, :6198-6210).
 enum { PS_REF = 4, PS_MVX = 5, PS_MVY = 6, PS_SUB = 7, PS_MERGE = 8, PS_CN = 9 };
 
+// One frame of a P launch whose frames are compacted inside the launch: the
+// block that finishes a unit's last macroblock row of the frame compacts that
+// unit's symbol streams, and the last unit of the frame to be compacted sets
+// the frame's host-mapped word, so the host can code the frame while the
+// launch goes on.
+struct FrameSync {
+    unsigned *ready;       // host-mapped; set to ready_val once the frame's streams are in place
+    unsigned ready_val;
+};
+
 }  // namespace fdvb

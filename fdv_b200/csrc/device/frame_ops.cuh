@@ -12,6 +12,7 @@
 //  * compact: per-macroblock symbol slots are concatenated, per stream, in
 //    raster order -- the order the reference appends them -- directly into
 //    host-mapped memory.
+#pragma once
 #include "common.cuh"
 #include "engine_dev.cuh"
 
@@ -225,6 +226,81 @@ __global__ void __launch_bounds__(1024) compact_kernel(const CompactTask *tasks,
     }
     if (T.hist)
         for (int i = tid; i < T.nstreams * 256; i += 1024) T.hist[i] = s_hist[i >> 8][i & 255];
+}
+
+// The same compaction by a block of NT threads inside another kernel (the
+// P-frame wavefront compacts a frame as soon as its last row is done): NT / 16
+// threads per stream.  The slots were written by other blocks of the launch,
+// which published them with a fence before counting their rows, so they are
+// read through L2.  Every thread of the block calls it.
+template <int NT> struct CompactScratch {
+    unsigned tot[16][NT / 16];
+    unsigned base[17];
+    unsigned hist[16][256];
+};
+template <int NT>
+__device__ __noinline__ void compact_block(const CompactTask &T, unsigned *err, CompactScratch<NT> &S, int tid) {
+    constexpr int TPS = NT / 16;
+    const int k = tid / TPS, t = tid % TPS;
+    for (int i = tid; i < 16 * 256; i += NT) (&S.hist[0][0])[i] = 0u;
+    const int nb = T.nslots, chunk = (nb + TPS - 1) / TPS, b0 = t * chunk, b1 = min(nb, b0 + chunk);
+    unsigned mine = 0;
+    if (k < T.nstreams)
+        for (int b = b0; b < b1; ++b)
+            mine += __ldcg(reinterpret_cast<const unsigned short *>(T.slots + (size_t)b * T.slot_bytes) + k);
+    S.tot[k][t] = mine;
+    __syncthreads();
+    if (tid < 16) {
+        unsigned acc = 0;
+        for (int i = 0; i < TPS; ++i) { const unsigned v = S.tot[tid][i]; S.tot[tid][i] = acc; acc += v; }
+        S.base[tid] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        unsigned acc = 0;
+        for (int s = 0; s < T.nstreams; ++s) { const unsigned tot = S.base[s]; S.base[s] = acc; acc += tot; }
+        S.base[16] = acc;
+    }
+    __syncthreads();
+    const size_t hdr = 4 * (size_t)T.nstreams, total = hdr + S.base[16];
+    if (total > T.cap) {
+        if (tid == 0) atomicOr(err, kErrOutCap);
+        __syncthreads();
+        return;
+    }
+    uint8_t *const asmb = T.tmp ? T.tmp : T.out;
+    if (tid < T.nstreams) {
+        const unsigned len = (tid + 1 < T.nstreams ? S.base[tid + 1] : S.base[16]) - S.base[tid];
+        reinterpret_cast<unsigned *>(asmb)[tid] = len;
+    }
+    if (k < T.nstreams) {
+        uint8_t *dst = asmb + hdr + S.base[k] + S.tot[k][t];
+        for (int b = b0; b < b1; ++b) {
+            const uint8_t *slot = T.slots + (size_t)b * T.slot_bytes;
+            const int n = __ldcg(reinterpret_cast<const unsigned short *>(slot) + k);
+            const uint8_t *src = slot + 32 + T.off[k];
+            for (int i = 0; i < n; ++i) {
+                const uint8_t v = __ldcg(src + i);
+                dst[i] = v;
+                if (T.hist) atomicAdd(&S.hist[k][v], 1u);
+            }
+            dst += n;
+        }
+    }
+    __syncthreads();
+    if (T.tmp) {
+        if (((reinterpret_cast<uintptr_t>(T.out) | reinterpret_cast<uintptr_t>(T.tmp)) & 15) == 0) {
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(T.tmp);
+            uint4 *d4 = reinterpret_cast<uint4 *>(T.out);
+            for (size_t i = tid; i < total / 16; i += NT) d4[i] = s4[i];
+            for (size_t i = total / 16 * 16 + tid; i < total; i += NT) T.out[i] = T.tmp[i];
+        } else {
+            for (size_t i = tid; i < total; i += NT) T.out[i] = T.tmp[i];
+        }
+    }
+    if (T.hist)
+        for (int i = tid; i < T.nstreams * 256; i += NT) T.hist[i] = S.hist[i >> 8][i & 255];
+    __syncthreads();
 }
 
 }  // namespace fdvb

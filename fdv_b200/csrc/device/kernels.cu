@@ -50,7 +50,8 @@ void launch_iframe(const void *planes, const void *tasks, int ntasks, int *ticke
 // search range allows it (up to 32); a range of 64 reads them from global
 // memory.  All units of one launch share the range.
 void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ticket, unsigned *err,
-                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st) {
+                   unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st,
+                   const FrameSync *fsync, const void *ctasks, int *fdone, int nu, int nunits) {
     static std::mutex mu;
     static bool attr[64][4] = {};
     int dev = 0;
@@ -58,7 +59,8 @@ void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ti
     const bool win = range <= 32;
     const int v = (win ? 1 : 0) + (learned ? 2 : 0);
     const size_t smem = win ? (size_t)kPWinOff + kPWinBytes : sizeof(PShared);
-    void (*const k[4])(const UnitDev *, const RowTask *, int, int *, unsigned *, unsigned long long) = {
+    void (*const k[4])(const UnitDev *, const RowTask *, int, int *, unsigned *, unsigned long long, const FrameSync *,
+                       const CompactTask *, int *, int, int) = {
         pframe_kernel<false, false>, pframe_kernel<true, false>, pframe_kernel<false, true>, pframe_kernel<true, true>};
     {
         std::lock_guard<std::mutex> lk(mu);
@@ -67,7 +69,8 @@ void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ti
             attr[dev][v] = true;
         }
     }
-    k[v]<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns);
+    k[v]<<<grid, PNT, smem, st>>>(units, rows, nrows, ticket, err, wait_ns, fsync,
+                                  static_cast<const CompactTask *>(ctasks), fdone, nu < 1 ? 1 : nu, nunits);
 }
 
 // The learned form's SKIP pre-analysis, one warp per macroblock of the P
@@ -322,7 +325,7 @@ extern "C" int fdvg_pframe_static(const uint8_t *cur, const uint8_t *near_ref, c
     if (!ok) return static_fail("descriptor upload failed");
     launch_refprep(base + o_prep, far_ref ? 2 : 1, w, h, B, st);
     launch_pframe(reinterpret_cast<const UnitDev *>(base + o_unit), reinterpret_cast<const RowTask *>(base + o_rows),
-                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, range, false, st);
+                  mbh, ticket, err, 4000000000ull, mbh < S.nsm ? mbh : S.nsm, range, false, st, nullptr, nullptr, nullptr, 1, 0);
     launch_deblock(base + o_db, 3, st);
     launch_compact(base + o_cmp, 1, err, st);
     if (cudaGetLastError() != cudaSuccess) return static_fail("kernel launch failed");

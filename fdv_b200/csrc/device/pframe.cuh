@@ -28,6 +28,7 @@
 //      chroma, reconstruction and the symbols of the chosen mode.
 #include "common.cuh"
 #include "engine_dev.cuh"
+#include "frame_ops.cuh"
 #include "inter.cuh"
 #include "intra.cuh"
 #include "post.cuh"
@@ -88,7 +89,13 @@ struct PShared {
     int rok[2];                  // row_ok
     int amz[2];                  // the above macroblock's mode is not SKIP
     int pok;                     // the row's first reference wait succeeded
-    PostScratch post;            // the reference output stage (post.cuh)
+    // the reference output stage (post.cuh) while a row runs; a finished
+    // frame's compaction (FrameSync launches) after the row's last tiles
+    union {
+        PostScratch post;
+        CompactScratch<512> cmp;
+    };
+    int lastrow;                 // this block finished the frame's last row
 };
 
 __device__ __forceinline__ uint8_t ldcg8(const uint8_t *p) { return __ldcg(p); }
@@ -242,10 +249,16 @@ constexpr int kLearnLd = 4;
 
 // LRN: the learned-proposal form (units carry hints); the plain instance has
 // none of its code.
+//
+// fsync (may be NULL): per frame of the launch (units j = frame * nu + i);
+// the block that finishes unit j's last row compacts ctasks[j], and the last
+// unit of a frame sets the frame's host-mapped ready word (FrameSync).  fdone:
+// per unit j its finished rows, then per frame its compacted units.
 template <bool WIN, bool LRN>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
-              int *ticket, unsigned *err, unsigned long long wait_ns) {
+              int *ticket, unsigned *err, unsigned long long wait_ns, const FrameSync *__restrict__ fsync,
+              const CompactTask *__restrict__ ctasks, int *fdone, int nu, int nunits) {
     extern __shared__ __align__(128) uint8_t psmem[];
     PShared &S = *reinterpret_cast<PShared *>(psmem);
     uint8_t *win = psmem + kPWinOff;
@@ -892,6 +905,29 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         // the row's last tiles (its last macroblock is finished)
         if (U.post_prog && mbx == mbw && tid >= kPostT0) post_upto(mbw, true);
         __syncthreads();
+        if (fsync) {
+            // the frame's rows done: the block that finishes the last one
+            // compacts the frame (every row's slots were published by the
+            // fence before its count) and tells the host
+            const int j = rows[t].unit, fk = j / nu;
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                S.lastrow = atomicAdd(&fdone[j], 1) + 1 == U.mbh;
+                __threadfence();
+            }
+            __syncthreads();
+            if (S.lastrow) {
+                compact_block<PNT>(ctasks[j], err, S.cmp, tid);
+                __threadfence_system();
+                __syncthreads();
+                if (tid == 0 && atomicAdd(&fdone[nunits + fk], 1) + 1 == nu) {
+                    __threadfence_system();
+                    *(volatile unsigned *)fsync[fk].ready = fsync[fk].ready_val;
+                }
+            }
+            __syncthreads();
+        }
     }
 }
 

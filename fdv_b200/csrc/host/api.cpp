@@ -410,22 +410,12 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     auto key_at = [&](int f) { return f == 0 || (keyint > 0 && f % keyint == 0) ? 1 : 0; };
     std::deque<int> types;    // frame types in flight, oldest first
     int rc = 0;
-    size_t prev = 0;          // frames of the previous submissions (in flight, not yet coded)
-    int ahead = -1;           // the key frame the lookahead was armed with
     // frames in one submission from f: a key frame alone, else a run of
-    // P-frames.  The host codes a run while the GPU analyses the next one, so
-    // the sequence's last run is coded after the GPU has finished: the final
-    // stretch goes in halving runs (each coded while the GPU runs the next,
-    // smaller one), down to a short last run.
+    // P-frames
     auto run_len = [&](int f) {
         int K = 1;
         if (!key_at(f))
             while (K < kmax && f + K < nframes && !key_at(f + K)) ++K;
-        constexpr int kTail = 6;
-        if (f + K == nframes) {
-            const int rem = nframes - f;
-            K = std::max(std::min(rem, kTail), (rem + 1) / 2);
-        }
         return K;
     };
     auto submit_at = [&](int f, int K) -> int {
@@ -452,7 +442,6 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
                     kplanes[3 * b + 2] = fv + (size_t)(Y0[b] / 2) * cw;
                 }
                 if (fdvb_engine_key_lookahead(E, kplanes.data(), qps.data()) != 0) { set_engine_err(); return -1; }
-                ahead = f2;
             }
         }
         if (fdvb_engine_submit_batch(E, K, planes.data(), intra.data(), qps.data(), nullptr, nullptr) != 0) {
@@ -463,34 +452,25 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         return 0;
     };
     // the caller's frames stay valid for the whole call: pinned ones are
-    // copied to the GPU without staging
+    // copied to the GPU without staging; P-frames are streamed out of their
+    // launches, so the host codes each frame while the GPU goes on
     fdvb_engine_direct_upload(E, 1);
+    fdvb_engine_stream_frames(E, 1);
     for (int f = 0; rc == 0;) {
-        size_t now = 0;
-        if (f < nframes) {
-            const bool analysed = f == ahead;   // a key frame whose analysis ran in an earlier launch
+        // keep the engine busy: whole runs, up to two runs' worth of frames in flight
+        while (f < nframes) {
             const int K = run_len(f);
+            if ((int)types.size() + K > 2 * kmax) break;
             if (submit_at(f, K) != 0) { rc = -1; break; }
-            now += (size_t)K;
             f += K;
-            // such a key frame keeps the GPU busy for a moment only: the run
-            // after it goes in now too, so the GPU has work while the host
-            // codes the previous run (within the frames the engine holds)
-            if (analysed && f < nframes && !key_at(f)) {
-                const int K2 = std::min(run_len(f), 2 * kmax - (int)(prev + now));
-                if (K2 >= 1) {
-                    if (submit_at(f, K2) != 0) { rc = -1; break; }
-                    now += (size_t)K2;
-                    f += K2;
-                }
-            }
         }
-        // code the previous batch while the GPU runs this one: collect its
-        // frames (their streams stay in their slots until the next
-        // submission), then every band codes them in order as one task
+        if (rc != 0 || types.empty()) break;
+        // the oldest frame as soon as it is ready, and any later ones ready
+        // by then; every band codes them in order as one task (their streams
+        // stay in their slots until the next submission)
         std::vector<int> btype;
         std::vector<std::vector<fdvb_streams>> bst(nb);
-        for (size_t c = 0; c < prev && rc == 0; ++c) {
+        do {
             const int ti = types.front();
             types.pop_front();
             if (fdvb_engine_collect(E) != 0) { set_engine_err(); rc = -1; break; }
@@ -501,7 +481,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
                     if (!s) { set_err("no streams for a collected frame"); rc = -1; break; }
                     bst[b].push_back(*s);
                 }
-        }
+        } while (rc == 0 && !types.empty() && btype.size() < 16 && fdvb_engine_ready(E) == 1);
         if (rc == 0 && !btype.empty()) {
             std::fill(urc.begin(), urc.end(), 0);
             pool.run(nb, [&](int u) {
@@ -518,8 +498,6 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             for (int r : urc)
                 if (r) { set_err(r == -2 ? "a band's stream outgrew the tiled encoder's capacity" : "entropy coding failed"); rc = -1; }
         }
-        if (now == 0) break;
-        prev = now;
     }
     while (!types.empty()) {
         types.pop_front();
@@ -527,6 +505,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     }
     fdvb_engine_key_lookahead(E, nullptr, nullptr);   // the next call's frames are other buffers
     fdvb_engine_direct_upload(E, 0);
+    fdvb_engine_stream_frames(E, 0);
     if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
     else fdvb_engine_destroy(E);
     return rc;

@@ -30,6 +30,8 @@ int fdvb_engine_set_refs(fdvb_engine *E, int unit, const uint8_t *near_i420, con
 const char *fdvb_engine_error(void);
 void fdvb_engine_src_on_device(fdvb_engine *E, int on);
 void fdvb_engine_direct_upload(fdvb_engine *E, int on);
+void fdvb_engine_stream_frames(fdvb_engine *E, int on);
+int fdvb_engine_ready(fdvb_engine *E);
 void fdvb_engine_stats(const fdvb_engine *E, double *step_ms, double *pk_ms, long long *pk_n, double *ik_ms,
                        long long *ik_n, long long *launches, long long *steps, long long *d2h_bytes);
 void fdvb_engine_stats_reset(fdvb_engine *E);
