@@ -1132,7 +1132,7 @@ extern "C" int fdvb_engine_collect(fdvb_engine *E) {
     if (!early) CK(cudaEventSynchronize(SL.ev[5]));
     E->steps += 1;
     if (SL.batch) {
-        // the batch's first frame carries its timing: whole step, and the
+        // the batch's last frame carries its timing: whole step, and the
         // P-frame kernel time counted per P-frame
         float ms = 0;
         cudaEventElapsedTime(&ms, SL.ev[0], SL.ev[5]);

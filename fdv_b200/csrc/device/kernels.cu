@@ -53,15 +53,17 @@ void launch_pframe(const UnitDev *units, const RowTask *rows, int nrows, int *ti
                    unsigned long long wait_ns, int grid, int range, bool learned, cudaStream_t st,
                    const FrameSync *fsync, const void *ctasks, int *fdone, int nu, int nunits) {
     static std::mutex mu;
-    static bool attr[64][4] = {};
+    static bool attr[64][8] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const bool win = range <= 32;
-    const int v = (win ? 1 : 0) + (learned ? 2 : 0);
+    const int v = (win ? 1 : 0) + (learned ? 2 : 0) + (fsync ? 4 : 0);
     const size_t smem = win ? (size_t)kPWinOff + kPWinBytes : sizeof(PShared);
-    void (*const k[4])(const UnitDev *, const RowTask *, int, int *, unsigned *, unsigned long long, const FrameSync *,
+    void (*const k[8])(const UnitDev *, const RowTask *, int, int *, unsigned *, unsigned long long, const FrameSync *,
                        const CompactTask *, int *, int, int) = {
-        pframe_kernel<false, false>, pframe_kernel<true, false>, pframe_kernel<false, true>, pframe_kernel<true, true>};
+        pframe_kernel<false, false, false>, pframe_kernel<true, false, false>, pframe_kernel<false, true, false>,
+        pframe_kernel<true, true, false>,   pframe_kernel<false, false, true>,  pframe_kernel<true, false, true>,
+        pframe_kernel<false, true, true>,   pframe_kernel<true, true, true>};
     {
         std::lock_guard<std::mutex> lk(mu);
         if (dev >= 0 && dev < 64 && !attr[dev][v]) {

@@ -250,11 +250,13 @@ constexpr int kLearnLd = 4;
 // LRN: the learned-proposal form (units carry hints); the plain instance has
 // none of its code.
 //
-// fsync (may be NULL): per frame of the launch (units j = frame * nu + i);
-// the block that finishes unit j's last row compacts ctasks[j], and the last
-// unit of a frame sets the frame's host-mapped ready word (FrameSync).  fdone:
-// per unit j its finished rows, then per frame its compacted units.
-template <bool WIN, bool LRN>
+// FS: the streaming form.  fsync holds per frame of the launch (units j =
+// frame * nu + i) its host-mapped ready word; the block that finishes unit
+// j's last row compacts ctasks[j], and the last unit of a frame sets the
+// frame's ready word (FrameSync).  fdone: per unit j its finished rows, then
+// per frame its compacted units.  The other instances ignore the three and
+// carry none of that code.
+template <bool WIN, bool LRN, bool FS>
 __global__ void __launch_bounds__(PNT, 1)
 pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ rows, int nrows,
               int *ticket, unsigned *err, unsigned long long wait_ns, const FrameSync *__restrict__ fsync,
@@ -905,7 +907,7 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
         // the row's last tiles (its last macroblock is finished)
         if (U.post_prog && mbx == mbw && tid >= kPostT0) post_upto(mbw, true);
         __syncthreads();
-        if (fsync) {
+        if (FS) {
             // the frame's rows done: the block that finishes the last one
             // compacts the frame (every row's slots were published by the
             // fence before its count) and tells the host
