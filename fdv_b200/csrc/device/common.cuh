@@ -59,6 +59,25 @@ __device__ __forceinline__ int leb_write(uint8_t *b, uint32_t u) {
     b[n++] = (uint8_t)u;
     return n;
 }
+// Exclusive prefix over the lanes selected by `mask` below this one, and the
+// total over them, of v in 0..7 (a level's byte count), from three ballots:
+// no chain of shuffles.
+__device__ __forceinline__ int ballot_prefix(int v, int lane, unsigned mask, int &total) {
+    const unsigned b0 = __ballot_sync(0xffffffffu, v & 1) & mask, b1 = __ballot_sync(0xffffffffu, v & 2) & mask,
+                   b2 = __ballot_sync(0xffffffffu, v & 4) & mask;
+    const unsigned lt = (1u << lane) - 1u;
+    total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+    return __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+}
+// The len-byte LEB128 form of u (len = leb_size(u), or 0: nothing) at dst,
+// without lane-dependent branches for len <= 3 (every 16-bit level): the
+// stores a lane does not need go to its own byte of junk.
+__device__ __forceinline__ void leb_put(uint8_t *dst, uint8_t *junk, uint32_t u, int len) {
+    *(len > 0 ? dst : junk) = (uint8_t)(len > 1 ? (u | 0x80u) : u);
+    *(len > 1 ? dst + 1 : junk) = (uint8_t)(len > 2 ? ((u >> 7) | 0x80u) : (u >> 7));
+    *(len > 2 ? dst + 2 : junk) = (uint8_t)(len > 3 ? ((u >> 14) | 0x80u) : (u >> 14));
+    if (__any_sync(0xffffffffu, len > 3) && len > 3) leb_write(dst, u);
+}
 __device__ __forceinline__ int pos_class(int idx) {
     int i = idx >> 2, j = idx & 3;
     if (!(i & 1) && !(j & 1)) return 0;
@@ -71,13 +90,23 @@ __device__ __forceinline__ double rd_cost(double D, double lambda, int bits) {
 }
 
 // ------------------------------------------------------------ 4x4 core --
+// Output m (0..3) of the 1-D forward / inverse butterflies.  Lanes of a warp
+// take different m, so the outputs are selected arithmetically: a chain of
+// conditionals on m compiles to divergent branches, several times slower.
+//   forward: m 0 a0 + a1, 1 2 a3 + a2, 2 a0 - a1, 3 a3 - 2 a2
+//   inverse: m 0 z0 + z3, 1 z1 + z2, 2 z1 - z2, 3 z0 - z3
 __device__ __forceinline__ int fwd1(int x0, int x1, int x2, int x3, int m) {
-    int a0 = x0 + x3, a3 = x0 - x3, a1 = x1 + x2, a2 = x1 - x2;
-    return m == 0 ? a0 + a1 : (m == 1 ? a3 * 2 + a2 : (m == 2 ? a0 - a1 : a3 - a2 * 2));
+    const int a0 = x0 + x3, a3 = x0 - x3, a1 = x1 + x2, a2 = x1 - x2;
+    const int sb = (m >> 1) & 1;
+    const int ev = a0 + ((a1 ^ -sb) + sb);
+    const int od = a3 * (2 - sb) + (((a2 * (1 + sb)) ^ -sb) + sb);
+    return ev + ((od - ev) & -(m & 1));
 }
 __device__ __forceinline__ int inv1(int d0, int d1, int d2, int d3, int m) {
-    int z0 = d0 + d2, z1 = d0 - d2, z2 = (d1 >> 1) - d3, z3 = d1 + (d3 >> 1);
-    return m == 0 ? z0 + z3 : (m == 1 ? z1 + z2 : (m == 2 ? z1 - z2 : z0 - z3));
+    const int z0 = d0 + d2, z1 = d0 - d2, z2 = (d1 >> 1) - d3, z3 = d1 + (d3 >> 1);
+    const int s0 = ((m + 1) >> 1) & 1, sg = (m >> 1) & 1;
+    const int A = z0 + ((z1 - z0) & -s0), B = z3 + ((z2 - z3) & -s0);
+    return A + ((B ^ -sg) + sg);
 }
 // Whole-block inverse on one thread (used by RDOQ candidate lanes).
 __device__ __forceinline__ void idct4_thread(const int d[16], int r[16]) {

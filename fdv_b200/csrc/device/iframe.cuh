@@ -277,6 +277,12 @@ __device__ __forceinline__ bool cell_done(int x, int y, int bx, int by) {
     if (x >= cx0 + 64) return false;
     return zidx4((x - cx0) >> 2, (y - cy0) >> 2) < zidx4((bx - cx0) >> 2, (by - cy0) >> 2);
 }
+// The allowed 4x4 modes as a mask (bit m: mode m), the same as mode_ok4:
+// lanes testing different modes take no divergent branch.
+__device__ __forceinline__ unsigned mode_mask4(int ht, int htr, int hl, int htl) {
+    const unsigned a = ht ? 1u : 0u, l = hl ? 1u : 0u, tr = (ht && htr) ? 1u : 0u, d = (ht && hl && htl) ? 1u : 0u;
+    return 1u | (a << 1) | (l << 2) | (l << 8) | (tr << 3) | (tr << 7) | (d * 0x70u);
+}
 __device__ __forceinline__ bool mode_ok4(int m, int ht, int htr, int hl, int htl) {
     switch (m) {
     case 0: return true;
@@ -309,18 +315,20 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     // neighbours (gather_neighbors fdv.h:3689-3706), one copy per screening
     // warp: N = L(3..0) T(-1) T(0..7) DC (pred4_table.h)
     if (w < 3) {
+        // one predicated load per lane -- lanes 0-7 the row above (4-7
+        // repeat T(3) without the above-right samples), 8-11 the column to
+        // the left, 12 the corner -- and one store at the lane's place in N:
+        // lane-dependent if/else chains would diverge, several times slower
         int *N = C.N4[w];
-        int v = 0;
-        if (lane < 8) v = ht ? ((lane < 4 || htr) ? TL(C, ty - 1, tx + lane) : TL(C, ty - 1, tx + 3)) : 0;
-        else if (lane < 12) v = hl ? TL(C, ty + lane - 8, tx - 1) : 0;
-        else if (lane == 12) v = htl ? TL(C, ty - 1, tx - 1) : 128;
+        const int ry = lane < 8 ? ty - 1 : (lane < 12 ? ty + lane - 8 : ty - 1);
+        const int rx = lane < 8 ? tx + ((lane < 4 || htr) ? lane : 3) : tx - 1;
+        const bool ok = lane < 8 ? ht : (lane < 12 ? hl : (lane == 12 && htl));
+        const int v = ok ? (int)TL(C, ry, rx) : (lane == 12 ? 128 : 0);
         const int sT = __reduce_add_sync(FDVB_FULL, lane < 4 ? v : 0);
         const int sL = __reduce_add_sync(FDVB_FULL, (lane >= 8 && lane < 12) ? v : 0);
-        if (lane < 8) N[5 + lane] = v;
-        else if (lane < 12) N[3 - (lane - 8)] = v;
-        else if (lane == 12) N[4] = v;
-        else if (lane == 13)
-            N[13] = (ht && hl) ? (sT + sL + 4) >> 3 : (ht ? (sT + 2) >> 2 : (hl ? (sL + 2) >> 2 : 128));
+        const int dc = (ht && hl) ? (sT + sL + 4) >> 3 : (ht ? (sT + 2) >> 2 : (hl ? (sL + 2) >> 2 : 128));
+        const int ni = lane < 8 ? 5 + lane : (lane < 12 ? 11 - lane : (lane == 12 ? 4 : 13));
+        if (lane < 14) N[ni] = lane == 13 ? dc : v;
         __syncwarp();
         // predictions and SATD (fdv.h:3803-3823): 8 lanes per mode, modes
         // 0-3 on warp 0, 4-7 on warp 1, 8 on warp 2; a lane holds two
@@ -329,10 +337,8 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
         const int q = lane & 7, i = q >> 1, h = q & 1, x0 = 2 * h;
         const uint16_t *op = &C.p4[m * 16 + i * 4 + x0];
         const int p0 = p4_eval(op[0], N), p1 = p4_eval(op[1], N);
-        if (w < 2 || lane < 8) {
-            C.cp[m][i * 4 + x0] = (uint8_t)p0;
-            C.cp[m][i * 4 + x0 + 1] = (uint8_t)p1;
-        }
+        C.cp[m][i * 4 + x0] = (uint8_t)p0;       // warp 2's lanes 8-31 repeat lanes 0-7
+        C.cp[m][i * 4 + x0 + 1] = (uint8_t)p1;
         const int d0 = C.src[(ty + i) * 64 + tx + x0] - p0, d1 = C.src[(ty + i) * 64 + tx + x0 + 1] - p1;
         // row transform: columns (0, 1) on h = 0, (2, 3) on h = 1
         const int s0 = d0 + d1, s1 = d0 - d1;
@@ -353,7 +359,7 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
         sa += __shfl_xor_sync(FDVB_FULL, sa, 1);
         sa += __shfl_xor_sync(FDVB_FULL, sa, 2);
         sa += __shfl_xor_sync(FDVB_FULL, sa, 4);
-        if (q == 0 && (w < 2 || lane < 8)) C.csat[m] = sa;
+        C.csat[m] = sa;                           // every lane of the mode's group holds the sum
     }
     cbar();
     long long tp = prof_t0(c.prof, t);
@@ -365,8 +371,8 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
         // minimum, then the first minimum of the rest in the order left by the
         // swap (the first candidate moved to the winner's place); the prune
         // keeps the second only if its SATD is within 5/4 of the first's.
-        const bool vm = lane < 9 && mode_ok4(lane, ht, htr, hl, htl);
-        const unsigned vmask = __ballot_sync(FDVB_FULL, vm);
+        const unsigned vmask = mode_mask4(ht, htr, hl, htl);
+        const bool vm = (vmask >> lane) & 1u;
         const unsigned sv = vm ? (unsigned)C.csat[lane] : 0u;
         const unsigned k0 = __reduce_min_sync(FDVB_FULL, vm ? (sv << 4) | lane : 0xffffffffu);
         const int m0 = k0 & 15, s0 = k0 >> 4;
@@ -433,7 +439,10 @@ __device__ double leaf4(CCtx &c, int bx, int by, ISink *tgt) {
     // (it reaches the barrier after that screen before the next trials
     // rewrite C.fin)
     const Blk4 &F = C.fin[fsel];
-    if (lane < 16) TL(C, ty + (lane >> 2), tx + (lane & 3)) = C.frec[fsel][lane];
+    {
+        const int l = lane & 15;                  // lanes 16-31 repeat lanes 0-15
+        TL(C, ty + (l >> 2), tx + (l & 3)) = C.frec[fsel][l];
+    }
     __syncwarp();
     if (t == 96) {
         cs_put1(&tgt->c, CS_N, (uint8_t)F.count, c.err);

@@ -78,16 +78,15 @@ __host__ __device__ constexpr P4Tab make_p4tab() {
     return t;
 }
 
-// One predicted sample from its packed entry.
+// One predicted sample from its packed entry: (a + f b + wc c + s) >> s with
+// the form's weights copy (f 0, wc 0, s 0), mean2 (1, 0, 1), tap121 (2, 1, 2),
+// tap13 (3, 0, 2) -- arithmetic in the form f, so that lanes evaluating
+// different forms take no divergent branch.
 __host__ __device__ __forceinline__ int p4_eval(unsigned op, const int *N) {
     const int f = (int)(op >> 12);
     const int a = N[op & 15], b = N[(op >> 4) & 15], c = N[(op >> 8) & 15];
-    // (a + wb b + wc c + r) >> s: copy (0,0,0,0), mean2 (1,0,1,1), tap121 (2,1,2,2), tap13 (3,0,2,2)
-    const int wb = f == P4_COPY ? 0 : (f == P4_TAP121 ? 2 : (f == P4_TAP13 ? 3 : 1));
-    const int wc = f == P4_TAP121 ? 1 : 0;
-    const int r = f == P4_COPY ? 0 : (f == P4_MEAN2 ? 1 : 2);
-    const int s = f == P4_COPY ? 0 : (f == P4_MEAN2 ? 1 : 2);
-    return (a + wb * b + wc * c + r) >> s;
+    const int wc = (f >> 1) & ~f & 1, s = f - ((f >> 1) & f & 1);
+    return (a + f * b + wc * c + s) >> s;
 }
 
 // The DC value (pred4_px's default case) from Tn = T(-1..7), Ln = L(-1..3).

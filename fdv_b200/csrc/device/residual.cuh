@@ -95,24 +95,29 @@ __device__ __forceinline__ int scan16(int v, int lane) {
 // the RDOQ truncation candidate L = lane - 1 in parallel, their rates come
 // from a suffix sum over the zigzag scan.  The reference's sequential
 // selection (bestJ < 0.0 || J < bestJ, in the order L = last .. -1) is a
-// butterfly minimum when no cost is negative and is replayed step by step
+// warp minimum when no cost is negative and is replayed step by step
 // otherwise (a rate can go negative).  Level bytes are packed in
-// parallel from a prefix sum of their LEB lengths.  Writes rec (stride rs).
+// parallel at offsets counted from ballots of their LEB lengths.  Writes rec
+// (stride rs).
 // Not inlined: the key-frame quadtree reaches it from many inlined node
 // levels, and one copy of its code keeps the kernels' instruction footprint
 // small (key frame 26.7 -> 22.6 ms on the hd720 bands).
 __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
                             uint8_t *rec, int rs, const QP4 &Q, double lambda, bool rdoq,
                             Blk4 *out, Blk4Scratch *sc, int lane) {
+    // Lanes 16-31 compute the same values as lanes 0-15 (every shuffle reads
+    // lanes 0-15), so their stores repeat those of lanes 0-15 and no store
+    // needs a lane-dependent branch.
     const int l = lane & 15, i = l >> 2, j = l & 3;
     const int cv = cur[i * cs + j], pv = pred[i * ps + j];
     const int res = cv - pv;
     int x0 = __shfl_sync(FDVB_FULL, res, i * 4 + 0), x1 = __shfl_sync(FDVB_FULL, res, i * 4 + 1);
     int x2 = __shfl_sync(FDVB_FULL, res, i * 4 + 2), x3 = __shfl_sync(FDVB_FULL, res, i * 4 + 3);
-    int t = fwd1(x0, x1, x2, x3, j);
+    const int t = fwd1(x0, x1, x2, x3, j);
     int y0 = __shfl_sync(FDVB_FULL, t, 0 * 4 + j), y1 = __shfl_sync(FDVB_FULL, t, 1 * 4 + j);
     int y2 = __shfl_sync(FDVB_FULL, t, 2 * 4 + j), y3 = __shfl_sync(FDVB_FULL, t, 3 * 4 + j);
     const int coef = fwd1(y0, y1, y2, y3, i);
+    const int dql = Q.dq[l];
     int lev;
     {
         int sign = coef < 0 ? -1 : 1;
@@ -125,29 +130,30 @@ __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8
     unsigned nzm = __ballot_sync(FDVB_FULL, lane < 16 && levz != 0);
     int last = nzm ? 31 - __clz(nzm) : -1;
     if (rdoq && last >= 0) {
+        // candidate c = lane (0..16): the levels at zigzag positions < c
+        // kept, the rate bits0 less 8 bits per byte of the dropped ones
         const uint32_t z = zz_enc(levz);
         const bool in = lane < 16 && kz <= last;
         const int bits0 = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
-        const int pre = scan16(in ? 8 * leb_size(z) : 0, lane);
-        const int tot = __shfl_sync(FDVB_FULL, pre, 15);
-        const int L = lane - 1;
-        int preL = __shfl_sync(FDVB_FULL, pre, L < 0 ? 0 : (L & 31));
-        if (L < 0) preL = 0;
-        const int bitsL = bits0 - (tot - preL);
-        const unsigned vmask = 1u | (nzm << 1);          // candidate c = L + 1
+        int tlen;
+        const int ex = ballot_prefix(in ? leb_size(z) : 0, lane, FDVB_FULL, tlen);
+        const int bitsL = bits0 - 8 * (tlen - ex);
+        const unsigned vmask = 1u | (nzm << 1);
         const bool valid = lane <= 16 && ((vmask >> lane) & 1u);
-        if (lane < 16) { sc->res[l] = res; sc->lev[l] = lev; }
+        sc->res[l] = res;
+        sc->lev[l] = lev * dql;          // the dequantised level
         __syncwarp();
-        double J = 0.0;
-        if (valid) {
+        double J;
+        {
+            const int L = lane - 1;
             int d[16], r[16];
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = (izz4(p) <= L ? sc->lev[p] : 0) * Q.dq[p];
+            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? sc->lev[p] : 0;
             idct4_thread(d, r);
             int D = 0;
 #pragma unroll
             for (int p = 0; p < 16; ++p) { int e = sc->res[p] - r[p]; D += e * e; }
-            J = rd_cost((double)D, lambda, bitsL);
+            J = valid ? rd_cost((double)D, lambda, bitsL) : 0.0;
         }
         int bestL = last;
         if (!__any_sync(FDVB_FULL, valid && J < 0.0)) {
@@ -160,7 +166,7 @@ __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8
             const unsigned mh = __reduce_min_sync(FDVB_FULL, hi);
             const unsigned lo = (valid && hi == mh) ? (unsigned)jb : 0xffffffffu;
             const unsigned ml = __reduce_min_sync(FDVB_FULL, lo);
-            const unsigned bc = __reduce_max_sync(FDVB_FULL, (valid && hi == mh && lo == ml) ? (unsigned)lane + 1u : 0u);
+            const unsigned bc = 32u - __clz(__ballot_sync(FDVB_FULL, valid && hi == mh && lo == ml));
             bestL = (int)bc - 2;
         } else {
             double bestJ = -1.0;
@@ -178,7 +184,7 @@ __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8
         __syncwarp();
     }
     // reconstruct from the final levels
-    const int dq = (lane < 16 ? lev : 0) * Q.dq[l];
+    const int dq = (lane < 16 ? lev : 0) * dql;
     int d0 = __shfl_sync(FDVB_FULL, dq, i * 4 + 0), d1 = __shfl_sync(FDVB_FULL, dq, i * 4 + 1);
     int d2 = __shfl_sync(FDVB_FULL, dq, i * 4 + 2), d3 = __shfl_sync(FDVB_FULL, dq, i * 4 + 3);
     int u = inv1(d0, d1, d2, d3, j);
@@ -186,23 +192,21 @@ __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8
     int e2 = __shfl_sync(FDVB_FULL, u, 2 * 4 + j), e3 = __shfl_sync(FDVB_FULL, u, 3 * 4 + j);
     const int rr = (int16_t)((inv1(e0, e1, e2, e3, i) + 32) >> 6);
     const int r = clipb(pv + rr);
-    if (lane < 16) rec[i * rs + j] = (uint8_t)r;
+    rec[i * rs + j] = (uint8_t)r;
     const int dd = cv - r;
-    const int ssd = __reduce_add_sync(FDVB_FULL, lane < 16 ? dd * dd : 0);
     // rate and level bytes, zigzag order
     const uint32_t z = zz_enc(levz);
     const bool in = lane < 16 && kz <= last;
-    const int bits = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
     const int len = in ? leb_size(z) : 0;
-    const int end = scan16(len, lane);
-    if (in) leb_write(out->bytes + (end - len), z);
-    const int nbytes = __shfl_sync(FDVB_FULL, end, 15);
-    if (lane == 0) {
-        out->count = last + 1;
-        out->nbytes = nbytes;
-        out->ssd = ssd;
-        out->bits = bits;
-    }
+    int nbytes;
+    const int ex = ballot_prefix(len, lane, FDVB_FULL, nbytes);
+    leb_put(out->bytes + ex, reinterpret_cast<uint8_t *>(sc->res) + lane, z, len);
+    const int ssd = __reduce_add_sync(FDVB_FULL, lane < 16 ? dd * dd : 0);
+    const int bits = bits_val((uint32_t)(last + 1)) + __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
+    out->count = last + 1;               // warp-uniform values
+    out->nbytes = nbytes;
+    out->ssd = ssd;
+    out->bits = bits;
     __syncwarp();
 }
 
@@ -227,6 +231,7 @@ __device__ void warp_block4x2(const uint8_t *cur0, const uint8_t *cur1, int cs, 
                               const uint8_t *pred1, int ps, uint8_t *rec0, uint8_t *rec1, int rs, const QP4 &Q,
                               double lambda, bool rdoq, Blk4 *out0, Blk4 *out1, Blk4Scratch *sc, int lane) {
     const int h = lane >> 4, hb = lane & 16, l = lane & 15, i = l >> 2, j = l & 3;
+    const unsigned hmask = h ? 0xffff0000u : 0x0000ffffu;
     const uint8_t *cur = h ? cur1 : cur0, *pred = h ? pred1 : pred0;
     const int cv = cur[i * cs + j], pv = pred[i * ps + j];
     const int res = cv - pv;
@@ -259,28 +264,26 @@ __device__ void warp_block4x2(const uint8_t *cur0, const uint8_t *cur1, int cs, 
         const uint32_t z = zz_enc(levz);
         const bool in = l <= last;
         const int bits0 = bits_val((uint32_t)(last + 1)) + half_sum(in ? bits_val(z) : 0, lane);
-        const int pre = scan16(in ? 8 * leb_size(z) : 0, lane);
-        const int tot = __shfl_sync(FDVB_FULL, pre, hb + 15);
+        int tlen;
+        const int ex = ballot_prefix(in ? leb_size(z) : 0, lane, hmask, tlen);
         const int L = l - 1;
-        int preL = __shfl_sync(FDVB_FULL, pre, hb + (L < 0 ? 0 : L));
-        if (L < 0) preL = 0;
-        const int bitsL = bits0 - (tot - preL);
+        const int bitsL = bits0 - 8 * (tlen - ex);    // the bytes of positions >= l dropped
         const unsigned vmask = 1u | (nzm << 1);           // candidate c = L + 1, c = 0..16
         const bool active = last >= 0;                      // this half truncates at all
         const bool valid = active && ((vmask >> l) & 1u);
         sc[h].res[l] = res;
-        sc[h].lev[l] = lev;
+        sc[h].lev[l] = lev * Q.dq[l];      // the dequantised level
         __syncwarp();
-        double J = 0.0;
-        if (valid) {
+        double J;
+        {   // every lane (no divergent branch); only valid candidates count
             int d[16], r[16];
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = (izz4(p) <= L ? sc[h].lev[p] : 0) * Q.dq[p];
+            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? sc[h].lev[p] : 0;
             idct4_thread(d, r);
             int D = 0;
 #pragma unroll
             for (int p = 0; p < 16; ++p) { const int e = sc[h].res[p] - r[p]; D += e * e; }
-            J = rd_cost((double)D, lambda, bitsL);
+            J = valid ? rd_cost((double)D, lambda, bitsL) : 0.0;
         }
         // candidate L = 15: every level kept
         const bool v16 = active && ((vmask >> 16) & 1u);
@@ -334,16 +337,14 @@ __device__ void warp_block4x2(const uint8_t *cur0, const uint8_t *cur1, int cs, 
     const bool in = l <= last;
     const int bits = bits_val((uint32_t)(last + 1)) + half_sum(in ? bits_val(z) : 0, lane);
     const int len = in ? leb_size(z) : 0;
-    const int end = scan16(len, lane);
+    int nbytes;
+    const int ex = ballot_prefix(len, lane, hmask, nbytes);
     Blk4 *out = h ? out1 : out0;
-    if (in) leb_write(out->bytes + (end - len), z);
-    const int nbytes = __shfl_sync(FDVB_FULL, end, hb + 15);
-    if (l == 0) {
-        out->count = last + 1;
-        out->nbytes = nbytes;
-        out->ssd = ssd;
-        out->bits = bits;
-    }
+    leb_put(out->bytes + ex, reinterpret_cast<uint8_t *>(sc[h].res) + l, z, len);
+    out->count = last + 1;               // uniform over the half
+    out->nbytes = nbytes;
+    out->ssd = ssd;
+    out->bits = bits;
     __syncwarp();
 }
 
@@ -525,18 +526,17 @@ __device__ void warp_region8(const uint8_t *cur, int cs, const uint8_t *pred, in
     const bool in0 = lane <= last, in1 = lane + 32 <= last;
     const int bsum = __reduce_add_sync(FDVB_FULL, (in0 ? bits_val(z0) : 0) + (in1 ? bits_val(z1) : 0));
     const int len0 = in0 ? leb_size(z0) : 0, len1 = in1 ? leb_size(z1) : 0;
-    const int end0 = warp_incl_scan(len0, lane);
-    const int tot0 = __shfl_sync(FDVB_FULL, end0, 31);
-    const int end1 = tot0 + warp_incl_scan(len1, lane);
-    if (in0) leb_write(out->bytes + end0 - len0, z0);
-    if (in1) leb_write(out->bytes + end1 - len1, z1);
-    const int nbytes = __shfl_sync(FDVB_FULL, end1, 31);
-    if (lane == 0) {
-        out->count = last + 1;
-        out->nbytes = nbytes;
-        out->bits = kBitsFlag + bits_val((uint32_t)(last + 1)) + bsum;
-        out->ssd = ssd;
-    }
+    int tot0, tot1;
+    const int ex0 = ballot_prefix(len0, lane, FDVB_FULL, tot0);
+    const int ex1 = tot0 + ballot_prefix(len1, lane, FDVB_FULL, tot1);
+    // every lane has read its levels (the ballots above): sc->L is junk now
+    uint8_t *const junk = reinterpret_cast<uint8_t *>(sc->L);
+    leb_put(out->bytes + ex0, junk + lane, z0, len0);
+    leb_put(out->bytes + ex1, junk + 32 + lane, z1, len1);
+    out->count = last + 1;               // warp-uniform values
+    out->nbytes = tot0 + tot1;
+    out->bits = kBitsFlag + bits_val((uint32_t)(last + 1)) + bsum;
+    out->ssd = ssd;
     __syncwarp();
 }
 
