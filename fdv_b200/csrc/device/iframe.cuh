@@ -219,47 +219,71 @@ __device__ void isink_put(ISink *s, int k, uint8_t v, unsigned *err) {
     if (s->slen[k] + 1 > s->scap[k]) { atomicOr(err, kErrSlotOverflow); return; }
     s->sbuf[k][s->slen[k]++] = v;
 }
-// dst += src, by the chain (lengths updated after a barrier).
-__device__ void chain_isink_append(ISink *dst, const ISink *src, unsigned *err) {
-    const int t = threadIdx.x;
-    for (int k = 0; k < IS_NS; ++k) {
-        const int n = src->slen[k], b = dst->slen[k];
-        if (b + n > dst->scap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        for (int i = t; i < n; i += kChainNT) dst->sbuf[k][b + i] = src->sbuf[k][i];
+// Copy n bytes from src to dst by the 32 lanes of a warp, four loads in
+// flight per lane.
+__device__ __forceinline__ void warp_copy_bytes(uint8_t *dst, const uint8_t *src, int n, int lane) {
+    int i = lane;
+    for (; i + 96 < n; i += 128) {
+        const uint8_t a = src[i], b = src[i + 32], c = src[i + 64], d = src[i + 96];
+        dst[i] = a; dst[i + 32] = b; dst[i + 64] = c; dst[i + 96] = d;
     }
-    for (int k = 0; k < CS_NUM; ++k) {
-        const int n = src->c.len[k], b = dst->c.len[k];
-        if (b + n > dst->c.cap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        for (int i = t; i < n; i += kChainNT) dst->c.buf[k][b + i] = src->c.buf[k][i];
+    for (; i < n; i += 32) dst[i] = src[i];
+}
+// dst += src, by the chain: lane s of every warp holds stream s's lengths
+// (the seven structure streams, then the coefficient streams), warp w copies
+// the w-th, (w + 4)-th, ... non-empty stream, and thread s updates stream s's
+// length after a barrier.  A stream that would overflow is left out and
+// reported.
+constexpr int kChainNS = IS_NS + CS_NUM;
+static_assert(kChainNS <= 32, "one lane per stream");
+__device__ void chain_isink_append(ISink *dst, const ISink *src, unsigned *err) {
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    int n = 0, b = 0, cap = 0;
+    if (lane < IS_NS) { n = src->slen[lane]; b = dst->slen[lane]; cap = dst->scap[lane]; }
+    else if (lane < kChainNS) { n = src->c.len[lane - IS_NS]; b = dst->c.len[lane - IS_NS]; cap = dst->c.cap[lane - IS_NS]; }
+    const bool fits = b + n <= cap;
+    if (w == 0 && n > 0 && !fits) atomicOr(err, kErrSlotOverflow);
+    unsigned todo = __ballot_sync(FDVB_FULL, n > 0 && fits);
+    for (int r = 0; todo; ++r) {
+        const int st = __ffs(todo) - 1;
+        todo &= todo - 1;
+        if ((r & 3) != w) continue;
+        const int ns = __shfl_sync(FDVB_FULL, n, st), bs = __shfl_sync(FDVB_FULL, b, st);
+        const uint8_t *sp = st < IS_NS ? src->sbuf[st] : src->c.buf[st - IS_NS];
+        uint8_t *dp = (st < IS_NS ? dst->sbuf[st] : dst->c.buf[st - IS_NS]) + bs;
+        warp_copy_bytes(dp, sp, ns, lane);
     }
     cbar();
-    if (t == 0) {
-        for (int k = 0; k < IS_NS; ++k) if (dst->slen[k] + src->slen[k] <= dst->scap[k]) dst->slen[k] += src->slen[k];
-        for (int k = 0; k < CS_NUM; ++k) if (dst->c.len[k] + src->c.len[k] <= dst->c.cap[k]) dst->c.len[k] += src->c.len[k];
+    if (t < kChainNS && n > 0 && fits) {
+        if (t < IS_NS) dst->slen[t] = b + n;
+        else dst->c.len[t - IS_NS] = b + n;
     }
     cbar();
 }
-// dst += the level-L team's sink `idx` (in cluster block `rank`), by the chain.
+// dst += the level-L team's sink `idx` (in cluster block `rank`), by the
+// chain, the same way (one lane per coefficient stream).
 __device__ void chain_append_leaf(CoefSink *dst, IShared *S, int L, int rank, int idx, unsigned *err) {
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     cg::cluster_group cl = cg::this_cluster();
     const bool s32 = L == 1;
     const CoefSink *ls = s32 ? &S->H.sink32[idx] : &S->H.sink[idx];
     const uint8_t *lm = s32 ? &S->H.sinkmem32[idx][0] : &S->H.sinkmem[idx][0];
     const CoefSink *rs = rank ? cl.map_shared_rank(ls, rank) : ls;
     const uint8_t *rm = rank ? cl.map_shared_rank(lm, rank) : lm;
-    int len[CS_NUM];
-    for (int k = 0; k < CS_NUM; ++k) len[k] = rs->len[k];
-    for (int k = 0; k < CS_NUM; ++k) {
-        const int n = len[k], b = dst->len[k];
-        if (n == 0) continue;
-        if (b + n > dst->cap[k]) { if (t == 0) atomicOr(err, kErrSlotOverflow); continue; }
-        const uint8_t *src = rm + (s32 ? leaf32_off(k) : leaf_off(k));
-        for (int i = t; i < n; i += kChainNT) dst->buf[k][b + i] = src[i];
+    int n = 0, b = 0, cap = 0;
+    if (lane < CS_NUM) { n = rs->len[lane]; b = dst->len[lane]; cap = dst->cap[lane]; }
+    const bool fits = b + n <= cap;
+    if (w == 0 && n > 0 && !fits) atomicOr(err, kErrSlotOverflow);
+    unsigned todo = __ballot_sync(FDVB_FULL, n > 0 && fits);
+    for (int r = 0; todo; ++r) {
+        const int k = __ffs(todo) - 1;
+        todo &= todo - 1;
+        if ((r & 3) != w) continue;
+        const int ns = __shfl_sync(FDVB_FULL, n, k), bs = __shfl_sync(FDVB_FULL, b, k);
+        warp_copy_bytes(dst->buf[k] + bs, rm + (s32 ? leaf32_off(k) : leaf_off(k)), ns, lane);
     }
     cbar();
-    if (t == 0)
-        for (int k = 0; k < CS_NUM; ++k) if (dst->len[k] + len[k] <= dst->cap[k]) dst->len[k] += len[k];
+    if (t < CS_NUM && n > 0 && fits) dst->len[t] = b + n;
     cbar();
 }
 

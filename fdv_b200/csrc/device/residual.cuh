@@ -66,7 +66,7 @@ struct Blk4 {
     uint8_t bytes[48];
 };
 // Per-warp scratch.
-struct Blk4Scratch {
+struct __align__(16) Blk4Scratch {
     int res[16];
     int lev[16];
 };
