@@ -129,12 +129,16 @@ __device__ __forceinline__ void gbar(int id, int n) { asm volatile("bar.sync %0,
 // that lanes of one warp can take different candidates without a divergent
 // table lookup: large diamond (0,8) (0,-8) (8,0) (-8,0) (4,4) (4,-4) (-4,4)
 // (-4,-4); small diamond (0,4) (0,-4) (4,0) (-4,0); cross (0,-1) (0,1) (-1,0) (1,0).
-__device__ __forceinline__ int ld_dx(int k) { return k == 2 ? 8 : (k == 3 ? -8 : (k == 4 || k == 5 ? 4 : (k >= 6 ? -4 : 0))); }
-__device__ __forceinline__ int ld_dy(int k) { return k == 0 ? 8 : (k == 1 ? -8 : (k == 4 || k == 6 ? 4 : (k == 5 || k == 7 ? -4 : 0))); }
-__device__ __forceinline__ int sd_dx(int k) { return k == 2 ? 4 : (k == 3 ? -4 : 0); }
-__device__ __forceinline__ int sd_dy(int k) { return k == 0 ? 4 : (k == 1 ? -4 : 0); }
-__device__ __forceinline__ int sp_dx(int k) { return k == 2 ? -1 : (k == 3 ? 1 : 0); }
-__device__ __forceinline__ int sp_dy(int k) { return k == 0 ? -1 : (k == 1 ? 1 : 0); }
+// Each offset is a signed nibble of a packed constant, picked by a shift, so
+// that lanes taking different candidates run the same instructions (nested
+// conditionals on k compile to divergent branches).
+__device__ __forceinline__ int nib(unsigned pack, int k) { return (int)(pack << (28 - 4 * k)) >> 28; }
+__device__ __forceinline__ int ld_dx(int k) { return 4 * nib(0xFF11E200u, k); }   //  0  0  8 -8  4  4 -4 -4
+__device__ __forceinline__ int ld_dy(int k) { return 4 * nib(0xF1F100E2u, k); }   //  8 -8  0  0  4 -4  4 -4
+__device__ __forceinline__ int sd_dx(int k) { return 4 * nib(0xF100u, k); }       //  0  0  4 -4
+__device__ __forceinline__ int sd_dy(int k) { return 4 * nib(0x00F1u, k); }       //  4 -4  0  0
+__device__ __forceinline__ int sp_dx(int k) { return nib(0x1F00u, k); }           //  0  0 -1  1
+__device__ __forceinline__ int sp_dy(int k) { return nib(0x001Fu, k); }           // -1  1  0  0
 
 // SAD of the BS x BS block whose source words this lane holds (c0, c1),
 // against the reference at (mvx, mvy).  BS = 16: the warp covers the block

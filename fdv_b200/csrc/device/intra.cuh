@@ -50,13 +50,18 @@ __device__ inline NNPred nn_setup(int mode, const uint8_t *top, const uint8_t *l
     }
     return P;
 }
+// Sample (x, y) of the prediction.  Lanes of a warp may hold different kinds
+// (one mode per half-warp in the screens), so the kinds' values are all
+// formed and one is selected arithmetically: a switch on the kind would
+// branch divergently on every sample.
 __device__ __forceinline__ int nn_px(const NNPred &P, const uint8_t *top, const uint8_t *left, int x, int y) {
-    switch (P.kind) {
-    case 1: return top[x];
-    case 2: return left[y];
-    case 3: return clipb((P.a + P.c * (y - P.c0) + 16 + P.b * (x - P.c0)) >> 5);
-    default: return P.dc;
-    }
+    const int k = P.kind;
+    const int pl = clipb((P.a + P.c * (y - P.c0) + 16 + P.b * (x - P.c0)) >> 5);
+    int v = P.dc;
+    v += ((int)top[x] - v) & -(int)(k == 1);
+    v += ((int)left[y] - v) & -(int)(k == 2);
+    v += (pl - v) & -(int)(k == 3);
+    return v;
 }
 
 // 4x4 directional prediction of pixel (x, y) from Tn = T(-1..7) and
