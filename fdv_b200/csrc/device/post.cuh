@@ -54,23 +54,20 @@ struct PostScratch {
 
 // The deblocked value of the sample at a[0], position x on a line of n samples
 // (a[k * step] the sample at x + k): the filter of the grid edge it touches,
-// as filter_edge (frame_ops.cuh) applies it.
+// as filter_edge (frame_ops.cuh) applies it.  Without lane-dependent
+// branches: a sample on no edge reads itself as all four taps, for which the
+// filter returns it unchanged (d = 0), and the side it is on is selected
+// arithmetically.
 __device__ __forceinline__ int dbk_sample(const uint8_t *a, int step, int x, int n, int alpha, int beta, int tc) {
-    int p1, p0, q0, q1;
-    bool pside;
-    if ((x & 7) == 7 && x + 1 < n) {
-        p1 = a[-step]; p0 = a[0]; q0 = a[step]; q1 = a[2 * step]; pside = true;
-    } else if ((x & 7) == 0 && x > 0) {
-        p1 = a[-2 * step]; p0 = a[-step]; q0 = a[0]; q1 = a[step]; pside = false;
-    } else {
-        return a[0];
-    }
-    if (abs(p0 - q0) < alpha && abs(p1 - p0) < beta && abs(q1 - q0) < beta) {
-        int d = ((q0 - p0) * 4 + (p1 - q1) + 4) >> 3;
-        d = d < -tc ? -tc : (d > tc ? tc : d);
-        return pside ? clipb(p0 + d) : clipb(q0 - d);
-    }
-    return a[0];
+    const int e7 = ((x & 7) == 7 && x + 1 < n) ? 1 : 0;   // p0 of the edge after it
+    const int e0 = ((x & 7) == 0 && x > 0) ? 1 : 0;       // q0 of the edge before it
+    const int p1 = a[-step * (e7 + 2 * e0)], p0 = a[-step * e0], q0 = a[step * e7], q1 = a[step * (2 * e7 + e0)];
+    int d = ((q0 - p0) * 4 + (p1 - q1) + 4) >> 3;
+    d = d < -tc ? -tc : (d > tc ? tc : d);
+    const int on = (abs(p0 - q0) < alpha && abs(p1 - p0) < beta && abs(q1 - q0) < beta) ? 1 : 0;
+    const int pv = clipb(p0 + d), qv = clipb(q0 - d), a0 = a[0];
+    const int fv = qv + ((pv - qv) & -e7);
+    return a0 + ((fv - a0) & -on);
 }
 
 __device__ __forceinline__ int tap6i(int a, int b, int c, int d, int e, int f) {

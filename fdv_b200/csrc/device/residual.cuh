@@ -427,11 +427,13 @@ __device__ void region8(const uint8_t *cur, int cs, const uint8_t *pred, int ps,
     const bool in = t <= last;
     const int bsum = __reduce_add_sync(FDVB_FULL, in ? bits_val(z) : 0);
     const int len = in ? leb_size(z) : 0;
-    const int end = warp_incl_scan(len, lane);
-    if (lane == 31) { sc->part[w][2] = end; sc->part[w][3] = bsum; }
+    int tot;
+    const int ex = ballot_prefix(len, lane, FDVB_FULL, tot);
+    if (lane == 31) { sc->part[w][2] = tot; sc->part[w][3] = bsum; }
     bar_sync64(bar);
     const int base = w ? sc->part[0][2] : 0;
-    if (in) leb_write(out->bytes + base + end - len, z);
+    // the residual (sc->X) is no longer read: its bytes take the unused stores
+    leb_put(out->bytes + base + ex, reinterpret_cast<uint8_t *>(sc->X) + t, z, len);
     if (t == 0) {
         out->count = last + 1;
         out->nbytes = sc->part[0][2] + sc->part[1][2];
