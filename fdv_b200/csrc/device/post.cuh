@@ -74,6 +74,15 @@ __device__ __forceinline__ int tap6i(int a, int b, int c, int d, int e, int f) {
     return a - 5 * b + 20 * c + 20 * d - 5 * e + f;
 }
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// n / d for 0 <= n < 2^22, 0 < d < 2^10, from r = 1.0f / d: the float
+// quotient is within one of the true one, and one correction each way makes
+// it exact (a runtime integer division is a long instruction sequence).
+__device__ __forceinline__ int fast_div(int n, int d, float r) {
+    int q = __float2int_rz(__fmul_rn((float)n, r));
+    q += (q + 1) * d <= n ? 1 : 0;
+    q -= q * d > n ? 1 : 0;
+    return q;
+}
 
 // Tiles tc0..tc1-1 (at most kPostRun) of tile row tr of frame U into its
 // reference output; t = thread index within the post threads (0..479).  Ends
@@ -91,22 +100,31 @@ __device__ __noinline__ void post_run(PostScratch &P, const UnitDev &U, int tr, 
     const int ccx0 = 8 * tc0, ccx1 = 8 * tc1;
     const int crx4 = max(0, ccx0 - 2) & ~3, crx1 = min(cw, ccx1 + 2);
     // a. the reconstruction (through L2: other blocks wrote most of it), in
-    // aligned 32-bit words (rows start 16-byte aligned, widths multiples of 8)
+    // aligned 32-bit words (rows start 16-byte aligned, widths multiples of 8);
+    // a thread's words are loaded before any is stored, so their L2 round
+    // trips overlap
     {
         const int nlw = (rx1 - rx4 + 3) >> 2, ncw = (crx1 - crx4 + 3) >> 2;
         const int nl = (vy1 - vy0) * (kPW / 4), nc = (cry1 - cry0) * (kCW / 4);
-        for (int i = t; i < nl + 2 * nc; i += kPostNT) {
+        auto word_at = [&](int i, uint32_t *&dst) -> uint32_t {
+            dst = nullptr;
             if (i < nl) {
                 const int y = i / (kPW / 4), q = i - y * (kPW / 4);
-                if (q < nlw)
-                    *reinterpret_cast<uint32_t *>(&P.rec[y][4 * q]) =
-                        __ldcg(reinterpret_cast<const uint32_t *>(&U.rec[0][(size_t)(vy0 + y) * w + rx4 + 4 * q]));
-            } else {
-                const int k = i - nl, pl = k >= nc ? 1 : 0, kk = k - pl * nc, y = kk / (kCW / 4), q = kk - y * (kCW / 4);
-                if (q < ncw)
-                    *reinterpret_cast<uint32_t *>(&P.crec[pl][y][4 * q]) = __ldcg(
-                        reinterpret_cast<const uint32_t *>(&U.rec[1 + pl][(size_t)(cry0 + y) * cw + crx4 + 4 * q]));
+                if (q >= nlw) return 0u;
+                dst = reinterpret_cast<uint32_t *>(&P.rec[y][4 * q]);
+                return __ldcg(reinterpret_cast<const uint32_t *>(&U.rec[0][(size_t)(vy0 + y) * w + rx4 + 4 * q]));
             }
+            if (i >= nl + 2 * nc) return 0u;
+            const int k = i - nl, pl = k >= nc ? 1 : 0, kk = k - pl * nc, y = kk / (kCW / 4), q = kk - y * (kCW / 4);
+            if (q >= ncw) return 0u;
+            dst = reinterpret_cast<uint32_t *>(&P.crec[pl][y][4 * q]);
+            return __ldcg(reinterpret_cast<const uint32_t *>(&U.rec[1 + pl][(size_t)(cry0 + y) * cw + crx4 + 4 * q]));
+        };
+        for (int i = t; i < nl + 2 * nc; i += 2 * kPostNT) {
+            uint32_t *d0, *d1;
+            const uint32_t v0 = word_at(i, d0), v1 = word_at(i + kPostNT, d1);
+            if (d0) *d0 = v0;
+            if (d1) *d1 = v1;
         }
     }
     post_bar();
@@ -186,17 +204,25 @@ __device__ __noinline__ void post_run(PostScratch &P, const UnitDev &U, int tr, 
         const int yca = tr == 0 ? -B : 8 * tr, ycb = tr == mbh - 1 ? ch + B : 8 * tr + 8;
         const int ncwx = (xcb - xca) >> 2, ncl = (ycb - yca) * ncwx;
         uint8_t *const lp[4] = {U.out.G, U.out.B, U.out.H, U.out.J};
+        const float rnpl = 1.0f / (float)npl, rnwx = 1.0f / (float)nwx, rncwx = 1.0f / (float)ncwx;
+        // core columns start at cx0: a word inside the plane whose samples
+        // are four aligned core bytes is one load
+        const bool core_al = (cx0 & 3) == 0;
         for (int i = t; i < nl + 2 * ncl; i += kPostNT) {
             if (i < nl) {
-                const int p = i / npl, k = i - p * npl, yy = k / nwx, q = k - yy * nwx;
+                const int p = fast_div(i, npl, rnpl), k = i - p * npl, yy = fast_div(k, nwx, rnwx), q = k - yy * nwx;
                 const int y = ya + yy, x = xa + 4 * q;
                 const uint8_t *cr = P.core[p][clampi(y, -3, h + 2) - cy0];
                 uint32_t word = 0;
+                if (core_al && x >= 0 && x + 3 < w) {
+                    word = *reinterpret_cast<const uint32_t *>(cr + x - cx0);
+                } else {
 #pragma unroll
-                for (int b = 0; b < 4; ++b) word |= (uint32_t)cr[clampi(x + b, -3, w + 2) - cx0] << (8 * b);
+                    for (int b = 0; b < 4; ++b) word |= (uint32_t)cr[clampi(x + b, -3, w + 2) - cx0] << (8 * b);
+                }
                 *reinterpret_cast<uint32_t *>(lp[p] + (long)y * U.out.ys + x) = word;
             } else {
-                const int k = i - nl, pl = k >= ncl ? 1 : 0, kk = k - pl * ncl, yy = kk / ncwx, q = kk - yy * ncwx;
+                const int k = i - nl, pl = k >= ncl ? 1 : 0, kk = k - pl * ncl, yy = fast_div(kk, ncwx, rncwx), q = kk - yy * ncwx;
                 const int y = yca + yy, x = xca + 4 * q;
                 const uint8_t *cr = P.cd[pl][clampi(y, 0, ch - 1) - 8 * tr];
                 uint32_t word = 0;
