@@ -66,6 +66,15 @@ struct Blk4 {
     uint8_t bytes[48];
 };
 // Per-warp scratch.
+// Sixteen ints of 16-byte aligned shared scratch, four vector loads.
+__device__ __forceinline__ void load16(const int *src, int v[16]) {
+    const int4 *s4 = reinterpret_cast<const int4 *>(src);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int4 a = s4[q];
+        v[4 * q] = a.x; v[4 * q + 1] = a.y; v[4 * q + 2] = a.z; v[4 * q + 3] = a.w;
+    }
+}
 struct __align__(16) Blk4Scratch {
     int res[16];
     int lev[16];
@@ -146,13 +155,15 @@ __device__ __noinline__ void warp_block4(const uint8_t *cur, int cs, const uint8
         double J;
         {
             const int L = lane - 1;
-            int d[16], r[16];
+            int d[16], r[16], rv[16];
+            load16(sc->lev, d);
+            load16(sc->res, rv);
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? sc->lev[p] : 0;
+            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? d[p] : 0;
             idct4_thread(d, r);
             int D = 0;
 #pragma unroll
-            for (int p = 0; p < 16; ++p) { int e = sc->res[p] - r[p]; D += e * e; }
+            for (int p = 0; p < 16; ++p) { int e = rv[p] - r[p]; D += e * e; }
             J = valid ? rd_cost((double)D, lambda, bitsL) : 0.0;
         }
         int bestL = last;
@@ -276,13 +287,15 @@ __device__ void warp_block4x2(const uint8_t *cur0, const uint8_t *cur1, int cs, 
         __syncwarp();
         double J;
         {   // every lane (no divergent branch); only valid candidates count
-            int d[16], r[16];
+            int d[16], r[16], rv[16];
+            load16(sc[h].lev, d);
+            load16(sc[h].res, rv);
 #pragma unroll
-            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? sc[h].lev[p] : 0;
+            for (int p = 0; p < 16; ++p) d[p] = izz4(p) <= L ? d[p] : 0;
             idct4_thread(d, r);
             int D = 0;
 #pragma unroll
-            for (int p = 0; p < 16; ++p) { const int e = sc[h].res[p] - r[p]; D += e * e; }
+            for (int p = 0; p < 16; ++p) { const int e = rv[p] - r[p]; D += e * e; }
             J = valid ? rd_cost((double)D, lambda, bitsL) : 0.0;
         }
         // candidate L = 15: every level kept
@@ -572,21 +585,25 @@ __device__ __forceinline__ void region_choice(const Blk4 *b4, const Reg8 &R, dou
 }
 
 // Copy region rg's symbols (flag, counts, level bytes) to the offsets its
-// decision reserved (one warp).
+// decision reserved (one warp).  The four 4x4 blocks' level bytes are one
+// copy over their concatenation, each byte's block found by comparing with
+// the running offsets (no loop per block waiting on the previous one's size).
 __device__ __forceinline__ void region_symbols(const RegDec &D, const Blk4 *b4, const Reg8 &R, CoefSink *sink,
                                                bool chroma, int lane) {
-    if (D.flv < 0) return;
-    if (lane == 0) sink->buf[CS_FL][D.ofl] = (uint8_t)D.flv;
-    if (D.flv == 1) {
+    const int flv = D.flv;
+    if (flv < 0) return;
+    if (lane == 0) sink->buf[CS_FL][D.ofl] = (uint8_t)flv;
+    if (flv == 1) {
         uint8_t *cnt = sink->buf[chroma ? CS_NC : CS_N] + D.oc;
         uint8_t *lv = sink->buf[chroma ? CS_LC : CS_L] + D.ol;
-        int o = 0;
-        for (int s2 = 0; s2 < 4; ++s2) {
-            if (lane == 0) cnt[s2] = (uint8_t)b4[s2].count;
-            for (int i = lane; i < b4[s2].nbytes; i += 32) lv[o + i] = b4[s2].bytes[i];
-            o += b4[s2].nbytes;
+        if (lane < 4) cnt[lane] = (uint8_t)b4[lane].count;
+        const int o1 = b4[0].nbytes, o2 = o1 + b4[1].nbytes, o3 = o2 + b4[2].nbytes, tot = o3 + b4[3].nbytes;
+        for (int i = lane; i < tot; i += 32) {
+            const int s1 = i >= o1 ? 1 : 0, s2 = i >= o2 ? 1 : 0, s3 = i >= o3 ? 1 : 0;
+            const int base = (o1 & -s1) + ((o2 - o1) & -s2) + ((o3 - o2) & -s3);
+            lv[i] = b4[s1 + s2 + s3].bytes[i - base];
         }
-    } else if (D.flv == 2) {
+    } else if (flv == 2) {
         if (lane == 0) sink->buf[CS_N8][D.oc] = (uint8_t)R.count;
         uint8_t *lv = sink->buf[CS_L8] + D.ol;
         for (int i = lane; i < D.nl; i += 32) lv[i] = R.bytes[i];
@@ -595,26 +612,32 @@ __device__ __forceinline__ void region_symbols(const RegDec &D, const Blk4 *b4, 
 
 // Reserve the stream offsets of regions dec[0..nreg) in order (one thread);
 // on overflow report it, clamp the lengths and mark the regions unwritten.
+// The five lengths a region can grow are kept in registers meanwhile.
 __device__ __forceinline__ void region_offsets(RegDec *dec, int nreg, CoefSink *sink, bool chroma,
                                                long long *e, int *b, unsigned *err) {
     const int kc = chroma ? CS_NC : CS_N, kl = chroma ? CS_LC : CS_L;
+    int lfl = sink->len[CS_FL], lc = sink->len[kc], ll = sink->len[kl], ln8 = sink->len[CS_N8], ll8 = sink->len[CS_L8];
     long long es = 0;
     int bs = 0;
+#pragma unroll 4
     for (int rg = 0; rg < nreg; ++rg) {
         RegDec &D = dec[rg];
-        D.ofl = sink->len[CS_FL]++;
-        if (D.flv == 1) { D.oc = sink->len[kc]; sink->len[kc] += 4; D.ol = sink->len[kl]; sink->len[kl] += D.nl; }
-        else if (D.flv == 2) { D.oc = sink->len[CS_N8]; sink->len[CS_N8] += 1; D.ol = sink->len[CS_L8]; sink->len[CS_L8] += D.nl; }
+        const int flv = D.flv, nl = D.nl;
+        D.ofl = lfl++;
+        if (flv == 1) { D.oc = lc; lc += 4; D.ol = ll; ll += nl; }
+        else if (flv == 2) { D.oc = ln8; ln8 += 1; D.ol = ll8; ll8 += nl; }
         es += D.e;
         bs += D.b;
     }
-    bool ovf = false;
-    for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) ovf = true;
+    const bool ovf = lfl > sink->cap[CS_FL] || lc > sink->cap[kc] || ll > sink->cap[kl] || ln8 > sink->cap[CS_N8] ||
+                     ll8 > sink->cap[CS_L8];
     if (ovf) {
         atomicOr(err, kErrSlotOverflow);
-        for (int k = 0; k < CS_NUM; ++k) if (sink->len[k] > sink->cap[k]) sink->len[k] = sink->cap[k];
+        lfl = min(lfl, sink->cap[CS_FL]); lc = min(lc, sink->cap[kc]); ll = min(ll, sink->cap[kl]);
+        ln8 = min(ln8, sink->cap[CS_N8]); ll8 = min(ll8, sink->cap[CS_L8]);
         for (int rg = 0; rg < nreg; ++rg) dec[rg].flv = -1;
     }
+    sink->len[CS_FL] = lfl; sink->len[kc] = lc; sink->len[kl] = ll; sink->len[CS_N8] = ln8; sink->len[CS_L8] = ll8;
     *e += es;
     *b += bs;
 }
