@@ -789,7 +789,11 @@ def main() -> None:
         tr = T.autotune([(W, bh) for _, bh in bands], RANGE, local)
         tuning = {k: tr[k] for k in ("max_batch", "p_grid", "p_ms_per_frame", "default_p_ms_per_frame", "cached")}
         tuning["gain_vs_default"] = round(tr["default_p_ms_per_frame"] / tr["p_ms_per_frame"], 4)
-        tuning["default"] = {"max_batch": 30, "p_grid": tr["nsm"]}
+        tuning["default"] = {"max_batch": T.BATCHES[-1], "p_grid": tr["nsm"]}
+        # against the earlier fixed shape (thirty frames per launch, one block per SM)
+        c30 = [c for c in tr["candidates"] if c["max_batch"] == 30 and c["p_grid"] == tr["nsm"]]
+        if c30:
+            tuning["gain_vs_30_frames"] = round(c30[0]["p_ms_per_frame"] / tr["p_ms_per_frame"], 4)
         tuning["candidates"] = tr["candidates"]
         tuning["sequence"] = tr["sequence"]
     g = F.Engine([(W, bh) for _, bh in bands], RANGE, local)

@@ -892,15 +892,15 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
             // ---- coefficient streams of the chosen mode into the slot (read
             // after the kernel; the sinks are reset only after the next
             // macroblock's first barrier)
-            if (chosen != 0) {
-                for (int k = 0; k < CS_NUM; ++k) {
-                    int n = M->len[k];
-                    if (n > c_SlotCap[PS_CN + k]) { if (tid == 0) atomicOr(err, kErrSlotOverflow); n = 0; }
-                    uint8_t *d = slot_data(slot, PS_CN + k);
-                    const uint8_t *s = M->buf[k];
-                    for (int i = tid; i < n; i += PNT) d[i] = s[i];
-                    if (tid == 0) slot_len(slot)[PS_CN + k] = (uint16_t)n;
-                }
+            // (warp k copies stream k: no stream waits for the one before)
+            if (chosen != 0 && (tid >> 5) < CS_NUM) {
+                const int k = tid >> 5, ln = tid & 31;
+                int n = M->len[k];
+                if (n > c_SlotCap[PS_CN + k]) { if (ln == 0) atomicOr(err, kErrSlotOverflow); n = 0; }
+                uint8_t *d = slot_data(slot, PS_CN + k);
+                const uint8_t *s = M->buf[k];
+                for (int i = ln; i < n; i += 32) d[i] = s[i];
+                if (ln == 0) slot_len(slot)[PS_CN + k] = (uint16_t)n;
             }
             pc.mark(PP_OUT);
         }
