@@ -655,8 +655,13 @@ pframe_kernel(const UnitDev *__restrict__ units, const RowTask *__restrict__ row
                     const int pw = warp < 8 ? warp : warp - 4;      // 0..11
                     const unsigned pmask = (l_intra ? 0u : 0xFu) | (navail > 1 && !lfast ? 0xF0u : 0u) |
                                            (S.isel >= 0 ? 0xF00u : 0u);
-                    for (int t = pw; t < 36; t += 12) {
-                        const int g = t / 3, j = t - 3 * g;
+                    // every warp takes two 4x4 pair tasks and one 8x8 task
+                    // (regions pw, pw + 4, pw + 8 mod 12): the warps finish
+                    // together instead of a third of them doing the three
+                    // shorter 8x8 tasks
+#pragma unroll 1
+                    for (int j = 0; j < 3; ++j) {
+                        const int g = (pw + 4 * j) % 12;
                         if ((pmask >> g) & 1u) resid_task(S, g, j, qp, lambda, warp, lane);
                     }
                     team_bar(BAR_POOL, 384);
