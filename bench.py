@@ -710,7 +710,7 @@ def pframe_roofline(pk_ms: float, pk_n: int, clocks: dict, local: int) -> dict:
                     "peak_source": "measured (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else "fallback"},
             "int_pipe": capture.get("int_pipe"),
             "capture": capture.get("capture"),
-            "note": "latency-bound wavefront (kernel time per P-frame, up to 30 P-frames overlapping per launch)"}
+            "note": "latency-bound wavefront (kernel time per P-frame, up to 60 P-frames overlapping per launch)"}
 
 
 def main() -> None:
