@@ -21,6 +21,7 @@
 #include <functional>
 #include <memory>
 #include <map>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -387,8 +388,33 @@ size_t fdv_wrap(uint8_t *out, size_t cap, int kind, int fps, const uint8_t *payl
 // tiled encoder gives it, twice the band's I420 frame size plus 64 KiB for all
 // frames (encode_band, fdv.h:7111-7113, checked per frame as fdv_video_encode
 // does, :6800-6804): a band that outgrows it fails the call, as there.
+// Host timing of the last whole-array encode (fdvb_encode_stats), ms since
+// its start: the first submission, the last frame collected, the end of its
+// coding, the end of the call; and the summed time the calling thread spent
+// waiting in collects and in the band coding.
+namespace {
+struct EncTiming {
+    double first_submit = 0, last_collect = 0, coded = 0, total = 0, collect_wait = 0, coding = 0;
+};
+EncTiming g_enc_timing;
+std::mutex g_enc_timing_mu;
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
+extern "C" void fdvb_encode_stats(double ms[6]) {
+    if (!ms) return;
+    std::lock_guard<std::mutex> lk(g_enc_timing_mu);
+    const EncTiming &t = g_enc_timing;
+    ms[0] = t.first_submit; ms[1] = t.last_collect; ms[2] = t.coded; ms[3] = t.total;
+    ms[4] = t.collect_wait; ms[5] = t.coding;
+}
+
 static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h, int qp, int keyint,
                         int bh_full, int nthreads, std::vector<UnitStream> &us, bool band_capped = false) {
+    const auto t_start = std::chrono::steady_clock::now();
+    EncTiming tm;
     const int nb = (h + bh_full - 1) / bh_full, cw = w / 2, ch = h / 2;
     std::vector<int> W(nb, w), H(nb), Y0(nb);
     for (int b = 0; b < nb; ++b) { Y0[b] = b * bh_full; H[b] = std::min(bh_full, h - Y0[b]); }
@@ -462,6 +488,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             const int K = run_len(f);
             if ((int)types.size() + K > 2 * kmax) break;
             if (submit_at(f, K) != 0) { rc = -1; break; }
+            if (f == 0) tm.first_submit = ms_since(t_start);
             f += K;
         }
         if (rc != 0 || types.empty()) break;
@@ -473,7 +500,10 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
         do {
             const int ti = types.front();
             types.pop_front();
+            const double tc0 = ms_since(t_start);
             if (fdvb_engine_collect(E) != 0) { set_engine_err(); rc = -1; break; }
+            tm.collect_wait += ms_since(t_start) - tc0;
+            if (types.empty() && f >= nframes) tm.last_collect = ms_since(t_start);
             btype.push_back(ti);
             for (int b = 0; b < nb; ++b)
                 for (int p = 0; p < (ti ? 3 : 1); ++p) {
@@ -483,6 +513,7 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
                 }
         } while (rc == 0 && !types.empty() && btype.size() < 16 && fdvb_engine_ready(E) == 1);
         if (rc == 0 && !btype.empty()) {
+            const double tp0 = ms_since(t_start);
             std::fill(urc.begin(), urc.end(), 0);
             pool.run(nb, [&](int u) {
                 size_t o = 0;
@@ -497,6 +528,8 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
             });
             for (int r : urc)
                 if (r) { set_err(r == -2 ? "a band's stream outgrew the tiled encoder's capacity" : "entropy coding failed"); rc = -1; }
+            tm.coding += ms_since(t_start) - tp0;
+            tm.coded = ms_since(t_start);
         }
     }
     while (!types.empty()) {
@@ -508,6 +541,11 @@ static int encode_bands(const uint8_t *const *frames, int nframes, int w, int h,
     fdvb_engine_stream_frames(E, 0);
     if (rc == 0) engine_release(E, nb, W.data(), H.data(), range, device);
     else fdvb_engine_destroy(E);
+    tm.total = ms_since(t_start);
+    {
+        std::lock_guard<std::mutex> lk(g_enc_timing_mu);
+        g_enc_timing = tm;
+    }
     return rc;
 }
 

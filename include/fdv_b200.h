@@ -76,6 +76,13 @@ const char *fdvd_last_error(void);
  * reset != 0 clears them. */
 void fdvd_timing(int on);
 void fdvd_stats(double ms[9], long long n[9], int reset);
+/* Host timing of the last whole-array encode (fdv_video_encode or
+ * fdv_vtile_encode; no counterpart in the reference), milliseconds since the
+ * call entered the encoder: ms[0] the first submission to the GPU, ms[1] the
+ * last frame collected, ms[2] the end of the last entropy coding, ms[3] the
+ * end; ms[4] the calling thread's summed waits in collects, ms[5] its summed
+ * time in the band-parallel entropy coding. */
+void fdvb_encode_stats(double ms[6]);
 
 /* Streaming encoder.  Replaces the fdv_enc_* family, fdv.h:1157-1198
  * (implementation fdv.h:8129-8459).  Output is byte-identical to
