@@ -901,6 +901,23 @@ extern "C" int fdvb_engine_submit_batch(fdvb_engine *E, int K, const uint8_t *co
         for (int r = 0; r < maxh; ++r)
             for (auto &t : frows) if (t.row == r) rows.push_back(t);
     }
+    // Frames of a launch overlap: row r of frame k needs the frame before
+    // only up to its row r + DR + 1 (the row that posts tile row r + DR,
+    // DR the reference rows the window reaches), so a frame can start about
+    // F macroblock steps after the one before, rows 2 steps apart.  Tickets
+    // in that order (frame k, row r at k F + 2 r) hand an SM the row that
+    // can run soonest: frame by frame, a tall frame's last rows, which start
+    // long after the next frame's first ones, would hold SMs while they
+    // wait.  F > 2 (DR + 1), so every row a task waits for still has an
+    // earlier ticket (no deadlock); bands of a few rows keep frame order.
+    if (K > 1 && !whole_frame_refs) {
+        const bool win = E->range <= 32;
+        const int dr = win ? (E->range + 19) / 16 : E->range / 16 + 2, dc = win ? 4 : E->range / 16 + 2;
+        const int F = 2 * (dr + 1) + dc + 6;
+        std::stable_sort(rows.begin(), rows.end(), [&](const RowTask &a, const RowTask &b) {
+            return (a.unit / nu) * F + 2 * a.row < (b.unit / nu) * F + 2 * b.row;
+        });
+    }
     // Key-frame CTU rows in ticket order: by row, a row's luma planes (the
     // longest chains) before its chroma planes.  A row waits only for the row
     // above in its own plane, which comes earlier in this order.
