@@ -80,23 +80,6 @@ struct __align__(16) Blk4Scratch {
     int lev[16];
 };
 
-__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(FDVB_FULL, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-// Inclusive scan over lanes 0..15 (lanes 16..31 hold partial sums).
-__device__ __forceinline__ int scan16(int v, int lane) {
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        int t = __shfl_up_sync(FDVB_FULL, v, o);
-        if ((lane & 15) >= o) v += t;
-    }
-    return v;
-}
 
 // One warp codes one 4x4 block: forward transform, quantisation, optional RDOQ
 // (fdv.h:2493-2536), dequantisation, inverse transform, reconstruction.  Lane
